@@ -1,0 +1,326 @@
+"""Benchmark: DOF-updates/s of the RK4 DG shallow-water step (SPOC cal_var path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl spoc|reference]
+                  [--config c2_fs_p6]
+
+Workload: configuration C2 of the reference's benchmark set (nonlinear
+free-slip calvarnl_fs, degree 6 = 28 modes, tri2_33 / legen7 quadrature,
+2 x 128 x 128 = 32768 jittered triangles on a 1000 km beta-plane basin,
+8 seeded geostrophic Gaussians), synthetic and seeded.  A step is one
+classical RK4 step (4 right-hand sides + update).  Metric:
+DOF-updates/s = 3 * nm * ne * steps / seconds (u, v, eta), whole job.
+
+`value`: device-resident state, CUDA events around every step on the
+launching stream, L2 flushed (256 MiB write) before every timed step, max
+over ranks.  `e2e`: the host-buffer entry point spoc_rk4_steps_host, one step
+per call with the state copied host->device and back from pinned memory
+inside the timed region.  N > 1 runs independent replicas (one per GPU, no
+collective on the data path): weak scaling.
+
+--impl reference times the CPU restatement of the reference (oracle/,
+OpenMP over all host cores) on the same workload: rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DOF-updates/s per RK4 step (plain FP64 vs mixed/adjoint) at stated L2 error"
+UNIT = "DOF-updates/s"
+
+
+def workload_desc(cfg, ne, nm):
+    return (f"{cfg.name}: cal_var {cfg.variant} degree {cfg.nc} (nm={nm}), tri2_{cfg.ng}/legen{cfg.ngf}, "
+            f"2x{cfg.n}x{cfg.n}={ne} triangles (jitter {cfg.jitter}), {cfg.length / 1e3:.0f} km basin, "
+            f"f0={cfg.f0}, beta={cfg.beta}, mu0={cfg.mu0}, mb0={cfg.mb0}, H={cfg.depth}, ic={cfg.ic}")
+
+
+def model_counts(cfg, ne, nf):
+    """Per-kernel algorithmic FP64 flops and compulsory HBM bytes of one RHS.
+
+    Flops count the reference's multiply-adds (2 flops each): cal_b N^2,
+    DTRSM4 N^2 per solve (two half sweeps), spectoxy/xytospec Q*N, tri_f 3*N*G,
+    cal_flu 2*N*G per face (both sides).  Bytes: each kernel's own-element
+    reads and writes of modal fields (neighbour data is an L2 re-read).
+    """
+    N, Q, G = cfg.nm, cfg.ng, cfg.ngf
+    if cfg.variant == "lin":
+        macs = ne * (6 * N * N + 3 * N * N + 4 * 3 * N * G) + nf * 3 * 2 * N * G
+        return {"k_lin": (2.0 * macs, 8.0 * ne * N * (3 + 9))}
+    return {
+        "k_qphase": (2.0 * (ne * (8 * N * N + 12 * N * G) + nf * 2 * 2 * N * G), 8.0 * ne * N * (2 + 4)),
+        "k_nlvol": (2.0 * ne * (2 * N * N + 17 * Q * N), 8.0 * ne * N * (11 + 8)),
+        "k_tend": (2.0 * (ne * (15 * N * N + 18 * N * G) + nf * 6 * 2 * N * G), 8.0 * ne * N * (8 + 12)),
+    }
+
+
+def sample_clocks_start(out: Path):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        f = open(out, "w")
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                 "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL), f
+    except Exception:
+        return None, None
+
+
+def sample_clocks_stop(proc, fh, out: Path, gpu_index: int):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    fh.close()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in out.read_text().splitlines():
+        parts = [p.strip() for p in line.split(",")]
+        if len(parts) < 9 or not parts[0].isdigit() or int(parts[0]) != gpu_index:
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = float(parts[2])
+        except ValueError:
+            continue
+        for name, val in zip(names, parts[5:9]):
+            if val.lower().startswith("active"):
+                reasons.add(name)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def run_reference(args, cfg, rank):
+    """CPU restatement of the reference (oracle/), all host threads, rank 0 only."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from spoc_b200 import workloads as W
+
+    p = W.build_problem(cfg)
+    T = p.T
+    OT = O.Tables(cfg.nc, cfg.ng, cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
+    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, cfg.nc, cfg.f0, cfg.beta)
+    threads = O.default_threads()
+    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+
+    def step():
+        O.rk4(cfg.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, cfg.mu0, cfg.mb0, cfg.g0,
+              p.dt, 1, threads)
+
+    t0 = time.perf_counter()
+    step()  # one warm-up step (bounded)
+    per = time.perf_counter() - t0
+    budget = 120.0
+    k = max(1, min(args.steps, int(budget / max(per, 1e-9))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        step()
+    sec = time.perf_counter() - t0
+    dof = 3.0 * T.nm * p.mesh.ne
+    val = dof * k / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": k, "warmup": 1, "ms_per_step": 1e3 * sec / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_desc(cfg, p.mesh.ne, T.nm), "ne": p.mesh.ne, "nm": T.nm},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{k} full RK4 steps of the workload ({args.steps} requested, "
+                                   f"capped at {budget:.0f} s)"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(cfg, p):
+    """Oracle on the host cores, bounded to ~10-30 s (rank 0, N=1)."""
+    from oracle import oracle as O
+    T = p.T
+    OT = O.Tables(cfg.nc, cfg.ng, cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
+    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, cfg.nc, cfg.f0, cfg.beta)
+    threads = O.default_threads()
+    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    k, t0 = 0, time.perf_counter()
+    while True:
+        O.rk4(cfg.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, cfg.mu0, cfg.mb0, cfg.g0,
+              p.dt, 1, threads)
+        k += 1
+        sec = time.perf_counter() - t0
+        if sec > 10.0 or k >= 50:
+            break
+    return {"value": 3.0 * T.nm * p.mesh.ne * k / sec, "unit": UNIT, "cores": threads,
+            "kind": "port", "sample": f"{k} full RK4 steps of the workload, OpenMP over elements"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="spoc", choices=["spoc", "reference"])
+    ap.add_argument("--config", default="c2_fs_p6")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from spoc_b200 import workloads as W
+    cfg = W.CONFIGS[args.config]
+
+    if args.impl == "reference":
+        run_reference(args, cfg, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from spoc_b200 import api
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    p = W.build_problem(cfg)
+    ne, nm = p.mesh.ne, p.T.nm
+    s = W.make_solver(p)
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, args.warmup)
+
+    # ---- timed region: device-resident state ----
+    clk_file = ROOT / "gpurun_out" / f"clocks_rank{rank}.csv"
+    clk_file.parent.mkdir(exist_ok=True)
+    proc, fh = sample_clocks_start(clk_file) if rank == 0 else (None, None)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = s.launches
+    times = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[i][0].record(stream)
+        s.rk4_steps(p.dt, 1)
+        with torch.cuda.stream(stream):
+            ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = s.launches - l0
+    clocks = sample_clocks_stop(proc, fh, clk_file, local) if rank == 0 else None
+    times = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(times))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    dof = 3.0 * nm * ne
+    value = dof * args.steps * world / (total_ms * 1e-3)
+
+    # ---- e2e: host buffers through spoc_rk4_steps_host ----
+    pin = [torch.from_numpy(a.copy()).pin_memory() for a in (p.u, p.v, p.h)]
+    host = [t.numpy() for t in pin]
+    e2e_steps = max(3, min(args.steps, 10))
+    s.rk4_steps_host(*host, p.dt, 1)  # warm-up
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e_times = []
+    for _ in range(e2e_steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.rk4_steps_host(*host, p.dt, 1)
+        b.record(stream)
+        b.synchronize()
+        e_times.append(a.elapsed_time(b))
+    e_ms = float(sum(e_times))
+    if world > 1:
+        t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e = {"value": dof * e2e_steps * world / (e_ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": 3 * ne * nm * 8, "d2h_bytes_per_step": 3 * ne * nm * 8}
+
+    # ---- per-kernel timing and roofline of the dominant kernel ----
+    s.set_state(p.u, p.v, p.h)
+    prof_steps = 2
+    kms = s.profile_rk4(p.dt, prof_steps)
+    counts = model_counts(cfg, ne, p.mesh.nf)
+    names = list(counts)
+    per_launch_ms = {n: float(kms[i]) / (4 * prof_steps) for i, n in enumerate(names)}
+    dom = max(per_launch_ms, key=per_launch_ms.get)
+    fl, by = counts[dom]
+    dur = per_launch_ms[dom] * 1e-3
+    fp64_fma = api.fp64_peak(0)
+    fp64_mul_add = api.fp64_peak(1)
+    hbm_peak = None
+    try:
+        hbm_peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
+        hbm_src = "measured"
+    except Exception:
+        hbm_peak, hbm_src = 6650.0, "fallback"
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(f"{cfg.name}:{dom}")
+    roof = {"kernel": dom, "bound": "hbm", "achieved": by / dur / 1e9, "peak": hbm_peak,
+            "unit": "GB/s", "frac": by / dur / 1e9 / hbm_peak, "traffic": traffic,
+            "peak_source": hbm_src, "algorithmic_bytes_per_launch": by}
+    roof_fp64 = {"kernel": dom, "bound": "fp64", "achieved": fl / dur / 1e12,
+                 "peak": fp64_fma, "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp64_fma,
+                 "peak_mul_add": fp64_mul_add, "frac_of_mul_add": fl / dur / 1e12 / fp64_mul_add,
+                 "algorithmic_flops_per_launch": fl,
+                 "peak_source": "measured live: spoc_fp64_peak (DFMA chains, 148 SMs)"}
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(cfg, ne, nm), "ne": ne, "nm": nm, "dt": p.dt,
+                       "precision": "fp64, reference operation order (bit-exact to the CPU oracle)",
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "kernel_ms_per_launch": per_launch_ms,
+            "roofline": roof,
+            "roofline_fp64": roof_fp64,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(cfg, p)
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

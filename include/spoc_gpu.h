@@ -1,0 +1,183 @@
+/*
+ * spoc_gpu.h -- C ABI of the B200 implementation of SPOC's RK4
+ * discontinuous-Galerkin shallow-water right-hand side.
+ *
+ * The reference selects its physics at link time: every src/calvar*.f defines
+ *   subroutine cal_var(nf,ne,u0,v0,h0,u1,v1,h1,tseg,pseg,ssit,itm,its,norm,
+ *                      nbdl,pbdl,nint,pint,bdl,cip,vect,normt,
+ *                      mu0,mb0,fc,beta,w0,z0,g0,hb,time)
+ * (src/calvarnl_fs.f:9-12, src/calvar_lin.f:7-10) and reads its tables from
+ * COMMON /const/ /gauss/ /gaussf/ /gauss2/ /gauss3/ /matrices/
+ * (src/calvarnl_fs.f:16-64).  This header exposes:
+ *   - spoc_create / spoc_cal_var / spoc_cal_var_dev / spoc_rk4_*: the handle
+ *     API (tables and mesh uploaded once, state optionally device-resident);
+ *   - cal_var_: the literal 31-argument drop-in with the gfortran by-reference
+ *     ABI, reading the COMMON contents registered by spoc_register_commons;
+ *   - spoc_build_* helpers: host restatements of the reference set-up routines
+ *     (tables, mesh pointers, corner fix, L2 projection) for callers that do
+ *     not keep the Fortran driver.
+ *
+ * Conventions: every integer connectivity array stores the reference's 1-based
+ * ids; every 2-D array is Fortran column-major with an explicit leading
+ * dimension; all functions return 0 on success or a positive SPOC_E* code and
+ * never throw.  A handle owns one CUDA stream and is not re-entrant.
+ */
+#ifndef SPOC_GPU_H
+#define SPOC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define SPOC_OK 0
+#define SPOC_E_ARG 1         /* bad argument or size */
+#define SPOC_E_CUDA 2        /* CUDA runtime error (see spoc_last_error) */
+#define SPOC_E_NONFINITE 3   /* the device non-finite flag was raised */
+#define SPOC_E_MATRIX 4      /* a mass matrix is not positive definite */
+#define SPOC_E_MESH 5        /* connectivity check failed */
+#define SPOC_E_NOMEM 6       /* host or device allocation failed */
+#define SPOC_E_UNSUPPORTED 7 /* variant / precision / size not built */
+
+/* physics variants: the four link-time plug-ins of the reference */
+#define SPOC_LIN 0 /* src/calvar_lin.f   */
+#define SPOC_FS 1  /* src/calvarnl_fs.f  */
+#define SPOC_NS 2  /* src/calvarnl_ns.f  */
+#define SPOC_INV 3 /* src/calvarnl_inv.f */
+
+/* precision modes */
+#define SPOC_FP64 0 /* reference operation order, no contraction: bit-exact to the CPU restatement */
+
+/* COMMON-block content, as the Fortran driver holds it (src/shwwnl.f:60-71).
+ * amm and amml hold the upper Cholesky factors (src/shwwnl.f:153-156). */
+typedef struct {
+  int nc, nm, ng, ngf;
+  const double *wi, *xi, *yi; /* [ng]  /gauss/  */
+  const double *wif, *tif;    /* [ngf] /gaussf/ */
+  const double *pi2;          /* pi2(ld_pi2, nm)            /gauss2/ */
+  int ld_pi2;
+  const double *pico;         /* pico(ld_pico1, ld_pico2, 3) /gauss3/ */
+  int ld_pico1, ld_pico2;
+  const double *amm, *amml, *agx, *agy, *ammo; /* (ld_mat, nm) /matrices/ */
+  int ld_mat;
+  const int *cip;             /* cip(2, 0:ncip-1), ncip >= nc+1 */
+} spoc_tables;
+
+/* mesh pointers, exactly as cal_var receives them (src/calvarnl_fs.f:22-61) */
+typedef struct {
+  int ne, nf;
+  const int *itm;      /* itm(3,ne)  */
+  const int *its;      /* its(3,ne)  */
+  const int *tseg;     /* tseg(2,nf) (0 = wall) */
+  const int *ssit;     /* ssit(2,nf) */
+  const double *norm;  /* norm(2,nf) */
+  const double *vect;  /* vect(5,ne) */
+  const double *normt; /* normt(2,ne) */
+  const int *bdl;      /* bdl(ne), LOGICAL*4 */
+} spoc_mesh;
+
+/* physical parameters and time-constant fields (ld, ne) */
+typedef struct {
+  double mu0, mb0, g0;
+  const double *fc, *w0, *z0, *hb;
+  int ld;
+} spoc_params;
+
+typedef struct spoc_handle spoc_handle;
+
+/* Upload tables and mesh; allocate device work space for ne elements.
+ * Replaces the per-call COMMON/argument reads of cal_var (src/calvarnl_fs.f:9-64). */
+int spoc_create(const spoc_tables *tables, const spoc_mesh *mesh, int variant, int precision,
+                spoc_handle **out);
+void spoc_destroy(spoc_handle *h);
+/* Use an external cudaStream_t (0 = the handle's own stream). */
+int spoc_set_stream(spoc_handle *h, void *stream);
+/* Upload mu0, mb0, g0 and fc, w0, z0, hb (arguments of cal_var, src/calvarnl_fs.f:12). */
+int spoc_set_params(spoc_handle *h, const spoc_params *p);
+
+/* One right-hand-side evaluation with HOST arrays (ld, ne): the literal
+ * replacement of `call cal_var(...)` in the RK4 loop (src/shwwnl.f:238-274). */
+int spoc_cal_var(spoc_handle *h, int ld, const double *u0, const double *v0, const double *h0,
+                 double *u1, double *v1, double *h1);
+/* Same with DEVICE arrays (ld, ne), on the handle's stream. */
+int spoc_cal_var_dev(spoc_handle *h, int ld, const double *u0, const double *v0,
+                     const double *h0, double *u1, double *v1, double *h1);
+
+/* Device-resident state (src/shwwnl.f:180-188 init.bin layout, ld = nm packed or 45). */
+int spoc_set_state(spoc_handle *h, int ld, const double *u, const double *v, const double *hh);
+int spoc_get_state(spoc_handle *h, int ld, double *u, double *v, double *hh);
+/* nsteps classical RK4 steps on the resident state (src/shwwnl.f:233-286). */
+int spoc_rk4_steps(spoc_handle *h, double dt, int nsteps);
+/* H2D of (u,v,hh), nsteps RK4 steps, D2H back: the host-buffer entry point. */
+int spoc_rk4_steps_host(spoc_handle *h, int ld, double *u, double *v, double *hh, double dt,
+                        int nsteps);
+/* Kinetic/potential energy and mass of the resident state (src/energy.f:3-96). */
+int spoc_energy(spoc_handle *h, double *ke, double *pe, double *mass);
+/* CFL time step of src/cfl.f:4-52 on the device (in(3,ne), node coordinates). */
+int spoc_cfl(spoc_handle *h, int nn, const int *in, const double *xgr, const double *ygr,
+             double *cflmin, double *dt);
+/* Number of kernels this handle launched so far (telemetry). */
+long long spoc_kernel_launches(spoc_handle *h);
+/* Diagnostics (no reference counterpart): run nsteps RK4 steps like
+ * spoc_rk4_steps, timing every kernel with CUDA events on the handle's stream;
+ * kernel_ms[k] receives the total milliseconds of kernel kind k (nonlinear:
+ * 0 q-phase, 1 nonlinear volume, 2 tendency+RK4; linear: 0), *nkinds the
+ * number of kinds. */
+int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms, int *nkinds);
+/* Measured FP64 throughput of this GPU in TFLOP/s (2 flops per multiply-add);
+ * mode 0: fused multiply-add, mode 1: separately rounded multiply and add. */
+int spoc_fp64_peak(int mode, double *tflops);
+/* Message for the last SPOC_E_CUDA / SPOC_E_ARG on this thread. */
+const char *spoc_last_error(void);
+
+/* ---- Fortran drop-in ----
+ * Register the COMMON contents once (after dpotrf), then link this library
+ * instead of calvar*.o: cal_var_ has the reference argument list
+ * (src/calvarnl_fs.f:9-12) with gfortran's by-reference, trailing-underscore
+ * ABI.  A handle is created on the first call for (nf, ne) and reused.
+ * Errors set *spoc_cal_var_status() (the reference `stop`s instead). */
+int spoc_register_commons(const spoc_tables *tables, int variant, int precision);
+void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, double *u1, double *v1,
+              double *h1, int *tseg, int *pseg, int *ssit, int *itm, int *its, double *norm,
+              int *nbdl, int *pbdl, int *nint, int *pint, int *bdl, int *cip, double *vect,
+              double *normt, double *mu0, double *mb0, double *fc, double *beta, double *w0,
+              double *z0, double *g0, double *hb, double *time);
+int *spoc_cal_var_status(void);
+void spoc_release_commons(void);
+
+/* ---- host set-up helpers (no CUDA) ----
+ * Tables: read_gauss values in, then cal_p2 (src/nonlin.f:10-30), cal_pico
+ * (src/mat1.f:214-259), calip (src/mat1.f:383-410), cal_mat x5
+ * (src/mat1.f:90-142), cal_matl (src/mat1.f:285-368) and the two dpotrf
+ * (src/shwwnl.f:153-156).  Output arrays, caller-allocated:
+ *   pi2[ng*nm] (ld ng), pico[ngf*nm*3] (ld ngf, nm), amm/amml/agx/agy/ammo/
+ *   ammx/ammy[nm*nm] (ld nm), cip[2*(nc+1)].
+ * Returns 0, or SPOC_E_MATRIX with *info = the dpotrf info (column of failure,
+ * +1000 for amml). */
+int spoc_build_tables(int nc, int ng, int ngf, const double *wi, const double *xi,
+                      const double *yi, const double *wif, const double *tif, double *pi2,
+                      double *pico, double *amm, double *amml, double *agx, double *agy,
+                      double *ammo, double *ammx, double *ammy, int *cip, int *info);
+/* Mesh pointers: pointer_mesh (src/cmal_s.f:88-216), check_mesh (:222-277),
+ * cal_rotnf (src/mat1.f:7-23), cal_its (:28-64), calpre (src/shwwnl.f:350-422)
+ * and coriolis (src/mat1.f:69-83).  Face arrays are sized for nfmax faces
+ * (3*ne suffices); fc is (ld, ne) and is zeroed first. */
+int spoc_build_mesh(int nn, int ne, const int *in, const double *xgr, const double *ygr,
+                    int nc, double f0, double beta, int nfmax, int *nf, int *itm, int *its,
+                    int *tseg, int *pseg, int *ssit, double *norm, double *vect, double *normt,
+                    int *bdl, double *fc, int ld);
+/* Corner fix of src/chmal.f:240-330: flip the diagonal of each element with
+ * two wall faces, then rotate local numbering so a wall face is side 1. */
+int spoc_fix_mesh(int nn, int ne, int *in);
+/* L2 projection of calh (src/init.f:290-344): vals(ng, ne) are the function at
+ * the points returned by spoc_projection_points; out is (ld, ne).  amm is the
+ * Cholesky factor from spoc_build_tables. */
+int spoc_projection_points(int ne, const int *in, const double *xgr, const double *ygr, int ng,
+                           const double *xi, const double *yi, double *px, double *py);
+int spoc_project(int nc, int ng, const double *wi, const double *pi2, const double *amm,
+                 int ne, const double *vals, double *out, int ld);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPOC_GPU_H */

@@ -1,0 +1,246 @@
+"""Python binding of the CPU oracle (oracle/libspoc_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker.  The product never imports it.
+
+The oracle builds its own tables and mesh pointers from raw inputs (quadrature
+points, node coordinates, element-to-node table), so a comparison against the
+product checks the product's set-up code as well as its kernels.
+Parity status: unpinned against reference output (no golden data ships with
+the reference and it cannot be compiled here); pinned by the known-answer
+tests in tests/test_oracle_pins.py.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "libspoc_oracle.so"
+
+LIN, FS, NS, INV = 0, 1, 2, 3
+VARIANTS = {"lin": LIN, "fs": FS, "ns": NS, "inv": INV}
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+
+
+class Common(C.Structure):
+    _fields_ = [
+        ("nc", C.c_int), ("nm", C.c_int), ("ng", C.c_int), ("ngf", C.c_int),
+        ("wi", _DP), ("xi", _DP), ("yi", _DP), ("wif", _DP), ("tif", _DP),
+        ("pi2", _DP), ("ldq", C.c_int), ("pico", _DP), ("ldg", C.c_int), ("ldp", C.c_int),
+        ("amm", _DP), ("amml", _DP), ("agx", _DP), ("agy", _DP), ("ammo", _DP), ("ldm", C.c_int),
+        ("cip", _IP),
+    ]
+
+
+class MeshS(C.Structure):
+    _fields_ = [
+        ("ne", C.c_int), ("nf", C.c_int), ("itm", _IP), ("its", _IP), ("tseg", _IP),
+        ("ssit", _IP), ("norm", _DP), ("vect", _DP), ("normt", _DP), ("bdl", _IP),
+    ]
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile if it is missing or stale."""
+    src = [HERE / "spoc_oracle.c", HERE / "spoc_oracle.h", HERE / "Makefile"]
+    if not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in src):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(str(LIB))
+        L = _lib
+        L.ora_po.restype = C.c_double
+        L.ora_po.argtypes = [C.c_int, C.c_double]
+        L.ora_dpo.restype = C.c_double
+        L.ora_dpo.argtypes = [C.c_int, C.c_double]
+        L.ora_checkcfl.restype = C.c_double
+        L.ora_checkcfl.argtypes = [C.c_int, C.c_int, C.c_int, _DP, _IP, C.c_double, _DP, _DP, _DP]
+        for name in ("ora_cal_var",):
+            getattr(L, name).argtypes = [C.c_int, C.POINTER(Common), C.POINTER(MeshS), C.c_int,
+                                         _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP,
+                                         C.c_double, C.c_double, C.c_double, C.c_int]
+        L.ora_rk4.argtypes = [C.c_int, C.POINTER(Common), C.POINTER(MeshS), C.c_int, _DP, _DP, _DP,
+                              _DP, _DP, _DP, _DP, C.c_double, C.c_double, C.c_double, C.c_double,
+                              C.c_int, C.c_int]
+        L.ora_energy.argtypes = [C.POINTER(Common), C.c_int, C.c_int, _DP, _DP, _DP, C.c_double, _DP,
+                                 _DP, _DP, _DP, _IP, _DP, _DP]
+    return _lib
+
+
+def d(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_DP)
+
+
+def i(a):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_IP)
+
+
+def default_threads() -> int:
+    return max(1, len(os.sched_getaffinity(0)))
+
+
+class Tables:
+    """Oracle restatement of the set-up of src/shwwnl.f:127-156."""
+
+    def __init__(self, nc, ng, ngf, wi, xi, yi, wif, tif):
+        L = lib()
+        self.nc, self.ng, self.ngf = nc, ng, ngf
+        self.nm = nm = (nc + 1) * (nc + 2) // 2
+        self.wi, self.xi, self.yi = (np.ascontiguousarray(a, dtype=np.float64) for a in (wi, xi, yi))
+        self.wif, self.tif = (np.ascontiguousarray(a, dtype=np.float64) for a in (wif, tif))
+        self.pi2 = np.zeros((nm, ng))
+        L.ora_cal_p2(nc, ng, d(self.xi), d(self.yi), d(self.pi2), ng)
+        self.pico = np.zeros((3, nm, ngf))
+        L.ora_cal_pico(nc, ngf, d(self.tif), d(self.pico), ngf, nm)
+        self.cip = np.zeros((nc + 1, 2), np.int32)
+        L.ora_calip(nc, i(self.cip))
+        mats = {}
+        for k, name in enumerate(("amm", "ammx", "ammy", "agx", "agy")):
+            m = np.zeros((nm, nm))
+            L.ora_cal_mat(nc, ng, k, d(self.xi), d(self.yi), d(self.wi), d(m), nm)
+            mats[name] = m
+        self.ammo = mats["amm"].copy()
+        self.amml = np.zeros((nm, nm))
+        L.ora_cal_matl(nc, d(self.ammo), d(self.amml), nm)
+        self.amml_raw = self.amml.copy()
+        self.amm = mats["amm"]
+        self.ammx, self.ammy, self.agx, self.agy = mats["ammx"], mats["ammy"], mats["agx"], mats["agy"]
+        self.info_amm = L.ora_dpotf2_upper(nm, d(self.amm), nm)
+        self.info_amml = L.ora_dpotf2_upper(nm - nc - 1, d(self.amml), nm)
+        self.common = Common(nc, nm, ng, ngf, d(self.wi), d(self.xi), d(self.yi), d(self.wif),
+                             d(self.tif), d(self.pi2), ng, d(self.pico), ngf, nm, d(self.amm),
+                             d(self.amml), d(self.agx), d(self.agy), d(self.ammo), nm, i(self.cip))
+
+
+class Mesh:
+    """Oracle restatement of pointer_mesh / check_mesh / cal_rotnf / cal_its /
+    calpre / coriolis (src/shwwnl.f:162-174)."""
+
+    def __init__(self, inn, xgr, ygr, nc, f0=0.0, beta=0.0, ld=None):
+        L = lib()
+        self.inn = np.ascontiguousarray(inn, dtype=np.int32)
+        self.xgr = np.ascontiguousarray(xgr, dtype=np.float64)
+        self.ygr = np.ascontiguousarray(ygr, dtype=np.float64)
+        self.ne, self.nn = self.inn.shape[0], self.xgr.shape[0]
+        nm = (nc + 1) * (nc + 2) // 2
+        self.ld = ld or nm
+        nfmax = 3 * self.ne
+        self.itm = np.zeros((self.ne, 3), np.int32)
+        tseg = np.zeros((nfmax, 2), np.int32)
+        pseg = np.zeros((nfmax, 2), np.int32)
+        nf = L.ora_pointer_mesh(self.nn, self.ne, i(self.inn), i(self.itm), i(tseg), i(pseg), nfmax)
+        if nf < 0:
+            raise RuntimeError("pointer_mesh overflow")
+        self.nf = nf
+        self.tseg = np.ascontiguousarray(tseg[:nf])
+        self.pseg = np.ascontiguousarray(pseg[:nf])
+        self.check = L.ora_check_mesh(self.ne, nf, i(self.itm), i(self.tseg))
+        self.norm = np.zeros((nf, 2))
+        L.ora_cal_rotnf(nf, d(self.xgr), d(self.ygr), d(self.norm), i(self.pseg))
+        self.its = np.zeros((self.ne, 3), np.int32)
+        self.ssit = np.zeros((nf, 2), np.int32)
+        self.its_rc = L.ora_cal_its(nf, i(self.itm), i(self.its), i(self.tseg), i(self.ssit))
+        self.vect = np.zeros((self.ne, 5))
+        self.normt = np.zeros((self.ne, 2))
+        self.bdl = np.zeros(self.ne, np.int32)
+        self.pint = np.zeros(self.ne, np.int32)
+        self.pbdl = np.zeros(self.ne, np.int32)
+        nint, nbdl, nebd = C.c_int(), C.c_int(), C.c_int()
+        L.ora_calpre(self.nn, self.ne, nf, i(self.inn), d(self.xgr), d(self.ygr), d(self.vect),
+                     i(self.itm), d(self.norm), d(self.normt), i(self.bdl), C.byref(nint),
+                     i(self.pint), C.byref(nbdl), i(self.pbdl), C.byref(nebd), i(self.tseg),
+                     i(self.pseg))
+        self.nint, self.nbdl, self.nebd = nint.value, nbdl.value, nebd.value
+        self.fc = np.zeros((self.ne, self.ld))
+        L.ora_coriolis.argtypes = [C.c_int, C.c_int, _IP, _DP, _DP, _DP, C.c_int, C.c_double, C.c_double]
+        L.ora_coriolis(nc, self.ne, i(self.inn), d(self.xgr), d(self.ygr), d(self.fc), self.ld, f0, beta)
+        self.s = MeshS(self.ne, nf, i(self.itm), i(self.its), i(self.tseg), i(self.ssit),
+                       d(self.norm), d(self.vect), d(self.normt), i(self.bdl))
+
+
+def cal_var(variant, T: Tables, M: Mesh, u0, v0, h0, fc, w0, z0, hb, mu0, mb0, g0, nthreads=None):
+    ld = u0.shape[1]
+    out = [np.zeros_like(u0) for _ in range(3)]
+    rc = lib().ora_cal_var(VARIANTS.get(variant, variant), C.byref(T.common), C.byref(M.s), ld,
+                           d(u0), d(v0), d(h0), *map(d, out), d(fc), d(w0), d(z0), d(hb),
+                           mu0, mb0, g0, nthreads or default_threads())
+    if rc:
+        raise RuntimeError(f"ora_cal_var rc={rc}")
+    return tuple(out)
+
+
+def rk4(variant, T: Tables, M: Mesh, u, v, h, fc, w0, z0, hb, mu0, mb0, g0, dt, nsteps,
+        nthreads=None):
+    """nsteps RK4 steps in place on (u, v, h)."""
+    rc = lib().ora_rk4(VARIANTS.get(variant, variant), C.byref(T.common), C.byref(M.s), u.shape[1],
+                       d(u), d(v), d(h), d(fc), d(w0), d(z0), d(hb), mu0, mb0, g0, dt, nsteps,
+                       nthreads or default_threads())
+    if rc:
+        raise RuntimeError(f"ora_rk4 rc={rc}")
+
+
+def energy(T: Tables, M: Mesh, u, v, h, hb, g0):
+    k, p, m = C.c_double(), C.c_double(), C.c_double()
+    lib().ora_energy(C.byref(T.common), M.ne, u.shape[1], d(u), d(v), d(h), g0, d(hb),
+                     C.byref(k), C.byref(p), C.byref(m), i(M.inn), d(M.xgr), d(M.ygr))
+    return k.value, p.value, m.value
+
+
+def checkcfl(nc, M: Mesh, hb, g0):
+    c = C.c_double()
+    dt = lib().ora_checkcfl(nc, M.ne, hb.shape[1], d(hb), i(M.inn), g0, d(M.xgr), d(M.ygr),
+                            C.byref(c))
+    return c.value, dt
+
+
+def calh(T: Tables, M: Mesh, f, ld=None):
+    """calh of src/init.f:290-344 for a vectorised f(x, y)."""
+    L = lib()
+    px = np.zeros((M.ne, T.ng))
+    py = np.zeros((M.ne, T.ng))
+    L.ora_calh_points(C.byref(T.common), M.ne, i(M.inn), d(M.xgr), d(M.ygr), d(px), d(py))
+    vals = np.ascontiguousarray(f(px, py), dtype=np.float64)
+    out = np.zeros((M.ne, ld or T.nm))
+    L.ora_calh(C.byref(T.common), M.ne, d(vals), d(out), out.shape[1])
+    return out, px, py
+
+
+def changemaille(inn, nn):
+    """chmal corner fix (src/chmal.f:240-330) on a copy of `in`."""
+    L = lib()
+    out = np.array(inn, dtype=np.int32, order="C", copy=True)
+    ne = out.shape[0]
+    nfmax = 3 * ne
+    itm = np.zeros((ne, 3), np.int32)
+    tseg = np.zeros((nfmax, 2), np.int32)
+    pseg = np.zeros((nfmax, 2), np.int32)
+    nf = L.ora_pointer_mesh(nn, ne, i(out), i(itm), i(tseg), i(pseg), nfmax)
+    rc = L.ora_changemaille(nn, ne, nf, i(out), i(itm), i(tseg), i(pseg))
+    if rc:
+        raise RuntimeError("changemaille failed")
+    return out
+
+
+def mass_norm(T: Tables, M: Mesh, a):
+    """Physical L2 norm sqrt(sum_e det_e a_e^T ammo a_e) of a modal field (ne, ld)."""
+    nm = T.nm
+    x = a[:, :nm]
+    det = M.vect[:, 0] * M.vect[:, 3] - M.vect[:, 2] * M.vect[:, 1]
+    G = T.ammo.T  # numpy [j, i] holds ammo(i, j); symmetric anyway
+    return float(np.sqrt(np.sum(det * np.einsum("ei,ij,ej->e", x, G, x))))

@@ -1,0 +1,400 @@
+"""ctypes binding of the C ABI in include/spoc_gpu.h (spoc_b200/libspoc_gpu.so).
+
+This is the host-side mirror of the reference's operator interface: the
+Fortran driver calls `cal_var` (src/calvarnl_fs.f:9-12) four times per RK4
+step (src/shwwnl.f:238-274); here `Solver.cal_var` is that call with host
+arrays, `Solver.rk4_steps` keeps the state on the device, and the set-up
+helpers restate read_gauss / cal_p2 / cal_pico / calip / cal_mat / cal_matl /
+dpotrf / pointer_mesh / calpre / coriolis / calh.
+
+Arrays follow the Fortran layout: a field of `ne` elements with leading
+dimension `ld` is a C-contiguous numpy array of shape (ne, ld); connectivity
+arrays hold 1-based ids.  Every call raises SpocError on a non-zero status.
+The library is required: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libspoc_gpu.so"
+
+LIN, FS, NS, INV = 0, 1, 2, 3
+VARIANTS = {"lin": LIN, "fs": FS, "ns": NS, "inv": INV}
+FP64 = 0
+
+_STATUS = {
+    0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-finite tendency",
+    4: "mass matrix not positive definite", 5: "mesh check failed", 6: "out of memory",
+    7: "unsupported configuration",
+}
+
+
+class SpocError(RuntimeError):
+    def __init__(self, code: int, where: str, detail: str = ""):
+        self.code = code
+        super().__init__(f"{where}: {_STATUS.get(code, code)} ({code}) {detail}".rstrip())
+
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+
+
+class _Tables(C.Structure):
+    _fields_ = [
+        ("nc", C.c_int), ("nm", C.c_int), ("ng", C.c_int), ("ngf", C.c_int),
+        ("wi", _DP), ("xi", _DP), ("yi", _DP), ("wif", _DP), ("tif", _DP),
+        ("pi2", _DP), ("ld_pi2", C.c_int),
+        ("pico", _DP), ("ld_pico1", C.c_int), ("ld_pico2", C.c_int),
+        ("amm", _DP), ("amml", _DP), ("agx", _DP), ("agy", _DP), ("ammo", _DP), ("ld_mat", C.c_int),
+        ("cip", _IP),
+    ]
+
+
+class _Mesh(C.Structure):
+    _fields_ = [
+        ("ne", C.c_int), ("nf", C.c_int),
+        ("itm", _IP), ("its", _IP), ("tseg", _IP), ("ssit", _IP),
+        ("norm", _DP), ("vect", _DP), ("normt", _DP), ("bdl", _IP),
+    ]
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("mu0", C.c_double), ("mb0", C.c_double), ("g0", C.c_double),
+        ("fc", _DP), ("w0", _DP), ("z0", _DP), ("hb", _DP), ("ld", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: Path | str | None = None) -> C.CDLL:
+    """Load libspoc_gpu.so (build it first with spoc_b200.build.build())."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: run `python -m spoc_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(str(p))
+    vp = C.c_void_p
+    sig = {
+        "spoc_create": (C.c_int, [C.POINTER(_Tables), C.POINTER(_Mesh), C.c_int, C.c_int, C.POINTER(vp)]),
+        "spoc_destroy": (None, [vp]),
+        "spoc_set_stream": (C.c_int, [vp, vp]),
+        "spoc_set_params": (C.c_int, [vp, C.POINTER(_Params)]),
+        "spoc_cal_var": (C.c_int, [vp, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP]),
+        "spoc_cal_var_dev": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, vp]),
+        "spoc_set_state": (C.c_int, [vp, C.c_int, _DP, _DP, _DP]),
+        "spoc_get_state": (C.c_int, [vp, C.c_int, _DP, _DP, _DP]),
+        "spoc_rk4_steps": (C.c_int, [vp, C.c_double, C.c_int]),
+        "spoc_rk4_steps_host": (C.c_int, [vp, C.c_int, _DP, _DP, _DP, C.c_double, C.c_int]),
+        "spoc_energy": (C.c_int, [vp, _DP, _DP, _DP]),
+        "spoc_cfl": (C.c_int, [vp, C.c_int, _IP, _DP, _DP, _DP, _DP]),
+        "spoc_kernel_launches": (C.c_longlong, [vp]),
+        "spoc_profile_rk4": (C.c_int, [vp, C.c_double, C.c_int, _DP, _IP]),
+        "spoc_fp64_peak": (C.c_int, [C.c_int, _DP]),
+        "spoc_last_error": (C.c_char_p, []),
+        "spoc_register_commons": (C.c_int, [C.POINTER(_Tables), C.c_int, C.c_int]),
+        "spoc_cal_var_status": (_IP, []),
+        "spoc_release_commons": (None, []),
+        "spoc_build_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP,
+                                        _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _IP]),
+        "spoc_build_mesh": (C.c_int, [C.c_int, C.c_int, _IP, _DP, _DP, C.c_int, C.c_double,
+                                      C.c_double, C.c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP,
+                                      _DP, _DP, _IP, _DP, C.c_int]),
+        "spoc_fix_mesh": (C.c_int, [C.c_int, C.c_int, _IP]),
+        "spoc_projection_points": (C.c_int, [C.c_int, _IP, _DP, _DP, C.c_int, _DP, _DP, _DP, _DP]),
+        "spoc_project": (C.c_int, [C.c_int, C.c_int, _DP, _DP, _DP, C.c_int, _DP, _DP, C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    # cal_var_ takes 31 pointers (gfortran by-reference ABI)
+    lib.cal_var_.restype = None
+    lib.cal_var_.argtypes = [vp] * 31
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _d(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_DP)
+
+
+def _i(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_IP)
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != 0:
+        msg = load_library().spoc_last_error()
+        raise SpocError(rc, where, msg.decode() if msg else "")
+
+
+# ---------------------------------------------------------------------------
+# quadrature data (src/readgauss.f)
+# ---------------------------------------------------------------------------
+_QUAD = None
+
+
+def quadrature(ng: int, ngf: int):
+    """(wi, xi, yi, wif, tif) of tri2_<ng>.dat and legen<ngf>.dat."""
+    global _QUAD
+    if _QUAD is None:
+        _QUAD = json.loads((HERE / "data" / "quadrature_tables.json").read_text())
+    tri = _QUAD["triangle"].get(str(ng))
+    edge = _QUAD["edge"].get(str(ngf))
+    if tri is None or edge is None:
+        raise ValueError(f"no quadrature table tri2_{ng}.dat / legen{ngf}.dat")
+    t = np.array([[float(v) for v in r] for r in tri], dtype=np.float64)
+    e = np.array([[float(v) for v in r] for r in edge], dtype=np.float64)
+    return (np.ascontiguousarray(t[:, 0]), np.ascontiguousarray(t[:, 1]),
+            np.ascontiguousarray(t[:, 2]), np.ascontiguousarray(e[:, 0]),
+            np.ascontiguousarray(e[:, 1]))
+
+
+@dataclass
+class Tables:
+    """Reference-element tables (the COMMON blocks of src/shwwnl.f:60-71)."""
+    nc: int
+    ng: int
+    ngf: int
+    wi: np.ndarray
+    xi: np.ndarray
+    yi: np.ndarray
+    wif: np.ndarray
+    tif: np.ndarray
+    pi2: np.ndarray   # (nm, ng): pi2(q, n) at [n, q]
+    pico: np.ndarray  # (3, nm, ngf): pico(j, n, s) at [s, n, j]
+    amm: np.ndarray   # (nm, nm) column-major storage: amm(i, j) at [j, i]; upper Cholesky factor
+    amml: np.ndarray
+    agx: np.ndarray
+    agy: np.ndarray
+    ammo: np.ndarray
+    ammx: np.ndarray
+    ammy: np.ndarray
+    cip: np.ndarray   # (nc+1, 2)
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def nm(self) -> int:
+        return (self.nc + 1) * (self.nc + 2) // 2
+
+    def struct(self) -> _Tables:
+        nm = self.nm
+        t = _Tables(self.nc, nm, self.ng, self.ngf, _d(self.wi), _d(self.xi), _d(self.yi),
+                    _d(self.wif), _d(self.tif), _d(self.pi2), self.ng, _d(self.pico), self.ngf,
+                    nm, _d(self.amm), _d(self.amml), _d(self.agx), _d(self.agy), _d(self.ammo),
+                    nm, _i(self.cip))
+        return t
+
+
+def fp64_peak(mode: int = 0) -> float:
+    """Measured FP64 TFLOP/s of the current GPU (0: FMA, 1: mul + add)."""
+    t = C.c_double()
+    _check(load_library().spoc_fp64_peak(mode, C.byref(t)), "fp64_peak")
+    return t.value
+
+
+def build_tables(nc: int, ng: int, ngf: int) -> Tables:
+    """Quadrature, basis tables, operators and Cholesky factors for degree nc."""
+    lib = load_library()
+    wi, xi, yi, wif, tif = quadrature(ng, ngf)
+    nm = (nc + 1) * (nc + 2) // 2
+    z = lambda *s: np.zeros(s, dtype=np.float64)
+    T = Tables(nc, ng, ngf, wi, xi, yi, wif, tif, z(nm, ng), z(3, nm, ngf), z(nm, nm), z(nm, nm),
+               z(nm, nm), z(nm, nm), z(nm, nm), z(nm, nm), z(nm, nm),
+               np.zeros((nc + 1, 2), dtype=np.int32))
+    info = C.c_int(0)
+    rc = lib.spoc_build_tables(nc, ng, ngf, _d(wi), _d(xi), _d(yi), _d(wif), _d(tif), _d(T.pi2),
+                               _d(T.pico), _d(T.amm), _d(T.amml), _d(T.agx), _d(T.agy),
+                               _d(T.ammo), _d(T.ammx), _d(T.ammy), _i(T.cip), C.byref(info))
+    if rc:
+        raise SpocError(rc, f"build_tables(nc={nc}, ng={ng})", f"dpotrf info {info.value}")
+    return T
+
+
+@dataclass
+class Mesh:
+    """Mesh pointers of pointer_mesh / cal_its / calpre (1-based ids)."""
+    nn: int
+    ne: int
+    nf: int
+    inn: np.ndarray   # (ne, 3) node ids
+    xgr: np.ndarray
+    ygr: np.ndarray
+    itm: np.ndarray   # (ne, 3)
+    its: np.ndarray   # (ne, 3)
+    tseg: np.ndarray  # (nf, 2)
+    pseg: np.ndarray  # (nf, 2)
+    ssit: np.ndarray  # (nf, 2)
+    norm: np.ndarray  # (nf, 2)
+    vect: np.ndarray  # (ne, 5)
+    normt: np.ndarray  # (ne, 2)
+    bdl: np.ndarray   # (ne,)
+    fc: np.ndarray    # (ne, ld)
+
+    def struct(self) -> _Mesh:
+        return _Mesh(self.ne, self.nf, _i(self.itm), _i(self.its), _i(self.tseg), _i(self.ssit),
+                     _d(self.norm), _d(self.vect), _d(self.normt), _i(self.bdl))
+
+    @property
+    def det(self) -> np.ndarray:
+        v = self.vect
+        return v[:, 0] * v[:, 3] - v[:, 2] * v[:, 1]
+
+
+def build_mesh(inn: np.ndarray, xgr: np.ndarray, ygr: np.ndarray, nc: int, f0: float = 0.0,
+               beta: float = 0.0, ld: int | None = None) -> Mesh:
+    lib = load_library()
+    inn = np.ascontiguousarray(inn, dtype=np.int32)
+    xgr = np.ascontiguousarray(xgr, dtype=np.float64)
+    ygr = np.ascontiguousarray(ygr, dtype=np.float64)
+    ne, nn = inn.shape[0], xgr.shape[0]
+    nm = (nc + 1) * (nc + 2) // 2
+    ld = ld or nm
+    nfmax = 3 * ne
+    nf = C.c_int(0)
+    itm = np.zeros((ne, 3), np.int32)
+    its = np.zeros((ne, 3), np.int32)
+    tseg = np.zeros((nfmax, 2), np.int32)
+    pseg = np.zeros((nfmax, 2), np.int32)
+    ssit = np.zeros((nfmax, 2), np.int32)
+    norm = np.zeros((nfmax, 2))
+    vect = np.zeros((ne, 5))
+    normt = np.zeros((ne, 2))
+    bdl = np.zeros(ne, np.int32)
+    fc = np.zeros((ne, ld))
+    rc = lib.spoc_build_mesh(nn, ne, _i(inn), _d(xgr), _d(ygr), nc, f0, beta, nfmax,
+                             C.byref(nf), _i(itm), _i(its), _i(tseg), _i(pseg), _i(ssit),
+                             _d(norm), _d(vect), _d(normt), _i(bdl), _d(fc), ld)
+    _check(rc, "build_mesh")
+    k = nf.value
+    return Mesh(nn, ne, k, inn, xgr, ygr, itm, its, np.ascontiguousarray(tseg[:k]),
+                np.ascontiguousarray(pseg[:k]), np.ascontiguousarray(ssit[:k]),
+                np.ascontiguousarray(norm[:k]), vect, normt, bdl, fc)
+
+
+def fix_mesh(inn: np.ndarray, nn: int) -> np.ndarray:
+    """Corner fix of src/chmal.f (returns a corrected copy of `in`)."""
+    out = np.array(inn, dtype=np.int32, order="C", copy=True)
+    _check(load_library().spoc_fix_mesh(nn, out.shape[0], _i(out)), "fix_mesh")
+    return out
+
+
+def projection_points(mesh: Mesh, T: Tables):
+    px = np.zeros((mesh.ne, T.ng))
+    py = np.zeros((mesh.ne, T.ng))
+    _check(load_library().spoc_projection_points(mesh.ne, _i(mesh.inn), _d(mesh.xgr), _d(mesh.ygr),
+                                                 T.ng, _d(T.xi), _d(T.yi), _d(px), _d(py)),
+           "projection_points")
+    return px, py
+
+
+def project(T: Tables, vals: np.ndarray, ld: int | None = None) -> np.ndarray:
+    """calh (src/init.f:290-344): L2 projection of point values (ne, ng)."""
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    ne = vals.shape[0]
+    ld = ld or T.nm
+    out = np.zeros((ne, ld))
+    _check(load_library().spoc_project(T.nc, T.ng, _d(T.wi), _d(T.pi2), _d(T.amm), ne, _d(vals),
+                                       _d(out), ld), "project")
+    return out
+
+
+class Solver:
+    """One device handle: tables and mesh resident, one CUDA stream."""
+
+    def __init__(self, T: Tables, mesh: Mesh, variant: int | str, precision: int = FP64):
+        self.lib = load_library()
+        self.T, self.mesh = T, mesh
+        self.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        self.nm = T.nm
+        self._h = C.c_void_p()
+        ts, ms = T.struct(), mesh.struct()
+        _check(self.lib.spoc_create(C.byref(ts), C.byref(ms), self.variant, precision,
+                                    C.byref(self._h)), "spoc_create")
+
+    def close(self) -> None:
+        if self._h:
+            self.lib.spoc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(self.lib.spoc_set_stream(self._h, C.c_void_p(stream_ptr)), "set_stream")
+
+    def set_params(self, mu0: float, mb0: float, g0: float, hb: np.ndarray, fc=None, w0=None,
+                   z0=None) -> None:
+        ld = hb.shape[1]
+        keep = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None
+                for a in (fc, w0, z0, hb)]
+        ptr = lambda a: _d(a) if a is not None else _DP()
+        p = _Params(mu0, mb0, g0, ptr(keep[0]), ptr(keep[1]), ptr(keep[2]), ptr(keep[3]), ld)
+        _check(self.lib.spoc_set_params(self._h, C.byref(p)), "set_params")
+
+    def cal_var(self, u0, v0, h0):
+        """One right-hand side with host arrays (ne, ld); returns (u1, v1, h1)."""
+        ld = u0.shape[1]
+        outs = [np.zeros_like(u0) for _ in range(3)]
+        _check(self.lib.spoc_cal_var(self._h, ld, _d(u0), _d(v0), _d(h0), *map(_d, outs)),
+               "spoc_cal_var")
+        return tuple(outs)
+
+    def cal_var_dev(self, ld: int, ptrs) -> None:
+        _check(self.lib.spoc_cal_var_dev(self._h, ld, *[C.c_void_p(p) for p in ptrs]),
+               "spoc_cal_var_dev")
+
+    def set_state(self, u, v, h) -> None:
+        _check(self.lib.spoc_set_state(self._h, u.shape[1], _d(u), _d(v), _d(h)), "set_state")
+
+    def get_state(self, ld: int | None = None):
+        ld = ld or self.nm
+        outs = [np.zeros((self.mesh.ne, ld)) for _ in range(3)]
+        _check(self.lib.spoc_get_state(self._h, ld, *map(_d, outs)), "get_state")
+        return tuple(outs)
+
+    def rk4_steps(self, dt: float, nsteps: int) -> None:
+        _check(self.lib.spoc_rk4_steps(self._h, dt, nsteps), "rk4_steps")
+
+    def rk4_steps_host(self, u, v, h, dt: float, nsteps: int) -> None:
+        _check(self.lib.spoc_rk4_steps_host(self._h, u.shape[1], _d(u), _d(v), _d(h), dt, nsteps),
+               "rk4_steps_host")
+
+    def energy(self):
+        k, p, m = C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib.spoc_energy(self._h, C.byref(k), C.byref(p), C.byref(m)), "energy")
+        return k.value, p.value, m.value
+
+    def cfl(self):
+        c, dt = C.c_double(), C.c_double()
+        m = self.mesh
+        _check(self.lib.spoc_cfl(self._h, m.nn, _i(m.inn), _d(m.xgr), _d(m.ygr), C.byref(c),
+                                 C.byref(dt)), "cfl")
+        return c.value, dt.value
+
+    def profile_rk4(self, dt: float, nsteps: int):
+        """Per-kernel-kind milliseconds over nsteps steps (advances the state)."""
+        ms = np.zeros(3)
+        nk = C.c_int()
+        _check(self.lib.spoc_profile_rk4(self._h, dt, nsteps, _d(ms), C.byref(nk)), "profile_rk4")
+        return ms[: nk.value]
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.spoc_kernel_launches(self._h))

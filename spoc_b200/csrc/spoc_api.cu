@@ -1,0 +1,748 @@
+// C ABI of the B200 SPOC right-hand side: handle life cycle, uploads, RK4
+// driver, diagnostics and the Fortran cal_var_ drop-in.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/spoc_gpu.h"
+#include "spoc_kernels.h"
+
+using namespace spoc;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *what, cudaError_t ce = cudaSuccess) {
+  char buf[512];
+  if (ce != cudaSuccess)
+    std::snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(ce));
+  else
+    std::snprintf(buf, sizeof buf, "%s", what);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call, what)                                  \
+  do {                                                  \
+    cudaError_t ce_ = (call);                           \
+    if (ce_ != cudaSuccess) return fail(SPOC_E_CUDA, what, ce_); \
+  } while (0)
+
+template <class T>
+cudaError_t dev_upload(T **dst, const std::vector<T> &src) {
+  cudaError_t e = cudaMalloc((void **)dst, sizeof(T) * (src.empty() ? 1 : src.size()));
+  if (e != cudaSuccess) return e;
+  if (!src.empty()) e = cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice);
+  return e;
+}
+
+}  // namespace
+
+struct spoc_handle {
+  int variant = 0, precision = 0;
+  int nc = 0, nm = 0, ng = 0, ngf = 0, nmr = 0, ne = 0, nf = 0;
+  int sms = 148;
+  cudaStream_t own = nullptr, st = nullptr;
+  long long launches = 0;
+  double mu0 = 0, mb0 = 0, g0 = 9.81, hh0 = 0;
+  bool have_params = false;
+  std::vector<void *> allocs;
+  DevOps op{};
+  DevMesh mesh{};
+  // fields, each ne*nm doubles
+  double *U0[3]{}, *SA[3]{}, *SB[3]{}, *ACC[3]{}, *TEND[3]{}, *SIN[3]{};
+  double *hb = nullptr, *w0 = nullptr, *z0 = nullptr, *fc = nullptr;
+  double *q = nullptr, *f = nullptr, *gx0 = nullptr, *gy0 = nullptr, *uh = nullptr, *vh = nullptr;
+  double *eterms = nullptr, *escal = nullptr;
+  int *flag = nullptr;
+  unsigned long long *cflbits = nullptr;
+
+  template <class T>
+  cudaError_t alloc(T **p, size_t n) {
+    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
+    if (e == cudaSuccess) allocs.push_back((void *)*p);
+    return e;
+  }
+  template <class T>
+  cudaError_t upload(const T **p, const std::vector<T> &v) {
+    T *d = nullptr;
+    cudaError_t e = dev_upload(&d, v);
+    if (d) allocs.push_back((void *)d);
+    *p = d;
+    return e;
+  }
+  ~spoc_handle() {
+    for (void *p : allocs) cudaFree(p);
+    if (own) cudaStreamDestroy(own);
+  }
+};
+
+namespace {
+
+size_t fsize(const spoc_handle *h) { return (size_t)h->ne * h->nm; }
+
+int build_ops(spoc_handle *h, const spoc_tables *t) {
+  const int nm = h->nm, ng = h->ng, G = h->ngf, nc = h->nc, nmr = h->nmr;
+  const int lm = t->ld_mat, lq = t->ld_pi2, lp1 = t->ld_pico1, lp2 = t->ld_pico2;
+  auto MAT = [&](const double *a, int i, int j) { return a[(size_t)j * lm + i]; };
+  std::vector<double> agx(nm * nm), agy(nm * nm), p2(nm * ng), p2t(ng * nm), wi(ng), wif(G);
+  std::vector<double> picoF(3 * nm * G), picoT(3 * G * nm), uT(nm * nm), uC(nm * nm), dia1(nm);
+  std::vector<double> ulT(nm * nm, 0.0), ulC(nm * nm, 0.0), dia2(nm, 0.0), ammo1(nm);
+  for (int j = 0; j < nm; ++j)
+    for (int i = 0; i < nm; ++i) {
+      agx[j * nm + i] = MAT(t->agx, j, i);
+      agy[j * nm + i] = MAT(t->agy, j, i);
+      uT[j * nm + i] = MAT(t->amm, j, i);
+      uC[j * nm + i] = MAT(t->amm, i, j);
+    }
+  for (int i = 0; i < nm; ++i) {
+    // dia1(i) = 1.d0/amm(i,i) (calvarnl_fs.f:72-74)
+    dia1[i] = 1.0 / MAT(t->amm, i, i);
+    ammo1[i] = MAT(t->ammo, i, 0);
+  }
+  for (int j = 0; j < nmr; ++j)
+    for (int i = 0; i < nmr; ++i) {
+      ulT[j * nm + i] = MAT(t->amml, j, i);
+      ulC[j * nm + i] = MAT(t->amml, i, j);
+    }
+  for (int i = 0; i < nmr; ++i) dia2[i] = 1.0 / MAT(t->amml, i, i);
+  for (int n = 0; n < nm; ++n)
+    for (int qp = 0; qp < ng; ++qp) {
+      p2[(size_t)n * ng + qp] = t->pi2[(size_t)n * lq + qp];
+      p2t[(size_t)qp * nm + n] = t->pi2[(size_t)n * lq + qp];
+    }
+  for (int qp = 0; qp < ng; ++qp) wi[qp] = t->wi[qp];
+  for (int j = 0; j < G; ++j) wif[j] = t->wif[j];
+  for (int s = 0; s < 3; ++s)
+    for (int n = 0; n < nm; ++n)
+      for (int j = 0; j < G; ++j) {
+        const double v = t->pico[((size_t)s * lp2 + n) * lp1 + j];
+        picoF[((size_t)s * nm + n) * G + j] = v;
+        picoT[((size_t)s * G + j) * nm + n] = v;
+      }
+  // reduc_gn / reduc_inv_gn index maps from cip (src/mat1.f:418-473)
+  std::vector<int> rk(nm, 0), ri0(nm, 0), rsg(nm, 1), ik(nm, 0), ia(nm, 0), icnt(nm, 0);
+  const int *cip = t->cip;
+  for (int j = 0; j <= nc - 1; ++j) {
+    const int c1 = cip[2 * j], c2 = cip[2 * j + 1];
+    for (int l = 0; l <= nc - 1 - j; ++l) {
+      const int r = c2 + l;
+      if (r < 0 || r >= nmr) return fail(SPOC_E_ARG, "cip table inconsistent with nc");
+      rk[r] = c1 + l + 1;
+      ri0[r] = c1;
+      rsg[r] = (l % 2 == 0) ? 1 : -1;
+    }
+    if (c1 < 0 || c1 >= nm) return fail(SPOC_E_ARG, "cip table inconsistent with nc");
+    ik[c1] = 1;
+    ia[c1] = c2;
+    icnt[c1] = nc - j;
+    for (int l = 0; l <= nc - j - 1; ++l) {
+      ik[c1 + l + 1] = 2;
+      ia[c1 + l + 1] = c2 + l;
+    }
+  }
+  ik[nm - 1] = 0;
+  DevOps &o = h->op;
+  o.nc = nc; o.nm = nm; o.nmr = nmr; o.ng = ng; o.ngf = G;
+  CK(h->upload(&o.agx, agx), "upload agx");
+  CK(h->upload(&o.agy, agy), "upload agy");
+  CK(h->upload(&o.p2, p2), "upload pi2");
+  CK(h->upload(&o.p2t, p2t), "upload pi2t");
+  CK(h->upload(&o.wi, wi), "upload wi");
+  CK(h->upload(&o.wif, wif), "upload wif");
+  CK(h->upload(&o.picoF, picoF), "upload pico");
+  CK(h->upload(&o.picoT, picoT), "upload picoT");
+  CK(h->upload(&o.uT, uT), "upload amm");
+  CK(h->upload(&o.uC, uC), "upload amm");
+  CK(h->upload(&o.dia1, dia1), "upload dia1");
+  CK(h->upload(&o.ulT, ulT), "upload amml");
+  CK(h->upload(&o.ulC, ulC), "upload amml");
+  CK(h->upload(&o.dia2, dia2), "upload dia2");
+  CK(h->upload(&o.red_k, rk), "upload reduc");
+  CK(h->upload(&o.red_i0, ri0), "upload reduc");
+  CK(h->upload(&o.red_sg, rsg), "upload reduc");
+  CK(h->upload(&o.inv_kind, ik), "upload reduc");
+  CK(h->upload(&o.inv_a, ia), "upload reduc");
+  CK(h->upload(&o.inv_cnt, icnt), "upload reduc");
+  CK(h->upload(&o.ammo1, ammo1), "upload ammo");
+  return SPOC_OK;
+}
+
+int build_mesh(spoc_handle *h, const spoc_mesh *m) {
+  const int ne = m->ne, nf = m->nf;
+  std::vector<int> itm(3 * (size_t)ne), its(3 * (size_t)ne), tseg(2 * (size_t)nf),
+      ssit(2 * (size_t)nf), bdl(ne);
+  std::vector<double> norm(2 * (size_t)nf), vect(5 * (size_t)ne), normt(2 * (size_t)ne);
+  for (int e = 0; e < ne; ++e) {
+    for (int k = 0; k < 3; ++k) {
+      const int f = m->itm[3 * (size_t)e + k];
+      if (f < 1 || f > nf) return fail(SPOC_E_MESH, "itm out of range");
+      itm[3 * (size_t)e + k] = f - 1;
+      const int s = m->its[3 * (size_t)e + k];
+      if (s != 1 && s != -1) return fail(SPOC_E_MESH, "its not +/-1");
+      its[3 * (size_t)e + k] = s;
+    }
+    for (int c = 0; c < 5; ++c) vect[5 * (size_t)e + c] = m->vect[5 * (size_t)e + c];
+    normt[2 * (size_t)e] = m->normt[2 * (size_t)e];
+    normt[2 * (size_t)e + 1] = m->normt[2 * (size_t)e + 1];
+    bdl[e] = m->bdl[e] != 0;
+  }
+  for (int f = 0; f < nf; ++f) {
+    const int t1 = m->tseg[2 * (size_t)f], t2 = m->tseg[2 * (size_t)f + 1];
+    if (t1 < 1 || t1 > ne || t2 < 0 || t2 > ne) return fail(SPOC_E_MESH, "tseg out of range");
+    tseg[2 * (size_t)f] = t1 - 1;
+    tseg[2 * (size_t)f + 1] = t2 - 1;  // wall -> -1
+    const int s1 = m->ssit[2 * (size_t)f], s2 = m->ssit[2 * (size_t)f + 1];
+    if (s1 < 1 || s1 > 3 || (t2 > 0 && (s2 < 1 || s2 > 3)))
+      return fail(SPOC_E_MESH, "ssit out of range");
+    ssit[2 * (size_t)f] = s1 - 1;
+    ssit[2 * (size_t)f + 1] = t2 > 0 ? s2 - 1 : 0;
+    // the reference traces a wall face with side 1 of its element (calflu.f:35-39)
+    if (t2 == 0 && s1 != 1) return fail(SPOC_E_MESH, "wall face is not side 1 of its element");
+    norm[2 * (size_t)f] = m->norm[2 * (size_t)f];
+    norm[2 * (size_t)f + 1] = m->norm[2 * (size_t)f + 1];
+  }
+  DevMesh &d = h->mesh;
+  d.ne = ne;
+  d.nf = nf;
+  CK(h->upload(&d.itm, itm), "upload itm");
+  CK(h->upload(&d.its, its), "upload its");
+  CK(h->upload(&d.tseg, tseg), "upload tseg");
+  CK(h->upload(&d.ssit, ssit), "upload ssit");
+  CK(h->upload(&d.norm, norm), "upload norm");
+  CK(h->upload(&d.vect, vect), "upload vect");
+  CK(h->upload(&d.normt, normt), "upload normt");
+  CK(h->upload(&d.bdl, bdl), "upload bdl");
+  return SPOC_OK;
+}
+
+// host (ld, ne) <-> device packed (nm, ne)
+cudaError_t copy_in(spoc_handle *h, double *dst, const double *src, int ld, cudaMemcpyKind k) {
+  return cudaMemcpy2DAsync(dst, sizeof(double) * h->nm, src, sizeof(double) * ld,
+                           sizeof(double) * h->nm, h->ne, k, h->st);
+}
+cudaError_t copy_out(spoc_handle *h, double *dst, const double *src, int ld, cudaMemcpyKind k) {
+  return cudaMemcpy2DAsync(dst, sizeof(double) * ld, src, sizeof(double) * h->nm,
+                           sizeof(double) * h->nm, h->ne, k, h->st);
+}
+
+RhsBuffers rhs_buffers(spoc_handle *h, double *const s[3]) {
+  RhsBuffers b;
+  b.su = s[0];
+  b.sv = s[1];
+  b.sh = s[2];
+  b.hb = h->hb;
+  b.w0 = h->w0;
+  b.z0 = h->z0;
+  b.fc = h->fc;
+  b.q = h->q;
+  b.f = h->f;
+  b.gx0 = h->gx0;
+  b.gy0 = h->gy0;
+  b.uh = h->uh;
+  b.vh = h->vh;
+  b.mu0 = h->mu0;
+  b.mb0 = h->mb0;
+  b.g0 = h->g0;
+  b.hh0 = h->hh0;
+  return b;
+}
+
+int check_flag(spoc_handle *h) {
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->st), "read flag");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  if (flag) {
+    CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->st), "clear flag");
+    return fail(SPOC_E_NONFINITE, "non-finite tendency detected");
+  }
+  return SPOC_OK;
+}
+
+int run_rhs_tend(spoc_handle *h, double *const s[3]) {
+  StageArgs sa{};
+  sa.stage = -1;
+  for (int c = 0; c < 3; ++c) sa.tend[c] = h->TEND[c];
+  sa.flag = h->flag;
+  CK(launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms, &h->launches),
+     "launch cal_var");
+  return SPOC_OK;
+}
+
+}  // namespace
+
+extern "C" const char *spoc_last_error(void) { return g_err.c_str(); }
+
+extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant, int precision,
+                           spoc_handle **out) {
+  if (!out) return fail(SPOC_E_ARG, "out is null");
+  *out = nullptr;
+  if (!t || !m) return fail(SPOC_E_ARG, "tables or mesh is null");
+  if (variant < SPOC_LIN || variant > SPOC_INV) return fail(SPOC_E_ARG, "unknown variant");
+  if (precision != SPOC_FP64) return fail(SPOC_E_UNSUPPORTED, "precision mode not built");
+  const int nc = t->nc, nm = (nc + 1) * (nc + 2) / 2;
+  if (nc < 1 || t->nm != nm) return fail(SPOC_E_ARG, "nm != (nc+1)(nc+2)/2");
+  if (nm > kMaxModes || t->ng < 1 || t->ng > kMaxQuad || t->ngf < 1 || t->ngf > kMaxEdge)
+    return fail(SPOC_E_UNSUPPORTED, "nm <= 64, ng <= 64 and ngf <= 10 are built");
+  if (!t->wi || !t->wif || !t->pi2 || !t->pico || !t->amm || !t->amml || !t->agx || !t->agy ||
+      !t->ammo || !t->cip || t->ld_mat < nm || t->ld_pi2 < t->ng || t->ld_pico1 < t->ngf ||
+      t->ld_pico2 < nm)
+    return fail(SPOC_E_ARG, "incomplete tables");
+  if (m->ne < 1 || m->nf < 1 || !m->itm || !m->its || !m->tseg || !m->ssit || !m->norm ||
+      !m->vect || !m->normt || !m->bdl)
+    return fail(SPOC_E_ARG, "incomplete mesh");
+  for (int i = 0; i < nm; ++i)
+    if (!(t->amm[(size_t)i * t->ld_mat + i] > 0.0)) return fail(SPOC_E_MATRIX, "amm factor has a non-positive diagonal");
+  for (int i = 0; i < nm - nc - 1; ++i)
+    if (!(t->amml[(size_t)i * t->ld_mat + i] > 0.0)) return fail(SPOC_E_MATRIX, "amml factor has a non-positive diagonal");
+
+  spoc_handle *h = new (std::nothrow) spoc_handle();
+  if (!h) return fail(SPOC_E_NOMEM, "host allocation");
+  h->variant = variant;
+  h->precision = precision;
+  h->nc = nc;
+  h->nm = nm;
+  h->ng = t->ng;
+  h->ngf = t->ngf;
+  h->nmr = nm - nc - 1;
+  h->ne = m->ne;
+  h->nf = m->nf;
+  int rc = SPOC_OK;
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) {
+    delete h;
+    return fail(SPOC_E_CUDA, "device set-up", ce);
+  }
+  h->st = h->own;
+  rc = build_ops(h, t);
+  if (!rc) rc = build_mesh(h, m);
+  if (!rc) {
+    const size_t n = fsize(h);
+    for (int c = 0; c < 3 && ce == cudaSuccess; ++c) {
+      ce = h->alloc(&h->U0[c], n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->SA[c], n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->SB[c], n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->ACC[c], n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->TEND[c], n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->SIN[c], n);
+    }
+    if (ce == cudaSuccess) ce = h->alloc(&h->hb, n);
+    if (ce == cudaSuccess) ce = h->alloc(&h->w0, n);
+    if (ce == cudaSuccess) ce = h->alloc(&h->z0, n);
+    if (ce == cudaSuccess) ce = h->alloc(&h->fc, n);
+    if (variant != SPOC_LIN) {
+      if (ce == cudaSuccess) ce = h->alloc(&h->q, 4 * n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->f, 4 * n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->gx0, n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->gy0, n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->uh, n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->vh, n);
+    }
+    if (ce == cudaSuccess) ce = h->alloc(&h->eterms, 3 * (size_t)h->ne);
+    if (ce == cudaSuccess) ce = h->alloc(&h->escal, 4);
+    if (ce == cudaSuccess) ce = h->alloc(&h->flag, 1);
+    if (ce == cudaSuccess) ce = h->alloc(&h->cflbits, 1);
+    for (int c = 0; c < 3 && ce == cudaSuccess; ++c)
+      ce = cudaMemsetAsync(h->U0[c], 0, sizeof(double) * n, h->st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->hb, 0, sizeof(double) * n, h->st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->w0, 0, sizeof(double) * n, h->st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->z0, 0, sizeof(double) * n, h->st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->fc, 0, sizeof(double) * n, h->st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->flag, 0, sizeof(int), h->st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+    if (ce != cudaSuccess) rc = fail(ce == cudaErrorMemoryAllocation ? SPOC_E_NOMEM : SPOC_E_CUDA, "device allocation", ce);
+  }
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return SPOC_OK;
+}
+
+extern "C" void spoc_destroy(spoc_handle *h) {
+  if (!h) return;
+  if (h->st) cudaStreamSynchronize(h->st);
+  delete h;
+}
+
+extern "C" int spoc_set_stream(spoc_handle *h, void *stream) {
+  if (!h) return fail(SPOC_E_ARG, "null handle");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  h->st = stream ? (cudaStream_t)stream : h->own;
+  return SPOC_OK;
+}
+
+extern "C" int spoc_set_params(spoc_handle *h, const spoc_params *p) {
+  if (!h || !p) return fail(SPOC_E_ARG, "null argument");
+  if (!p->hb || p->ld < h->nm) return fail(SPOC_E_ARG, "hb missing or ld < nm");
+  h->mu0 = p->mu0;
+  h->mb0 = p->mb0;
+  h->g0 = p->g0;
+  h->hh0 = p->hb[0];  // hh0 = hb(1,1) (calvar_lin.f:65)
+  CK(copy_in(h, h->hb, p->hb, p->ld, cudaMemcpyHostToDevice), "upload hb");
+  const size_t n = fsize(h);
+  if (p->w0) CK(copy_in(h, h->w0, p->w0, p->ld, cudaMemcpyHostToDevice), "upload w0");
+  else CK(cudaMemsetAsync(h->w0, 0, sizeof(double) * n, h->st), "zero w0");
+  if (p->z0) CK(copy_in(h, h->z0, p->z0, p->ld, cudaMemcpyHostToDevice), "upload z0");
+  else CK(cudaMemsetAsync(h->z0, 0, sizeof(double) * n, h->st), "zero z0");
+  if (p->fc) CK(copy_in(h, h->fc, p->fc, p->ld, cudaMemcpyHostToDevice), "upload fc");
+  else CK(cudaMemsetAsync(h->fc, 0, sizeof(double) * n, h->st), "zero fc");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  h->have_params = true;
+  return SPOC_OK;
+}
+
+extern "C" int spoc_cal_var(spoc_handle *h, int ld, const double *u0, const double *v0,
+                            const double *h0, double *u1, double *v1, double *h1) {
+  if (!h || !u0 || !v0 || !h0 || !u1 || !v1 || !h1) return fail(SPOC_E_ARG, "null argument");
+  if (ld < h->nm) return fail(SPOC_E_ARG, "ld < nm");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  CK(copy_in(h, h->SIN[0], u0, ld, cudaMemcpyHostToDevice), "upload u0");
+  CK(copy_in(h, h->SIN[1], v0, ld, cudaMemcpyHostToDevice), "upload v0");
+  CK(copy_in(h, h->SIN[2], h0, ld, cudaMemcpyHostToDevice), "upload h0");
+  int rc = run_rhs_tend(h, h->SIN);
+  if (rc) return rc;
+  CK(copy_out(h, u1, h->TEND[0], ld, cudaMemcpyDeviceToHost), "download u1");
+  CK(copy_out(h, v1, h->TEND[1], ld, cudaMemcpyDeviceToHost), "download v1");
+  CK(copy_out(h, h1, h->TEND[2], ld, cudaMemcpyDeviceToHost), "download h1");
+  return check_flag(h);
+}
+
+extern "C" int spoc_cal_var_dev(spoc_handle *h, int ld, const double *u0, const double *v0,
+                                const double *h0, double *u1, double *v1, double *h1) {
+  if (!h || !u0 || !v0 || !h0 || !u1 || !v1 || !h1) return fail(SPOC_E_ARG, "null argument");
+  if (ld < h->nm) return fail(SPOC_E_ARG, "ld < nm");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  CK(copy_in(h, h->SIN[0], u0, ld, cudaMemcpyDeviceToDevice), "copy u0");
+  CK(copy_in(h, h->SIN[1], v0, ld, cudaMemcpyDeviceToDevice), "copy v0");
+  CK(copy_in(h, h->SIN[2], h0, ld, cudaMemcpyDeviceToDevice), "copy h0");
+  int rc = run_rhs_tend(h, h->SIN);
+  if (rc) return rc;
+  CK(copy_out(h, u1, h->TEND[0], ld, cudaMemcpyDeviceToDevice), "copy u1");
+  CK(copy_out(h, v1, h->TEND[1], ld, cudaMemcpyDeviceToDevice), "copy v1");
+  CK(copy_out(h, h1, h->TEND[2], ld, cudaMemcpyDeviceToDevice), "copy h1");
+  return check_flag(h);
+}
+
+extern "C" int spoc_set_state(spoc_handle *h, int ld, const double *u, const double *v,
+                              const double *hh) {
+  if (!h || !u || !v || !hh || ld < (h ? h->nm : 1)) return fail(SPOC_E_ARG, "bad argument");
+  CK(copy_in(h, h->U0[0], u, ld, cudaMemcpyHostToDevice), "upload u");
+  CK(copy_in(h, h->U0[1], v, ld, cudaMemcpyHostToDevice), "upload v");
+  CK(copy_in(h, h->U0[2], hh, ld, cudaMemcpyHostToDevice), "upload h");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  return SPOC_OK;
+}
+
+extern "C" int spoc_get_state(spoc_handle *h, int ld, double *u, double *v, double *hh) {
+  if (!h || !u || !v || !hh || ld < (h ? h->nm : 1)) return fail(SPOC_E_ARG, "bad argument");
+  CK(copy_out(h, u, h->U0[0], ld, cudaMemcpyDeviceToHost), "download u");
+  CK(copy_out(h, v, h->U0[1], ld, cudaMemcpyDeviceToHost), "download v");
+  CK(copy_out(h, hh, h->U0[2], ld, cudaMemcpyDeviceToHost), "download h");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  return SPOC_OK;
+}
+
+namespace {
+int enqueue_steps(spoc_handle *h, double dt, int nsteps) {
+  StageArgs sa{};
+  sa.dt = dt;
+  sa.dt6 = dt / 6.0;  // dt / 6.d0 (src/shwwnl.f:277)
+  sa.flag = h->flag;
+  for (int c = 0; c < 3; ++c) {
+    sa.base[c] = h->U0[c];
+    sa.acc[c] = h->ACC[c];
+  }
+  for (int it = 0; it < nsteps; ++it) {
+    for (int s = 0; s < 4; ++s) {
+      double *const *in = s == 0 ? h->U0 : (s == 2 ? h->SB : h->SA);
+      double *const *out = s == 1 ? h->SB : h->SA;
+      sa.stage = s;
+      for (int c = 0; c < 3; ++c) sa.out[c] = out[c];
+      CK(launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, in), sa, h->st, h->sms,
+                    &h->launches),
+         "launch RK4 stage");
+    }
+  }
+  return SPOC_OK;
+}
+}  // namespace
+
+extern "C" int spoc_rk4_steps(spoc_handle *h, double dt, int nsteps) {
+  if (!h || nsteps < 0) return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  int rc = enqueue_steps(h, dt, nsteps);
+  if (rc) return rc;
+  return check_flag(h);
+}
+
+extern "C" int spoc_rk4_steps_host(spoc_handle *h, int ld, double *u, double *v, double *hh,
+                                   double dt, int nsteps) {
+  if (!h || !u || !v || !hh || nsteps < 0 || ld < (h ? h->nm : 1))
+    return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  CK(copy_in(h, h->U0[0], u, ld, cudaMemcpyHostToDevice), "upload u");
+  CK(copy_in(h, h->U0[1], v, ld, cudaMemcpyHostToDevice), "upload v");
+  CK(copy_in(h, h->U0[2], hh, ld, cudaMemcpyHostToDevice), "upload h");
+  int rc = enqueue_steps(h, dt, nsteps);
+  if (rc) return rc;
+  CK(copy_out(h, u, h->U0[0], ld, cudaMemcpyDeviceToHost), "download u");
+  CK(copy_out(h, v, h->U0[1], ld, cudaMemcpyDeviceToHost), "download v");
+  CK(copy_out(h, hh, h->U0[2], ld, cudaMemcpyDeviceToHost), "download h");
+  return check_flag(h);
+}
+
+extern "C" int spoc_energy(spoc_handle *h, double *ke, double *pe, double *mass) {
+  if (!h || !ke || !pe || !mass) return fail(SPOC_E_ARG, "null argument");
+  CK(launch_energy(h->op, h->mesh, h->U0[0], h->U0[1], h->U0[2], h->hb, h->g0, h->eterms,
+                   h->escal, h->st, h->sms, &h->launches),
+     "launch energy");
+  double out[3];
+  CK(cudaMemcpyAsync(out, h->escal, sizeof out, cudaMemcpyDeviceToHost, h->st), "read energy");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  *ke = out[0];
+  *pe = out[1];
+  *mass = out[2];
+  return SPOC_OK;
+}
+
+extern "C" int spoc_cfl(spoc_handle *h, int nn, const int *in, const double *xgr,
+                        const double *ygr, double *cflmin, double *dt) {
+  if (!h || !in || !xgr || !ygr || nn < 3 || !cflmin || !dt) return fail(SPOC_E_ARG, "bad argument");
+  for (size_t i = 0; i < 3 * (size_t)h->ne; ++i)
+    if (in[i] < 1 || in[i] > nn) return fail(SPOC_E_MESH, "node id out of range");
+  int *din = nullptr;
+  double *dx = nullptr, *dy = nullptr;
+  cudaError_t ce = cudaMalloc(&din, sizeof(int) * 3 * (size_t)h->ne);
+  if (ce == cudaSuccess) ce = cudaMalloc(&dx, sizeof(double) * nn);
+  if (ce == cudaSuccess) ce = cudaMalloc(&dy, sizeof(double) * nn);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(din, in, sizeof(int) * 3 * (size_t)h->ne, cudaMemcpyHostToDevice, h->st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(dx, xgr, sizeof(double) * nn, cudaMemcpyHostToDevice, h->st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(dy, ygr, sizeof(double) * nn, cudaMemcpyHostToDevice, h->st);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(h->cflbits, 0xff, sizeof(unsigned long long), h->st);
+  if (ce == cudaSuccess)
+    ce = launch_cfl(h->ne, h->nc, din, dx, dy, h->hb, h->nm, h->g0, h->cflbits, h->st, h->sms,
+                    &h->launches);
+  unsigned long long bits = 0;
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&bits, h->cflbits, sizeof bits, cudaMemcpyDeviceToHost, h->st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+  cudaFree(din);
+  cudaFree(dx);
+  cudaFree(dy);
+  if (ce != cudaSuccess) return fail(SPOC_E_CUDA, "cfl", ce);
+  double c;
+  std::memcpy(&c, &bits, sizeof c);
+  *cflmin = c;
+  // rounding of src/cfl.f:34-42 (the last branch is an integer division)
+  double d = 0.0;
+  if (c >= 100) d = (double)(10 * (int)(c / 10));
+  else if (c >= 10 && c < 100) d = (double)(2 * (int)(c / 2));
+  else if (c < 10 && c >= 1) d = (double)((int)c);
+  else if (c < 1) d = (double)((int)(c * 10) / 10);
+  *dt = d;
+  return SPOC_OK;
+}
+
+extern "C" long long spoc_kernel_launches(spoc_handle *h) { return h ? h->launches : -1; }
+
+extern "C" int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms,
+                                int *nkinds) {
+  if (!h || nsteps < 1 || !kernel_ms || !nkinds) return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  const int nk = h->variant == SPOC_LIN ? 1 : 3;
+  cudaEvent_t ev[4];
+  for (int i = 0; i < 4; ++i) CK(cudaEventCreate(&ev[i]), "event");
+  for (int k = 0; k < nk; ++k) kernel_ms[k] = 0.0;
+  StageArgs sa{};
+  sa.dt = dt;
+  sa.dt6 = dt / 6.0;
+  sa.flag = h->flag;
+  for (int c = 0; c < 3; ++c) {
+    sa.base[c] = h->U0[c];
+    sa.acc[c] = h->ACC[c];
+  }
+  int rc = SPOC_OK;
+  for (int it = 0; it < nsteps && !rc; ++it)
+    for (int s = 0; s < 4 && !rc; ++s) {
+      double *const *in = s == 0 ? h->U0 : (s == 2 ? h->SB : h->SA);
+      double *const *out = s == 1 ? h->SB : h->SA;
+      sa.stage = s;
+      for (int c = 0; c < 3; ++c) sa.out[c] = out[c];
+      cudaError_t ce = launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, in), sa, h->st,
+                                  h->sms, &h->launches, ev);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[nk]);
+      for (int k = 0; k < nk && ce == cudaSuccess; ++k) {
+        float ms = 0.f;
+        ce = cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        kernel_ms[k] += ms;
+      }
+      if (ce != cudaSuccess) rc = fail(SPOC_E_CUDA, "profile", ce);
+    }
+  for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+  *nkinds = nk;
+  if (rc) return rc;
+  return check_flag(h);
+}
+
+extern "C" int spoc_fp64_peak(int mode, double *tflops) {
+  if (!tflops || (mode != 0 && mode != 1)) return fail(SPOC_E_ARG, "bad argument");
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev), "device");
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+  double *out = nullptr;
+  CK(cudaMalloc(&out, sizeof(double)), "alloc");
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int iters = 4096;
+  cudaError_t ce = launch_fp64_peak(mode, sms, iters, out, 0);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5 && ce == cudaSuccess; ++r) {
+    cudaEventRecord(a, 0);
+    ce = launch_fp64_peak(mode, sms, iters, out, 0);
+    cudaEventRecord(b, 0);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, a, b);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  if (ce != cudaSuccess) return fail(SPOC_E_CUDA, "fp64 peak", ce);
+  const double ops = (double)sms * 8 * 256 * 8 * (double)iters;  // multiply-adds
+  *tflops = 2.0 * ops / (best * 1e-3) / 1e12;
+  return SPOC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Fortran drop-in: cal_var_ with the reference's 31 by-reference arguments
+// ---------------------------------------------------------------------------
+namespace {
+struct Commons {
+  bool have = false;
+  int variant = 0, precision = 0;
+  int nc = 0, nm = 0, ng = 0, ngf = 0, ld = 0;
+  std::vector<double> wi, xi, yi, wif, tif, pi2, pico, amm, amml, agx, agy, ammo;
+  std::vector<int> cip;
+  int ld_pi2 = 0, ld_p1 = 0, ld_p2 = 0;
+  spoc_handle *h = nullptr;
+  int h_ne = 0, h_nf = 0;
+  const void *h_keys[8] = {};
+  int status = 0;
+};
+Commons g_commons;
+std::mutex g_commons_mu;
+}  // namespace
+
+extern "C" int *spoc_cal_var_status(void) { return &g_commons.status; }
+
+extern "C" int spoc_register_commons(const spoc_tables *t, int variant, int precision) {
+  std::lock_guard<std::mutex> lk(g_commons_mu);
+  if (!t || !t->wi || !t->xi || !t->yi || !t->wif || !t->tif || !t->pi2 || !t->pico || !t->amm ||
+      !t->amml || !t->agx || !t->agy || !t->ammo || !t->cip)
+    return fail(SPOC_E_ARG, "incomplete tables");
+  Commons &c = g_commons;
+  if (c.h) {
+    spoc_destroy(c.h);
+    c.h = nullptr;
+  }
+  c.variant = variant;
+  c.precision = precision;
+  c.nc = t->nc;
+  c.nm = t->nm;
+  c.ng = t->ng;
+  c.ngf = t->ngf;
+  c.ld = t->ld_mat;
+  c.ld_pi2 = t->ld_pi2;
+  c.ld_p1 = t->ld_pico1;
+  c.ld_p2 = t->ld_pico2;
+  c.wi.assign(t->wi, t->wi + t->ng);
+  c.xi.assign(t->xi, t->xi + t->ng);
+  c.yi.assign(t->yi, t->yi + t->ng);
+  c.wif.assign(t->wif, t->wif + t->ngf);
+  c.tif.assign(t->tif, t->tif + t->ngf);
+  c.pi2.assign(t->pi2, t->pi2 + (size_t)t->ld_pi2 * t->nm);
+  c.pico.assign(t->pico, t->pico + (size_t)t->ld_pico1 * t->ld_pico2 * 3);
+  const size_t mm = (size_t)t->ld_mat * t->nm;
+  c.amm.assign(t->amm, t->amm + mm);
+  c.amml.assign(t->amml, t->amml + mm);
+  c.agx.assign(t->agx, t->agx + mm);
+  c.agy.assign(t->agy, t->agy + mm);
+  c.ammo.assign(t->ammo, t->ammo + mm);
+  c.cip.assign(t->cip, t->cip + 2 * (t->nc + 1));
+  c.have = true;
+  c.status = 0;
+  return SPOC_OK;
+}
+
+extern "C" void spoc_release_commons(void) {
+  std::lock_guard<std::mutex> lk(g_commons_mu);
+  if (g_commons.h) spoc_destroy(g_commons.h);
+  g_commons = Commons();
+}
+
+extern "C" void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, double *u1,
+                         double *v1, double *h1, int *tseg, int *pseg, int *ssit, int *itm,
+                         int *its, double *norm, int *nbdl, int *pbdl, int *nint, int *pint,
+                         int *bdl, int *cip, double *vect, double *normt, double *mu0,
+                         double *mb0, double *fc, double *beta, double *w0, double *z0,
+                         double *g0, double *hb, double *time) {
+  (void)pseg; (void)nbdl; (void)pbdl; (void)nint; (void)pint; (void)cip; (void)beta; (void)time;
+  std::lock_guard<std::mutex> lk(g_commons_mu);
+  Commons &c = g_commons;
+  if (!c.have) {
+    c.status = fail(SPOC_E_ARG, "spoc_register_commons not called");
+    return;
+  }
+  const void *keys[8] = {tseg, itm, its, norm, vect, fc, w0, hb};
+  bool same = c.h && c.h_ne == *ne && c.h_nf == *nf;
+  for (int i = 0; i < 8 && same; ++i) same = keys[i] == c.h_keys[i];
+  if (!same) {
+    if (c.h) {
+      spoc_destroy(c.h);
+      c.h = nullptr;
+    }
+    spoc_tables t{};
+    t.nc = c.nc; t.nm = c.nm; t.ng = c.ng; t.ngf = c.ngf;
+    t.wi = c.wi.data(); t.xi = c.xi.data(); t.yi = c.yi.data();
+    t.wif = c.wif.data(); t.tif = c.tif.data();
+    t.pi2 = c.pi2.data(); t.ld_pi2 = c.ld_pi2;
+    t.pico = c.pico.data(); t.ld_pico1 = c.ld_p1; t.ld_pico2 = c.ld_p2;
+    t.amm = c.amm.data(); t.amml = c.amml.data(); t.agx = c.agx.data(); t.agy = c.agy.data();
+    t.ammo = c.ammo.data(); t.ld_mat = c.ld; t.cip = c.cip.data();
+    spoc_mesh m{};
+    m.ne = *ne; m.nf = *nf; m.itm = itm; m.its = its; m.tseg = tseg; m.ssit = ssit;
+    m.norm = norm; m.vect = vect; m.normt = normt; m.bdl = bdl;
+    int rc = spoc_create(&t, &m, c.variant, c.precision, &c.h);
+    if (!rc) {
+      spoc_params p{*mu0, *mb0, *g0, fc, w0, z0, hb, c.ld};
+      rc = spoc_set_params(c.h, &p);
+    }
+    if (rc) {
+      if (c.h) spoc_destroy(c.h);
+      c.h = nullptr;
+      c.status = rc;
+      return;
+    }
+    c.h_ne = *ne;
+    c.h_nf = *nf;
+    for (int i = 0; i < 8; ++i) c.h_keys[i] = keys[i];
+  } else {
+    c.h->mu0 = *mu0;
+    c.h->mb0 = *mb0;
+    c.h->g0 = *g0;
+  }
+  c.status = spoc_cal_var(c.h, c.ld, u0, v0, h0, u1, v1, h1);
+}

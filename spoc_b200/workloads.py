@@ -1,0 +1,217 @@
+"""Synthetic meshes, initial states and the benchmark configurations.
+
+No mesh, initial state or oc.inp ships with the reference, so each
+configuration is generated here from seeded inputs:
+  * mesh: a square basin cut into n x n cells, each split into two right
+    triangles as src/rmal.f:30-46 does, interior vertices optionally jittered
+    by U(-j, j) * cell size with numpy's PCG64, then the corner fix of
+    src/chmal.f:240-330 (spoc_fix_mesh);
+  * state: analytic fields L2-projected onto the modal basis with the calh
+    method of src/init.f:290-344 (spoc_project); depth hb = H constant as in
+    src/init.f:246-252.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import api
+
+
+@dataclass
+class Config:
+    name: str
+    variant: str
+    nc: int
+    ng: int
+    ngf: int
+    n: int                 # cells per side: ne = 2 n^2
+    length: float = 1.0e6  # basin side (m), centred on the origin
+    jitter: float = 0.0    # interior vertex jitter, fraction of the cell size
+    f0: float = 1.0e-4
+    beta: float = 0.0
+    g0: float = 9.81
+    depth: float = 4000.0
+    mu0: float = 0.0
+    mb0: float = 0.0
+    ic: str = "gauss"
+    steps: int = 100
+    seed: int = 0
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def nm(self) -> int:
+        return (self.nc + 1) * (self.nc + 2) // 2
+
+    @property
+    def ne(self) -> int:
+        return 2 * self.n * self.n
+
+
+# The reference's own configuration space (see the survey of the benchmark
+# configurations): C1 linear p3, C2 free-slip p6, C3 inviscid, C4 no-slip p4.
+# C3 asks for degree 8 with the 42-point rule, whose mass matrix has rank
+# <= 42 < 45 (dpotrf fails); C3 here runs degree 7 with the same rules.
+CONFIGS = {
+    "c1_lin_p3": Config("c1_lin_p3", "lin", 3, 12, 4, 32, ic="gauss", steps=1000, seed=1),
+    "c2_fs_p6": Config("c2_fs_p6", "fs", 6, 33, 7, 128, jitter=0.2, beta=2.0e-11, mu0=100.0,
+                       mb0=1.0e-3, ic="gauss8", steps=2000, seed=2),
+    "c3_inv_p7": Config("c3_inv_p7", "inv", 7, 42, 9, 256, jitter=0.2, mu0=0.0, ic="kminus3",
+                        steps=1000, seed=3),
+    "c4_ns_p4": Config("c4_ns_p4", "ns", 4, 25, 5, 128, jitter=0.2, beta=2.0e-11, mu0=100.0,
+                       mb0=1.0e-3, ic="gauss8", steps=200, seed=4),
+}
+
+
+def small(cfg: Config, n: int, **kw) -> Config:
+    """The same physics, discretisation and cell size on an n x n cell basin."""
+    d = dict(cfg.__dict__)
+    d.update(n=n, length=cfg.length * n / cfg.n)
+    d.update(**kw)
+    d["extra"] = dict(cfg.extra)
+    return Config(**d)
+
+
+def square_mesh(n: int, length: float = 1.0e6, jitter: float = 0.0, seed: int = 0):
+    """(nn, inn (ne,3) 1-based, xgr, ygr) of the rmal split, jittered, corner-fixed."""
+    nx = n + 1
+    h = length / n
+    xs = -0.5 * length + h * np.arange(nx)
+    X, Y = np.meshgrid(xs, xs, indexing="xy")  # node j*nx + i at (xs[i], xs[j])
+    x, y = X.ravel().copy(), Y.ravel().copy()
+    if jitter > 0.0:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        d = rng.uniform(-jitter, jitter, size=(x.size, 2)) * h
+        ii = np.arange(x.size)
+        interior = (ii % nx > 0) & (ii % nx < nx - 1) & (ii // nx > 0) & (ii // nx < nx - 1)
+        x[interior] += d[interior, 0]
+        y[interior] += d[interior, 1]
+    cells = np.arange(n * n)
+    ci, cj = cells % n, cells // n
+    ne1 = ci + 1 + nx * cj  # 1-based lower-left node (src/rmal.f:174)
+    t1 = np.stack([ne1, ne1 + 1, ne1 + nx], axis=1)
+    t2 = np.stack([ne1 + 1, ne1 + 1 + nx, ne1 + nx], axis=1)
+    inn = np.empty((2 * n * n, 3), dtype=np.int32)
+    inn[0::2] = t1
+    inn[1::2] = t2
+    nn = nx * nx
+    inn = api.fix_mesh(inn, nn)
+    return nn, inn, x, y
+
+
+def _gauss8(cfg: Config, rng):
+    L = cfg.length
+    cx = rng.uniform(-0.35 * L, 0.35 * L, 8)
+    cy = rng.uniform(-0.35 * L, 0.35 * L, 8)
+    amp = rng.uniform(-2.0, 2.0, 8)
+    wid = rng.uniform(0.05 * L, 0.15 * L, 8)  # 50-150 km on the 1000 km basin
+    return cx, cy, amp, wid
+
+
+def _kminus3(cfg: Config, rng, kmax: int = 12):
+    k = np.arange(-kmax, kmax + 1)
+    KX, KY = np.meshgrid(k, k, indexing="ij")
+    kk = np.hypot(KX, KY)
+    keep = (kk > 0) & (kk <= kmax)
+    kx, ky, kk = KX[keep], KY[keep], kk[keep]
+    amp = kk ** -2.0  # |eta_k|^2 ~ k^-4, E(k) ~ k |eta_k|^2 ~ k^-3
+    phase = rng.uniform(0.0, 2.0 * np.pi, kx.size)
+    return kx, ky, amp, phase
+
+
+def _fields(cfg: Config, px, py, rng_state):
+    """(eta, u, v) at physical points; u, v geostrophic where the IC asks."""
+    g, L = cfg.g0, cfg.length
+    if cfg.ic == "gauss":  # ftourbh-like Gaussian, 1 m, e-folding L/10 = 100 km (src/fonc.f:42-50)
+        eta = np.exp(-(px ** 2 + py ** 2) / (0.1 * L) ** 2)
+        return eta, np.zeros_like(eta), np.zeros_like(eta)
+    f = cfg.f0 + cfg.beta * py
+    if cfg.ic == "gauss8":
+        cx, cy, amp, wid = rng_state
+        eta = np.zeros_like(px)
+        ex = np.zeros_like(px)
+        ey = np.zeros_like(px)
+        for a, x0, y0, w in zip(amp, cx, cy, wid):
+            gsh = a * np.exp(-((px - x0) ** 2 + (py - y0) ** 2) / w ** 2)
+            eta += gsh
+            ex += gsh * (-2.0 * (px - x0) / w ** 2)
+            ey += gsh * (-2.0 * (py - y0) / w ** 2)
+    elif cfg.ic == "kminus3":
+        kx, ky, amp, phase = rng_state
+        two_pi_l = 2.0 * np.pi / L
+        eta = np.zeros_like(px)
+        ex = np.zeros_like(px)
+        ey = np.zeros_like(px)
+        for a, p, qx, qy in zip(amp, phase, kx, ky):
+            arg = two_pi_l * (qx * px + qy * py) + p
+            eta += a * np.cos(arg)
+            ex -= a * two_pi_l * qx * np.sin(arg)
+            ey -= a * two_pi_l * qy * np.sin(arg)
+        s = 0.5 / np.sqrt(np.mean(eta ** 2))
+        eta, ex, ey = eta * s, ex * s, ey * s
+    else:
+        raise ValueError(cfg.ic)
+    return eta, -g / f * ey, g / f * ex
+
+
+@dataclass
+class Problem:
+    cfg: Config
+    T: api.Tables
+    mesh: api.Mesh
+    u: np.ndarray
+    v: np.ndarray
+    h: np.ndarray
+    hb: np.ndarray
+    fc: np.ndarray
+    w0: np.ndarray
+    z0: np.ndarray
+    dt: float
+
+
+def build_problem(cfg: Config, ld: int | None = None, tables: api.Tables | None = None) -> Problem:
+    T = tables or api.build_tables(cfg.nc, cfg.ng, cfg.ngf)
+    nm = T.nm
+    ld = ld or nm
+    nn, inn, x, y = square_mesh(cfg.n, cfg.length, cfg.jitter, cfg.seed)
+    mesh = api.build_mesh(inn, x, y, cfg.nc, cfg.f0, cfg.beta, ld)
+    rng = np.random.Generator(np.random.PCG64(1000 + cfg.seed))
+    state = {"gauss": None, "gauss8": _gauss8, "kminus3": _kminus3}[cfg.ic]
+    rs = state(cfg, rng) if state else None
+    px, py = api.projection_points(mesh, T)
+    eta, uu, vv = _fields(cfg, px, py, rs)
+    h = api.project(T, eta, ld)
+    u = api.project(T, uu, ld)
+    v = api.project(T, vv, ld)
+    hb = np.zeros((mesh.ne, ld))
+    hb[:, 0] = cfg.depth
+    w0 = np.zeros((mesh.ne, ld))
+    z0 = np.zeros((mesh.ne, ld))
+    # time step of checkcfl (src/cfl.f:4-52), evaluated on the host
+    dt = cfl_dt(cfg.nc, mesh, cfg.g0, cfg.depth)
+    return Problem(cfg, T, mesh, u, v, h, hb, mesh.fc, w0, z0, dt)
+
+
+def cfl_dt(nc: int, mesh: api.Mesh, g0: float, depth: float) -> float:
+    x, y, inn = mesh.xgr, mesh.ygr, mesh.inn - 1
+    cc0 = np.sqrt(g0 * depth)
+    best = 6000.0
+    for a, b in ((0, 1), (0, 2), (1, 2)):
+        dx = x[inn[:, b]] - x[inn[:, a]]
+        dy = y[inn[:, b]] - y[inn[:, a]]
+        dd = np.sqrt(dx * dx + dy * dy) / float(nc) * 0.30
+        best = min(best, float(np.min(dd / cc0)))
+    if best >= 100:
+        return float(10 * int(best / 10))
+    if best >= 10:
+        return float(2 * int(best / 2))
+    if best >= 1:
+        return float(int(best))
+    return float(int(best * 10) // 10)
+
+
+def make_solver(p: Problem) -> api.Solver:
+    s = api.Solver(p.T, p.mesh, p.cfg.variant)
+    s.set_params(p.cfg.mu0, p.cfg.mb0, p.cfg.g0, p.hb, p.fc, p.w0, p.z0)
+    return s

@@ -1,0 +1,220 @@
+"""GPU parity: the CUDA path against the CPU oracle, through the C ABI.
+
+The FP64 path evaluates every sum in the reference order with separately
+rounded products, so the comparison is bit-for-bit (np.array_equal) for the
+right-hand side, the RK4 steps and the CFL bound; the energy diagnostic is
+summed in a different order (fixed-order tree) and is compared at 1e-13
+relative.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from spoc_b200 import api
+from spoc_b200 import workloads as W
+
+NAMES = ["c1_lin_p3", "c2_fs_p6", "c4_ns_p4", "c3_inv_p7"]
+
+
+def oracle_for(p):
+    T = p.T
+    OT = O.Tables(p.cfg.nc, p.cfg.ng, p.cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
+    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, p.cfg.nc, p.cfg.f0, p.cfg.beta,
+                ld=p.u.shape[1])
+    return OT, OM
+
+
+def oracle_rhs(p, OT, OM, u, v, h):
+    c = p.cfg
+    return O.cal_var(c.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0)
+
+
+def assert_bitwise(got, ref, nm):
+    for g, r in zip(got, ref):
+        g, r = g[:, :nm], r[:, :nm]
+        bad = ~((g == r) | (np.isnan(g) & np.isnan(r)))
+        assert not bad.any(), f"{bad.sum()} coefficients differ; max |d| = {np.abs(g - r).max():.3e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("ld", [None, 45])
+def test_cal_var_bitwise(gpu_lib, name, ld):
+    p = W.build_problem(W.small(W.CONFIGS[name], 6), ld=ld)
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    got = s.cal_var(p.u, p.v, p.h)
+    ref = oracle_rhs(p, OT, OM, p.u, p.v, p.h)
+    assert_bitwise(got, ref, p.T.nm)
+    assert any(np.abs(r).max() > 0 for r in ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_cal_var_random_state_bitwise(gpu_lib, name):
+    """Rough random state: exercises every branch with O(1) values everywhere."""
+    p = W.build_problem(W.small(W.CONFIGS[name], 5))
+    rng = np.random.default_rng(7)
+    u, v = rng.normal(size=p.u.shape), rng.normal(size=p.v.shape)
+    h = rng.normal(size=p.h.shape)
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    assert_bitwise(s.cal_var(u, v, h), oracle_rhs(p, OT, OM, u, v, h), p.T.nm)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_rk4_device_resident_bitwise(gpu_lib, name):
+    p = W.build_problem(W.small(W.CONFIGS[name], 6))
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, 5)
+    got = s.get_state()
+    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    c = p.cfg
+    O.rk4(c.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0, p.dt, 5)
+    assert_bitwise(got, (u, v, h), p.T.nm)
+
+
+@pytest.mark.gpu
+def test_rk4_host_entry_matches_resident(gpu_lib):
+    p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 8), ld=45)
+    s = W.make_solver(p)
+    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    s.rk4_steps_host(u, v, h, p.dt, 3)
+    s2 = W.make_solver(p)
+    s2.set_state(p.u, p.v, p.h)
+    s2.rk4_steps(p.dt, 3)
+    assert_bitwise((u, v, h), s2.get_state(45), p.T.nm)
+
+
+@pytest.mark.gpu
+def test_c1_full_1000_steps_bitwise(gpu_lib):
+    """Configuration C1 as specified: 2048 triangles, p3, 1000 RK4 steps at the cfl.f step."""
+    p = W.build_problem(W.CONFIGS["c1_lin_p3"])
+    assert p.mesh.ne == 2048 and p.dt == 14.0
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, 1000)
+    got = s.get_state()
+    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    c = p.cfg
+    O.rk4(c.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0, p.dt, 1000)
+    assert_bitwise(got, (u, v, h), p.T.nm)
+    # the state moved: this is not a trivially stationary run
+    assert O.mass_norm(OT, OM, h - p.h) > 1e-3 * O.mass_norm(OT, OM, p.h)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c2_fs_p6", "c4_ns_p4"])
+def test_medium_mesh_steps_bitwise(gpu_lib, name):
+    p = W.build_problem(W.small(W.CONFIGS[name], 16))
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, 10)
+    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    c = p.cfg
+    O.rk4(c.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0, p.dt, 10)
+    assert_bitwise(s.get_state(), (u, v, h), p.T.nm)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c1_lin_p3", "c2_fs_p6"])
+def test_energy_and_cfl(gpu_lib, name):
+    p = W.build_problem(W.small(W.CONFIGS[name], 10))
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    s.set_state(p.u, p.v, p.h)
+    ke, pe, mass = s.energy()
+    rke, rpe, rmass = O.energy(OT, OM, p.u, p.v, p.h, p.hb, p.cfg.g0)
+    assert ke == pytest.approx(rke, rel=1e-13, abs=1e-300)
+    assert pe == pytest.approx(rpe, rel=1e-13)
+    scale = abs(rpe) ** 0.5 + abs(rmass) + 1.0
+    assert abs(mass - rmass) <= 1e-13 * scale * p.mesh.ne
+    cmin, dt = s.cfl()
+    rcmin, rdt = O.checkcfl(p.cfg.nc, OM, p.hb, p.cfg.g0)
+    assert cmin == rcmin and dt == rdt == p.dt
+
+
+@pytest.mark.gpu
+def test_fortran_drop_in_cal_var_(gpu_lib):
+    """cal_var_ with the reference's 31 by-reference arguments (src/calvarnl_fs.f:9-12)."""
+    p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 6))
+    lib = api.load_library()
+    ts = p.T.struct()
+    assert lib.spoc_register_commons(C.byref(ts), api.FS, api.FP64) == 0
+    m, c = p.mesh, p.cfg
+    outs = [np.zeros_like(p.u) for _ in range(3)]
+    keep = []
+
+    def ints(x):
+        keep.append(C.c_int(x))
+        return C.c_void_p(C.addressof(keep[-1]))
+
+    def dbl(x):
+        keep.append(C.c_double(x))
+        return C.c_void_p(C.addressof(keep[-1]))
+
+    ptr = lambda a: C.c_void_p(a.ctypes.data)
+    nbdl, nint = int(m.bdl.sum()), int(m.ne - m.bdl.sum())
+    pbdl = np.zeros(m.ne, np.int32)
+    pint = np.zeros(m.ne, np.int32)
+    args = [ints(m.nf), ints(m.ne), ptr(p.u), ptr(p.v), ptr(p.h), *map(ptr, outs), ptr(m.tseg),
+            ptr(m.pseg), ptr(m.ssit), ptr(m.itm), ptr(m.its), ptr(m.norm), ints(nbdl), ptr(pbdl),
+            ints(nint), ptr(pint), ptr(m.bdl), ptr(p.T.cip), ptr(m.vect), ptr(m.normt),
+            dbl(c.mu0), dbl(c.mb0), ptr(p.fc), dbl(c.beta), ptr(p.w0), ptr(p.z0), dbl(c.g0),
+            ptr(p.hb), dbl(0.0)]
+    for _ in range(2):  # second call reuses the cached handle
+        lib.cal_var_(*args)
+        assert lib.spoc_cal_var_status()[0] == 0
+    OT, OM = oracle_for(p)
+    assert_bitwise(outs, oracle_rhs(p, OT, OM, p.u, p.v, p.h), p.T.nm)
+    lib.spoc_release_commons()
+
+
+@pytest.mark.gpu
+def test_nonfinite_state_is_reported(gpu_lib):
+    p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 4))
+    s = W.make_solver(p)
+    h = p.h.copy()
+    h[3, 0] = np.nan
+    s.set_state(p.u, p.v, h)
+    with pytest.raises(api.SpocError) as ei:
+        s.rk4_steps(p.dt, 1)
+    assert ei.value.code == 3
+    # the handle stays usable after the error
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, 1)
+
+
+@pytest.mark.gpu
+def test_full_c2_deterministic_and_conservative(gpu_lib):
+    """C2 at full size: repeatable bit for bit, and mass conserved to round-off."""
+    p = W.build_problem(W.CONFIGS["c2_fs_p6"])
+    s = W.make_solver(p)
+    runs = []
+    for _ in range(2):
+        s.set_state(p.u, p.v, p.h)
+        s.rk4_steps(p.dt, 3)
+        runs.append(s.get_state())
+    assert_bitwise(runs[0], runs[1], p.T.nm)
+    s.set_state(p.u, p.v, p.h)
+    _, _, m0 = s.energy()
+    s.rk4_steps(p.dt, 3)
+    _, _, m1 = s.energy()
+    # mass = sum_e det_e sum_j ammo(j,1) h_j (src/energy.f:327-329); walls carry no flux
+    scale = float(np.sum(np.abs(p.mesh.det[:, None] * p.T.ammo[0, :][None, :] * p.h)))
+    assert abs(m1 - m0) <= 1e-12 * scale
+
+
+@pytest.mark.gpu
+def test_singular_mass_matrix_rejected(gpu_lib):
+    """Degree 8 with the 42-point rule: 45 modes, rank <= 42; dpotrf fails as in the reference."""
+    with pytest.raises(api.SpocError) as ei:
+        api.build_tables(8, 42, 9)
+    assert ei.value.code == 4
