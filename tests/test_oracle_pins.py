@@ -1,0 +1,224 @@
+"""Known-answer pins of the CPU oracle (no GPU).
+
+The reference ships no tests, fixtures or golden vectors, and it cannot be
+compiled here, so the oracle is pinned by properties with exact answers:
+quadrature exactness, closed-form integrals of Legendre products, the
+Cholesky factorisation, polynomial exactness of the face trace, invariance of
+a state at rest, exact mass conservation, an analytic standing wave, and
+serial/parallel bit-identity.
+"""
+from fractions import Fraction
+from math import comb, factorial
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from spoc_b200 import api
+from spoc_b200 import workloads as W
+
+TRI_DEGREE = {6: 4, 12: 6, 25: 10, 27: 11, 33: 12, 42: 14}  # Dunavant-type rules
+
+
+def tri_monomial(a, b):
+    """Exact integral of x^a y^b over the triangle (-1,-1), (1,-1), (-1,1)."""
+    # x = 2s - 1, y = 2t - 1 on the unit triangle; dA = 4 ds dt
+    tot = Fraction(0)
+    for i in range(a + 1):
+        for j in range(b + 1):
+            c = comb(a, i) * comb(b, j) * (2 ** i) * (2 ** j) * (-1) ** (a - i + b - j)
+            tot += c * Fraction(factorial(i) * factorial(j), factorial(i + j + 2))
+    return 4 * tot
+
+
+@pytest.mark.parametrize("ng", sorted(TRI_DEGREE))
+def test_triangle_rule_exactness(ng):
+    wi, xi, yi, _, _ = api.quadrature(ng, 3)
+    assert abs(wi.sum() - 2.0) < 1e-14
+    deg = TRI_DEGREE[ng]
+    for a in range(deg + 1):
+        for b in range(deg + 1 - a):
+            exact = float(tri_monomial(a, b))
+            got = float(np.sum(wi * xi ** a * yi ** b))
+            assert abs(got - exact) < 2e-14, (ng, a, b, got, exact)
+
+
+@pytest.mark.parametrize("ngf", range(3, 10))
+def test_gauss_legendre_edge_rules(ngf):
+    _, _, _, wif, tif = api.quadrature(12, ngf)
+    x, w = np.polynomial.legendre.leggauss(ngf)
+    assert np.allclose(np.sort(tif), x, atol=1e-15, rtol=0)
+    assert np.allclose(wif[np.argsort(tif)], w, atol=1e-14, rtol=0)  # table noise is ulp-level
+
+
+def test_legendre_recurrence():
+    L = O.lib()
+    for n in range(9):
+        c = np.zeros(n + 1)
+        c[n] = 1
+        for x in (-1.0, -0.3, 0.0, 0.71, 1.0):
+            assert abs(L.ora_po(n, x) - np.polynomial.legendre.legval(x, c)) < 1e-14
+            dc = np.polynomial.legendre.legder(c)
+            assert abs(L.ora_dpo(n, x) - np.polynomial.legendre.legval(x, dc)) < 1e-12
+
+
+def _exact_mass(nc):
+    """Exact mass / x-derivative matrices of the P_k1(x) P_k2(y) basis."""
+    modes = [(a, b) for a in range(nc + 1) for b in range(nc + 1 - a)]
+    leg = [np.polynomial.legendre.leg2poly(np.eye(nc + 1)[k]) for k in range(nc + 1)]
+    der = [np.polynomial.polynomial.polyder(p) if len(p) > 1 else np.zeros(1) for p in leg]
+
+    def integ(px, py):
+        return sum(float(cx) * float(cy) * float(tri_monomial(i, j))
+                   for i, cx in enumerate(px) for j, cy in enumerate(py) if cx and cy)
+
+    mul = np.polynomial.polynomial.polymul
+    n = len(modes)
+    M = np.zeros((n, n))
+    D = np.zeros((n, n))
+    for r, (a, b) in enumerate(modes):
+        for s, (c, d) in enumerate(modes):
+            M[r, s] = integ(mul(leg[a], leg[c]), mul(leg[b], leg[d]))
+            D[r, s] = integ(mul(leg[a], der[c]), mul(leg[b], leg[d]))
+    return M, D
+
+
+@pytest.mark.parametrize("nc,ng", [(3, 12), (4, 25), (5, 27)])
+def test_operators_match_closed_form(nc, ng):
+    """cal_mat (src/mat1.f:90-142) equals the exact integrals where the rule is exact."""
+    wi, xi, yi, wif, tif = api.quadrature(ng, nc + 1)
+    T = O.Tables(nc, ng, nc + 1, wi, xi, yi, wif, tif)
+    M, D = _exact_mass(nc)
+    # numpy [j, i] holds mat(i, j)
+    assert np.allclose(T.ammo.T, M, atol=1e-13, rtol=0)
+    assert np.allclose(T.agx.T, D, atol=1e-13, rtol=0)
+
+
+@pytest.mark.parametrize("nc,ng", [(3, 12), (4, 25), (6, 33), (7, 42)])
+def test_cholesky_reconstructs_mass_matrix(nc, ng):
+    wi, xi, yi, wif, tif = api.quadrature(ng, 9)
+    T = O.Tables(nc, ng, 9, wi, xi, yi, wif, tif)
+    assert T.info_amm == 0 and T.info_amml == 0
+    U = np.triu(T.amm.T)  # numpy [j, i] holds amm(i, j): transpose to (i, j)
+    A = T.ammo.T
+    assert np.abs(U.T @ U - A).max() < 1e-14 * np.abs(A).max() * T.nm
+    nmr = T.nm - nc - 1
+    Ul = np.triu(T.amml.T[:nmr, :nmr])
+    Al = T.amml_raw.T[:nmr, :nmr]
+    assert np.abs(Ul.T @ Ul - Al).max() < 1e-13 * np.abs(Al).max() * T.nm
+
+
+def test_singular_high_degree_rule_fails_like_dpotrf():
+    """Degree 8 (45 modes) with 42 points: the quadrature Gram matrix has rank <= 42."""
+    wi, xi, yi, wif, tif = api.quadrature(42, 9)
+    T = O.Tables(8, 42, 9, wi, xi, yi, wif, tif)
+    assert T.info_amm == 43
+
+
+def _problem(name, n, **kw):
+    p = W.build_problem(W.small(W.CONFIGS[name], n, **kw))
+    T = p.T
+    OT = O.Tables(p.cfg.nc, p.cfg.ng, p.cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
+    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, p.cfg.nc, p.cfg.f0, p.cfg.beta)
+    return p, OT, OM
+
+
+def test_face_trace_is_exact_for_polynomials():
+    """cal_flu (src/calflu.f) at edge points equals the polynomial evaluated there."""
+    p, OT, OM = _problem("c2_fs_p6", 4)
+    rng = np.random.default_rng(0)
+    c = rng.normal(size=6)
+    s = 1.0 / p.cfg.length  # O(1) polynomial on the basin
+
+    def f(x, y):
+        x, y = x * s, y * s
+        return c[0] + c[1] * x + c[2] * y + c[3] * x * y + c[4] * x ** 2 + c[5] * y ** 3
+    a, _, _ = O.calh(OT, OM, f)
+    nf = OM.nf
+    fb = np.zeros((nf, OT.ngf))
+    L = O.lib()
+    L.ora_cal_flu(O.C.byref(OT.common), nf, O.i(OM.tseg), O.d(fb), OT.ngf, O.d(a), a.shape[1],
+                  O.i(OM.ssit), 1)
+    # physical edge points of face k: tseg(1) element, side ssit(1), parameter t
+    for face in range(nf):
+        e, side = OM.tseg[face, 0] - 1, OM.ssit[face, 0]
+        n1, n2, n3 = OM.inn[e] - 1
+        X = np.array([OM.xgr[n1], OM.xgr[n2], OM.xgr[n3]])
+        Y = np.array([OM.ygr[n1], OM.ygr[n2], OM.ygr[n3]])
+        t = OT.tif
+        xi, eta = {1: (t, -np.ones_like(t)), 2: (-t, t), 3: (-np.ones_like(t), -t)}[side]
+        px = X[0] + (X[1] - X[0]) * (xi + 1) / 2 + (X[2] - X[0]) * (eta + 1) / 2
+        py = Y[0] + (Y[1] - Y[0]) * (xi + 1) / 2 + (Y[2] - Y[0]) * (eta + 1) / 2
+        assert np.allclose(fb[face], f(px, py), rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("name", ["c1_lin_p3", "c2_fs_p6", "c4_ns_p4", "c3_inv_p7"])
+def test_state_at_rest_stays_at_rest(name):
+    p, OT, OM = _problem(name, 5)
+    z = np.zeros_like(p.u)
+    h = np.zeros_like(p.h)
+    h[:, 0] = 0.37  # flat free surface
+    c = p.cfg
+    r = O.cal_var(c.variant, OT, OM, z, z, h, np.zeros_like(OM.fc), p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0)
+    # a flat surface produces no tendency: compare with the tendency of a bump
+    rb = O.cal_var(c.variant, OT, OM, z, z, p.h, np.zeros_like(OM.fc), p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0)
+    scale = max(np.abs(x).max() for x in rb)
+    assert max(np.abs(x).max() for x in r) < 1e-6 * scale
+    assert np.abs(r[2]).max() == 0.0
+
+
+@pytest.mark.parametrize("name", ["c1_lin_p3", "c2_fs_p6", "c4_ns_p4", "c3_inv_p7"])
+def test_rhs_conserves_mass(name):
+    """sum_e det_e sum_j ammo(j,1) dh_j = 0: flux form, central flux, closed basin."""
+    p, OT, OM = _problem(name, 6)
+    c = p.cfg
+    rng = np.random.default_rng(3)
+    u = p.u + 0.01 * rng.normal(size=p.u.shape)
+    v = p.v + 0.01 * rng.normal(size=p.v.shape)
+    if c.variant == "lin":
+        # the linear h flux uses u itself, which must satisfy u.n = 0 at walls:
+        # take the velocity the linear dynamics builds from rest
+        u, v, h = np.zeros_like(u), np.zeros_like(v), p.h.copy()
+        O.rk4("lin", OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, 0.0, 0.0, c.g0, p.dt, 3)
+        assert np.abs(u).max() > 0
+    du, dv, dh = O.cal_var(c.variant, OT, OM, u, v, p.h, OM.fc, p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0)
+    det = OM.vect[:, 0] * OM.vect[:, 3] - OM.vect[:, 2] * OM.vect[:, 1]
+    terms = det[:, None] * OT.ammo[0, :][None, :] * dh
+    assert np.abs(terms).sum() > 0
+    assert abs(terms.sum()) < 1e-11 * np.abs(terms).sum()
+
+
+def test_linear_standing_wave_known_answer():
+    """Fundamental basin mode (walls at x = +-L/2), as compare.f checks:
+    h = A cos(k x') cos(w t), u = A g k / w sin(k x') sin(w t), w = k sqrt(g H)."""
+    cfg = W.small(W.CONFIGS["c1_lin_p3"], 16)
+    p, OT, OM = _problem("c1_lin_p3", 16)
+    L, g, H, A = cfg.length, cfg.g0, cfg.depth, 0.5
+    k = np.pi / L
+    w = k * np.sqrt(g * H)
+    h, px, py = O.calh(OT, OM, lambda x, y: A * np.cos(k * (x + L / 2)))
+    u = np.zeros_like(h)
+    v = np.zeros_like(h)
+    nsteps = 200
+    O.rk4("lin", OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, 0.0, 0.0, g, p.dt, nsteps)
+    t = p.dt * nsteps
+    href = A * np.cos(k * (px + L / 2)) * np.cos(w * t)
+    uref = A * g * k / w * np.sin(k * (px + L / 2)) * np.sin(w * t)
+    hq = h @ OT.pi2
+    uq = u @ OT.pi2
+    vq = v @ OT.pi2
+    assert np.sqrt(np.mean((hq - href) ** 2)) < 1e-4 * A
+    assert np.sqrt(np.mean((uq - uref) ** 2)) < 1e-4 * A * g * k / w
+    assert np.abs(vq).max() < 1e-4 * A * g * k / w
+
+
+def test_openmp_and_serial_are_bit_identical():
+    p, OT, OM = _problem("c2_fs_p6", 8)
+    c = p.cfg
+    outs = []
+    for nt in (1, 4):
+        u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+        O.rk4(c.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0, p.dt, 2, nt)
+        outs.append((u, v, h))
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
