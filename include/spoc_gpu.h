@@ -90,6 +90,13 @@ typedef struct spoc_handle spoc_handle;
 int spoc_create(const spoc_tables *tables, const spoc_mesh *mesh, int variant, int precision,
                 spoc_handle **out);
 void spoc_destroy(spoc_handle *h);
+/* Kernel family (no reference counterpart; results are identical):
+ * SPOC_PATH_AUTO picks the compile-time-sized kernels when (nc, ng, ngf) is
+ * one of the tabulated combinations, else the generic runtime-sized ones. */
+#define SPOC_PATH_AUTO 0
+#define SPOC_PATH_GENERIC 1
+#define SPOC_PATH_TEMPLATED 2
+int spoc_set_kernel_path(spoc_handle *h, int path);
 /* Use an external cudaStream_t (0 = the handle's own stream). */
 int spoc_set_stream(spoc_handle *h, void *stream);
 /* Upload mu0, mb0, g0 and fc, w0, z0, hb (arguments of cal_var, src/calvarnl_fs.f:12). */

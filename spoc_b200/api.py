@@ -88,6 +88,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "spoc_create": (C.c_int, [C.POINTER(_Tables), C.POINTER(_Mesh), C.c_int, C.c_int, C.POINTER(vp)]),
         "spoc_destroy": (None, [vp]),
         "spoc_set_stream": (C.c_int, [vp, vp]),
+        "spoc_set_kernel_path": (C.c_int, [vp, C.c_int]),
         "spoc_set_params": (C.c_int, [vp, C.POINTER(_Params)]),
         "spoc_cal_var": (C.c_int, [vp, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP]),
         "spoc_cal_var_dev": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, vp]),
@@ -335,6 +336,11 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+    def set_kernel_path(self, path: str) -> None:
+        """'auto', 'generic' (runtime-sized kernels) or 'templated' (compile-time sized)."""
+        code = {"auto": 0, "generic": 1, "templated": 2}[path]
+        _check(self.lib.spoc_set_kernel_path(self._h, code), "set_kernel_path")
 
     def set_stream(self, stream_ptr: int) -> None:
         _check(self.lib.spoc_set_stream(self._h, C.c_void_p(stream_ptr)), "set_stream")

@@ -49,6 +49,7 @@ struct spoc_handle {
   int variant = 0, precision = 0;
   int nc = 0, nm = 0, ng = 0, ngf = 0, nmr = 0, ne = 0, nf = 0;
   int sms = 148;
+  int path = SPOC_PATH_AUTO;
   cudaStream_t own = nullptr, st = nullptr;
   long long launches = 0;
   double mu0 = 0, mb0 = 0, g0 = 9.81, hh0 = 0;
@@ -255,6 +256,15 @@ RhsBuffers rhs_buffers(spoc_handle *h, double *const s[3]) {
   return b;
 }
 
+cudaError_t launch(spoc_handle *h, double *const s[3], const StageArgs &sa, cudaEvent_t *ev) {
+  const bool fast = h->path != SPOC_PATH_GENERIC && fast_available(h->nc, h->ng, h->ngf);
+  if (fast)
+    return launch_rhs_fast(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms,
+                           &h->launches, ev);
+  return launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms,
+                    &h->launches, ev);
+}
+
 int check_flag(spoc_handle *h) {
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->st), "read flag");
@@ -271,8 +281,7 @@ int run_rhs_tend(spoc_handle *h, double *const s[3]) {
   sa.stage = -1;
   for (int c = 0; c < 3; ++c) sa.tend[c] = h->TEND[c];
   sa.flag = h->flag;
-  CK(launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms, &h->launches),
-     "launch cal_var");
+  CK(launch(h, s, sa, nullptr), "launch cal_var");
   return SPOC_OK;
 }
 
@@ -376,6 +385,14 @@ extern "C" void spoc_destroy(spoc_handle *h) {
   delete h;
 }
 
+extern "C" int spoc_set_kernel_path(spoc_handle *h, int path) {
+  if (!h || path < SPOC_PATH_AUTO || path > SPOC_PATH_TEMPLATED) return fail(SPOC_E_ARG, "bad argument");
+  if (path == SPOC_PATH_TEMPLATED && !fast_available(h->nc, h->ng, h->ngf))
+    return fail(SPOC_E_UNSUPPORTED, "no compile-time-sized kernels for this (nc, ng, ngf)");
+  h->path = path;
+  return SPOC_OK;
+}
+
 extern "C" int spoc_set_stream(spoc_handle *h, void *stream) {
   if (!h) return fail(SPOC_E_ARG, "null handle");
   CK(cudaStreamSynchronize(h->st), "synchronize");
@@ -470,9 +487,7 @@ int enqueue_steps(spoc_handle *h, double dt, int nsteps) {
       double *const *out = s == 1 ? h->SB : h->SA;
       sa.stage = s;
       for (int c = 0; c < 3; ++c) sa.out[c] = out[c];
-      CK(launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, in), sa, h->st, h->sms,
-                    &h->launches),
-         "launch RK4 stage");
+      CK(launch(h, in, sa, nullptr), "launch RK4 stage");
     }
   }
   return SPOC_OK;
@@ -579,8 +594,7 @@ extern "C" int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *k
       double *const *out = s == 1 ? h->SB : h->SA;
       sa.stage = s;
       for (int c = 0; c < 3; ++c) sa.out[c] = out[c];
-      cudaError_t ce = launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, in), sa, h->st,
-                                  h->sms, &h->launches, ev);
+      cudaError_t ce = launch(h, in, sa, ev);
       if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[nk]);
       for (int k = 0; k < nk && ce == cudaSuccess; ++k) {
         float ms = 0.f;

@@ -1,0 +1,1084 @@
+// Compile-time-sized FP64 kernels of the SPOC RK4 DG right-hand side.
+//
+// Same arithmetic as spoc_kernels.cu (every sum in the reference order, every
+// product separately rounded, bit-identical results), organised for
+// throughput:
+//   * dimensions (nm, ng, ngf) are template parameters, so every loop is
+//     unrolled and every shared-memory offset is an immediate;
+//   * the reference-element operators are staged once per block in shared
+//     memory (persistent blocks loop over elements);
+//   * the modal coefficients of the element and of its three neighbours are
+//     staged with coalesced loads before the face-value chains;
+//   * independent chains are batched so each lane carries several at once:
+//     the mat-vecs of one kernel share their operator loads, the face values
+//     of all traced fields run together, the lifts of all fields and sides
+//     run together, and the mass solves of one element run together.
+// One warp still handles one element; lanes map to modes, quadrature points
+// or face points.
+#include <cuda_runtime.h>
+
+#include "spoc_device.cuh"
+#include "spoc_kernels.h"
+
+namespace spoc {
+namespace {
+
+template <int NC_, int Q_, int G_>
+struct Dims {
+  static constexpr int N = (NC_ + 1) * (NC_ + 2) / 2;
+  static constexpr int NMR = NC_ * (NC_ + 1) / 2;
+  static constexpr int Q = Q_;
+  static constexpr int G = G_;
+  static constexpr int R = (N + 31) / 32;    // modal rows per lane
+  static constexpr int RQ = (Q + 31) / 32;   // quadrature rows per lane
+  static constexpr int TRI = N * (N + 1) / 2;
+  static constexpr int TRIR = NMR * (NMR + 1) / 2;
+  static_assert(3 * G <= 32, "face points must fit one warp");
+  static_assert(N <= 64 && Q <= 64, "two rows per lane at most");
+};
+
+// Packed upper-triangular factor U (row k of U is U(k, k..m-1); column k is
+// U(0..k, k)).  Row k starts at k*m - k*(k-1)/2; column k at k*(k+1)/2.
+__host__ __device__ constexpr int row_off(int k, int m) { return k * m - k * (k - 1) / 2; }
+__host__ __device__ constexpr int col_off(int k) { return k * (k + 1) / 2; }
+
+// Operators of the q-phase, tendency and linear kernels.
+template <class Dm>
+struct SOps {
+  double agx[Dm::N * Dm::N];      // [j*N + i] = agx(j,i)
+  double agy[Dm::N * Dm::N];
+  double pf[3 * Dm::N * Dm::G];   // [(s*N + n)*G + j] = pico(j,n,s)
+  double pt[3 * Dm::G * Dm::N];   // [(s*G + j)*N + n] = pico(j,n,s)
+  double urow[Dm::TRI];           // U(k,i), i >= k, row-packed
+  double ucol[Dm::TRI];           // U(i,k), i <= k, column-packed
+  double lrow[Dm::TRIR];          // Ul(k,i)
+  double lcol[Dm::TRIR];          // Ul(i,k)
+  double dia1[Dm::N];
+  double dia2[Dm::NMR > 0 ? Dm::NMR : 1];
+  double wif[Dm::G];
+  int red_k[Dm::NMR > 0 ? Dm::NMR : 1], red_i0[Dm::NMR > 0 ? Dm::NMR : 1],
+      red_sg[Dm::NMR > 0 ? Dm::NMR : 1];
+  int inv_kind[Dm::N], inv_a[Dm::N], inv_cnt[Dm::N];
+};
+
+// Operators of the quadrature-point kernel.
+template <class Dm>
+struct SOpsQ {
+  double p2[Dm::N * Dm::Q];       // [n*Q + q] = pi2(q,n)
+  double p2t[Dm::Q * Dm::N];      // [q*N + n] = pi2(q,n)
+  double wi[Dm::Q];
+  double urow[Dm::TRI];
+  double ucol[Dm::TRI];
+  double lrow[Dm::TRIR];
+  double lcol[Dm::TRIR];
+  double dia1[Dm::N];
+  double dia2[Dm::NMR > 0 ? Dm::NMR : 1];
+  int red_k[Dm::NMR > 0 ? Dm::NMR : 1], red_i0[Dm::NMR > 0 ? Dm::NMR : 1],
+      red_sg[Dm::NMR > 0 ? Dm::NMR : 1];
+  int inv_kind[Dm::N], inv_a[Dm::N], inv_cnt[Dm::N];
+};
+
+template <class Dm, class S>
+__device__ void stage_solve_ops(S &s, const DevOps &op) {
+  constexpr int N = Dm::N, NMR = Dm::NMR;
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int k = 0; k < N; ++k)
+    for (int i = k + t; i < N; i += nt) s.urow[row_off(k, N) + i - k] = op.uT[k * N + i];
+  for (int k = 0; k < N; ++k)
+    for (int i = t; i <= k; i += nt) s.ucol[col_off(k) + i] = op.uC[k * N + i];
+  for (int k = 0; k < NMR; ++k)
+    for (int i = k + t; i < NMR; i += nt) s.lrow[row_off(k, NMR) + i - k] = op.ulT[k * N + i];
+  for (int k = 0; k < NMR; ++k)
+    for (int i = t; i <= k; i += nt) s.lcol[col_off(k) + i] = op.ulC[k * N + i];
+  for (int i = t; i < N; i += nt) {
+    s.dia1[i] = op.dia1[i];
+    s.inv_kind[i] = op.inv_kind[i];
+    s.inv_a[i] = op.inv_a[i];
+    s.inv_cnt[i] = op.inv_cnt[i];
+  }
+  for (int i = t; i < NMR; i += nt) {
+    s.dia2[i] = op.dia2[i];
+    s.red_k[i] = op.red_k[i];
+    s.red_i0[i] = op.red_i0[i];
+    s.red_sg[i] = op.red_sg[i];
+  }
+}
+
+template <class Dm>
+__device__ void stage_ops(SOps<Dm> &s, const DevOps &op) {
+  constexpr int N = Dm::N, G = Dm::G;
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int i = t; i < N * N; i += nt) {
+    s.agx[i] = op.agx[i];
+    s.agy[i] = op.agy[i];
+  }
+  for (int i = t; i < 3 * N * G; i += nt) {
+    s.pf[i] = op.picoF[i];
+    s.pt[i] = op.picoT[i];
+  }
+  for (int i = t; i < G; i += nt) s.wif[i] = op.wif[i];
+  stage_solve_ops<Dm>(s, op);
+}
+
+template <class Dm>
+__device__ void stage_ops_q(SOpsQ<Dm> &s, const DevOps &op) {
+  constexpr int N = Dm::N, Q = Dm::Q;
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int i = t; i < N * Q; i += nt) {
+    s.p2[i] = op.p2[i];
+    s.p2t[i] = op.p2t[i];
+  }
+  for (int i = t; i < Q; i += nt) s.wi[i] = op.wi[i];
+  stage_solve_ops<Dm>(s, op);
+}
+
+__device__ __forceinline__ int warp_in_block() { return threadIdx.x >> 5; }
+__device__ __forceinline__ int warp_global() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ int warp_count() { return (gridDim.x * blockDim.x) >> 5; }
+
+// ---------------------------------------------------------------------------
+// warp building blocks (lanes over modes unless stated otherwise)
+// ---------------------------------------------------------------------------
+
+// own field: lanes load v[e*N + i] into sm[i]
+template <class Dm>
+__device__ __forceinline__ void load_vec(double *sm, const double *__restrict__ g, int e) {
+  const int l = lane_id();
+#pragma unroll
+  for (int r = 0; r < Dm::R; ++r) {
+    const int i = l + 32 * r;
+    if (i < Dm::N) sm[i] = g[(size_t)e * Dm::N + i];
+  }
+}
+
+template <class Dm>
+__device__ __forceinline__ void load_reg(double (&x)[Dm::R], const double *__restrict__ g, int e) {
+  const int l = lane_id();
+#pragma unroll
+  for (int r = 0; r < Dm::R; ++r) {
+    const int i = l + 32 * r;
+    x[r] = i < Dm::N ? g[(size_t)e * Dm::N + i] : 0.0;
+  }
+}
+
+template <class Dm>
+__device__ __forceinline__ void store_reg(double *g, const double (&x)[Dm::R], int e) {
+  const int l = lane_id();
+#pragma unroll
+  for (int r = 0; r < Dm::R; ++r) {
+    const int i = l + 32 * r;
+    if (i < Dm::N) g[(size_t)e * Dm::N + i] = x[r];
+  }
+}
+
+template <class Dm>
+__device__ __forceinline__ void reg_to_sm(double *sm, const double (&x)[Dm::R]) {
+  const int l = lane_id();
+#pragma unroll
+  for (int r = 0; r < Dm::R; ++r) {
+    const int i = l + 32 * r;
+    if (i < Dm::N) sm[i] = x[r];
+  }
+}
+
+// Neighbour across each side k of element e (-1 for a wall) and whether e is
+// tseg(1) of that face.
+struct Sides {
+  int face[3], nb[3];
+  bool first[3];
+};
+__device__ __forceinline__ Sides sides_of(const DevMesh &m, int e) {
+  Sides s;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int f = __ldg(m.itm + 3 * e + k);
+    const int t1 = __ldg(m.tseg + 2 * f), t2 = __ldg(m.tseg + 2 * f + 1);
+    s.face[k] = f;
+    s.first[k] = (t1 == e);
+    s.nb[k] = s.first[k] ? t2 : t1;
+  }
+  return s;
+}
+
+// Stage NF fields of the three neighbours: nb[(k*NF + f)*N + i].
+template <class Dm, int NF, class Fetch>
+__device__ __forceinline__ void stage_neighbours(const Sides &sd, double *nb, Fetch fetch) {
+  const int l = lane_id();
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int t = sd.nb[k];
+    if (t < 0) continue;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int r = 0; r < Dm::R; ++r) {
+        const int i = l + 32 * r;
+        if (i < Dm::N) nb[(k * NF + f) * Dm::N + i] = fetch(f, t, i);
+      }
+  }
+}
+
+// Face values of NF fields by the cal_flu chain (src/calflu.f:31-62): lane
+// k*G + j computes point j of the face of side k; fb[f*32 + k*G + j].
+template <class Dm, int NF>
+__device__ __forceinline__ void face_values(const double *pf, const DevMesh &m, const Sides &sd,
+                                            const double *own, const double *nb, double *fb) {
+  constexpr int N = Dm::N, G = Dm::G;
+  const int l = lane_id();
+  if (l < 3 * G) {
+    const int k = l / G, j = l - k * G;
+    const int f = sd.face[k];
+    double acc[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = 0.0;
+    if (sd.nb[k] < 0) {
+      const double *p = pf + j;  // wall faces are traced on side 1 of their element
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        const double pv = p[n * G];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) acc[q] = add(acc[q], mul(own[q * N + n], pv));
+      }
+    } else {
+      const double *nbk = nb + k * NF * N;
+      const double *a1 = sd.first[k] ? own : nbk;
+      const double *a2 = sd.first[k] ? nbk : own;
+      const int s1 = __ldg(m.ssit + 2 * f), s2 = __ldg(m.ssit + 2 * f + 1);
+      const double *p1 = pf + s1 * N * G + j;
+      const double *p2 = pf + s2 * N * G + (G - 1 - j);
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        const double pv = p1[n * G];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) acc[q] = add(acc[q], mul(a1[q * N + n], pv));
+      }
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        const double pv = p2[n * G];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) acc[q] = add(acc[q], mul(a2[q * N + n], pv));
+      }
+#pragma unroll
+      for (int q = 0; q < NF; ++q) acc[q] = mul(0.5, acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < NF; ++q) fb[q * 32 + l] = acc[q];
+  }
+}
+
+// ax[f] = agx^T x_f, bx[f] = agy^T x_f for NF smem vectors x_f = X + f*XS
+template <class Dm, int NF>
+__device__ __forceinline__ void matvec2(const double *A, const double *B, const double *X, int XS,
+                                        double (&ax)[NF][Dm::R], double (&bx)[NF][Dm::R]) {
+  constexpr int N = Dm::N, R = Dm::R;
+  const int l = lane_id();
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int r = 0; r < R; ++r) ax[f][r] = bx[f][r] = 0.0;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    double a[R], b[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = l + 32 * r;
+      a[r] = (i < N) ? A[j * N + i] : 0.0;
+      b[r] = (i < N) ? B[j * N + i] : 0.0;
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const double x = X[f * XS + j];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        ax[f][r] = add(ax[f][r], mul(a[r], x));
+        bx[f][r] = add(bx[f][r], mul(b[r], x));
+      }
+    }
+  }
+}
+
+// b := b + ans * c (cal_b epilogue, src/calb2.f:91)
+template <int R>
+__device__ __forceinline__ void axpy(double (&b)[R], const double (&ans)[R], double c) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) b[r] = add(b[r], mul(ans[r], c));
+}
+
+// Lift sums of tri_f (src/mat1.f:189-206) for NF face-value sets:
+// t[f][k][r] = sum_j wif(j) * (pico(j1,n,k) * fb[f*32 + k*G + j]).
+template <class Dm, int NF>
+__device__ __forceinline__ void lift_sums(const SOps<Dm> &s, const int (&isg)[3], const double *fb,
+                                          double (&t)[NF][3][Dm::R]) {
+  constexpr int N = Dm::N, G = Dm::G, R = Dm::R;
+  const int l = lane_id();
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int isg2 = (G + 1) * (1 - isg[k]) / 2;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int r = 0; r < R; ++r) t[f][k][r] = 0.0;
+#pragma unroll
+    for (int jj = 1; jj <= G; ++jj) {
+      const int j1 = isg2 + isg[k] * jj;
+      const double w = s.wif[jj - 1];
+      const double *pr = s.pt + (k * G + j1 - 1) * N;
+      double p[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = l + 32 * r;
+        p[r] = i < N ? pr[i] : 0.0;
+      }
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const double fv = fb[f * 32 + k * G + jj - 1];
+#pragma unroll
+        for (int r = 0; r < R; ++r) t[f][k][r] = add(t[f][k][r], mul(w, mul(p[r], fv)));
+      }
+    }
+  }
+}
+
+// b := b + t_k * sig_k, k = 1..3, sig_k = (isg_k * coeff) * 0.5
+template <int R>
+__device__ __forceinline__ void apply_lift(double (&b)[R], const double (&t)[3][R],
+                                           const int (&isg)[3], double coeff) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double sig = mul(mul((double)isg[k], coeff), 0.5);
+#pragma unroll
+    for (int r = 0; r < R; ++r) b[r] = add(b[r], mul(t[k][r], sig));
+  }
+}
+
+// S simultaneous DTRSM4 solves (src/dtrsm1.f:47-82) of size M with a packed
+// factor; rows i = lane + 32 r.
+template <int M, int R, int S>
+__device__ __forceinline__ void solve_batch(double (&t)[S][R], const double *row, const double *col,
+                                            const double *dia) {
+  const int l = lane_id();
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    const int kl = k & 31, kr = k >> 5;
+    const double d = dia[k];
+    double xk[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      if (l == kl) t[s][kr] = mul(t[s][kr], d);
+      xk[s] = __shfl_sync(0xffffffffu, t[s][kr], kl);
+    }
+    const double *u = row + row_off(k, M) - k;  // u[i] = U(k,i)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = l + 32 * r;
+      if (i > k && i < M) {
+        const double uk = u[i];
+#pragma unroll
+        for (int s = 0; s < S; ++s) t[s][r] = sub(t[s][r], mul(uk, xk[s]));
+      }
+    }
+  }
+#pragma unroll
+  for (int k = M - 1; k >= 0; --k) {
+    const int kl = k & 31, kr = k >> 5;
+    const double d = dia[k];
+    double bk[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      if (l == kl) t[s][kr] = mul(t[s][kr], d);
+      bk[s] = __shfl_sync(0xffffffffu, t[s][kr], kl);
+    }
+    const double *u = col + col_off(k);  // u[i] = U(i,k)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = l + 32 * r;
+      if (i < k) {
+        const double uk = u[i];
+#pragma unroll
+        for (int s = 0; s < S; ++s) t[s][r] = sub(t[s][r], mul(bk[s], uk));
+      }
+    }
+  }
+}
+
+template <class Dm, class Ops, int S>
+__device__ __forceinline__ void solve_full_b(const Ops &s, double (&t)[S][Dm::R]) {
+  solve_batch<Dm::N, Dm::R, S>(t, s.urow, s.ucol, s.dia1);
+}
+template <class Dm, class Ops, int S>
+__device__ __forceinline__ void solve_red_b(const Ops &s, double (&t)[S][Dm::R]) {
+  solve_batch<Dm::NMR, Dm::R, S>(t, s.lrow, s.lcol, s.dia2);
+}
+
+// reduc_gn (src/mat1.f:418-439) through a warp scratch vector
+template <class Dm, class Ops>
+__device__ __forceinline__ void reduc(const Ops &s, const double (&gn)[Dm::R], double (&r)[Dm::R],
+                                      double *sm) {
+  const int l = lane_id();
+  reg_to_sm<Dm>(sm, gn);
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < Dm::R; ++h) {
+    const int rr = l + 32 * h;
+    double v = 0.0;
+    if (rr < Dm::NMR) {
+      const double a = sm[s.red_k[rr]], c = sm[s.red_i0[rr]];
+      v = s.red_sg[rr] > 0 ? add(a, c) : sub(a, c);
+    }
+    r[h] = v;
+  }
+  __syncwarp();
+}
+
+// reduc_inv_gn (src/mat1.f:445-473)
+template <class Dm, class Ops>
+__device__ __forceinline__ void reduc_inv(const Ops &s, const double (&gr)[Dm::R],
+                                          double (&gn)[Dm::R], double *sm) {
+  const int l = lane_id();
+#pragma unroll
+  for (int h = 0; h < Dm::R; ++h) {
+    const int i = l + 32 * h;
+    if (i < Dm::NMR) sm[i] = gr[h];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < Dm::R; ++h) {
+    const int n = l + 32 * h;
+    double v = 0.0;
+    if (n < Dm::N) {
+      const int kind = s.inv_kind[n];
+      if (kind == 1) {
+        const int a = s.inv_a[n], cnt = s.inv_cnt[n];
+        for (int ll = 0; ll < cnt; ll += 2) v = add(v, sm[a + ll]);
+        for (int ll = 1; ll < cnt; ll += 2) v = sub(v, sm[a + ll]);
+      } else if (kind == 2) {
+        v = sm[s.inv_a[n]];
+      }
+    }
+    gn[h] = v;
+  }
+  __syncwarp();
+}
+
+template <int R>
+__device__ __forceinline__ void rot(double (&gn)[R], double (&gt)[R], const double (&gx)[R],
+                                    const double (&gy)[R], double dnx, double dny) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const double a = gx[r], b = gy[r];
+    gn[r] = add(mul(a, dnx), mul(b, dny));
+    gt[r] = sub(mul(a, dny), mul(b, dnx));
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void copy(double (&d)[R], const double (&s)[R]) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) d[r] = s[r];
+}
+
+struct Geo {
+  double ax, bx, ay, by, detai;
+};
+__device__ __forceinline__ Geo geo(const DevMesh &m, int e) {
+  const double *v = m.vect + 5 * (size_t)e;
+  return Geo{__ldg(v), __ldg(v + 1), __ldg(v + 2), __ldg(v + 3), __ldg(v + 4)};
+}
+
+// scaled face values: out[l] = fb[l] * norm(c, face of side l/G) [* scale]
+template <class Dm>
+__device__ __forceinline__ void scale_face(const DevMesh &m, const Sides &sd, const double *fb,
+                                           double *out, int c) {
+  const int l = lane_id();
+  if (l < 3 * Dm::G) out[l] = mul(fb[l], __ldg(m.norm + 2 * sd.face[l / Dm::G] + c));
+}
+template <class Dm>
+__device__ __forceinline__ void scale_face_h(const DevMesh &m, const Sides &sd, const double *fb,
+                                             double *out, int c, double scale) {
+  const int l = lane_id();
+  if (l < 3 * Dm::G) out[l] = mul(mul(fb[l], __ldg(m.norm + 2 * sd.face[l / Dm::G] + c)), scale);
+}
+
+// RK4 stage bookkeeping (src/shwwnl.f:242-284)
+template <class Dm>
+__device__ __forceinline__ void stage_update(const StageArgs &sa, int fld, int e,
+                                             const double (&d)[Dm::R]) {
+  const int l = lane_id();
+#pragma unroll
+  for (int r = 0; r < Dm::R; ++r) {
+    const int n = l + 32 * r;
+    if (n >= Dm::N) continue;
+    const size_t i = (size_t)e * Dm::N + n;
+    const double dd = d[r];
+    if (!isfinite(dd)) atomicOr(sa.flag, 1);
+    if (sa.stage < 0) {
+      sa.tend[fld][i] = dd;
+      continue;
+    }
+    const double u0 = sa.base[fld][i];
+    if (sa.stage == 0) {
+      sa.acc[fld][i] = dd;
+      sa.out[fld][i] = add(u0, mul(mul(sa.dt, dd), 0.5));
+    } else if (sa.stage == 1) {
+      sa.acc[fld][i] = add(sa.acc[fld][i], mul(2.0, dd));
+      sa.out[fld][i] = add(u0, mul(mul(sa.dt, dd), 0.5));
+    } else if (sa.stage == 2) {
+      sa.acc[fld][i] = add(sa.acc[fld][i], mul(2.0, dd));
+      sa.out[fld][i] = add(u0, mul(sa.dt, dd));
+    } else {
+      sa.base[fld][i] = add(u0, mul(sa.dt6, add(sa.acc[fld][i], dd)));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// q-phase (calvarnl_fs.f:88-226)
+// ---------------------------------------------------------------------------
+template <class Dm>
+struct QWarp {
+  double own[2 * Dm::N];
+  double nb[3 * 2 * Dm::N];
+  double fr[2 * 32];
+  double fb[4 * 32];
+  double sm[64];
+};
+
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const double *__restrict__ su,
+                                                 const double *__restrict__ sv, double *q) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
+  QWarp<Dm> &W = reinterpret_cast<QWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, R = Dm::R;
+  stage_ops(S, op);
+  __syncthreads();
+  const size_t fs = (size_t)m.ne * N;
+  for (int e = warp_global(); e < m.ne; e += warp_count()) {
+    const Sides sd = sides_of(m, e);
+    const Geo g = geo(m, e);
+    int isg[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
+    load_vec<Dm>(W.own, su, e);
+    load_vec<Dm>(W.own + N, sv, e);
+    stage_neighbours<Dm, 2>(sd, W.nb, [&](int f, int t, int i) {
+      return (f == 0 ? su : sv)[(size_t)t * N + i];
+    });
+    __syncwarp();
+    face_values<Dm, 2>(S.pf, m, sd, W.own, W.nb, W.fr);
+    __syncwarp();
+    scale_face<Dm>(m, sd, W.fr, W.fb + 0, 0);
+    scale_face<Dm>(m, sd, W.fr, W.fb + 32, 1);
+    scale_face<Dm>(m, sd, W.fr + 32, W.fb + 64, 0);
+    scale_face<Dm>(m, sd, W.fr + 32, W.fb + 96, 1);
+    double ax[2][R], bx[2][R];
+    matvec2<Dm, 2>(S.agx, S.agy, W.own, N, ax, bx);
+    __syncwarp();
+    double gq[4][R];  // gxx, gxy, gyx, gyy
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double gx1 = add(0.0, mul(ax[c][r], -1.0)), gy1 = add(0.0, mul(bx[c][r], -1.0));
+        gq[2 * c][r] = mul(sub(mul(g.by, gx1), mul(g.ay, gy1)), g.detai);
+        gq[2 * c + 1][r] = mul(add(-mul(g.bx, gx1), mul(g.ax, gy1)), g.detai);
+      }
+    double t[4][3][R];
+    lift_sums<Dm, 4>(S, isg, W.fb, t);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) apply_lift<R>(gq[c], t[c], isg, g.detai);
+    if (VAR == kFS && __ldg(m.bdl + e)) {
+      // calvarnl_fs.f:171-204
+      const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+      double gnx[R], gtx[R], gny[R], gty[R], gtn[R], bu[1][R];
+      double fs3[3][R];  // gnn, gnt, gtt
+      rot<R>(gnx, gtx, gq[0], gq[2], dnx, dny);
+      rot<R>(gny, gty, gq[1], gq[3], dnx, dny);
+      rot<R>(fs3[0], fs3[1], gnx, gny, dnx, dny);
+      rot<R>(gtn, fs3[2], gtx, gty, dnx, dny);
+      reduc<Dm>(S, gtn, bu[0], W.sm);
+      solve_full_b<Dm, SOps<Dm>, 3>(S, fs3);
+      solve_red_b<Dm, SOps<Dm>, 1>(S, bu);
+      reduc_inv<Dm>(S, bu[0], gtn, W.sm);
+      rot<R>(gnx, gny, fs3[0], fs3[1], dnx, dny);
+      rot<R>(gtx, gty, gtn, fs3[2], dnx, dny);
+      rot<R>(gq[0], gq[2], gnx, gtx, dnx, dny);
+      rot<R>(gq[1], gq[3], gny, gty, dnx, dny);
+    } else {
+      solve_full_b<Dm, SOps<Dm>, 4>(S, gq);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) store_reg<Dm>(q + c * fs, gq[c], e);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// nonlinear terms at quadrature points (calvarnl_fs.f:243-348)
+// ---------------------------------------------------------------------------
+template <class Dm>
+struct BWarp {
+  double vin[9 * Dm::N];
+  double wp[8 * Dm::Q];
+  double sm[64];
+};
+
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SOpsQ<Dm> &S = *reinterpret_cast<SOpsQ<Dm> *>(smem);
+  BWarp<Dm> &W = reinterpret_cast<BWarp<Dm> *>(smem + sizeof(SOpsQ<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, Q = Dm::Q, R = Dm::R, RQ = Dm::RQ;
+  stage_ops_q(S, op);
+  __syncthreads();
+  const int l = lane_id();
+  const size_t fs = (size_t)m.ne * N;
+  for (int e = warp_global(); e < m.ne; e += warp_count()) {
+    double uk[R], vk[R], hh[R], qq[4][R], fc[R], hb[R], w0[R], z0[R];
+    load_reg<Dm>(uk, a.su, e);
+    load_reg<Dm>(vk, a.sv, e);
+    load_reg<Dm>(hh, a.sh, e);
+    load_reg<Dm>(hb, a.hb, e);
+    load_reg<Dm>(w0, a.w0, e);
+    load_reg<Dm>(z0, a.z0, e);
+    load_reg<Dm>(fc, a.fc, e);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) load_reg<Dm>(qq[c], a.q + c * fs, e);
+    // uk,vk,hk=h+hb,wk=w-mb0 u,zk=z-mb0 v,gxx=qxx,gxy=qxy-fc,gyx=qyx+fc,gyy=qyy (:245-255)
+    {
+      double v9[9][R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        v9[0][r] = uk[r];
+        v9[1][r] = vk[r];
+        v9[2][r] = qq[0][r];
+        v9[3][r] = sub(qq[1][r], fc[r]);
+        v9[4][r] = add(qq[2][r], fc[r]);
+        v9[5][r] = qq[3][r];
+        v9[6][r] = add(hh[r], hb[r]);
+        v9[7][r] = sub(w0[r], mul(a.mb0, uk[r]));
+        v9[8][r] = sub(z0[r], mul(a.mb0, vk[r]));
+      }
+#pragma unroll
+      for (int f = 0; f < 9; ++f) reg_to_sm<Dm>(W.vin + f * N, v9[f]);
+    }
+    __syncwarp();
+    // spectoxy (src/nonlin.f:62-86) for the nine fields; lanes over points
+#pragma unroll
+    for (int h = 0; h < RQ; ++h) {
+      const int qp = l + 32 * h;
+      if (qp < Q) {
+        double mv[9];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) mv[f] = 0.0;
+#pragma unroll 4
+        for (int n = 0; n < N; ++n) {
+          const double p = S.p2[n * Q + qp];
+#pragma unroll
+          for (int f = 0; f < 9; ++f) mv[f] = add(mv[f], mul(W.vin[f * N + n], p));
+        }
+        const double w = S.wi[qp];
+        W.wp[0 * Q + qp] = mul(w, mul(mv[0], mv[2]));
+        W.wp[1 * Q + qp] = mul(w, mul(mv[1], mv[3]));
+        W.wp[2 * Q + qp] = mul(w, mul(mv[0], mv[4]));
+        W.wp[3 * Q + qp] = mul(w, mul(mv[1], mv[5]));
+        W.wp[4 * Q + qp] = mul(w, mul(mv[0], mv[6]));
+        W.wp[5 * Q + qp] = mul(w, mul(mv[1], mv[6]));
+        W.wp[6 * Q + qp] = mul(w, __ddiv_rn(mv[7], mv[6]));
+        W.wp[7 * Q + qp] = mul(w, __ddiv_rn(mv[8], mv[6]));
+      }
+    }
+    __syncwarp();
+    // xytospec (src/nonlin.f:35-57, :91-107); lanes over modes
+    double X[8][R];
+#pragma unroll
+    for (int f = 0; f < 8; ++f)
+#pragma unroll
+      for (int r = 0; r < R; ++r) X[f][r] = 0.0;
+#pragma unroll 4
+    for (int qp = 0; qp < Q; ++qp) {
+      double p[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int n = l + 32 * r;
+        p[r] = n < N ? S.p2t[qp * N + n] : 0.0;
+      }
+#pragma unroll
+      for (int f = 0; f < 8; ++f) {
+        const double wv = W.wp[f * Q + qp];
+#pragma unroll
+        for (int r = 0; r < R; ++r) X[f][r] = add(X[f][r], mul(wv, p[r]));
+      }
+    }
+    double uv[2][R];
+    copy<R>(uv[0], X[4]);
+    copy<R>(uv[1], X[5]);
+    if (__ldg(m.bdl + e)) {
+      if (VAR == kNS) {
+        double bu[2][R];  // calvarnl_ns.f:249-265
+        reduc<Dm>(S, uv[0], bu[0], W.sm);
+        reduc<Dm>(S, uv[1], bu[1], W.sm);
+        solve_red_b<Dm, SOpsQ<Dm>, 2>(S, bu);
+        reduc_inv<Dm>(S, bu[0], uv[0], W.sm);
+        reduc_inv<Dm>(S, bu[1], uv[1], W.sm);
+      } else {
+        const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+        double gn[R], gt[1][R], bu[1][R];
+        rot<R>(gn, gt[0], uv[0], uv[1], dnx, dny);
+        reduc<Dm>(S, gn, bu[0], W.sm);
+        solve_red_b<Dm, SOpsQ<Dm>, 1>(S, bu);
+        solve_full_b<Dm, SOpsQ<Dm>, 1>(S, gt);
+        reduc_inv<Dm>(S, bu[0], gn, W.sm);
+        rot<R>(uv[0], uv[1], gn, gt[0], dnx, dny);
+      }
+    } else {
+      solve_full_b<Dm, SOpsQ<Dm>, 2>(S, uv);
+    }
+    double gx0[R], gy0[R], f4[4][R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      gx0[r] = add(-add(X[0][r], X[1][r]), X[6][r]);
+      gy0[r] = add(-add(X[2][r], X[3][r]), X[7][r]);
+      f4[0][r] = sub(mul(a.mu0, qq[0][r]), mul(a.g0, hh[r]));
+      f4[1][r] = mul(a.mu0, qq[1][r]);
+      f4[2][r] = mul(a.mu0, qq[2][r]);
+      f4[3][r] = sub(mul(a.mu0, qq[3][r]), mul(a.g0, hh[r]));
+    }
+    store_reg<Dm>(a.gx0, gx0, e);
+    store_reg<Dm>(a.gy0, gy0, e);
+    store_reg<Dm>(a.uh, uv[0], e);
+    store_reg<Dm>(a.vh, uv[1], e);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) store_reg<Dm>(a.f + c * fs, f4[c], e);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tendencies and the RK4 stage update (calvarnl_fs.f:350-544)
+// ---------------------------------------------------------------------------
+template <class Dm>
+struct TWarp {
+  double own[6 * Dm::N];       // fxx, fxy, fyx, fyy, uh, vh
+  double nb[3 * 6 * Dm::N];
+  double fr[6 * 32];
+  double fb[6 * 32];           // fbdxx, fbdxy, fbdyx, fbdyy, fbdx, fbdy
+  double sm[64];
+};
+
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
+  TWarp<Dm> &W = reinterpret_cast<TWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, R = Dm::R;
+  stage_ops(S, op);
+  __syncthreads();
+  const size_t fs = (size_t)m.ne * N;
+  const double *src[6] = {a.f, a.f + fs, a.f + 2 * fs, a.f + 3 * fs, a.uh, a.vh};
+  for (int e = warp_global(); e < m.ne; e += warp_count()) {
+    const Sides sd = sides_of(m, e);
+    const Geo g = geo(m, e);
+    int isg[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) load_vec<Dm>(W.own + f * N, src[f], e);
+    stage_neighbours<Dm, 6>(sd, W.nb, [&](int f, int t, int i) { return src[f][(size_t)t * N + i]; });
+    __syncwarp();
+    face_values<Dm, 6>(S.pf, m, sd, W.own, W.nb, W.fr);
+    __syncwarp();
+#pragma unroll
+    for (int f = 0; f < 6; ++f) scale_face<Dm>(m, sd, W.fr + 32 * f, W.fb + 32 * f, f & 1);
+    double ax[6][R], bx[6][R];
+    matvec2<Dm, 6>(S.agx, S.agy, W.own, N, ax, bx);
+    double gx[R], gy[R], hb[R];
+    load_reg<Dm>(gx, a.gx0, e);
+    load_reg<Dm>(gy, a.gy0, e);
+    const double cby = mul(g.by, g.detai), cay = mul(g.ay, g.detai);
+    const double cbx = mul(g.bx, g.detai), cax = mul(g.ax, g.detai);
+    axpy<R>(gx, ax[0], -cby);
+    axpy<R>(gx, bx[0], cay);
+    axpy<R>(gx, ax[1], cbx);
+    axpy<R>(gx, bx[1], -cax);
+    axpy<R>(gy, ax[2], -cby);
+    axpy<R>(gy, bx[2], cay);
+    axpy<R>(gy, ax[3], cbx);
+    axpy<R>(gy, bx[3], -cax);
+#pragma unroll
+    for (int r = 0; r < R; ++r) hb[r] = 0.0;
+    axpy<R>(hb, ax[4], cby);
+    axpy<R>(hb, bx[4], -cay);
+    axpy<R>(hb, ax[5], -cbx);
+    axpy<R>(hb, bx[5], cax);
+    __syncwarp();
+    double t[6][3][R];
+    lift_sums<Dm, 6>(S, isg, W.fb, t);
+    apply_lift<R>(gx, t[0], isg, g.detai);
+    apply_lift<R>(gx, t[1], isg, g.detai);
+    apply_lift<R>(gy, t[2], isg, g.detai);
+    apply_lift<R>(gy, t[3], isg, g.detai);
+    apply_lift<R>(hb, t[4], isg, -g.detai);
+    apply_lift<R>(hb, t[5], isg, -g.detai);
+    if (__ldg(m.bdl + e)) {
+      if (VAR == kNS) {
+        double bu[2][R], hs[1][R];
+        reduc<Dm>(S, gx, bu[0], W.sm);
+        reduc<Dm>(S, gy, bu[1], W.sm);
+        solve_red_b<Dm, SOps<Dm>, 2>(S, bu);
+        copy<R>(hs[0], hb);
+        solve_full_b<Dm, SOps<Dm>, 1>(S, hs);
+        copy<R>(hb, hs[0]);
+        reduc_inv<Dm>(S, bu[0], gx, W.sm);
+        reduc_inv<Dm>(S, bu[1], gy, W.sm);
+      } else {
+        const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+        double gn[R], full2[2][R], bu[1][R];
+        rot<R>(gn, full2[0], gx, gy, dnx, dny);
+        copy<R>(full2[1], hb);
+        reduc<Dm>(S, gn, bu[0], W.sm);
+        solve_red_b<Dm, SOps<Dm>, 1>(S, bu);
+        solve_full_b<Dm, SOps<Dm>, 2>(S, full2);
+        reduc_inv<Dm>(S, bu[0], gn, W.sm);
+        rot<R>(gx, gy, gn, full2[0], dnx, dny);
+        copy<R>(hb, full2[1]);
+      }
+    } else {
+      double s3[3][R];
+      copy<R>(s3[0], gx);
+      copy<R>(s3[1], gy);
+      copy<R>(s3[2], hb);
+      solve_full_b<Dm, SOps<Dm>, 3>(S, s3);
+      copy<R>(gx, s3[0]);
+      copy<R>(gy, s3[1]);
+      copy<R>(hb, s3[2]);
+    }
+    stage_update<Dm>(sa, 0, e, gx);
+    stage_update<Dm>(sa, 1, e, gy);
+    stage_update<Dm>(sa, 2, e, hb);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// linear variant (calvar_lin.f:7-287)
+// ---------------------------------------------------------------------------
+template <class Dm>
+struct LWarp {
+  double own[3 * Dm::N];  // fxx = -g0 h, u, v
+  double nb[3 * 3 * Dm::N];
+  double xs[2 * Dm::N];   // u*hh0, v*hh0
+  double fr[3 * 32];
+  double fb[4 * 32];      // fbdxx, fbdyy, fbdx, fbdy
+  double sm[64];
+};
+
+template <class Dm>
+__global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, StageArgs sa) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
+  LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, R = Dm::R;
+  stage_ops(S, op);
+  __syncthreads();
+  const int l = lane_id();
+  const double mg0 = -a.g0, hh0 = a.hh0;
+  for (int e = warp_global(); e < m.ne; e += warp_count()) {
+    const Sides sd = sides_of(m, e);
+    const Geo g = geo(m, e);
+    int isg[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
+    double uk[R], vk[R], hk[R];
+    load_reg<Dm>(uk, a.su, e);
+    load_reg<Dm>(vk, a.sv, e);
+    load_reg<Dm>(hk, a.sh, e);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = l + 32 * r;
+      if (i < N) {
+        W.own[i] = mul(mg0, hk[r]);  // fxx = fyy = -g0 h (calvar_lin.f:76-79)
+        W.own[N + i] = uk[r];
+        W.own[2 * N + i] = vk[r];
+        W.xs[i] = mul(uk[r], hh0);
+        W.xs[N + i] = mul(vk[r], hh0);
+      }
+    }
+    stage_neighbours<Dm, 3>(sd, W.nb, [&](int f, int t, int i) {
+      const size_t o = (size_t)t * N + i;
+      return f == 0 ? mul(mg0, a.sh[o]) : (f == 1 ? a.su[o] : a.sv[o]);
+    });
+    __syncwarp();
+    face_values<Dm, 3>(S.pf, m, sd, W.own, W.nb, W.fr);
+    __syncwarp();
+    scale_face<Dm>(m, sd, W.fr, W.fb, 0);        // fbdxx
+    scale_face<Dm>(m, sd, W.fr, W.fb + 32, 1);   // fbdyy
+    scale_face_h<Dm>(m, sd, W.fr + 32, W.fb + 64, 0, hh0);  // fbdx
+    scale_face_h<Dm>(m, sd, W.fr + 64, W.fb + 96, 1, hh0);  // fbdy
+    double af[1][R], bf[1][R], ah[2][R], bh[2][R];
+    matvec2<Dm, 1>(S.agx, S.agy, W.own, N, af, bf);
+    matvec2<Dm, 2>(S.agx, S.agy, W.xs, N, ah, bh);
+    __syncwarp();
+    const double cby = mul(g.by, g.detai), cay = mul(g.ay, g.detai);
+    const double cbx = mul(g.bx, g.detai), cax = mul(g.ax, g.detai);
+    double gx[R], gy[R], hb[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) gx[r] = gy[r] = hb[r] = 0.0;
+    // u, v (calvar_lin.f:143-166); the zero fields fxy, fyx contribute exact zeros
+    axpy<R>(gx, af[0], -cby);
+    axpy<R>(gx, bf[0], cay);
+    axpy<R>(gy, af[0], cbx);
+    axpy<R>(gy, bf[0], -cax);
+    // h (calvar_lin.f:256-270)
+    axpy<R>(hb, ah[0], cby);
+    axpy<R>(hb, bh[0], -cay);
+    axpy<R>(hb, ah[1], -cbx);
+    axpy<R>(hb, bh[1], cax);
+    double t[4][3][R];
+    lift_sums<Dm, 4>(S, isg, W.fb, t);
+    apply_lift<R>(gx, t[0], isg, g.detai);
+    apply_lift<R>(gy, t[1], isg, g.detai);
+    apply_lift<R>(hb, t[2], isg, -g.detai);
+    apply_lift<R>(hb, t[3], isg, -g.detai);
+    if (__ldg(m.bdl + e)) {
+      const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+      double gn[R], full2[2][R], bu[1][R];
+      rot<R>(gn, full2[0], gx, gy, dnx, dny);
+      copy<R>(full2[1], hb);
+      reduc<Dm>(S, gn, bu[0], W.sm);
+      solve_red_b<Dm, SOps<Dm>, 1>(S, bu);
+      solve_full_b<Dm, SOps<Dm>, 2>(S, full2);
+      reduc_inv<Dm>(S, bu[0], gn, W.sm);
+      rot<R>(gx, gy, gn, full2[0], dnx, dny);
+      copy<R>(hb, full2[1]);
+    } else {
+      double s3[3][R];
+      copy<R>(s3[0], gx);
+      copy<R>(s3[1], gy);
+      copy<R>(s3[2], hb);
+      solve_full_b<Dm, SOps<Dm>, 3>(S, s3);
+      copy<R>(gx, s3[0]);
+      copy<R>(gy, s3[1]);
+      copy<R>(hb, s3[2]);
+    }
+    stage_update<Dm>(sa, 0, e, gx);
+    stage_update<Dm>(sa, 1, e, gy);
+    stage_update<Dm>(sa, 2, e, hb);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launch plumbing
+// ---------------------------------------------------------------------------
+template <class K>
+cudaError_t prepare(K kernel, size_t smem) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// warps per block so that the per-block shared memory stays under ~113 KB
+// (two blocks per SM) when possible, else one block up to 8 warps.
+inline int pick_warps(size_t ops, size_t per_warp) {
+  for (int w = 8; w >= 2; --w)
+    if (ops + w * per_warp <= 113 * 1024) return w;
+  for (int w = 8; w >= 1; --w)
+    if (ops + w * per_warp <= 220 * 1024) return w;
+  return 1;
+}
+
+template <class Dm, int VAR>
+cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
+                   cudaStream_t st, int sms, cudaEvent_t *ev) {
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], st);
+  };
+  NlArgs na{b.su, b.sv, b.sh, b.hb, b.w0, b.z0, b.fc, b.q, b.gx0, b.gy0, b.uh, b.vh, b.f,
+            b.mu0, b.mb0, b.g0};
+  TendArgs ta{b.gx0, b.gy0, b.uh, b.vh, b.f};
+  const int wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
+  const int wb = pick_warps(sizeof(SOpsQ<Dm>), sizeof(BWarp<Dm>));
+  const int wt = pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>));
+  const size_t sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
+  const size_t sb = sizeof(SOpsQ<Dm>) + wb * sizeof(BWarp<Dm>);
+  const size_t stt = sizeof(SOps<Dm>) + wt * sizeof(TWarp<Dm>);
+  static bool ready = false;
+  if (!ready) {
+    cudaError_t e = prepare(kf_qphase<Dm, VAR>, sq);
+    if (e == cudaSuccess) e = prepare(kf_nlvol<Dm, VAR>, sb);
+    if (e == cudaSuccess) e = prepare(kf_tend<Dm, VAR>, stt);
+    if (e != cudaSuccess) return e;
+    ready = true;
+  }
+  auto blocks = [&](size_t smem, int w) {
+    int per_sm = (int)((227 * 1024) / (smem + 1024));
+    if (per_sm < 1) per_sm = 1;
+    const int need = (m.ne + w - 1) / w;
+    const int cap = sms * per_sm;
+    return need < cap ? need : cap;
+  };
+  mark(0);
+  kf_qphase<Dm, VAR><<<blocks(sq, wq), 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
+  mark(1);
+  kf_nlvol<Dm, VAR><<<blocks(sb, wb), 32 * wb, sb, st>>>(op, m, na);
+  mark(2);
+  kf_tend<Dm, VAR><<<blocks(stt, wt), 32 * wt, stt, st>>>(op, m, ta, sa);
+  mark(3);
+  return cudaGetLastError();
+}
+
+template <class Dm>
+cudaError_t run_lin(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
+                    cudaStream_t st, int sms, cudaEvent_t *ev) {
+  const int w = pick_warps(sizeof(SOps<Dm>), sizeof(LWarp<Dm>));
+  const size_t sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
+  static bool ready = false;
+  if (!ready) {
+    cudaError_t e = prepare(kf_lin<Dm>, sm);
+    if (e != cudaSuccess) return e;
+    ready = true;
+  }
+  int per_sm = (int)((227 * 1024) / (sm + 1024));
+  if (per_sm < 1) per_sm = 1;
+  const int need = (m.ne + w - 1) / w;
+  const int grid = need < sms * per_sm ? need : sms * per_sm;
+  LinArgs la{b.su, b.sv, b.sh, b.g0, b.hh0};
+  if (ev) cudaEventRecord(ev[0], st);
+  kf_lin<Dm><<<grid, 32 * w, sm, st>>>(op, m, la, sa);
+  if (ev) cudaEventRecord(ev[1], st);
+  return cudaGetLastError();
+}
+
+template <class Dm>
+cudaError_t run_any(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
+                    const StageArgs &sa, cudaStream_t st, int sms, cudaEvent_t *ev) {
+  switch (variant) {
+    case kLIN: return run_lin<Dm>(op, m, b, sa, st, sms, ev);
+    case kFS: return run_nl<Dm, kFS>(op, m, b, sa, st, sms, ev);
+    case kNS: return run_nl<Dm, kNS>(op, m, b, sa, st, sms, ev);
+    default: return run_nl<Dm, kINV>(op, m, b, sa, st, sms, ev);
+  }
+}
+
+}  // namespace
+
+bool fast_available(int nc, int ng, int ngf) {
+  return (nc == 3 && ng == 12 && ngf == 4) || (nc == 4 && ng == 25 && ngf == 5) ||
+         (nc == 5 && ng == 27 && ngf == 6) || (nc == 6 && ng == 33 && ngf == 7) ||
+         (nc == 7 && ng == 42 && ngf == 9);
+}
+
+cudaError_t launch_rhs_fast(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
+                            const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
+                            cudaEvent_t *ev) {
+  cudaError_t e = cudaErrorNotSupported;
+  const int nc = op.nc, ng = op.ng, ngf = op.ngf;
+  if (nc == 3 && ng == 12 && ngf == 4) e = run_any<Dims<3, 12, 4>>(variant, op, m, b, sa, st, sms, ev);
+  else if (nc == 4 && ng == 25 && ngf == 5) e = run_any<Dims<4, 25, 5>>(variant, op, m, b, sa, st, sms, ev);
+  else if (nc == 5 && ng == 27 && ngf == 6) e = run_any<Dims<5, 27, 6>>(variant, op, m, b, sa, st, sms, ev);
+  else if (nc == 6 && ng == 33 && ngf == 7) e = run_any<Dims<6, 33, 7>>(variant, op, m, b, sa, st, sms, ev);
+  else if (nc == 7 && ng == 42 && ngf == 9) e = run_any<Dims<7, 42, 9>>(variant, op, m, b, sa, st, sms, ev);
+  if (e == cudaSuccess) *launches += variant == kLIN ? 1 : 3;
+  return e;
+}
+
+}  // namespace spoc

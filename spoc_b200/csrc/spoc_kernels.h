@@ -52,6 +52,13 @@ cudaError_t launch_cfl(int ne, int nc, const int *in, const double *xg, const do
                        const double *hb, int nm, double g0, unsigned long long *out,
                        cudaStream_t st, int sms, long long *launches);
 
+// Compile-time-sized kernels (spoc_fast.cu) for the tabulated degree /
+// quadrature combinations; identical results to launch_rhs.
+bool fast_available(int nc, int ng, int ngf);
+cudaError_t launch_rhs_fast(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
+                            const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
+                            cudaEvent_t *ev = nullptr);
+
 // 8 independent chains of `iters` FP64 operations per thread, sms*8 blocks of 256
 cudaError_t launch_fp64_peak(int mode, int sms, int iters, double *out, cudaStream_t st);
 

@@ -38,13 +38,18 @@ def assert_bitwise(got, ref, nm):
         assert not bad.any(), f"{bad.sum()} coefficients differ; max |d| = {np.abs(g - r).max():.3e}"
 
 
+PATHS = ["generic", "templated"]
+
+
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("ld", [None, 45])
-def test_cal_var_bitwise(gpu_lib, name, ld):
+def test_cal_var_bitwise(gpu_lib, name, ld, path):
     p = W.build_problem(W.small(W.CONFIGS[name], 6), ld=ld)
     OT, OM = oracle_for(p)
     s = W.make_solver(p)
+    s.set_kernel_path(path)
     got = s.cal_var(p.u, p.v, p.h)
     ref = oracle_rhs(p, OT, OM, p.u, p.v, p.h)
     assert_bitwise(got, ref, p.T.nm)
@@ -52,8 +57,9 @@ def test_cal_var_bitwise(gpu_lib, name, ld):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("name", NAMES)
-def test_cal_var_random_state_bitwise(gpu_lib, name):
+def test_cal_var_random_state_bitwise(gpu_lib, name, path):
     """Rough random state: exercises every branch with O(1) values everywhere."""
     p = W.build_problem(W.small(W.CONFIGS[name], 5))
     rng = np.random.default_rng(7)
@@ -61,15 +67,18 @@ def test_cal_var_random_state_bitwise(gpu_lib, name):
     h = rng.normal(size=p.h.shape)
     OT, OM = oracle_for(p)
     s = W.make_solver(p)
+    s.set_kernel_path(path)
     assert_bitwise(s.cal_var(u, v, h), oracle_rhs(p, OT, OM, u, v, h), p.T.nm)
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("name", NAMES)
-def test_rk4_device_resident_bitwise(gpu_lib, name):
+def test_rk4_device_resident_bitwise(gpu_lib, name, path):
     p = W.build_problem(W.small(W.CONFIGS[name], 6))
     OT, OM = oracle_for(p)
     s = W.make_solver(p)
+    s.set_kernel_path(path)
     s.set_state(p.u, p.v, p.h)
     s.rk4_steps(p.dt, 5)
     got = s.get_state()
@@ -210,6 +219,20 @@ def test_full_c2_deterministic_and_conservative(gpu_lib):
     # mass = sum_e det_e sum_j ammo(j,1) h_j (src/energy.f:327-329); walls carry no flux
     scale = float(np.sum(np.abs(p.mesh.det[:, None] * p.T.ammo[0, :][None, :] * p.h)))
     assert abs(m1 - m0) <= 1e-12 * scale
+
+
+@pytest.mark.gpu
+def test_untabulated_degree_runs_generic_kernels(gpu_lib):
+    """Degree 2 with the 6-point rule has no compile-time-sized kernels: auto
+    selects the generic ones, and asking for the templated ones is refused."""
+    cfg = W.small(W.CONFIGS["c2_fs_p6"], 5, nc=2, ng=6, ngf=3)
+    p = W.build_problem(cfg)
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    with pytest.raises(api.SpocError) as ei:
+        s.set_kernel_path("templated")
+    assert ei.value.code == 7
+    assert_bitwise(s.cal_var(p.u, p.v, p.h), oracle_rhs(p, OT, OM, p.u, p.v, p.h), p.T.nm)
 
 
 @pytest.mark.gpu
