@@ -761,8 +761,7 @@ template <class Dm>
 struct TWarp {
   double own[6 * Dm::N];       // fxx, fxy, fyx, fyy, uh, vh
   double nb[3 * 6 * Dm::N];
-  double fr[6 * 32];
-  double fb[6 * 32];           // fbdxx, fbdxy, fbdyx, fbdyy, fbdx, fbdy
+  double fb[6 * 32];           // face values, then fbdxx, fbdxy, fbdyx, fbdyy, fbdx, fbdy
   double sm[64];
 };
 
@@ -786,10 +785,11 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
     for (int f = 0; f < 6; ++f) load_vec<Dm>(W.own + f * N, src[f], e);
     stage_neighbours<Dm, 6>(sd, W.nb, [&](int f, int t, int i) { return src[f][(size_t)t * N + i]; });
     __syncwarp();
-    face_values<Dm, 6>(S.pf, m, sd, W.own, W.nb, W.fr);
+    face_values<Dm, 6>(S.pf, m, sd, W.own, W.nb, W.fb);
     __syncwarp();
+    // each lane scales the values it computed (fbd * norm(1|2, face))
 #pragma unroll
-    for (int f = 0; f < 6; ++f) scale_face<Dm>(m, sd, W.fr + 32 * f, W.fb + 32 * f, f & 1);
+    for (int f = 0; f < 6; ++f) scale_face<Dm>(m, sd, W.fb + 32 * f, W.fb + 32 * f, f & 1);
     double ax[6][R], bx[6][R];
     matvec2<Dm, 6>(S.agx, S.agy, W.own, N, ax, bx);
     double gx[R], gy[R], hb[R];
@@ -986,6 +986,18 @@ inline int pick_warps(size_t ops, size_t per_warp) {
   return 1;
 }
 
+// Persistent grid: exactly the number of blocks that can be resident.
+template <class K>
+int resident_grid(K kernel, int threads, size_t smem, int sms, int ne, int warps) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const int need = (ne + warps - 1) / warps;
+  const int cap = sms * per_sm;
+  return need < cap ? need : cap;
+}
+
 template <class Dm, int VAR>
 cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
                    cudaStream_t st, int sms, cudaEvent_t *ev) {
@@ -995,33 +1007,30 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   NlArgs na{b.su, b.sv, b.sh, b.hb, b.w0, b.z0, b.fc, b.q, b.gx0, b.gy0, b.uh, b.vh, b.f,
             b.mu0, b.mb0, b.g0};
   TendArgs ta{b.gx0, b.gy0, b.uh, b.vh, b.f};
-  const int wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
-  const int wb = pick_warps(sizeof(SOpsQ<Dm>), sizeof(BWarp<Dm>));
-  const int wt = pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>));
-  const size_t sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
-  const size_t sb = sizeof(SOpsQ<Dm>) + wb * sizeof(BWarp<Dm>);
-  const size_t stt = sizeof(SOps<Dm>) + wt * sizeof(TWarp<Dm>);
-  static bool ready = false;
-  if (!ready) {
+  static int wq = 0, wb = 0, wt = 0, gq = 0, gb = 0, gt = 0, ne_cached = -1;
+  static size_t sq = 0, sb = 0, stt = 0;
+  if (ne_cached != m.ne) {
+    wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
+    wb = pick_warps(sizeof(SOpsQ<Dm>), sizeof(BWarp<Dm>));
+    wt = pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>));
+    sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
+    sb = sizeof(SOpsQ<Dm>) + wb * sizeof(BWarp<Dm>);
+    stt = sizeof(SOps<Dm>) + wt * sizeof(TWarp<Dm>);
     cudaError_t e = prepare(kf_qphase<Dm, VAR>, sq);
     if (e == cudaSuccess) e = prepare(kf_nlvol<Dm, VAR>, sb);
     if (e == cudaSuccess) e = prepare(kf_tend<Dm, VAR>, stt);
     if (e != cudaSuccess) return e;
-    ready = true;
+    gq = resident_grid(kf_qphase<Dm, VAR>, 32 * wq, sq, sms, m.ne, wq);
+    gb = resident_grid(kf_nlvol<Dm, VAR>, 32 * wb, sb, sms, m.ne, wb);
+    gt = resident_grid(kf_tend<Dm, VAR>, 32 * wt, stt, sms, m.ne, wt);
+    ne_cached = m.ne;
   }
-  auto blocks = [&](size_t smem, int w) {
-    int per_sm = (int)((227 * 1024) / (smem + 1024));
-    if (per_sm < 1) per_sm = 1;
-    const int need = (m.ne + w - 1) / w;
-    const int cap = sms * per_sm;
-    return need < cap ? need : cap;
-  };
   mark(0);
-  kf_qphase<Dm, VAR><<<blocks(sq, wq), 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
+  kf_qphase<Dm, VAR><<<gq, 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
   mark(1);
-  kf_nlvol<Dm, VAR><<<blocks(sb, wb), 32 * wb, sb, st>>>(op, m, na);
+  kf_nlvol<Dm, VAR><<<gb, 32 * wb, sb, st>>>(op, m, na);
   mark(2);
-  kf_tend<Dm, VAR><<<blocks(stt, wt), 32 * wt, stt, st>>>(op, m, ta, sa);
+  kf_tend<Dm, VAR><<<gt, 32 * wt, stt, st>>>(op, m, ta, sa);
   mark(3);
   return cudaGetLastError();
 }
@@ -1029,18 +1038,16 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
 template <class Dm>
 cudaError_t run_lin(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
                     cudaStream_t st, int sms, cudaEvent_t *ev) {
-  const int w = pick_warps(sizeof(SOps<Dm>), sizeof(LWarp<Dm>));
-  const size_t sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
-  static bool ready = false;
-  if (!ready) {
+  static int w = 0, grid = 0, ne_cached = -1;
+  static size_t sm = 0;
+  if (ne_cached != m.ne) {
+    w = pick_warps(sizeof(SOps<Dm>), sizeof(LWarp<Dm>));
+    sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
     cudaError_t e = prepare(kf_lin<Dm>, sm);
     if (e != cudaSuccess) return e;
-    ready = true;
+    grid = resident_grid(kf_lin<Dm>, 32 * w, sm, sms, m.ne, w);
+    ne_cached = m.ne;
   }
-  int per_sm = (int)((227 * 1024) / (sm + 1024));
-  if (per_sm < 1) per_sm = 1;
-  const int need = (m.ne + w - 1) / w;
-  const int grid = need < sms * per_sm ? need : sms * per_sm;
   LinArgs la{b.su, b.sv, b.sh, b.g0, b.hh0};
   if (ev) cudaEventRecord(ev[0], st);
   kf_lin<Dm><<<grid, 32 * w, sm, st>>>(op, m, la, sa);
