@@ -134,6 +134,24 @@ int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms, i
 /* Measured FP64 throughput of this GPU in TFLOP/s (2 flops per multiply-add);
  * mode 0: fused multiply-add, mode 1: separately rounded multiply and add. */
 int spoc_fp64_peak(int mode, double *tflops);
+/* Energy diagnostic that allocates nothing.  No counterpart in the reference
+ * (it computes what src/energy.f:3-96 computes, like spoc_energy).  For
+ * callers that cannot call cudaMalloc: it synchronises the device and is not
+ * allowed during stream capture, or the host program owns all device memory.
+ * Every argument is a DEVICE pointer owned by the caller: u, v, h, hb are
+ * (ld, ne) fields, vect is (5, ne), pi2 is (ng, nm), wi is [ng], ammo1 is
+ * column 1 of the mass matrix ammo [nm]; out receives (ke, pe, mass).  Work
+ * is queued on `stream` (0 = legacy default stream) and nothing is allocated:
+ * the per-element scratch is a static device array holding at most
+ * SPOC_NOALLOC_MAX_NE elements (3 MiB on every GPU that loads the library);
+ * larger ne returns SPOC_E_UNSUPPORTED.  The first call on a device looks up
+ * that array's address and should come before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race on it. */
+#define SPOC_NOALLOC_MAX_NE 131072
+int spoc_energy_noalloc(int nc, int ng, int ne, int ld, double g0, const double *u,
+                        const double *v, const double *h, const double *hb, const double *vect,
+                        const double *pi2, const double *wi, const double *ammo1, double *out,
+                        void *stream);
 /* Message for the last SPOC_E_CUDA / SPOC_E_ARG on this thread. */
 const char *spoc_last_error(void);
 

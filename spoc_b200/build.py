@@ -26,7 +26,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
     "-Xptxas", "-v",
 ]
-SOURCES = ["spoc_kernels.cu", "spoc_fast.cu", "spoc_api.cu"]
+SOURCES = ["spoc_kernels.cu", "spoc_fast.cu", "spoc_api.cu", "spoc_noalloc.cu"]
 HOST_SOURCES = ["spoc_host.cpp"]
 HEADERS = ["spoc_device.cuh", "spoc_kernels.h"]
 
