@@ -18,6 +18,15 @@
 #include <omp.h>
 #endif
 
+/* Contraction precision: 64 (default) evaluates the reference in double; 32
+ * rounds both operands of every contraction (cal_b, spectoxy, xytospec,
+ * cal_flu, tri_f) to float and accumulates in float, leaving the solves, the
+ * pointwise terms and RK4 in double.  32 models the best case of a tensor-core
+ * form that computes the contractions to FP32 accuracy (TF32 with a hi/lo
+ * split); it exists to measure how the mass solves amplify that error. */
+static int g_contract32 = 0;
+void ora_set_contraction_precision(int bits) { g_contract32 = (bits == 32); }
+
 #define NNMAX 66   /* local vector capacity: degree <= 10 */
 #define NGMAX 80   /* triangle quadrature points */
 #define NGFMAX 16  /* edge quadrature points */
@@ -531,6 +540,22 @@ void ora_cal_flu(const ora_common *c, int nf, const int *tseg, double *fbdy, int
   for (int i = 1; i <= nf; i++) {
     for (int j = 1; j <= ngf; j++) M2(fbdy, ldf, j, i) = 0.0;
     int k1 = I2(tseg, 1, i, 2), k2 = I2(tseg, 2, i, 2);
+    if (g_contract32) {
+      for (int j = 1; j <= ngf; j++) {
+        float t1 = 0.f, t2 = 0.f;
+        int s1 = k2 == 0 ? 1 : I2(ssit, 1, i, 2);
+        for (int i1 = 1; i1 <= nm; i1++) t1 = t1 + (float)M2(a0, ld, i1, k1) * (float)PICO(c, j, i1, s1);
+        if (k2 != 0) {
+          int s2 = I2(ssit, 2, i, 2);
+          for (int i1 = 1; i1 <= nm; i1++)
+            t2 = t2 + (float)M2(a0, ld, i1, k2) * (float)PICO(c, ngf - j + 1, i1, s2);
+          M2(fbdy, ldf, j, i) = 0.5f * (t1 + t2);
+        } else {
+          M2(fbdy, ldf, j, i) = t1;
+        }
+      }
+      continue;
+    }
     if (k2 == 0) {
       for (int i1 = 1; i1 <= nm; i1++)
         for (int j = 1; j <= ngf; j++)
@@ -560,6 +585,14 @@ void ora_tri_f(const ora_common *c, int tk, const int *itm, const int *its,
     double sig = (double)isg * coeff * 0.5;
     for (int i1 = 1; i1 <= nm; i1++) {
       double ans = 0.0;
+      if (g_contract32) {
+        float a = 0.f;
+        for (int j = 1; j <= ngf; j++) {
+          int j1 = isg2 + isg * j;
+          a = a + (float)(c->wif[j - 1] * PICO(c, j1, i1, k)) * (float)M2(fbdy, ldf, j, ns1);
+        }
+        ans = a;
+      } else
       for (int j = 1; j <= ngf; j++) {
         int j1 = isg2 + isg * j;
         double var = PICO(c, j1, i1, k) * M2(fbdy, ldf, j, ns1);
@@ -575,7 +608,13 @@ void ora_cal_b(const ora_common *c, double *b, const double *ak, const double *m
   const int nm = c->nm, ldm = c->ldm;
   for (int i = 1; i <= nm; i++) {
     double ans = 0.0;
-    for (int j = 1; j <= nm; j++) ans = ans + M2(mat, ldm, j, i) * ak[j - 1];
+    if (g_contract32) {
+      float a = 0.f;
+      for (int j = 1; j <= nm; j++) a = a + (float)M2(mat, ldm, j, i) * (float)ak[j - 1];
+      ans = a;
+    } else {
+      for (int j = 1; j <= nm; j++) ans = ans + M2(mat, ldm, j, i) * ak[j - 1];
+    }
     b[i - 1] = b[i - 1] + ans * coeff;
   }
 }
@@ -584,6 +623,14 @@ void ora_cal_b(const ora_common *c, double *b, const double *ak, const double *m
 void ora_spectoxy(const ora_common *c, double *mff, const double *ak) {
   const int ng = c->ng, nm = c->nm;
   for (int j = 1; j <= ng; j++) mff[j - 1] = 0.0;
+  if (g_contract32) {
+    for (int j = 1; j <= ng; j++) {
+      float a = 0.f;
+      for (int i1 = 1; i1 <= nm; i1++) a = a + (float)ak[i1 - 1] * (float)PI2(c, j, i1);
+      mff[j - 1] = a;
+    }
+    return;
+  }
   for (int i1 = 1; i1 <= nm; i1++)
     for (int j = 1; j <= ng; j++) mff[j - 1] = mff[j - 1] + ak[i1 - 1] * PI2(c, j, i1);
 }
@@ -593,7 +640,13 @@ void ora_xytospec(const ora_common *c, double *b, const double *mff) {
   const int ng = c->ng, nm = c->nm;
   for (int i1 = 1; i1 <= nm; i1++) {
     double ans = 0.0;
-    for (int i = 1; i <= ng; i++) ans = ans + c->wi[i - 1] * mff[i - 1] * PI2(c, i, i1);
+    if (g_contract32) {
+      float a = 0.f;
+      for (int i = 1; i <= ng; i++) a = a + (float)(c->wi[i - 1] * mff[i - 1]) * (float)PI2(c, i, i1);
+      ans = a;
+    } else {
+      for (int i = 1; i <= ng; i++) ans = ans + c->wi[i - 1] * mff[i - 1] * PI2(c, i, i1);
+    }
     b[i1 - 1] = ans;
   }
 }

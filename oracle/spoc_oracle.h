@@ -54,6 +54,11 @@ typedef struct {
 
 enum { ORA_LIN = 0, ORA_FS = 1, ORA_NS = 2, ORA_INV = 3 };
 
+/* Contraction precision of the study mode: 64 (default, the reference) or 32
+ * (float operands and accumulation in every contraction; solves and RK4 stay
+ * double).  See tests/test_precision_study.py. */
+void ora_set_contraction_precision(int bits);
+
 /* ---- L1: basis, quadrature tables and reference operators ---- */
 double ora_po(int n, double x);
 double ora_dpo(int n, double x);

@@ -65,11 +65,16 @@ CONFIGS = {
 
 
 def small(cfg: Config, n: int, **kw) -> Config:
-    """The same physics, discretisation and cell size on an n x n cell basin."""
+    """The same physics, discretisation and cell size on an n x n cell basin.
+
+    The initial-condition length scales (Gaussian widths, wavelengths) stay
+    those of the full basin, so the fields remain resolved on the small one.
+    """
     d = dict(cfg.__dict__)
     d.update(n=n, length=cfg.length * n / cfg.n)
     d.update(**kw)
     d["extra"] = dict(cfg.extra)
+    d["extra"].setdefault("ic_length", cfg.length)
     return Config(**d)
 
 
@@ -100,12 +105,16 @@ def square_mesh(n: int, length: float = 1.0e6, jitter: float = 0.0, seed: int = 
     return nn, inn, x, y
 
 
+def _ic_length(cfg: Config) -> float:
+    return cfg.extra.get("ic_length", cfg.length)
+
+
 def _gauss8(cfg: Config, rng):
-    L = cfg.length
+    L, Lic = cfg.length, _ic_length(cfg)
     cx = rng.uniform(-0.35 * L, 0.35 * L, 8)
     cy = rng.uniform(-0.35 * L, 0.35 * L, 8)
     amp = rng.uniform(-2.0, 2.0, 8)
-    wid = rng.uniform(0.05 * L, 0.15 * L, 8)  # 50-150 km on the 1000 km basin
+    wid = rng.uniform(0.05 * Lic, 0.15 * Lic, 8)  # 50-150 km for the 1000 km basin
     return cx, cy, amp, wid
 
 
@@ -123,8 +132,8 @@ def _kminus3(cfg: Config, rng, kmax: int = 12):
 def _fields(cfg: Config, px, py, rng_state):
     """(eta, u, v) at physical points; u, v geostrophic where the IC asks."""
     g, L = cfg.g0, cfg.length
-    if cfg.ic == "gauss":  # ftourbh-like Gaussian, 1 m, e-folding L/10 = 100 km (src/fonc.f:42-50)
-        eta = np.exp(-(px ** 2 + py ** 2) / (0.1 * L) ** 2)
+    if cfg.ic == "gauss":  # ftourbh-like Gaussian, 1 m, 100 km e-folding (src/fonc.f:42-50)
+        eta = np.exp(-(px ** 2 + py ** 2) / (0.1 * _ic_length(cfg)) ** 2)
         return eta, np.zeros_like(eta), np.zeros_like(eta)
     f = cfg.f0 + cfg.beta * py
     if cfg.ic == "gauss8":
@@ -139,7 +148,7 @@ def _fields(cfg: Config, px, py, rng_state):
             ey += gsh * (-2.0 * (py - y0) / w ** 2)
     elif cfg.ic == "kminus3":
         kx, ky, amp, phase = rng_state
-        two_pi_l = 2.0 * np.pi / L
+        two_pi_l = 2.0 * np.pi / _ic_length(cfg)
         eta = np.zeros_like(px)
         ex = np.zeros_like(px)
         ey = np.zeros_like(px)
@@ -194,6 +203,9 @@ def build_problem(cfg: Config, ld: int | None = None, tables: api.Tables | None 
 
 
 def cfl_dt(nc: int, mesh: api.Mesh, g0: float, depth: float) -> float:
+    """checkcfl (src/cfl.f:4-52).  Below 1 s the reference's last branch,
+    dfloat(int(cflmin*10)/10), is an integer division and always gives 0;
+    the bound rounded down to one decimal is used there instead."""
     x, y, inn = mesh.xgr, mesh.ygr, mesh.inn - 1
     cc0 = np.sqrt(g0 * depth)
     best = 6000.0
@@ -208,7 +220,7 @@ def cfl_dt(nc: int, mesh: api.Mesh, g0: float, depth: float) -> float:
         return float(2 * int(best / 2))
     if best >= 1:
         return float(int(best))
-    return float(int(best * 10) // 10)
+    return float(int(best * 10)) / 10.0
 
 
 def make_solver(p: Problem) -> api.Solver:

@@ -160,10 +160,10 @@ def test_state_at_rest_stays_at_rest(name):
     h[:, 0] = 0.37  # flat free surface
     c = p.cfg
     r = O.cal_var(c.variant, OT, OM, z, z, h, np.zeros_like(OM.fc), p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0)
-    # a flat surface produces no tendency: compare with the tendency of a bump
-    rb = O.cal_var(c.variant, OT, OM, z, z, p.h, np.zeros_like(OM.fc), p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0)
-    scale = max(np.abs(x).max() for x in rb)
-    assert max(np.abs(x).max() for x in r) < 1e-6 * scale
+    # a flat surface produces no tendency; the round-off left over is relative
+    # to the gravity-wave scale g * h / cell and grows with cond(amm)
+    scale = c.g0 * 0.37 / (c.length / c.n)
+    assert max(np.abs(x).max() for x in r) < 1e-5 * scale
     assert np.abs(r[2]).max() == 0.0
 
 
