@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--impl", default="spoc", choices=["spoc", "reference"])
     ap.add_argument("--config", default="c2_fs_p6")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma"],
+                    help="fp64: bit-exact reference order (headline); fp64_fma: fused multiply-adds")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -201,7 +203,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     p = W.build_problem(cfg)
     ne, nm = p.mesh.ne, p.T.nm
-    s = W.make_solver(p)
+    s = W.make_solver(p, args.precision)
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -296,6 +298,41 @@ def main():
                  "algorithmic_flops_per_launch": fl,
                  "peak_source": "measured live: spoc_fp64_peak (DFMA chains, 148 SMs)"}
 
+    # the other precision mode on the same workload, and its distance from the
+    # bit-exact result after the timed steps
+    other = "fp64_fma" if args.precision == "fp64" else "fp64"
+    s2 = W.make_solver(p, other)
+    s2.set_stream(stream.cuda_stream)
+    s2.set_state(p.u, p.v, p.h)
+    s2.rk4_steps(p.dt, args.warmup)
+    o_times = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            a.record(stream)
+        s2.rk4_steps(p.dt, 1)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        b.synchronize()
+        o_times.append(a.elapsed_time(b))
+    s.set_state(p.u, p.v, p.h)
+    s2.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, 100)
+    s2.rk4_steps(p.dt, 100)
+    sa_, sb_ = s.get_state(), s2.get_state()
+    det = p.mesh.det
+    A = p.T.ammo.T
+
+    def mnorm(x):
+        return float(np.sqrt(np.sum(det * np.einsum("ei,ij,ej->e", x, A, x))))
+
+    diff = max(mnorm(x - y) / mnorm(x) for x, y in zip(sa_, sb_))
+    s2.close()
+    other_line = {"precision": other, "value": dof * args.steps / (sum(o_times) * 1e-3),
+                  "ms_per_step": sum(o_times) / args.steps,
+                  "rel_l2_diff_vs_other_after_100_steps": diff}
+
     line = None
     if rank == 0:
         line = {
@@ -303,7 +340,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_desc(cfg, ne, nm), "ne": ne, "nm": nm, "dt": p.dt,
-                       "precision": "fp64, reference operation order (bit-exact to the CPU oracle)",
+                       "precision": ("fp64, reference operation order (bit-exact to the CPU oracle)"
+                                     if args.precision == "fp64" else
+                                     "fp64 with fused multiply-adds (not bit-exact)"),
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "e2e": e2e,
@@ -311,6 +350,7 @@ def main():
             "kernel_ms_per_launch": per_launch_ms,
             "roofline": roof,
             "roofline_fp64": roof_fp64,
+            "other_precision": other_line,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -46,7 +46,10 @@ extern "C" {
 #define SPOC_INV 3 /* src/calvarnl_inv.f */
 
 /* precision modes */
-#define SPOC_FP64 0 /* reference operation order, no contraction: bit-exact to the CPU restatement */
+#define SPOC_FP64 0     /* reference operation order, no contraction: bit-exact to the CPU restatement */
+#define SPOC_FP64_FMA 1 /* reference order with fused multiply-adds in the contractions and
+                           solves: FP64 accuracy, not bit-exact; untabulated (nc, ng, ngf)
+                           run the SPOC_FP64 kernels */
 
 /* COMMON-block content, as the Fortran driver holds it (src/shwwnl.f:60-71).
  * amm and amml hold the upper Cholesky factors (src/shwwnl.f:153-156). */

@@ -27,6 +27,8 @@ LIB_PATH = HERE / "libspoc_gpu.so"
 LIN, FS, NS, INV = 0, 1, 2, 3
 VARIANTS = {"lin": LIN, "fs": FS, "ns": NS, "inv": INV}
 FP64 = 0
+FP64_FMA = 1
+PRECISIONS = {"fp64": FP64, "fp64_fma": FP64_FMA}
 
 _STATUS = {
     0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-finite tendency",
@@ -316,7 +318,9 @@ def project(T: Tables, vals: np.ndarray, ld: int | None = None) -> np.ndarray:
 class Solver:
     """One device handle: tables and mesh resident, one CUDA stream."""
 
-    def __init__(self, T: Tables, mesh: Mesh, variant: int | str, precision: int = FP64):
+    def __init__(self, T: Tables, mesh: Mesh, variant: int | str, precision: int | str = FP64):
+        if isinstance(precision, str):
+            precision = PRECISIONS[precision]
         self.lib = load_library()
         self.T, self.mesh = T, mesh
         self.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)

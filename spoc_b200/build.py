@@ -27,6 +27,8 @@ NVCC_FLAGS = [
     "-Xptxas", "-v",
 ]
 SOURCES = ["spoc_kernels.cu", "spoc_fast.cu", "spoc_api.cu", "spoc_noalloc.cu"]
+# spoc_fast.cu is compiled a second time with fused multiply-adds
+VARIANT_SOURCES = [("spoc_fast.cu", "spoc_fast_fma", ["-DSPOC_FMA=1"])]
 HOST_SOURCES = ["spoc_host.cpp"]
 HEADERS = ["spoc_device.cuh", "spoc_kernels.h"]
 
@@ -53,25 +55,27 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     nvcc = _nvcc()
     bdir = HERE / "_build"
     bdir.mkdir(exist_ok=True)
-    objs = []
-    log = []
+    jobs = []
     for src in SOURCES:
-        obj = bdir / (src + ".o")
-        cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        log.append(r.stdout + r.stderr)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
-        objs.append(obj)
+        jobs.append((src, bdir / (src + ".o"),
+                     [nvcc, *ARCH, *NVCC_FLAGS, "-c", str(CSRC / src), "-o", str(bdir / (src + ".o"))]))
+    for src, stem, defs in VARIANT_SOURCES:
+        jobs.append((src, bdir / (stem + ".o"),
+                     [nvcc, *ARCH, *NVCC_FLAGS, *defs, "-c", str(CSRC / src), "-o", str(bdir / (stem + ".o"))]))
     for src in HOST_SOURCES:
-        obj = bdir / (src + ".o")
-        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
-               "-Wall", "-c", str(CSRC / src), "-o", str(obj)]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        jobs.append((src, bdir / (src + ".o"),
+                     ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+                      "-Wall", "-c", str(CSRC / src), "-o", str(bdir / (src + ".o"))]))
+    # the translation units are independent: compile them concurrently
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: subprocess.run(j[2], capture_output=True, text=True), jobs))
+    log = []
+    for (src, _, cmd), r in zip(jobs, results):
         log.append(r.stdout + r.stderr)
         if r.returncode != 0:
-            raise RuntimeError(f"g++ failed on {src}:\n{r.stderr}")
-        objs.append(obj)
+            raise RuntimeError(f"compile failed on {src} ({' '.join(cmd[-6:])}):\n{r.stderr}")
+    objs = [j[1] for j in jobs]
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -258,6 +258,9 @@ RhsBuffers rhs_buffers(spoc_handle *h, double *const s[3]) {
 
 cudaError_t launch(spoc_handle *h, double *const s[3], const StageArgs &sa, cudaEvent_t *ev) {
   const bool fast = h->path != SPOC_PATH_GENERIC && fast_available(h->nc, h->ng, h->ngf);
+  if (fast && h->precision == SPOC_FP64_FMA)
+    return launch_rhs_fast_fma(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms,
+                               &h->launches, ev);
   if (fast)
     return launch_rhs_fast(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms,
                            &h->launches, ev);
@@ -295,7 +298,8 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
   *out = nullptr;
   if (!t || !m) return fail(SPOC_E_ARG, "tables or mesh is null");
   if (variant < SPOC_LIN || variant > SPOC_INV) return fail(SPOC_E_ARG, "unknown variant");
-  if (precision != SPOC_FP64) return fail(SPOC_E_UNSUPPORTED, "precision mode not built");
+  if (precision != SPOC_FP64 && precision != SPOC_FP64_FMA)
+    return fail(SPOC_E_UNSUPPORTED, "precision mode not built");
   const int nc = t->nc, nm = (nc + 1) * (nc + 2) / 2;
   if (nc < 1 || t->nm != nm) return fail(SPOC_E_ARG, "nm != (nc+1)(nc+2)/2");
   if (nm > kMaxModes || t->ng < 1 || t->ng > kMaxQuad || t->ngf < 1 || t->ngf > kMaxEdge)

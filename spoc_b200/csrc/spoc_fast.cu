@@ -20,8 +20,25 @@
 #include "spoc_device.cuh"
 #include "spoc_kernels.h"
 
+// SPOC_FMA selects the arithmetic of the multiply-add chains: 0 (default)
+// rounds every product separately, as the reference; 1 fuses each
+// multiply-add (one rounding), which halves the FP64 instructions of the
+// contractions and solves but no longer reproduces the reference bit for bit.
+// This file is compiled once per setting.
+#ifndef SPOC_FMA
+#define SPOC_FMA 0
+#endif
+
 namespace spoc {
 namespace {
+
+#if SPOC_FMA
+__device__ __forceinline__ double macc(double acc, double a, double b) { return __fma_rn(a, b, acc); }
+__device__ __forceinline__ double msub(double acc, double a, double b) { return __fma_rn(-a, b, acc); }
+#else
+__device__ __forceinline__ double macc(double acc, double a, double b) { return add(acc, mul(a, b)); }
+__device__ __forceinline__ double msub(double acc, double a, double b) { return sub(acc, mul(a, b)); }
+#endif
 
 template <int NC_, int Q_, int G_>
 struct Dims {
@@ -237,7 +254,7 @@ __device__ __forceinline__ void face_values(const double *pf, const DevMesh &m, 
       for (int n = 0; n < N; ++n) {
         const double pv = p[n * G];
 #pragma unroll
-        for (int q = 0; q < NF; ++q) acc[q] = add(acc[q], mul(own[q * N + n], pv));
+        for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], own[q * N + n], pv);
       }
     } else {
       const double *nbk = nb + k * NF * N;
@@ -250,13 +267,13 @@ __device__ __forceinline__ void face_values(const double *pf, const DevMesh &m, 
       for (int n = 0; n < N; ++n) {
         const double pv = p1[n * G];
 #pragma unroll
-        for (int q = 0; q < NF; ++q) acc[q] = add(acc[q], mul(a1[q * N + n], pv));
+        for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], a1[q * N + n], pv);
       }
 #pragma unroll
       for (int n = 0; n < N; ++n) {
         const double pv = p2[n * G];
 #pragma unroll
-        for (int q = 0; q < NF; ++q) acc[q] = add(acc[q], mul(a2[q * N + n], pv));
+        for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], a2[q * N + n], pv);
       }
 #pragma unroll
       for (int q = 0; q < NF; ++q) acc[q] = mul(0.5, acc[q]);
@@ -290,8 +307,8 @@ __device__ __forceinline__ void matvec2(const double *A, const double *B, const 
       const double x = X[f * XS + j];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        ax[f][r] = add(ax[f][r], mul(a[r], x));
-        bx[f][r] = add(bx[f][r], mul(b[r], x));
+        ax[f][r] = macc(ax[f][r], a[r], x);
+        bx[f][r] = macc(bx[f][r], b[r], x);
       }
     }
   }
@@ -301,7 +318,7 @@ __device__ __forceinline__ void matvec2(const double *A, const double *B, const 
 template <int R>
 __device__ __forceinline__ void axpy(double (&b)[R], const double (&ans)[R], double c) {
 #pragma unroll
-  for (int r = 0; r < R; ++r) b[r] = add(b[r], mul(ans[r], c));
+  for (int r = 0; r < R; ++r) b[r] = macc(b[r], ans[r], c);
 }
 
 // Lift sums of tri_f (src/mat1.f:189-206) for NF face-value sets:
@@ -333,7 +350,7 @@ __device__ __forceinline__ void lift_sums(const SOps<Dm> &s, const int (&isg)[3]
       for (int f = 0; f < NF; ++f) {
         const double fv = fb[f * 32 + k * G + jj - 1];
 #pragma unroll
-        for (int r = 0; r < R; ++r) t[f][k][r] = add(t[f][k][r], mul(w, mul(p[r], fv)));
+        for (int r = 0; r < R; ++r) t[f][k][r] = macc(t[f][k][r], w, mul(p[r], fv));
       }
     }
   }
@@ -347,7 +364,7 @@ __device__ __forceinline__ void apply_lift(double (&b)[R], const double (&t)[3][
   for (int k = 0; k < 3; ++k) {
     const double sig = mul(mul((double)isg[k], coeff), 0.5);
 #pragma unroll
-    for (int r = 0; r < R; ++r) b[r] = add(b[r], mul(t[k][r], sig));
+    for (int r = 0; r < R; ++r) b[r] = macc(b[r], t[k][r], sig);
   }
 }
 
@@ -374,7 +391,7 @@ __device__ __forceinline__ void solve_batch(double (&t)[S][R], const double *row
       if (i > k && i < M) {
         const double uk = u[i];
 #pragma unroll
-        for (int s = 0; s < S; ++s) t[s][r] = sub(t[s][r], mul(uk, xk[s]));
+        for (int s = 0; s < S; ++s) t[s][r] = msub(t[s][r], uk, xk[s]);
       }
     }
   }
@@ -395,7 +412,7 @@ __device__ __forceinline__ void solve_batch(double (&t)[S][R], const double *row
       if (i < k) {
         const double uk = u[i];
 #pragma unroll
-        for (int s = 0; s < S; ++s) t[s][r] = sub(t[s][r], mul(bk[s], uk));
+        for (int s = 0; s < S; ++s) t[s][r] = msub(t[s][r], bk[s], uk);
       }
     }
   }
@@ -675,7 +692,7 @@ __global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) 
         for (int n = 0; n < N; ++n) {
           const double p = S.p2[n * Q + qp];
 #pragma unroll
-          for (int f = 0; f < 9; ++f) mv[f] = add(mv[f], mul(W.vin[f * N + n], p));
+          for (int f = 0; f < 9; ++f) mv[f] = macc(mv[f], W.vin[f * N + n], p);
         }
         const double w = S.wi[qp];
         W.wp[0 * Q + qp] = mul(w, mul(mv[0], mv[2]));
@@ -707,7 +724,7 @@ __global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) 
       for (int f = 0; f < 8; ++f) {
         const double wv = W.wp[f * Q + qp];
 #pragma unroll
-        for (int r = 0; r < R; ++r) X[f][r] = add(X[f][r], mul(wv, p[r]));
+        for (int r = 0; r < R; ++r) X[f][r] = macc(X[f][r], wv, p[r]);
       }
     }
     double uv[2][R];
@@ -1068,15 +1085,23 @@ cudaError_t run_any(int variant, const DevOps &op, const DevMesh &m, const RhsBu
 
 }  // namespace
 
-bool fast_available(int nc, int ng, int ngf) {
+#if SPOC_FMA
+#define FAST_AVAILABLE fast_available_fma
+#define LAUNCH_FAST launch_rhs_fast_fma
+#else
+#define FAST_AVAILABLE fast_available
+#define LAUNCH_FAST launch_rhs_fast
+#endif
+
+bool FAST_AVAILABLE(int nc, int ng, int ngf) {
   return (nc == 3 && ng == 12 && ngf == 4) || (nc == 4 && ng == 25 && ngf == 5) ||
          (nc == 5 && ng == 27 && ngf == 6) || (nc == 6 && ng == 33 && ngf == 7) ||
          (nc == 7 && ng == 42 && ngf == 9);
 }
 
-cudaError_t launch_rhs_fast(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
-                            const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
-                            cudaEvent_t *ev) {
+cudaError_t LAUNCH_FAST(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
+                        const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
+                        cudaEvent_t *ev) {
   cudaError_t e = cudaErrorNotSupported;
   const int nc = op.nc, ng = op.ng, ngf = op.ngf;
   if (nc == 3 && ng == 12 && ngf == 4) e = run_any<Dims<3, 12, 4>>(variant, op, m, b, sa, st, sms, ev);

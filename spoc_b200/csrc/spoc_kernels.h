@@ -59,6 +59,12 @@ cudaError_t launch_rhs_fast(int variant, const DevOps &op, const DevMesh &m, con
                             const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
                             cudaEvent_t *ev = nullptr);
 
+// The same kernels with fused multiply-adds (spoc_fast.cu built with SPOC_FMA=1).
+bool fast_available_fma(int nc, int ng, int ngf);
+cudaError_t launch_rhs_fast_fma(int variant, const DevOps &op, const DevMesh &m,
+                                const RhsBuffers &b, const StageArgs &sa, cudaStream_t st, int sms,
+                                long long *launches, cudaEvent_t *ev = nullptr);
+
 // 8 independent chains of `iters` FP64 operations per thread, sms*8 blocks of 256
 cudaError_t launch_fp64_peak(int mode, int sms, int iters, double *out, cudaStream_t st);
 

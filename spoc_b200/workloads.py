@@ -223,7 +223,7 @@ def cfl_dt(nc: int, mesh: api.Mesh, g0: float, depth: float) -> float:
     return float(int(best * 10)) / 10.0
 
 
-def make_solver(p: Problem) -> api.Solver:
-    s = api.Solver(p.T, p.mesh, p.cfg.variant)
+def make_solver(p: Problem, precision: str = "fp64") -> api.Solver:
+    s = api.Solver(p.T, p.mesh, p.cfg.variant, precision)
     s.set_params(p.cfg.mu0, p.cfg.mb0, p.cfg.g0, p.hb, p.fc, p.w0, p.z0)
     return s
