@@ -168,6 +168,51 @@ def cpu_baseline(cfg, p):
             "kind": "port", "sample": f"{k} full RK4 steps of the workload, OpenMP over elements"}
 
 
+def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
+    """Configuration C4: gradient of the observation cost over a 200-step
+    window of calvarnl_ns (p4, 32768 triangles) with 20 binomial snapshots;
+    500 seeded points observed at steps 50/100/150/200 against a truth run."""
+    from spoc_b200 import workloads as W
+    cfg = W.CONFIGS["c4_ns_p4"]
+    p = W.build_problem(cfg)
+    s = W.make_solver(p)
+    s.set_stream(stream.cuda_stream)
+    elem, basis, _, _ = W.random_observations(p, nobs, seed=cfg.seed)
+    steps = np.array([50, 100, 150, 200], dtype=np.int32)
+    rng = np.random.Generator(np.random.PCG64(7))
+    truth = (p.u, p.v, p.h + 0.05 * rng.normal(size=p.h.shape) * (np.arange(p.h.shape[1]) < 1))
+    s.set_state(*truth)
+    vals, t_prev = [], 0
+    for st in steps:
+        s.rk4_steps(p.dt, int(st - t_prev))
+        t_prev = st
+        vals.append(np.sum(s.get_state()[2][elem - 1] * basis, axis=1))
+    s.set_observations(elem, basis, steps, np.array(vals))
+    x0 = (p.u, p.v, p.h)
+    s.fwd_window(x0, p.dt, nsteps)  # warm-up
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        b.synchronize()
+        return out, a.elapsed_time(b)
+
+    J, t_fwd = timed(lambda: s.fwd_window(x0, p.dt, nsteps))
+    s.adjoint_counters()
+    (J2, g), t_bwd = timed(lambda: s.bwd_window(x0, p.dt, nsteps, snaps))
+    nf, na = s.adjoint_counters()
+    s.close()
+    return {"config": f"c4_ns_p4: {p.mesh.ne} triangles, nm={p.T.nm}, window {nsteps} steps, "
+                      f"{snaps} binomial snapshots, {nobs} observation points at steps 50/100/150/200",
+            "cost": J, "forward_window_ms": t_fwd, "gradient_ms": t_bwd,
+            "gradient_over_forward": t_bwd / t_fwd,
+            "forward_steps_run_by_gradient": nf, "adjoint_steps": na,
+            "checks": "dot-product, central differences (20 directions) and checkpointing invariance in tests/test_gpu_adjoint.py"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -176,6 +221,7 @@ def main():
     ap.add_argument("--impl", default="spoc", choices=["spoc", "reference"])
     ap.add_argument("--config", default="c2_fs_p6")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma"],
                     help="fp64: bit-exact reference order (headline); fp64_fma: fused multiply-adds")
     args = ap.parse_args()
@@ -333,6 +379,10 @@ def main():
                   "ms_per_step": sum(o_times) / args.steps,
                   "rel_l2_diff_vs_other_after_100_steps": diff}
 
+    adjoint = None
+    if world == 1 and not args.no_adjoint:
+        adjoint = adjoint_measure(torch, stream)
+
     line = None
     if rank == 0:
         line = {
@@ -351,6 +401,7 @@ def main():
             "roofline": roof,
             "roofline_fp64": roof_fp64,
             "other_precision": other_line,
+            "adjoint": adjoint,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -158,6 +158,44 @@ int spoc_energy_noalloc(int nc, int ng, int ne, int ld, double g0, const double 
 /* Message for the last SPOC_E_CUDA / SPOC_E_ARG on this thread. */
 const char *spoc_last_error(void);
 
+/* ---- tangent-linear model, adjoint, gradient (no reference counterpart) ----
+ * All arrays are HOST arrays (ld, ne).  These calls use the handle's resident
+ * state buffers as work space (call spoc_set_state again afterwards).
+ * spoc_tlm_rhs: (ou,ov,oh) = J(u,v,hh) (du,dv,dh), J the Jacobian of cal_var.
+ * spoc_adj_rhs: (ou,ov,oh) = J(u,v,hh)^T (bu,bv,bh).
+ * spoc_tlm_steps: (du,dv,dh) <- the perturbation after nsteps RK4 steps from
+ *   the base state (u0,v0,h0).
+ * spoc_adj_steps: (bu,bv,bh) <- the adjoint at step 0 of the adjoint given at
+ *   step nsteps (recomputing the trajectory from (u0,v0,h0)).
+ * spoc_set_observations: nobs points, point o in element elem[o] (1-based)
+ *   with basis values basis[o*nm + n] = phi_n(xi_o, eta_o); observed eta
+ *   values[t*nobs + o] at RK4 step steps[t].
+ * spoc_fwd_window / spoc_bwd_window: the forward / backward pair of the cost
+ *   J = 1/2 sum_t sum_o (eta(x_o, step_t) - values[t*nobs+o])^2 over nsteps
+ *   RK4 steps from (u0,v0,h0): fwd returns J; bwd returns J and its gradient
+ *   with respect to the initial modal coefficients (gu,gv,gh), reversing the
+ *   window with binomial checkpointing in `snaps` device snapshots.
+ * spoc_adjoint_counters: forward and adjoint RK4 steps run since the last
+ *   call (recomputation included). */
+int spoc_tlm_rhs(spoc_handle *h, int ld, const double *u, const double *v, const double *hh,
+                 const double *du, const double *dv, const double *dh, double *ou, double *ov,
+                 double *oh);
+int spoc_adj_rhs(spoc_handle *h, int ld, const double *u, const double *v, const double *hh,
+                 const double *bu, const double *bv, const double *bh, double *ou, double *ov,
+                 double *oh);
+int spoc_tlm_steps(spoc_handle *h, int ld, const double *u0, const double *v0, const double *h0,
+                   double *du, double *dv, double *dh, double dt, int nsteps);
+int spoc_adj_steps(spoc_handle *h, int ld, const double *u0, const double *v0, const double *h0,
+                   double *bu, double *bv, double *bh, double dt, int nsteps);
+int spoc_set_observations(spoc_handle *h, int nobs, const int *elem, const double *basis,
+                          int ntimes, const int *steps, const double *values);
+int spoc_fwd_window(spoc_handle *h, int ld, const double *u0, const double *v0, const double *h0,
+                    double dt, int nsteps, double *cost);
+int spoc_bwd_window(spoc_handle *h, int ld, const double *u0, const double *v0, const double *h0,
+                    double dt, int nsteps, int snaps, double *cost, double *gu, double *gv,
+                    double *gh);
+int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long long *adj_steps);
+
 /* ---- Fortran drop-in ----
  * Register the COMMON contents once (after dpotrf), then link this library
  * instead of calvar*.o: cal_var_ has the reference argument list

@@ -103,6 +103,15 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "spoc_kernel_launches": (C.c_longlong, [vp]),
         "spoc_profile_rk4": (C.c_int, [vp, C.c_double, C.c_int, _DP, _IP]),
         "spoc_fp64_peak": (C.c_int, [C.c_int, _DP]),
+        "spoc_tlm_rhs": (C.c_int, [vp, C.c_int] + [_DP] * 9),
+        "spoc_adj_rhs": (C.c_int, [vp, C.c_int] + [_DP] * 9),
+        "spoc_tlm_steps": (C.c_int, [vp, C.c_int] + [_DP] * 6 + [C.c_double, C.c_int]),
+        "spoc_adj_steps": (C.c_int, [vp, C.c_int] + [_DP] * 6 + [C.c_double, C.c_int]),
+        "spoc_set_observations": (C.c_int, [vp, C.c_int, _IP, _DP, C.c_int, _IP, _DP]),
+        "spoc_fwd_window": (C.c_int, [vp, C.c_int, _DP, _DP, _DP, C.c_double, C.c_int, _DP]),
+        "spoc_bwd_window": (C.c_int, [vp, C.c_int, _DP, _DP, _DP, C.c_double, C.c_int, C.c_int,
+                                      _DP, _DP, _DP, _DP]),
+        "spoc_adjoint_counters": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "spoc_last_error": (C.c_char_p, []),
         "spoc_register_commons": (C.c_int, [C.POINTER(_Tables), C.c_int, C.c_int]),
         "spoc_cal_var_status": (_IP, []),
@@ -404,6 +413,67 @@ class Solver:
         nk = C.c_int()
         _check(self.lib.spoc_profile_rk4(self._h, dt, nsteps, _d(ms), C.byref(nk)), "profile_rk4")
         return ms[: nk.value]
+
+    # ---- tangent-linear model, adjoint, observation cost ----
+    def _c(self, a):
+        return np.ascontiguousarray(a, dtype=np.float64)
+
+    def tlm_rhs(self, x, d):
+        """J(x) d for x = (u, v, h), d = (du, dv, dh), arrays (ne, ld)."""
+        x, d = [self._c(a) for a in x], [self._c(a) for a in d]
+        out = [np.zeros_like(x[0]) for _ in range(3)]
+        _check(self.lib.spoc_tlm_rhs(self._h, x[0].shape[1], *map(_d, x), *map(_d, d),
+                                     *map(_d, out)), "tlm_rhs")
+        return tuple(out)
+
+    def adj_rhs(self, x, b):
+        """J(x)^T b."""
+        x, b = [self._c(a) for a in x], [self._c(a) for a in b]
+        out = [np.zeros_like(x[0]) for _ in range(3)]
+        _check(self.lib.spoc_adj_rhs(self._h, x[0].shape[1], *map(_d, x), *map(_d, b),
+                                     *map(_d, out)), "adj_rhs")
+        return tuple(out)
+
+    def tlm_steps(self, x0, d, dt: float, nsteps: int):
+        x0, d = [self._c(a) for a in x0], [self._c(a).copy() for a in d]
+        _check(self.lib.spoc_tlm_steps(self._h, x0[0].shape[1], *map(_d, x0), *map(_d, d), dt,
+                                       nsteps), "tlm_steps")
+        return tuple(d)
+
+    def adj_steps(self, x0, b, dt: float, nsteps: int):
+        x0, b = [self._c(a) for a in x0], [self._c(a).copy() for a in b]
+        _check(self.lib.spoc_adj_steps(self._h, x0[0].shape[1], *map(_d, x0), *map(_d, b), dt,
+                                       nsteps), "adj_steps")
+        return tuple(b)
+
+    def set_observations(self, elem, basis, steps, values):
+        elem = np.ascontiguousarray(elem, dtype=np.int32)
+        basis = self._c(basis)
+        steps = np.ascontiguousarray(steps, dtype=np.int32)
+        values = self._c(values)
+        self._obs = (elem, basis, steps, values)
+        _check(self.lib.spoc_set_observations(self._h, elem.size, _i(elem), _d(basis), steps.size,
+                                              _i(steps), _d(values)), "set_observations")
+
+    def fwd_window(self, x0, dt: float, nsteps: int) -> float:
+        x0 = [self._c(a) for a in x0]
+        J = C.c_double()
+        _check(self.lib.spoc_fwd_window(self._h, x0[0].shape[1], *map(_d, x0), dt, nsteps,
+                                        C.byref(J)), "fwd_window")
+        return J.value
+
+    def bwd_window(self, x0, dt: float, nsteps: int, snaps: int):
+        x0 = [self._c(a) for a in x0]
+        g = [np.zeros_like(x0[0]) for _ in range(3)]
+        J = C.c_double()
+        _check(self.lib.spoc_bwd_window(self._h, x0[0].shape[1], *map(_d, x0), dt, nsteps, snaps,
+                                        C.byref(J), *map(_d, g)), "bwd_window")
+        return J.value, tuple(g)
+
+    def adjoint_counters(self):
+        f, a = C.c_longlong(), C.c_longlong()
+        _check(self.lib.spoc_adjoint_counters(self._h, C.byref(f), C.byref(a)), "adjoint_counters")
+        return f.value, a.value
 
     @property
     def launches(self) -> int:

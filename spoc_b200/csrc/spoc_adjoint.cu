@@ -1,0 +1,688 @@
+// Tangent-linear and adjoint kernels of the SPOC right-hand side (FP64).
+//
+// The right-hand side (calvarnl_*.f, calvar_lin.f) is linear in the state
+// except for the pointwise products and divisions at quadrature points
+// (calvarnl_fs.f:263-296).  Hence
+//   * tangent-linear model: the forward q-phase, tendency and linear kernels
+//     applied to the perturbation (they are linear in their inputs) plus one
+//     linearised quadrature-point kernel (k_nlvol_tlm);
+//   * adjoint: the transpose of every stage, in reverse order.  The mass
+//     solves and every wall projection are self-adjoint (the rotations are
+//     symmetric reflections and reduc_inv_gn is the transpose of reduc_gn), so
+//     the adjoint reuses the forward solve code.  Face-flux transposes are
+//     done in two kernels without atomics: each element writes the adjoint of
+//     its three side lifts (in face-point order), then each element gathers
+//     both sides of its faces and applies the transposed trace.
+// One warp per element, lanes over modes / points, as the generic forward
+// kernels.  Fused multiply-adds are used freely: these kernels are checked
+// by dot-product and finite-difference tests, not bit for bit.
+#include <cuda_runtime.h>
+
+#include "spoc_device.cuh"
+#include "spoc_kernels.h"
+
+namespace spoc {
+namespace {
+
+constexpr int kT = 256;
+constexpr int kWB = kT / kWarp;
+
+__device__ __forceinline__ int wg() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ int wc() { return (gridDim.x * blockDim.x) >> 5; }
+__device__ __forceinline__ double fmac(double acc, double a, double b) { return __fma_rn(a, b, acc); }
+
+__device__ __forceinline__ V2 vadd(V2 a, V2 b) { return V2{a.a + b.a, a.b + b.b}; }
+__device__ __forceinline__ V2 vscale(V2 a, double c) { return V2{a.a * c, a.b * c}; }
+// c1*a + c2*b
+__device__ __forceinline__ V2 vlin(double c1, V2 a, double c2, V2 b) {
+  return V2{fmac(c1 * a.a, c2, b.a), fmac(c1 * a.b, c2, b.b)};
+}
+
+struct Geo {
+  double ax, bx, ay, by, detai;
+};
+__device__ __forceinline__ Geo geo(const DevMesh &m, int e) {
+  const double *v = m.vect + 5 * (size_t)e;
+  return Geo{__ldg(v), __ldg(v + 1), __ldg(v + 2), __ldg(v + 3), __ldg(v + 4)};
+}
+
+// Adjoint of the three side lifts of tri_f (src/mat1.f:189-206) for one
+// load vector g (smem, nm): L[(e*3+k)*G + j] = sig_k * wif(j) * sum_n
+// pico(j1(j), n, k) g(n), j in face-point order, sig_k = its_k * coeff / 2.
+__device__ __forceinline__ void side_lift_adj(const DevOps &op, const DevMesh &m, int e,
+                                              const double *g, double coeff, double *L) {
+  const int l = lane_id(), G = op.ngf, nm = op.nm;
+  if (l < 3 * G) {
+    const int k = l / G, j = l - k * G;  // j 0-based face point
+    const int isg = __ldg(m.its + 3 * e + k);
+    const int j1 = isg > 0 ? j : G - 1 - j;  // element-local point
+    const double sig = isg * coeff * 0.5;
+    const double *p = op.picoF + (size_t)k * nm * G + j1;
+    double s = 0.0;
+    for (int n = 0; n < nm; ++n) s = fmac(s, __ldg(p + n * G), g[n]);
+    L[(3 * (size_t)e + k) * G + j] = sig * __ldg(op.wif + j) * s;
+  }
+}
+
+// Sum over the (one or two) elements of each face of element e of their side
+// lift adjoints, in face-point order: S[k*G + j].  Also returns the trace
+// weight (0.5 interior, 1 wall) per side through wt[k].
+__device__ __forceinline__ void face_sums(const DevOps &op, const DevMesh &m, int e,
+                                          const double *L, double *S) {
+  const int l = lane_id(), G = op.ngf;
+  if (l < 3 * G) {
+    const int k = l / G, j = l - k * G;
+    const int f = __ldg(m.itm + 3 * e + k);
+    const int t1 = __ldg(m.tseg + 2 * f), t2 = __ldg(m.tseg + 2 * f + 1);
+    double s = L[(3 * (size_t)e + k) * G + j];
+    if (t2 >= 0) {
+      const int nb = (t1 == e) ? t2 : t1;
+      const int kn = (t1 == e) ? __ldg(m.ssit + 2 * f + 1) : __ldg(m.ssit + 2 * f);
+      s += L[(3 * (size_t)nb + kn) * G + j];
+    }
+    S[l] = s;
+  }
+}
+
+// Transposed cal_flu (src/calflu.f:31-62) for element e: a(n) = sum_k w_k
+// sum_j pico(j_e(j), n, k) * c_k(j) * S[k*G + j], with c_k(j) = norm(comp,
+// face_k) * scale and w_k = 0.5 (interior) or 1 (wall, traced on side 1).
+__device__ __forceinline__ V2 trace_adj(const DevOps &op, const DevMesh &m, int e, const double *S,
+                                        int comp, double scale) {
+  const int l = lane_id(), G = op.ngf, nm = op.nm;
+  V2 a = vzero();
+  for (int k = 0; k < 3; ++k) {
+    const int f = __ldg(m.itm + 3 * e + k);
+    const int t1 = __ldg(m.tseg + 2 * f), t2 = __ldg(m.tseg + 2 * f + 1);
+    const double w = (t2 < 0 ? 1.0 : 0.5) * __ldg(m.norm + 2 * f + comp) * scale;
+    const bool first = (t1 == e);
+    const double *pk = op.picoT + (size_t)k * G * nm;
+    for (int j = 0; j < G; ++j) {
+      const int je = first ? j : G - 1 - j;
+      const double c = w * S[k * G + j];
+      const double *pr = pk + (size_t)je * nm;
+      if (l < nm) a.a = fmac(a.a, __ldg(pr + l), c);
+      if (l + kWarp < nm) a.b = fmac(a.b, __ldg(pr + l + kWarp), c);
+    }
+  }
+  return a;
+}
+
+// ans_i = sum_j A(i,j) x_j through the non-transposed copy (AN[j*nm + i] = A(i,j))
+__device__ __forceinline__ V2 matvecN(const double *AN, const double *x, int nm) {
+  const int l = lane_id();
+  double s0 = 0.0, s1 = 0.0;
+  for (int j = 0; j < nm; ++j) {
+    const double xj = x[j];
+    if (l < nm) s0 = fmac(s0, __ldg(AN + j * nm + l), xj);
+    if (l + kWarp < nm) s1 = fmac(s1, __ldg(AN + j * nm + l + kWarp), xj);
+  }
+  return V2{s0, s1};
+}
+
+// FS q-phase wall transform (calvarnl_fs.f:171-204): symmetric, used both ways.
+__device__ __forceinline__ void qwall_fs(const DevOps &op, V2 &gxx, V2 &gxy, V2 &gyx, V2 &gyy,
+                                         double dnx, double dny, double *sm) {
+  V2 gnx, gtx, gny, gty, gnn, gnt, gtn, gtt;
+  rot_vec(gnx, gtx, gxx, gyx, dnx, dny);
+  rot_vec(gny, gty, gxy, gyy, dnx, dny);
+  rot_vec(gnn, gnt, gnx, gny, dnx, dny);
+  rot_vec(gtn, gtt, gtx, gty, dnx, dny);
+  V2 bu = reduc_gn(op, gtn, sm);
+  gnn = solve_full(op, gnn);
+  gnt = solve_full(op, gnt);
+  bu = solve_red(op, bu);
+  gtt = solve_full(op, gtt);
+  gtn = reduc_inv_gn(op, bu, sm);
+  rot_vec(gnx, gny, gnn, gnt, dnx, dny);
+  rot_vec(gtx, gty, gtn, gtt, dnx, dny);
+  rot_vec(gxx, gyx, gnx, gtx, dnx, dny);
+  rot_vec(gxy, gyy, gny, gty, dnx, dny);
+}
+
+// Mass solve of a vector pair with the variant's wall projection (symmetric).
+template <int VAR>
+__device__ __forceinline__ void pair_solve(const DevOps &op, const DevMesh &m, int e, V2 &gx,
+                                           V2 &gy, double *sm) {
+  if (__ldg(m.bdl + e)) {
+    if (VAR == kNS)
+      wall_solve_zero(op, gx, gy, sm);
+    else
+      wall_solve_rot(op, gx, gy, __ldg(m.normt + 2 * e), __ldg(m.normt + 2 * e + 1), sm);
+  } else {
+    gx = solve_full(op, gx);
+    gy = solve_full(op, gy);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tangent-linear quadrature-point kernel (linearisation of k_nlvol)
+// ---------------------------------------------------------------------------
+struct TlmSmem {
+  double vin[18][kMaxModes];  // 9 base + 9 perturbation modal inputs
+  double wp[8][kMaxQuad];
+  double sm[kMaxModes];
+};
+
+template <int VAR>
+__global__ void __launch_bounds__(64) k_nlvol_tlm(DevOps op, DevMesh m, TlmArgs a) {
+  __shared__ TlmSmem sall[2];
+  TlmSmem &S = sall[threadIdx.x >> 5];
+  const int nm = op.nm, ng = op.ng, ne = m.ne, l = lane_id();
+  const size_t fs = (size_t)ne * nm;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    const V2 uk = vload(a.su + o, nm), vk = vload(a.sv + o, nm), hh = vload(a.sh + o, nm);
+    const V2 hb = vload(a.hb + o, nm), w0 = vload(a.w0 + o, nm), z0 = vload(a.z0 + o, nm);
+    const V2 fc = vload(a.fc + o, nm);
+    const V2 q0 = vload(a.q + o, nm), q1 = vload(a.q + fs + o, nm);
+    const V2 q2 = vload(a.q + 2 * fs + o, nm), q3 = vload(a.q + 3 * fs + o, nm);
+    const V2 du = vload(a.du + o, nm), dv = vload(a.dv + o, nm), dh = vload(a.dh + o, nm);
+    const V2 d0 = vload(a.dq + o, nm), d1 = vload(a.dq + fs + o, nm);
+    const V2 d2 = vload(a.dq + 2 * fs + o, nm), d3 = vload(a.dq + 3 * fs + o, nm);
+    vstore(S.vin[0], uk, nm);
+    vstore(S.vin[1], vk, nm);
+    vstore(S.vin[2], q0, nm);
+    vstore(S.vin[3], V2{q1.a - fc.a, q1.b - fc.b}, nm);
+    vstore(S.vin[4], V2{q2.a + fc.a, q2.b + fc.b}, nm);
+    vstore(S.vin[5], q3, nm);
+    vstore(S.vin[6], vadd(hh, hb), nm);
+    vstore(S.vin[7], V2{w0.a - a.mb0 * uk.a, w0.b - a.mb0 * uk.b}, nm);
+    vstore(S.vin[8], V2{z0.a - a.mb0 * vk.a, z0.b - a.mb0 * vk.b}, nm);
+    vstore(S.vin[9], du, nm);
+    vstore(S.vin[10], dv, nm);
+    vstore(S.vin[11], d0, nm);
+    vstore(S.vin[12], d1, nm);
+    vstore(S.vin[13], d2, nm);
+    vstore(S.vin[14], d3, nm);
+    vstore(S.vin[15], dh, nm);
+    vstore(S.vin[16], vscale(du, -a.mb0), nm);
+    vstore(S.vin[17], vscale(dv, -a.mb0), nm);
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int qp = l + h * kWarp;
+      if (qp < ng) {
+        double b[9], d[9];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) b[f] = d[f] = 0.0;
+        for (int n = 0; n < nm; ++n) {
+          const double p = __ldg(op.p2 + (size_t)n * ng + qp);
+#pragma unroll
+          for (int f = 0; f < 9; ++f) {
+            b[f] = fmac(b[f], S.vin[f][n], p);
+            d[f] = fmac(d[f], S.vin[9 + f][n], p);
+          }
+        }
+        const double w = __ldg(op.wi + qp), ih = 1.0 / b[6];
+        // d(products) of calvarnl_fs.f:263-296
+        S.wp[0][qp] = w * (d[0] * b[2] + b[0] * d[2]);
+        S.wp[1][qp] = w * (d[1] * b[3] + b[1] * d[3]);
+        S.wp[2][qp] = w * (d[0] * b[4] + b[0] * d[4]);
+        S.wp[3][qp] = w * (d[1] * b[5] + b[1] * d[5]);
+        S.wp[4][qp] = w * (d[0] * b[6] + b[0] * d[6]);
+        S.wp[5][qp] = w * (d[1] * b[6] + b[1] * d[6]);
+        S.wp[6][qp] = w * (d[7] - b[7] * ih * d[6]) * ih;
+        S.wp[7][qp] = w * (d[8] - b[8] * ih * d[6]) * ih;
+      }
+    }
+    __syncwarp();
+    double X[8][2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int n = l + h * kWarp;
+#pragma unroll
+      for (int f = 0; f < 8; ++f) X[f][h] = 0.0;
+      if (n < nm)
+        for (int qp = 0; qp < ng; ++qp) {
+          const double p = __ldg(op.p2t + (size_t)qp * nm + n);
+#pragma unroll
+          for (int f = 0; f < 8; ++f) X[f][h] = fmac(X[f][h], S.wp[f][qp], p);
+        }
+    }
+    V2 uhk{X[4][0], X[4][1]}, vhk{X[5][0], X[5][1]};
+    pair_solve<VAR>(op, m, e, uhk, vhk, S.sm);
+    V2 gx0{-(X[0][0] + X[1][0]) + X[6][0], -(X[0][1] + X[1][1]) + X[6][1]};
+    V2 gy0{-(X[2][0] + X[3][0]) + X[7][0], -(X[2][1] + X[3][1]) + X[7][1]};
+    vstore(a.gx0 + o, gx0, nm);
+    vstore(a.gy0 + o, gy0, nm);
+    vstore(a.uh + o, uhk, nm);
+    vstore(a.vh + o, vhk, nm);
+    const double mu0 = a.mu0, g0 = a.g0;
+    vstore(a.f + o, vlin(mu0, d0, -g0, dh), nm);
+    vstore(a.f + fs + o, vscale(d1, mu0), nm);
+    vstore(a.f + 2 * fs + o, vscale(d2, mu0), nm);
+    vstore(a.f + 3 * fs + o, vlin(mu0, d3, -g0, dh), nm);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the tendency stage (calvarnl_fs.f:382-544)
+// ---------------------------------------------------------------------------
+struct TaSmem {
+  double g[3][kMaxModes];
+};
+
+template <int VAR>
+__global__ void __launch_bounds__(kT) k_adj_tend_a(DevOps op, DevMesh m, AdjTendArgs a) {
+  __shared__ TaSmem sall[kWB];
+  __shared__ double smw[kWB][kMaxModes];
+  TaSmem &S = sall[threadIdx.x >> 5];
+  double *sm = smw[threadIdx.x >> 5];
+  const int nm = op.nm, ne = m.ne;
+  const size_t fs = (size_t)ne * nm;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    const Geo g = geo(m, e);
+    V2 gx = vload(a.bu + o, nm), gy = vload(a.bv + o, nm), b = vload(a.bh + o, nm);
+    pair_solve<VAR>(op, m, e, gx, gy, sm);
+    b = solve_full(op, b);
+    vstore(a.gx0b + o, gx, nm);
+    vstore(a.gy0b + o, gy, nm);
+    vstore(S.g[0], gx, nm);
+    vstore(S.g[1], gy, nm);
+    vstore(S.g[2], b, nm);
+    __syncwarp();
+    const V2 axg = matvecN(op.agxN, S.g[0], nm), ayg = matvecN(op.agyN, S.g[0], nm);
+    const V2 bxg = matvecN(op.agxN, S.g[1], nm), byg = matvecN(op.agyN, S.g[1], nm);
+    const V2 ah = matvecN(op.agxN, S.g[2], nm), bh = matvecN(op.agyN, S.g[2], nm);
+    const double cby = g.by * g.detai, cay = g.ay * g.detai, cbx = g.bx * g.detai, cax = g.ax * g.detai;
+    vstore(a.fb + o, vlin(-cby, axg, cay, ayg), nm);
+    vstore(a.fb + fs + o, vlin(cbx, axg, -cax, ayg), nm);
+    vstore(a.fb + 2 * fs + o, vlin(-cby, bxg, cay, byg), nm);
+    vstore(a.fb + 3 * fs + o, vlin(cbx, bxg, -cax, byg), nm);
+    vstore(a.uhb + o, vlin(cby, ah, -cay, bh), nm);
+    vstore(a.vhb + o, vlin(-cbx, ah, cax, bh), nm);
+    side_lift_adj(op, m, e, S.g[0], g.detai, a.lx);
+    side_lift_adj(op, m, e, S.g[1], g.detai, a.ly);
+    side_lift_adj(op, m, e, S.g[2], -g.detai, a.lh);
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(kT) k_adj_tend_b(DevOps op, DevMesh m, AdjTendArgs a) {
+  __shared__ double sall[kWB][3][32];
+  double(*S)[32] = sall[threadIdx.x >> 5];
+  const int nm = op.nm, ne = m.ne;
+  const size_t fs = (size_t)ne * nm;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    face_sums(op, m, e, a.lx, S[0]);
+    face_sums(op, m, e, a.ly, S[1]);
+    face_sums(op, m, e, a.lh, S[2]);
+    __syncwarp();
+    // fbdxx = fbd(fxx)*n1, fbdxy = fbd(fxy)*n2 lifted into gx; likewise gy, h
+    vstore(a.fb + o, vadd(vload(a.fb + o, nm), trace_adj(op, m, e, S[0], 0, 1.0)), nm);
+    vstore(a.fb + fs + o, vadd(vload(a.fb + fs + o, nm), trace_adj(op, m, e, S[0], 1, 1.0)), nm);
+    vstore(a.fb + 2 * fs + o, vadd(vload(a.fb + 2 * fs + o, nm), trace_adj(op, m, e, S[1], 0, 1.0)), nm);
+    vstore(a.fb + 3 * fs + o, vadd(vload(a.fb + 3 * fs + o, nm), trace_adj(op, m, e, S[1], 1, 1.0)), nm);
+    vstore(a.uhb + o, vadd(vload(a.uhb + o, nm), trace_adj(op, m, e, S[2], 0, 1.0)), nm);
+    vstore(a.vhb + o, vadd(vload(a.vhb + o, nm), trace_adj(op, m, e, S[2], 1, 1.0)), nm);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the quadrature-point stage (calvarnl_fs.f:243-348)
+// ---------------------------------------------------------------------------
+struct NaSmem {
+  double vin[9][kMaxModes];
+  double xb[8][kMaxModes];
+  double qb[9][kMaxQuad];  // quadrature-point adjoints: U V Gxx Gxy Gyx Gyy H Wk Zk
+  double sm[kMaxModes];
+};
+
+template <int VAR>
+__global__ void __launch_bounds__(64) k_nlvol_adj(DevOps op, DevMesh m, AdjNlArgs a) {
+  __shared__ NaSmem sall[2];
+  NaSmem &S = sall[threadIdx.x >> 5];
+  const int nm = op.nm, ng = op.ng, ne = m.ne, l = lane_id();
+  const size_t fs = (size_t)ne * nm;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    const V2 uk = vload(a.su + o, nm), vk = vload(a.sv + o, nm), hh = vload(a.sh + o, nm);
+    const V2 hb = vload(a.hb + o, nm), w0 = vload(a.w0 + o, nm), z0 = vload(a.z0 + o, nm);
+    const V2 fc = vload(a.fc + o, nm);
+    const V2 q0 = vload(a.q + o, nm), q1 = vload(a.q + fs + o, nm);
+    const V2 q2 = vload(a.q + 2 * fs + o, nm), q3 = vload(a.q + 3 * fs + o, nm);
+    const V2 f0 = vload(a.fb + o, nm), f1 = vload(a.fb + fs + o, nm);
+    const V2 f2 = vload(a.fb + 2 * fs + o, nm), f3 = vload(a.fb + 3 * fs + o, nm);
+    const V2 gx0 = vload(a.gx0b + o, nm), gy0 = vload(a.gy0b + o, nm);
+    V2 uhb = vload(a.uhb + o, nm), vhb = vload(a.vhb + o, nm);
+    vstore(S.vin[0], uk, nm);
+    vstore(S.vin[1], vk, nm);
+    vstore(S.vin[2], q0, nm);
+    vstore(S.vin[3], V2{q1.a - fc.a, q1.b - fc.b}, nm);
+    vstore(S.vin[4], V2{q2.a + fc.a, q2.b + fc.b}, nm);
+    vstore(S.vin[5], q3, nm);
+    vstore(S.vin[6], vadd(hh, hb), nm);
+    vstore(S.vin[7], V2{w0.a - a.mb0 * uk.a, w0.b - a.mb0 * uk.b}, nm);
+    vstore(S.vin[8], V2{z0.a - a.mb0 * vk.a, z0.b - a.mb0 * vk.b}, nm);
+    // uh = W(uhk) (self-adjoint)
+    pair_solve<VAR>(op, m, e, uhb, vhb, S.sm);
+    const V2 ngx = vscale(gx0, -1.0), ngy = vscale(gy0, -1.0);
+    vstore(S.xb[0], ngx, nm);
+    vstore(S.xb[1], ngx, nm);
+    vstore(S.xb[2], ngy, nm);
+    vstore(S.xb[3], ngy, nm);
+    vstore(S.xb[4], uhb, nm);
+    vstore(S.xb[5], vhb, nm);
+    vstore(S.xb[6], gx0, nm);
+    vstore(S.xb[7], gy0, nm);
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int qp = l + h * kWarp;
+      if (qp < ng) {
+        double b[9], pb[8];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) b[f] = 0.0;
+#pragma unroll
+        for (int f = 0; f < 8; ++f) pb[f] = 0.0;
+        for (int n = 0; n < nm; ++n) {
+          const double p = __ldg(op.p2 + (size_t)n * ng + qp);
+#pragma unroll
+          for (int f = 0; f < 9; ++f) b[f] = fmac(b[f], S.vin[f][n], p);
+#pragma unroll
+          for (int f = 0; f < 8; ++f) pb[f] = fmac(pb[f], S.xb[f][n], p);
+        }
+        const double w = __ldg(op.wi + qp), ih = 1.0 / b[6];
+#pragma unroll
+        for (int f = 0; f < 8; ++f) pb[f] *= w;  // xytospec^T
+        S.qb[0][qp] = pb[0] * b[2] + pb[2] * b[4] + pb[4] * b[6];  // U
+        S.qb[1][qp] = pb[1] * b[3] + pb[3] * b[5] + pb[5] * b[6];  // V
+        S.qb[2][qp] = pb[0] * b[0];                                // Gxx
+        S.qb[3][qp] = pb[1] * b[1];                                // Gxy
+        S.qb[4][qp] = pb[2] * b[0];                                // Gyx
+        S.qb[5][qp] = pb[3] * b[1];                                // Gyy
+        S.qb[6][qp] = pb[4] * b[0] + pb[5] * b[1] - (pb[6] * b[7] + pb[7] * b[8]) * ih * ih;  // H
+        S.qb[7][qp] = pb[6] * ih;                                  // Wk
+        S.qb[8][qp] = pb[7] * ih;                                  // Zk
+      }
+    }
+    __syncwarp();
+    // spectoxy^T: modal adjoint a(n) = sum_q pi2(q,n) qb(q)
+    double M[9][2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int n = l + h * kWarp;
+#pragma unroll
+      for (int f = 0; f < 9; ++f) M[f][h] = 0.0;
+      if (n < nm)
+        for (int qp = 0; qp < ng; ++qp) {
+          const double p = __ldg(op.p2t + (size_t)qp * nm + n);
+#pragma unroll
+          for (int f = 0; f < 9; ++f) M[f][h] = fmac(M[f][h], S.qb[f][qp], p);
+        }
+    }
+    const double mu0 = a.mu0, g0 = a.g0, mb0 = a.mb0;
+    V2 ub{M[0][0] - mb0 * M[7][0], M[0][1] - mb0 * M[7][1]};
+    V2 vb{M[1][0] - mb0 * M[8][0], M[1][1] - mb0 * M[8][1]};
+    V2 hbar{M[6][0] - g0 * (f0.a + f3.a), M[6][1] - g0 * (f0.b + f3.b)};
+    vstore(a.ub + o, ub, nm);
+    vstore(a.vb + o, vb, nm);
+    vstore(a.hbo + o, hbar, nm);
+    vstore(a.qb + o, V2{M[2][0] + mu0 * f0.a, M[2][1] + mu0 * f0.b}, nm);
+    vstore(a.qb + fs + o, V2{M[3][0] + mu0 * f1.a, M[3][1] + mu0 * f1.b}, nm);
+    vstore(a.qb + 2 * fs + o, V2{M[4][0] + mu0 * f2.a, M[4][1] + mu0 * f2.b}, nm);
+    vstore(a.qb + 3 * fs + o, V2{M[5][0] + mu0 * f3.a, M[5][1] + mu0 * f3.b}, nm);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the q-phase (calvarnl_fs.f:88-226)
+// ---------------------------------------------------------------------------
+template <int VAR>
+__global__ void __launch_bounds__(kT) k_adj_qphase_a(DevOps op, DevMesh m, AdjQArgs a) {
+  __shared__ double sall[kWB][5][kMaxModes];
+  double(*S)[kMaxModes] = sall[threadIdx.x >> 5];
+  const int nm = op.nm, ne = m.ne;
+  const size_t fs = (size_t)ne * nm;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    const Geo g = geo(m, e);
+    V2 gxx = vload(a.qb + o, nm), gxy = vload(a.qb + fs + o, nm);
+    V2 gyx = vload(a.qb + 2 * fs + o, nm), gyy = vload(a.qb + 3 * fs + o, nm);
+    if (VAR == kFS && __ldg(m.bdl + e)) {
+      qwall_fs(op, gxx, gxy, gyx, gyy, __ldg(m.normt + 2 * e), __ldg(m.normt + 2 * e + 1), S[4]);
+    } else {
+      gxx = solve_full(op, gxx);
+      gxy = solve_full(op, gxy);
+      gyx = solve_full(op, gyx);
+      gyy = solve_full(op, gyy);
+    }
+    // gxx = (by gx1 - ay gy1) detai, gxy = (-bx gx1 + ax gy1) detai, gx1 = -agx^T u ...
+    const double d = g.detai;
+    const V2 gx1u = vlin(d * g.by, gxx, -d * g.bx, gxy), gy1u = vlin(-d * g.ay, gxx, d * g.ax, gxy);
+    const V2 gx1v = vlin(d * g.by, gyx, -d * g.bx, gyy), gy1v = vlin(-d * g.ay, gyx, d * g.ax, gyy);
+    vstore(S[0], gx1u, nm);
+    vstore(S[1], gy1u, nm);
+    vstore(S[2], gx1v, nm);
+    vstore(S[3], gy1v, nm);
+    __syncwarp();
+    const V2 uvol = vscale(vadd(matvecN(op.agxN, S[0], nm), matvecN(op.agyN, S[1], nm)), -1.0);
+    const V2 vvol = vscale(vadd(matvecN(op.agxN, S[2], nm), matvecN(op.agyN, S[3], nm)), -1.0);
+    vstore(a.ub + o, vadd(vload(a.ub + o, nm), uvol), nm);
+    vstore(a.vb + o, vadd(vload(a.vb + o, nm), vvol), nm);
+    __syncwarp();
+    vstore(S[0], gxx, nm);
+    vstore(S[1], gxy, nm);
+    vstore(S[2], gyx, nm);
+    vstore(S[3], gyy, nm);
+    __syncwarp();
+    for (int c = 0; c < 4; ++c) side_lift_adj(op, m, e, S[c], d, a.lq + (size_t)c * ne * 3 * op.ngf);
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(kT) k_adj_qphase_b(DevOps op, DevMesh m, AdjQArgs a) {
+  __shared__ double sall[kWB][4][32];
+  double(*S)[32] = sall[threadIdx.x >> 5];
+  const int nm = op.nm, ne = m.ne;
+  const size_t ls = (size_t)ne * 3 * op.ngf;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    for (int c = 0; c < 4; ++c) face_sums(op, m, e, a.lq + c * ls, S[c]);
+    __syncwarp();
+    // u is traced into fbdxx (n1, lifted into gxx) and fbdxy (n2, into gxy)
+    V2 ut = vadd(trace_adj(op, m, e, S[0], 0, 1.0), trace_adj(op, m, e, S[1], 1, 1.0));
+    V2 vt = vadd(trace_adj(op, m, e, S[2], 0, 1.0), trace_adj(op, m, e, S[3], 1, 1.0));
+    vstore(a.ub + o, vadd(vload(a.ub + o, nm), ut), nm);
+    vstore(a.vb + o, vadd(vload(a.vb + o, nm), vt), nm);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the linear variant (calvar_lin.f:7-287)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kT) k_adj_lin_a(DevOps op, DevMesh m, AdjLinArgs a) {
+  __shared__ double sall[kWB][3][kMaxModes];
+  __shared__ double smw[kWB][kMaxModes];
+  double(*S)[kMaxModes] = sall[threadIdx.x >> 5];
+  double *sm = smw[threadIdx.x >> 5];
+  const int nm = op.nm, ne = m.ne;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    const Geo g = geo(m, e);
+    V2 gx = vload(a.bu + o, nm), gy = vload(a.bv + o, nm), b = vload(a.bh + o, nm);
+    if (__ldg(m.bdl + e)) {
+      wall_solve_rot(op, gx, gy, __ldg(m.normt + 2 * e), __ldg(m.normt + 2 * e + 1), sm);
+    } else {
+      gx = solve_full(op, gx);
+      gy = solve_full(op, gy);
+    }
+    b = solve_full(op, b);
+    vstore(S[0], gx, nm);
+    vstore(S[1], gy, nm);
+    vstore(S[2], b, nm);
+    __syncwarp();
+    const double cby = g.by * g.detai, cay = g.ay * g.detai, cbx = g.bx * g.detai, cax = g.ax * g.detai;
+    const V2 axg = matvecN(op.agxN, S[0], nm), ayg = matvecN(op.agyN, S[0], nm);
+    const V2 bxg = matvecN(op.agxN, S[1], nm), byg = matvecN(op.agyN, S[1], nm);
+    const V2 ah = matvecN(op.agxN, S[2], nm), bh = matvecN(op.agyN, S[2], nm);
+    // fxx = fyy = -g0 h: gx uses (agx,-by d), (agy, ay d); gy uses (agx, bx d), (agy, -ax d)
+    const V2 fb = vadd(vlin(-cby, axg, cay, ayg), vlin(cbx, bxg, -cax, byg));
+    vstore(a.hbo + o, vscale(fb, -a.g0), nm);
+    vstore(a.ub + o, vscale(vlin(cby, ah, -cay, bh), a.hh0), nm);
+    vstore(a.vb + o, vscale(vlin(-cbx, ah, cax, bh), a.hh0), nm);
+    side_lift_adj(op, m, e, S[0], g.detai, a.lx);
+    side_lift_adj(op, m, e, S[1], g.detai, a.ly);
+    side_lift_adj(op, m, e, S[2], -g.detai, a.lh);
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(kT) k_adj_lin_b(DevOps op, DevMesh m, AdjLinArgs a) {
+  __shared__ double sall[kWB][3][32];
+  double(*S)[32] = sall[threadIdx.x >> 5];
+  const int nm = op.nm, ne = m.ne;
+  for (int e = wg(); e < ne; e += wc()) {
+    const size_t o = (size_t)e * nm;
+    face_sums(op, m, e, a.lx, S[0]);
+    face_sums(op, m, e, a.ly, S[1]);
+    face_sums(op, m, e, a.lh, S[2]);
+    __syncwarp();
+    const V2 ht = vadd(trace_adj(op, m, e, S[0], 0, 1.0), trace_adj(op, m, e, S[1], 1, 1.0));
+    vstore(a.hbo + o, vadd(vload(a.hbo + o, nm), vscale(ht, -a.g0)), nm);
+    vstore(a.ub + o, vadd(vload(a.ub + o, nm), trace_adj(op, m, e, S[2], 0, a.hh0)), nm);
+    vstore(a.vb + o, vadd(vload(a.vb + o, nm), trace_adj(op, m, e, S[2], 1, a.hh0)), nm);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// element-wise helpers of the RK4 tangent-linear / adjoint steps
+// ---------------------------------------------------------------------------
+// out = x + c * y (n doubles)
+__global__ void k_axpy(size_t n, const double *x, double c, const double *y, double *out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = fma(c, y[i], x[i]);
+}
+
+// out = a*x + b*y
+__global__ void k_axpby(size_t n, double a, const double *x, double b, const double *y,
+                        double *out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = fma(a, x[i], b * y[i]);
+}
+
+// Observation values: obs o lies in element elem[o] with basis values
+// basis[o*nm + n]; val[o] = sum_n h(elem, n) basis(n).
+__global__ void k_obs_eval(int nobs, int nm, const int *elem, const double *basis, const double *h,
+                           double *val) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o < nobs) {
+    const double *hv = h + (size_t)elem[o] * nm;
+    double s = 0.0;
+    for (int n = 0; n < nm; ++n) s = fma(hv[n], basis[(size_t)o * nm + n], s);
+    val[o] = s;
+  }
+}
+
+// Adjoint forcing of 0.5 sum_o (val_o - y_o)^2: hb(elem, n) += sum over the
+// observations of that element (CSR, fixed order) of r_o basis(o, n).
+__global__ void k_obs_adj(int nel, int nm, const int *el_list, const int *el_start,
+                          const int *obs_of, const double *basis, const double *resid, double *hb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nel * nm) {
+    const int k = i / nm, n = i - k * nm;
+    double s = 0.0;
+    for (int p = el_start[k]; p < el_start[k + 1]; ++p) {
+      const int o = obs_of[p];
+      s = fma(resid[o], basis[(size_t)o * nm + n], s);
+    }
+    hb[(size_t)el_list[k] * nm + n] += s;
+  }
+}
+
+inline int grid_for(int ne, int sms, int wpb) {
+  const int need = (ne + wpb - 1) / wpb;
+  return need < sms * 8 ? need : sms * 8;
+}
+
+}  // namespace
+
+cudaError_t launch_nlvol_tlm(int variant, const DevOps &op, const DevMesh &m, const TlmArgs &a,
+                             cudaStream_t st, int sms) {
+  const int grid = grid_for(m.ne, sms, 2);
+  switch (variant) {
+    case kFS: k_nlvol_tlm<kFS><<<grid, 64, 0, st>>>(op, m, a); break;
+    case kNS: k_nlvol_tlm<kNS><<<grid, 64, 0, st>>>(op, m, a); break;
+    default: k_nlvol_tlm<kINV><<<grid, 64, 0, st>>>(op, m, a); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_nl(int variant, const DevOps &op, const DevMesh &m, const AdjTendArgs &ta,
+                          const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int sms) {
+  const int g8 = grid_for(m.ne, sms, kWB), g2 = grid_for(m.ne, sms, 2);
+  switch (variant) {
+    case kFS:
+      k_adj_tend_a<kFS><<<g8, kT, 0, st>>>(op, m, ta);
+      k_adj_tend_b<<<g8, kT, 0, st>>>(op, m, ta);
+      k_nlvol_adj<kFS><<<g2, 64, 0, st>>>(op, m, na);
+      k_adj_qphase_a<kFS><<<g8, kT, 0, st>>>(op, m, qa);
+      break;
+    case kNS:
+      k_adj_tend_a<kNS><<<g8, kT, 0, st>>>(op, m, ta);
+      k_adj_tend_b<<<g8, kT, 0, st>>>(op, m, ta);
+      k_nlvol_adj<kNS><<<g2, 64, 0, st>>>(op, m, na);
+      k_adj_qphase_a<kNS><<<g8, kT, 0, st>>>(op, m, qa);
+      break;
+    default:
+      k_adj_tend_a<kINV><<<g8, kT, 0, st>>>(op, m, ta);
+      k_adj_tend_b<<<g8, kT, 0, st>>>(op, m, ta);
+      k_nlvol_adj<kINV><<<g2, 64, 0, st>>>(op, m, na);
+      k_adj_qphase_a<kINV><<<g8, kT, 0, st>>>(op, m, qa);
+      break;
+  }
+  k_adj_qphase_b<<<g8, kT, 0, st>>>(op, m, qa);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_lin(const DevOps &op, const DevMesh &m, const AdjLinArgs &a,
+                           cudaStream_t st, int sms) {
+  const int g = grid_for(m.ne, sms, kWB);
+  k_adj_lin_a<<<g, kT, 0, st>>>(op, m, a);
+  k_adj_lin_b<<<g, kT, 0, st>>>(op, m, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(size_t n, const double *x, double c, const double *y, double *out,
+                        cudaStream_t st, int sms) {
+  size_t blocks = (n + 255) / 256;
+  if (blocks > (size_t)sms * 16) blocks = (size_t)sms * 16;
+  if (blocks < 1) blocks = 1;
+  k_axpy<<<(unsigned)blocks, 256, 0, st>>>(n, x, c, y, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpby(size_t n, double a, const double *x, double b, const double *y,
+                         double *out, cudaStream_t st, int sms) {
+  size_t blocks = (n + 255) / 256;
+  if (blocks > (size_t)sms * 16) blocks = (size_t)sms * 16;
+  if (blocks < 1) blocks = 1;
+  k_axpby<<<(unsigned)blocks, 256, 0, st>>>(n, a, x, b, y, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_obs_eval(int nobs, int nm, const int *elem, const double *basis,
+                            const double *h, double *val, cudaStream_t st) {
+  k_obs_eval<<<(nobs + 127) / 128, 128, 0, st>>>(nobs, nm, elem, basis, h, val);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_obs_adj(int nel, int nm, const int *el_list, const int *el_start,
+                           const int *obs_of, const double *basis, const double *resid, double *hb,
+                           cudaStream_t st) {
+  const int n = nel * nm;
+  k_obs_adj<<<(n + 127) / 128, 128, 0, st>>>(nel, nm, el_list, el_start, obs_of, basis, resid, hb);
+  return cudaGetLastError();
+}
+
+}  // namespace spoc

@@ -2,6 +2,7 @@
 // driver, diagnostics and the Fortran cal_var_ drop-in.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -93,13 +94,16 @@ int build_ops(spoc_handle *h, const spoc_tables *t) {
   const int nm = h->nm, ng = h->ng, G = h->ngf, nc = h->nc, nmr = h->nmr;
   const int lm = t->ld_mat, lq = t->ld_pi2, lp1 = t->ld_pico1, lp2 = t->ld_pico2;
   auto MAT = [&](const double *a, int i, int j) { return a[(size_t)j * lm + i]; };
-  std::vector<double> agx(nm * nm), agy(nm * nm), p2(nm * ng), p2t(ng * nm), wi(ng), wif(G);
+  std::vector<double> agx(nm * nm), agy(nm * nm), agxN(nm * nm), agyN(nm * nm), p2(nm * ng),
+      p2t(ng * nm), wi(ng), wif(G);
   std::vector<double> picoF(3 * nm * G), picoT(3 * G * nm), uT(nm * nm), uC(nm * nm), dia1(nm);
   std::vector<double> ulT(nm * nm, 0.0), ulC(nm * nm, 0.0), dia2(nm, 0.0), ammo1(nm);
   for (int j = 0; j < nm; ++j)
     for (int i = 0; i < nm; ++i) {
       agx[j * nm + i] = MAT(t->agx, j, i);
       agy[j * nm + i] = MAT(t->agy, j, i);
+      agxN[i * nm + j] = MAT(t->agx, j, i);
+      agyN[i * nm + j] = MAT(t->agy, j, i);
       uT[j * nm + i] = MAT(t->amm, j, i);
       uC[j * nm + i] = MAT(t->amm, i, j);
     }
@@ -154,6 +158,8 @@ int build_ops(spoc_handle *h, const spoc_tables *t) {
   o.nc = nc; o.nm = nm; o.nmr = nmr; o.ng = ng; o.ngf = G;
   CK(h->upload(&o.agx, agx), "upload agx");
   CK(h->upload(&o.agy, agy), "upload agy");
+  CK(h->upload(&o.agxN, agxN), "upload agx");
+  CK(h->upload(&o.agyN, agyN), "upload agy");
   CK(h->upload(&o.p2, p2), "upload pi2");
   CK(h->upload(&o.p2t, p2t), "upload pi2t");
   CK(h->upload(&o.wi, wi), "upload wi");
@@ -383,9 +389,12 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
   return SPOC_OK;
 }
 
+void adj_forget(spoc_handle *h);
+
 extern "C" void spoc_destroy(spoc_handle *h) {
   if (!h) return;
   if (h->st) cudaStreamSynchronize(h->st);
+  adj_forget(h);
   delete h;
 }
 
@@ -763,4 +772,498 @@ extern "C" void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, d
     c.h->g0 = *g0;
   }
   c.status = spoc_cal_var(c.h, c.ld, u0, v0, h0, u1, v1, h1);
+}
+
+// ---------------------------------------------------------------------------
+// Tangent-linear model, adjoint and gradient of an observation cost
+// (no reference counterpart; see include/spoc_gpu.h)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct AdjCtx {
+  int ready = 0;
+  size_t n = 0;  // ne * nm
+  // right-hand-side scratch
+  double *qb = nullptr, *qd = nullptr, *tgx0 = nullptr, *tgy0 = nullptr, *tuh = nullptr,
+         *tvh = nullptr, *tf = nullptr;
+  double *agx0 = nullptr, *agy0 = nullptr, *auh = nullptr, *avh = nullptr, *af = nullptr,
+         *aq = nullptr, *lx = nullptr, *ly = nullptr, *lh = nullptr, *lq = nullptr;
+  // RK4 step work: states x, s2, s3, s4 (3 fields each), tendencies, vectors
+  double *S[4][3] = {}, *K[4][3] = {}, *V[6][3] = {};
+  // observations
+  int nobs = 0, ntimes = 0, nel = 0;
+  int *d_elem = nullptr, *d_el_list = nullptr, *d_el_start = nullptr, *d_obs_of = nullptr;
+  double *d_basis = nullptr, *d_val = nullptr, *d_resid = nullptr;
+  std::vector<int> steps;
+  std::vector<double> values;          // ntimes * nobs
+  std::vector<double> resid;           // ntimes * nobs, from the last forward window
+  // checkpoints
+  std::vector<double *> snaps;
+  long long fwd_steps = 0, adj_steps = 0;
+};
+
+std::mutex g_adj_mu;
+std::vector<std::pair<spoc_handle *, AdjCtx *>> g_adj;
+
+AdjCtx *ctx_of(spoc_handle *h) {
+  std::lock_guard<std::mutex> lk(g_adj_mu);
+  for (auto &p : g_adj)
+    if (p.first == h) return p.second;
+  AdjCtx *c = new AdjCtx();
+  g_adj.push_back({h, c});
+  return c;
+}
+
+}  // namespace
+
+// Drop the adjoint context of a handle being destroyed (its device buffers
+// are owned by the handle and freed with it).
+void adj_forget(spoc_handle *h) {
+  std::lock_guard<std::mutex> lk(g_adj_mu);
+  for (size_t i = 0; i < g_adj.size(); ++i)
+    if (g_adj[i].first == h) {
+      delete g_adj[i].second;
+      g_adj.erase(g_adj.begin() + i);
+      return;
+    }
+}
+
+namespace {
+
+int adj_init(spoc_handle *h, AdjCtx *c) {
+  if (c->ready) return SPOC_OK;
+  const size_t n = fsize(h), ls = (size_t)h->ne * 3 * h->ngf;
+  c->n = n;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](double **p, size_t k) {
+    if (e == cudaSuccess) e = h->alloc(p, k);
+  };
+  A(&c->qb, 4 * n); A(&c->qd, 4 * n); A(&c->tgx0, n); A(&c->tgy0, n); A(&c->tuh, n);
+  A(&c->tvh, n); A(&c->tf, 4 * n); A(&c->agx0, n); A(&c->agy0, n); A(&c->auh, n);
+  A(&c->avh, n); A(&c->af, 4 * n); A(&c->aq, 4 * n); A(&c->lx, ls); A(&c->ly, ls);
+  A(&c->lh, ls); A(&c->lq, 4 * ls);
+  for (int i = 0; i < 4; ++i)
+    for (int f = 0; f < 3; ++f) {
+      A(&c->S[i][f], n);
+      A(&c->K[i][f], n);
+    }
+  for (int i = 0; i < 6; ++i)
+    for (int f = 0; f < 3; ++f) A(&c->V[i][f], n);
+  if (e != cudaSuccess) return fail(SPOC_E_NOMEM, "adjoint work space", e);
+  c->ready = 1;
+  return SPOC_OK;
+}
+
+// forward tendency k = f(s) with the handle's precision and kernel family
+int fwd_rhs(spoc_handle *h, double *const s[3], double *const k[3]) {
+  StageArgs sa{};
+  sa.stage = -1;
+  for (int f = 0; f < 3; ++f) sa.tend[f] = k[f];
+  sa.flag = h->flag;
+  CK(launch(h, s, sa, nullptr), "forward rhs");
+  return SPOC_OK;
+}
+
+// tangent-linear tendency: out = J(s) d
+int tlm_rhs(spoc_handle *h, AdjCtx *c, double *const s[3], double *const d[3],
+            double *const out[3]) {
+  StageArgs sa{};
+  sa.stage = -1;
+  for (int f = 0; f < 3; ++f) sa.tend[f] = out[f];
+  sa.flag = h->flag;
+  if (h->variant == SPOC_LIN) {
+    LinArgs la{d[0], d[1], d[2], h->g0, h->hh0};
+    CK(launch_lin(h->op, h->mesh, la, sa, h->st, h->sms), "tlm linear");
+    return SPOC_OK;
+  }
+  CK(launch_qphase(h->variant, h->op, h->mesh, s[0], s[1], c->qb, h->st, h->sms), "tlm base q");
+  CK(launch_qphase(h->variant, h->op, h->mesh, d[0], d[1], c->qd, h->st, h->sms), "tlm q");
+  TlmArgs ta{s[0], s[1], s[2], h->hb, h->w0, h->z0, h->fc, c->qb, d[0], d[1], d[2], c->qd,
+             c->tgx0, c->tgy0, c->tuh, c->tvh, c->tf, h->mu0, h->mb0, h->g0};
+  CK(launch_nlvol_tlm(h->variant, h->op, h->mesh, ta, h->st, h->sms), "tlm nlvol");
+  TendArgs td{c->tgx0, c->tgy0, c->tuh, c->tvh, c->tf};
+  CK(launch_tend(h->variant, h->op, h->mesh, td, sa, h->st, h->sms), "tlm tend");
+  return SPOC_OK;
+}
+
+// adjoint tendency: out = J(s)^T b
+int adj_rhs(spoc_handle *h, AdjCtx *c, double *const s[3], double *const b[3],
+            double *const out[3]) {
+  if (h->variant == SPOC_LIN) {
+    AdjLinArgs la{b[0], b[1], b[2], out[0], out[1], out[2], c->lx, c->ly, c->lh, h->g0, h->hh0};
+    CK(launch_adj_lin(h->op, h->mesh, la, h->st, h->sms), "adjoint linear");
+    return SPOC_OK;
+  }
+  CK(launch_qphase(h->variant, h->op, h->mesh, s[0], s[1], c->qb, h->st, h->sms), "adjoint base q");
+  AdjTendArgs ta{b[0], b[1], b[2], c->agx0, c->agy0, c->af, c->auh, c->avh, c->lx, c->ly, c->lh};
+  AdjNlArgs na{s[0], s[1], s[2], h->hb, h->w0, h->z0, h->fc, c->qb, c->af, c->agx0, c->agy0,
+               c->auh, c->avh, out[0], out[1], out[2], c->aq, h->mu0, h->mb0, h->g0};
+  AdjQArgs qa{c->aq, out[0], out[1], c->lq};
+  CK(launch_adj_nl(h->variant, h->op, h->mesh, ta, na, qa, h->st, h->sms), "adjoint");
+  return SPOC_OK;
+}
+
+int axpy3(spoc_handle *h, double *const x[3], double a, double *const y[3], double *const o[3]) {
+  for (int f = 0; f < 3; ++f)
+    CK(launch_axpy(fsize(h), x[f], a, y[f], o[f], h->st, h->sms), "axpy");
+  return SPOC_OK;
+}
+
+int copy3(spoc_handle *h, double *const dst[3], double *const src[3]) {
+  for (int f = 0; f < 3; ++f)
+    CK(cudaMemcpyAsync(dst[f], src[f], sizeof(double) * fsize(h), cudaMemcpyDeviceToDevice, h->st),
+       "copy");
+  return SPOC_OK;
+}
+
+int zero3(spoc_handle *h, double *const x[3]) {
+  for (int f = 0; f < 3; ++f)
+    CK(cudaMemsetAsync(x[f], 0, sizeof(double) * fsize(h), h->st), "zero");
+  return SPOC_OK;
+}
+
+// Stage states of the RK4 step from x (S[0] = x given): S[1..3], K[0..2].
+int stages(spoc_handle *h, AdjCtx *c, double dt) {
+  int rc;
+  if ((rc = fwd_rhs(h, c->S[0], c->K[0]))) return rc;
+  if ((rc = axpy3(h, c->S[0], 0.5 * dt, c->K[0], c->S[1]))) return rc;
+  if ((rc = fwd_rhs(h, c->S[1], c->K[1]))) return rc;
+  if ((rc = axpy3(h, c->S[0], 0.5 * dt, c->K[1], c->S[2]))) return rc;
+  if ((rc = fwd_rhs(h, c->S[2], c->K[2]))) return rc;
+  return axpy3(h, c->S[0], dt, c->K[2], c->S[3]);
+}
+
+// Advance a state by nsteps forward RK4 steps in place (the handle's RK4
+// kernels on its own buffers).
+int advance(spoc_handle *h, AdjCtx *c, double *const x[3], double dt, int nsteps) {
+  if (nsteps <= 0) return SPOC_OK;
+  int rc = copy3(h, h->U0, x);
+  if (rc) return rc;
+  if ((rc = enqueue_steps(h, dt, nsteps))) return rc;
+  c->fwd_steps += nsteps;
+  return copy3(h, x, h->U0);
+}
+
+// out = a*x + b*y for the three fields
+int axpby3(spoc_handle *h, double a, double *const x[3], double b, double *const y[3],
+           double *const o[3]) {
+  for (int f = 0; f < 3; ++f)
+    CK(launch_axpby(fsize(h), a, x[f], b, y[f], o[f], h->st, h->sms), "axpby");
+  return SPOC_OK;
+}
+
+// Adjoint of one RK4 step at state x: lam <- (dx'/dx)^T lam.  With stage
+// states s1 = x, s2, s3, s4 and kbar_i the adjoints of the stage tendencies:
+// kbar4 = dt/6 lam, s4bar = J(s4)^T kbar4, kbar3 = dt/3 lam + dt s4bar,
+// s3bar = J(s3)^T kbar3, kbar2 = dt/3 lam + dt/2 s3bar, s2bar = J(s2)^T kbar2,
+// kbar1 = dt/6 lam + dt/2 s2bar, s1bar = J(s1)^T kbar1, lam += sum sbar.
+int adj_step(spoc_handle *h, AdjCtx *c, double *const x[3], double *const lam[3], double dt) {
+  int rc;
+  if ((rc = copy3(h, c->S[0], x))) return rc;
+  if ((rc = stages(h, c, dt))) return rc;
+  double *const *L = lam;
+  double *const *kb = c->V[0], *const *sb = c->V[1], *const *acc = c->V[2];
+  if ((rc = axpby3(h, dt / 6.0, L, 0.0, L, kb))) return rc;
+  if ((rc = adj_rhs(h, c, c->S[3], kb, sb))) return rc;
+  if ((rc = copy3(h, acc, sb))) return rc;
+  if ((rc = axpby3(h, dt, sb, dt / 3.0, L, kb))) return rc;
+  if ((rc = adj_rhs(h, c, c->S[2], kb, sb))) return rc;
+  if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
+  if ((rc = axpby3(h, 0.5 * dt, sb, dt / 3.0, L, kb))) return rc;
+  if ((rc = adj_rhs(h, c, c->S[1], kb, sb))) return rc;
+  if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
+  if ((rc = axpby3(h, 0.5 * dt, sb, dt / 6.0, L, kb))) return rc;
+  if ((rc = adj_rhs(h, c, c->S[0], kb, sb))) return rc;
+  if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
+  if ((rc = axpy3(h, L, 1.0, acc, L))) return rc;
+  c->adj_steps += 1;
+  return SPOC_OK;
+}
+
+// Tangent-linear RK4 step at x: d <- (dx'/dx) d.
+int tlm_step(spoc_handle *h, AdjCtx *c, double *const x[3], double *const d[3], double dt) {
+  int rc;
+  if ((rc = copy3(h, c->S[0], x))) return rc;
+  if ((rc = stages(h, c, dt))) return rc;
+  double *const *ds = c->V[0], *const *dk = c->V[1], *const *acc = c->V[2];
+  if ((rc = tlm_rhs(h, c, c->S[0], d, dk))) return rc;      // dk1
+  if ((rc = copy3(h, acc, dk))) return rc;
+  if ((rc = axpy3(h, d, 0.5 * dt, dk, ds))) return rc;      // ds2
+  if ((rc = tlm_rhs(h, c, c->S[1], ds, dk))) return rc;     // dk2
+  if ((rc = axpy3(h, acc, 2.0, dk, acc))) return rc;
+  if ((rc = axpy3(h, d, 0.5 * dt, dk, ds))) return rc;      // ds3
+  if ((rc = tlm_rhs(h, c, c->S[2], ds, dk))) return rc;     // dk3
+  if ((rc = axpy3(h, acc, 2.0, dk, acc))) return rc;
+  if ((rc = axpy3(h, d, dt, dk, ds))) return rc;            // ds4
+  if ((rc = tlm_rhs(h, c, c->S[3], ds, dk))) return rc;     // dk4
+  if ((rc = axpy3(h, acc, 1.0, dk, acc))) return rc;
+  return axpy3(h, d, dt / 6.0, acc, d);
+}
+
+int obs_index(AdjCtx *c, int step) {
+  for (size_t t = 0; t < c->steps.size(); ++t)
+    if (c->steps[t] == step) return (int)t;
+  return -1;
+}
+
+// cost term and residuals at observation time t for state x
+int obs_eval(spoc_handle *h, AdjCtx *c, int t, double *const x[3], double *cost) {
+  CK(launch_obs_eval(c->nobs, h->nm, c->d_elem, c->d_basis, x[2], c->d_val, h->st), "obs");
+  std::vector<double> val(c->nobs);
+  CK(cudaMemcpyAsync(val.data(), c->d_val, sizeof(double) * c->nobs, cudaMemcpyDeviceToHost, h->st),
+     "obs read");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  double s = 0.0;
+  for (int o = 0; o < c->nobs; ++o) {
+    const double r = val[o] - c->values[(size_t)t * c->nobs + o];
+    c->resid[(size_t)t * c->nobs + o] = r;
+    s += 0.5 * r * r;
+  }
+  *cost += s;
+  return SPOC_OK;
+}
+
+int obs_force(spoc_handle *h, AdjCtx *c, int t, double *const lam[3]) {
+  CK(cudaMemcpyAsync(c->d_resid, c->resid.data() + (size_t)t * c->nobs, sizeof(double) * c->nobs,
+                     cudaMemcpyHostToDevice, h->st),
+     "residual upload");
+  CK(launch_obs_adj(c->nel, h->nm, c->d_el_list, c->d_el_start, c->d_obs_of, c->d_basis,
+                    c->d_resid, lam[2], h->st),
+     "obs adjoint");
+  return SPOC_OK;
+}
+
+long long binom(int n, int k) {
+  if (k < 0 || k > n) return 0;
+  long long r = 1;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+
+// Reverse steps [i0, i1) given the state at i0 in `base`, with `free_snaps`
+// snapshot buffers available (binomial checkpointing).  lam enters as the
+// adjoint of the state at i1 and leaves as the adjoint of the state at i0,
+// observation forcing included.
+int reverse(spoc_handle *h, AdjCtx *c, int i0, int i1, double *const base[3], int free_snaps,
+            double *const lam[3], double dt) {
+  int rc;
+  const int l = i1 - i0;
+  if (l <= 0) return SPOC_OK;
+  double *const *work = c->V[3];
+  if (l == 1 || free_snaps == 0) {
+    for (int j = i1 - 1; j >= i0; --j) {
+      if ((rc = copy3(h, work, base))) return rc;
+      if ((rc = advance(h, c, work, dt, j - i0))) return rc;
+      if ((rc = adj_step(h, c, work, lam, dt))) return rc;
+      const int t = obs_index(c, j);
+      if (t >= 0 && (rc = obs_force(h, c, t, lam))) return rc;
+    }
+    return SPOC_OK;
+  }
+  int r = 1;
+  while (binom(free_snaps + r, free_snaps) < l) ++r;
+  long long right = binom(free_snaps - 1 + r, free_snaps - 1);
+  int k = (int)std::max<long long>(1, l - std::min<long long>(right, l - 1));
+  double *slot[3];
+  double *snap = c->snaps[free_snaps - 1];
+  for (int f = 0; f < 3; ++f) slot[f] = snap + f * c->n;
+  if ((rc = copy3(h, slot, base))) return rc;
+  if ((rc = advance(h, c, slot, dt, k))) return rc;
+  if ((rc = reverse(h, c, i0 + k, i1, slot, free_snaps - 1, lam, dt))) return rc;
+  return reverse(h, c, i0, i0 + k, base, free_snaps, lam, dt);
+}
+
+int host_to_dev3(spoc_handle *h, double *const dst[3], int ld, const double *a, const double *b,
+                 const double *cc) {
+  CK(copy_in(h, dst[0], a, ld, cudaMemcpyHostToDevice), "upload");
+  CK(copy_in(h, dst[1], b, ld, cudaMemcpyHostToDevice), "upload");
+  CK(copy_in(h, dst[2], cc, ld, cudaMemcpyHostToDevice), "upload");
+  return SPOC_OK;
+}
+
+int dev_to_host3(spoc_handle *h, double *a, double *b, double *cc, int ld, double *const src[3]) {
+  CK(copy_out(h, a, src[0], ld, cudaMemcpyDeviceToHost), "download");
+  CK(copy_out(h, b, src[1], ld, cudaMemcpyDeviceToHost), "download");
+  CK(copy_out(h, cc, src[2], ld, cudaMemcpyDeviceToHost), "download");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  return SPOC_OK;
+}
+
+}  // namespace
+
+extern "C" int spoc_tlm_rhs(spoc_handle *h, int ld, const double *u, const double *v,
+                            const double *hh, const double *du, const double *dv,
+                            const double *dh, double *ou, double *ov, double *oh) {
+  if (!h || !u || !v || !hh || !du || !dv || !dh || !ou || !ov || !oh || ld < (h ? h->nm : 1))
+    return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  AdjCtx *c = ctx_of(h);
+  int rc = adj_init(h, c);
+  if (!rc) rc = host_to_dev3(h, c->S[0], ld, u, v, hh);
+  if (!rc) rc = host_to_dev3(h, c->V[4], ld, du, dv, dh);
+  if (!rc) rc = tlm_rhs(h, c, c->S[0], c->V[4], c->V[5]);
+  if (!rc) rc = dev_to_host3(h, ou, ov, oh, ld, c->V[5]);
+  return rc ? rc : check_flag(h);
+}
+
+extern "C" int spoc_adj_rhs(spoc_handle *h, int ld, const double *u, const double *v,
+                            const double *hh, const double *bu, const double *bv,
+                            const double *bh, double *ou, double *ov, double *oh) {
+  if (!h || !u || !v || !hh || !bu || !bv || !bh || !ou || !ov || !oh || ld < (h ? h->nm : 1))
+    return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  AdjCtx *c = ctx_of(h);
+  int rc = adj_init(h, c);
+  if (!rc) rc = host_to_dev3(h, c->S[0], ld, u, v, hh);
+  if (!rc) rc = host_to_dev3(h, c->V[4], ld, bu, bv, bh);
+  if (!rc) rc = adj_rhs(h, c, c->S[0], c->V[4], c->V[5]);
+  if (!rc) rc = dev_to_host3(h, ou, ov, oh, ld, c->V[5]);
+  return rc ? rc : check_flag(h);
+}
+
+extern "C" int spoc_tlm_steps(spoc_handle *h, int ld, const double *u0, const double *v0,
+                              const double *h0, double *du, double *dv, double *dh, double dt,
+                              int nsteps) {
+  if (!h || !u0 || !v0 || !h0 || !du || !dv || !dh || nsteps < 0 || ld < (h ? h->nm : 1))
+    return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  AdjCtx *c = ctx_of(h);
+  int rc = adj_init(h, c);
+  double *const *x = c->V[3], *const *d = c->V[4];
+  if (!rc) rc = host_to_dev3(h, x, ld, u0, v0, h0);
+  if (!rc) rc = host_to_dev3(h, d, ld, du, dv, dh);
+  for (int i = 0; i < nsteps && !rc; ++i) {
+    rc = tlm_step(h, c, x, d, dt);
+    if (!rc) rc = advance(h, c, x, dt, 1);
+  }
+  if (!rc) rc = dev_to_host3(h, du, dv, dh, ld, d);
+  return rc ? rc : check_flag(h);
+}
+
+extern "C" int spoc_adj_steps(spoc_handle *h, int ld, const double *u0, const double *v0,
+                              const double *h0, double *bu, double *bv, double *bh, double dt,
+                              int nsteps) {
+  if (!h || !u0 || !v0 || !h0 || !bu || !bv || !bh || nsteps < 0 || ld < (h ? h->nm : 1))
+    return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  AdjCtx *c = ctx_of(h);
+  int rc = adj_init(h, c);
+  double *const *x = c->V[4], *const *lam = c->V[5];
+  if (!rc) rc = host_to_dev3(h, x, ld, u0, v0, h0);
+  if (!rc) rc = host_to_dev3(h, lam, ld, bu, bv, bh);
+  std::vector<int> saved;
+  saved.swap(c->steps);  // no observation forcing inside this call
+  if (!rc) rc = reverse(h, c, 0, nsteps, x, 0, lam, dt);
+  c->steps.swap(saved);
+  if (!rc) rc = dev_to_host3(h, bu, bv, bh, ld, lam);
+  return rc ? rc : check_flag(h);
+}
+
+extern "C" int spoc_set_observations(spoc_handle *h, int nobs, const int *elem,
+                                     const double *basis, int ntimes, const int *steps,
+                                     const double *values) {
+  if (!h || nobs < 1 || !elem || !basis || ntimes < 1 || !steps || !values)
+    return fail(SPOC_E_ARG, "bad argument");
+  AdjCtx *c = ctx_of(h);
+  int rc = adj_init(h, c);
+  if (rc) return rc;
+  for (int o = 0; o < nobs; ++o)
+    if (elem[o] < 1 || elem[o] > h->ne) return fail(SPOC_E_ARG, "observation element out of range");
+  // CSR of observations by element, in observation order (fixed summation order)
+  std::vector<int> el0(nobs);
+  for (int o = 0; o < nobs; ++o) el0[o] = elem[o] - 1;
+  std::vector<int> order(nobs);
+  for (int o = 0; o < nobs; ++o) order[o] = o;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return el0[a] < el0[b]; });
+  std::vector<int> el_list, el_start, obs_of;
+  for (int i = 0; i < nobs; ++i) {
+    const int o = order[i];
+    if (el_list.empty() || el_list.back() != el0[o]) {
+      el_list.push_back(el0[o]);
+      el_start.push_back(i);
+    }
+    obs_of.push_back(o);
+  }
+  el_start.push_back(nobs);
+  std::vector<double> bas(basis, basis + (size_t)nobs * h->nm);
+  c->nobs = nobs;
+  c->ntimes = ntimes;
+  c->nel = (int)el_list.size();
+  c->steps.assign(steps, steps + ntimes);
+  c->values.assign(values, values + (size_t)ntimes * nobs);
+  c->resid.assign((size_t)ntimes * nobs, 0.0);
+  auto upi = [&](int **d, const std::vector<int> &v) { return dev_upload(d, v); };
+  auto upd = [&](double **d, const std::vector<double> &v) { return dev_upload(d, v); };
+  cudaError_t e = upi(&c->d_elem, el0);
+  if (e == cudaSuccess) e = upi(&c->d_el_list, el_list);
+  if (e == cudaSuccess) e = upi(&c->d_el_start, el_start);
+  if (e == cudaSuccess) e = upi(&c->d_obs_of, obs_of);
+  if (e == cudaSuccess) e = upd(&c->d_basis, bas);
+  if (e == cudaSuccess) e = upd(&c->d_val, std::vector<double>(nobs, 0.0));
+  if (e == cudaSuccess) e = upd(&c->d_resid, std::vector<double>(nobs, 0.0));
+  for (void *p : {(void *)c->d_elem, (void *)c->d_el_list, (void *)c->d_el_start,
+                  (void *)c->d_obs_of, (void *)c->d_basis, (void *)c->d_val, (void *)c->d_resid})
+    if (p) h->allocs.push_back(p);
+  if (e != cudaSuccess) return fail(SPOC_E_CUDA, "observation upload", e);
+  return SPOC_OK;
+}
+
+extern "C" int spoc_fwd_window(spoc_handle *h, int ld, const double *u0, const double *v0,
+                               const double *h0, double dt, int nsteps, double *cost) {
+  if (!h || !u0 || !v0 || !h0 || !cost || nsteps < 0 || ld < (h ? h->nm : 1))
+    return fail(SPOC_E_ARG, "bad argument");
+  AdjCtx *c = ctx_of(h);
+  if (!c->nobs) return fail(SPOC_E_ARG, "spoc_set_observations not called");
+  int rc = adj_init(h, c);
+  double *const *x = c->V[4];
+  if (!rc) rc = host_to_dev3(h, x, ld, u0, v0, h0);
+  double J = 0.0;
+  int t = obs_index(c, 0);
+  if (!rc && t >= 0) rc = obs_eval(h, c, t, x, &J);
+  for (int i = 1; i <= nsteps && !rc; ++i) {
+    rc = advance(h, c, x, dt, 1);
+    t = obs_index(c, i);
+    if (!rc && t >= 0) rc = obs_eval(h, c, t, x, &J);
+  }
+  *cost = J;
+  return rc ? rc : check_flag(h);
+}
+
+extern "C" int spoc_bwd_window(spoc_handle *h, int ld, const double *u0, const double *v0,
+                               const double *h0, double dt, int nsteps, int snaps, double *cost,
+                               double *gu, double *gv, double *gh) {
+  if (!h || !u0 || !v0 || !h0 || !cost || !gu || !gv || !gh || nsteps < 1 || snaps < 0 ||
+      ld < (h ? h->nm : 1))
+    return fail(SPOC_E_ARG, "bad argument");
+  AdjCtx *c = ctx_of(h);
+  if (!c->nobs) return fail(SPOC_E_ARG, "spoc_set_observations not called");
+  int rc = adj_init(h, c);
+  if (rc) return rc;
+  // snapshot buffers
+  while ((int)c->snaps.size() < snaps) {
+    double *p = nullptr;
+    cudaError_t e = h->alloc(&p, 3 * c->n);
+    if (e != cudaSuccess) return fail(SPOC_E_NOMEM, "checkpoint buffers", e);
+    c->snaps.push_back(p);
+  }
+  // forward sweep: cost and residuals at the observation times
+  rc = spoc_fwd_window(h, ld, u0, v0, h0, dt, nsteps, cost);
+  if (rc) return rc;
+  double *const *x0 = c->V[4], *const *lam = c->V[5];
+  rc = host_to_dev3(h, x0, ld, u0, v0, h0);
+  if (!rc) rc = zero3(h, lam);
+  int t = obs_index(c, nsteps);
+  if (!rc && t >= 0) rc = obs_force(h, c, t, lam);
+  if (!rc) rc = reverse(h, c, 0, nsteps, x0, snaps, lam, dt);
+  if (!rc) rc = dev_to_host3(h, gu, gv, gh, ld, lam);
+  return rc ? rc : check_flag(h);
+}
+
+extern "C" int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long long *adj_steps) {
+  if (!h || !fwd_steps || !adj_steps) return fail(SPOC_E_ARG, "bad argument");
+  AdjCtx *c = ctx_of(h);
+  *fwd_steps = c->fwd_steps;
+  *adj_steps = c->adj_steps;
+  c->fwd_steps = c->adj_steps = 0;
+  return SPOC_OK;
 }

@@ -23,6 +23,8 @@ struct DevOps {
   int nc, nm, nmr, ng, ngf;
   const double *agx;    // [j*nm + i] = agx(j,i)
   const double *agy;    // [j*nm + i] = agy(j,i)
+  const double *agxN;   // [i*nm + j] = agx(j,i)  (non-transposed products, adjoint)
+  const double *agyN;   // [i*nm + j] = agy(j,i)
   const double *p2;     // [n*ng + q] = pi2(q,n)       (spectoxy)
   const double *p2t;    // [q*nm + n] = pi2(q,n)       (xytospec)
   const double *wi;     // [ng]

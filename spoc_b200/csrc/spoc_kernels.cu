@@ -623,6 +623,34 @@ cudaError_t launch_rhs(int variant, const DevOps &op, const DevMesh &m, const Rh
   return cudaGetLastError();
 }
 
+cudaError_t launch_qphase(int variant, const DevOps &op, const DevMesh &m, const double *su,
+                          const double *sv, double *q, cudaStream_t st, int sms) {
+  const int grid = grid_for(m.ne, sms);
+  switch (variant) {
+    case kFS: k_qphase<kFS><<<grid, kThreads, 0, st>>>(op, m, su, sv, q); break;
+    case kNS: k_qphase<kNS><<<grid, kThreads, 0, st>>>(op, m, su, sv, q); break;
+    default: k_qphase<kINV><<<grid, kThreads, 0, st>>>(op, m, su, sv, q); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tend(int variant, const DevOps &op, const DevMesh &m, const TendArgs &ta,
+                        const StageArgs &sa, cudaStream_t st, int sms) {
+  const int grid = grid_for(m.ne, sms);
+  switch (variant) {
+    case kFS: k_tend<kFS><<<grid, kThreads, 0, st>>>(op, m, ta, sa); break;
+    case kNS: k_tend<kNS><<<grid, kThreads, 0, st>>>(op, m, ta, sa); break;
+    default: k_tend<kINV><<<grid, kThreads, 0, st>>>(op, m, ta, sa); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lin(const DevOps &op, const DevMesh &m, const LinArgs &la, const StageArgs &sa,
+                       cudaStream_t st, int sms) {
+  k_lin<<<grid_for(m.ne, sms), kThreads, 0, st>>>(op, m, la, sa);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_energy(const DevOps &op, const DevMesh &m, const double *su, const double *sv,
                           const double *sh, const double *hb, double g0, double *terms,
                           double *out, cudaStream_t st, int sms, long long *launches) {

@@ -35,6 +35,49 @@ struct LinArgs {
   double g0, hh0;
 };
 
+// Tangent-linear quadrature-point stage: base state (su.., q) and perturbation
+// (du, dv, dh, dq) in; perturbations of gx0, gy0, uh, vh, F out.
+struct TlmArgs {
+  const double *su, *sv, *sh, *hb, *w0, *z0, *fc, *q;
+  const double *du, *dv, *dh, *dq;
+  double *gx0, *gy0, *uh, *vh, *f;
+  double mu0, mb0, g0;
+};
+
+// Adjoint of the tendency stage: adjoints (bu, bv, bh) of the tendencies in;
+// adjoints of gx0, gy0, F (4 fields), uh, vh out; side-lift scratch lx, ly, lh
+// (ne*3*ngf each).
+struct AdjTendArgs {
+  const double *bu, *bv, *bh;
+  double *gx0b, *gy0b, *fb, *uhb, *vhb;
+  double *lx, *ly, *lh;
+};
+
+// Adjoint of the quadrature-point stage: base state and the adjoints from the
+// tendency stage in; adjoints of u, v, h (written) and q (4 fields) out.
+struct AdjNlArgs {
+  const double *su, *sv, *sh, *hb, *w0, *z0, *fc, *q;
+  const double *fb, *gx0b, *gy0b, *uhb, *vhb;
+  double *ub, *vb, *hbo, *qb;
+  double mu0, mb0, g0;
+};
+
+// Adjoint of the q-phase: adjoint of q in; adjoints of u, v accumulated;
+// side-lift scratch lq (4 * ne*3*ngf).
+struct AdjQArgs {
+  const double *qb;
+  double *ub, *vb;
+  double *lq;
+};
+
+// Adjoint of the linear variant.
+struct AdjLinArgs {
+  const double *bu, *bv, *bh;
+  double *ub, *vb, *hbo;
+  double *lx, *ly, *lh;
+  double g0, hh0;
+};
+
 struct RhsBuffers {
   const double *su, *sv, *sh;          // stage input
   const double *hb, *w0, *z0, *fc;     // time-constant fields
@@ -45,12 +88,38 @@ struct RhsBuffers {
 cudaError_t launch_rhs(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
                        const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
                        cudaEvent_t *ev = nullptr);
+// Single generic kernels (the tangent-linear model reuses them: the q-phase,
+// the tendency kernel and the linear kernel are linear in their inputs).
+cudaError_t launch_qphase(int variant, const DevOps &op, const DevMesh &m, const double *su,
+                          const double *sv, double *q, cudaStream_t st, int sms);
+cudaError_t launch_tend(int variant, const DevOps &op, const DevMesh &m, const TendArgs &ta,
+                        const StageArgs &sa, cudaStream_t st, int sms);
+cudaError_t launch_lin(const DevOps &op, const DevMesh &m, const LinArgs &la, const StageArgs &sa,
+                       cudaStream_t st, int sms);
+
 cudaError_t launch_energy(const DevOps &op, const DevMesh &m, const double *su, const double *sv,
                           const double *sh, const double *hb, double g0, double *terms,
                           double *out, cudaStream_t st, int sms, long long *launches);
 cudaError_t launch_cfl(int ne, int nc, const int *in, const double *xg, const double *yg,
                        const double *hb, int nm, double g0, unsigned long long *out,
                        cudaStream_t st, int sms, long long *launches);
+
+// Tangent-linear and adjoint kernels (spoc_adjoint.cu).
+cudaError_t launch_nlvol_tlm(int variant, const DevOps &op, const DevMesh &m, const TlmArgs &a,
+                             cudaStream_t st, int sms);
+cudaError_t launch_adj_nl(int variant, const DevOps &op, const DevMesh &m, const AdjTendArgs &ta,
+                          const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int sms);
+cudaError_t launch_adj_lin(const DevOps &op, const DevMesh &m, const AdjLinArgs &a,
+                           cudaStream_t st, int sms);
+cudaError_t launch_axpy(size_t n, const double *x, double c, const double *y, double *out,
+                        cudaStream_t st, int sms);
+cudaError_t launch_axpby(size_t n, double a, const double *x, double b, const double *y,
+                         double *out, cudaStream_t st, int sms);
+cudaError_t launch_obs_eval(int nobs, int nm, const int *elem, const double *basis,
+                            const double *h, double *val, cudaStream_t st);
+cudaError_t launch_obs_adj(int nel, int nm, const int *el_list, const int *el_start,
+                           const int *obs_of, const double *basis, const double *resid, double *hb,
+                           cudaStream_t st);
 
 // Compile-time-sized kernels (spoc_fast.cu) for the tabulated degree /
 // quadrature combinations; identical results to launch_rhs.

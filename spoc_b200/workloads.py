@@ -227,3 +227,52 @@ def make_solver(p: Problem, precision: str = "fp64") -> api.Solver:
     s = api.Solver(p.T, p.mesh, p.cfg.variant, precision)
     s.set_params(p.cfg.mu0, p.cfg.mb0, p.cfg.g0, p.hb, p.fc, p.w0, p.z0)
     return s
+
+
+def locate(mesh: api.Mesh, px: np.ndarray, py: np.ndarray):
+    """Element (1-based) and reference coordinates (xi, eta) of each point.
+
+    The element map is x = x1 + ax (xi + 1) + bx (eta + 1) (src/shwwnl.f:384-397,
+    src/init.f:330-331); a point belongs to the first element whose reference
+    coordinates lie in the triangle xi, eta >= -1, xi + eta <= 0.
+    """
+    inn = mesh.inn - 1
+    x1, y1 = mesh.xgr[inn[:, 0]], mesh.ygr[inn[:, 0]]
+    ax, bx, ay, by, detai = (mesh.vect[:, k] for k in range(5))
+    elem = np.zeros(px.size, dtype=np.int32)
+    xi = np.zeros(px.size)
+    eta = np.zeros(px.size)
+    for o, (x, y) in enumerate(zip(px, py)):
+        dx, dy = x - x1, y - y1
+        s = (by * dx - bx * dy) * detai - 1.0
+        t = (-ay * dx + ax * dy) * detai - 1.0
+        inside = (s >= -1 - 1e-12) & (t >= -1 - 1e-12) & (s + t <= 1e-12)
+        k = int(np.argmax(inside))
+        if not inside[k]:
+            raise ValueError(f"point {o} ({x}, {y}) is outside the mesh")
+        elem[o], xi[o], eta[o] = k + 1, s[k], t[k]
+    return elem, xi, eta
+
+
+def basis_at(nc: int, xi: np.ndarray, eta: np.ndarray) -> np.ndarray:
+    """phi_n(xi, eta) = P_k1(xi) P_k2(eta), modes kc1 outer, kc2 inner (src/nonlin.f:325-331)."""
+    from numpy.polynomial import legendre as L
+    cols = []
+    for a in range(nc + 1):
+        for b in range(nc + 1 - a):
+            ca = np.zeros(a + 1)
+            ca[a] = 1
+            cb = np.zeros(b + 1)
+            cb[b] = 1
+            cols.append(L.legval(xi, ca) * L.legval(eta, cb))
+    return np.stack(cols, axis=1)
+
+
+def random_observations(p: Problem, nobs: int, seed: int):
+    """nobs points uniform in the basin (seeded), with their elements and basis values."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    L = p.cfg.length
+    px = rng.uniform(-0.5 * L, 0.5 * L, nobs)
+    py = rng.uniform(-0.5 * L, 0.5 * L, nobs)
+    elem, xi, eta = locate(p.mesh, px, py)
+    return elem, basis_at(p.cfg.nc, xi, eta), px, py
