@@ -50,6 +50,10 @@ extern "C" {
 #define SPOC_FP64_FMA 1 /* reference order with fused multiply-adds in the contractions and
                            solves: FP64 accuracy, not bit-exact; untabulated (nc, ng, ngf)
                            run the SPOC_FP64 kernels */
+#define SPOC_MIXED 2    /* FP32 contractions in the orthonormal basis psi = U^-T phi
+                           (amm = U^T U), FP64 RK4 state and basis changes; tabulated
+                           (nc, ng, ngf) only.  State, inputs and outputs stay in the
+                           reference basis at the ABI. */
 
 /* COMMON-block content, as the Fortran driver holds it (src/shwwnl.f:60-71).
  * amm and amml hold the upper Cholesky factors (src/shwwnl.f:153-156). */

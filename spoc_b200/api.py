@@ -28,7 +28,8 @@ LIN, FS, NS, INV = 0, 1, 2, 3
 VARIANTS = {"lin": LIN, "fs": FS, "ns": NS, "inv": INV}
 FP64 = 0
 FP64_FMA = 1
-PRECISIONS = {"fp64": FP64, "fp64_fma": FP64_FMA}
+MIXED = 2  # FP32 contractions in the orthonormal basis, FP64 RK4 state
+PRECISIONS = {"fp64": FP64, "fp64_fma": FP64_FMA, "mixed": MIXED}
 
 _STATUS = {
     0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-finite tendency",

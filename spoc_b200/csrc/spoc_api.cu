@@ -13,6 +13,7 @@
 
 #include "../../include/spoc_gpu.h"
 #include "spoc_kernels.h"
+#include "spoc_mixed.h"
 
 using namespace spoc;
 
@@ -65,6 +66,7 @@ struct spoc_handle {
   double *eterms = nullptr, *escal = nullptr;
   int *flag = nullptr;
   unsigned long long *cflbits = nullptr;
+  MixedCtx *mx = nullptr;  // SPOC_MIXED: the resident state lives here (psi basis)
 
   template <class T>
   cudaError_t alloc(T **p, size_t n) {
@@ -81,6 +83,7 @@ struct spoc_handle {
     return e;
   }
   ~spoc_handle() {
+    if (mx) mixed_destroy(mx);
     for (void *p : allocs) cudaFree(p);
     if (own) cudaStreamDestroy(own);
   }
@@ -286,6 +289,10 @@ int check_flag(spoc_handle *h) {
 }
 
 int run_rhs_tend(spoc_handle *h, double *const s[3]) {
+  if (h->mx) {
+    CK(mixed_rhs(h->mx, h->mesh, s, h->TEND, h->flag, h->st, &h->launches), "mixed cal_var");
+    return SPOC_OK;
+  }
   StageArgs sa{};
   sa.stage = -1;
   for (int c = 0; c < 3; ++c) sa.tend[c] = h->TEND[c];
@@ -304,7 +311,7 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
   *out = nullptr;
   if (!t || !m) return fail(SPOC_E_ARG, "tables or mesh is null");
   if (variant < SPOC_LIN || variant > SPOC_INV) return fail(SPOC_E_ARG, "unknown variant");
-  if (precision != SPOC_FP64 && precision != SPOC_FP64_FMA)
+  if (precision != SPOC_FP64 && precision != SPOC_FP64_FMA && precision != SPOC_MIXED)
     return fail(SPOC_E_UNSUPPORTED, "precision mode not built");
   const int nc = t->nc, nm = (nc + 1) * (nc + 2) / 2;
   if (nc < 1 || t->nm != nm) return fail(SPOC_E_ARG, "nm != (nc+1)(nc+2)/2");
@@ -381,6 +388,16 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
     if (ce != cudaSuccess) rc = fail(ce == cudaErrorMemoryAllocation ? SPOC_E_NOMEM : SPOC_E_CUDA, "device allocation", ce);
   }
+  if (!rc && precision == SPOC_MIXED) {
+    std::string err;
+    rc = mixed_create(&h->mx, t, variant, h->ne, h->sms, &err);
+    if (rc) rc = fail(rc, err.c_str());
+    if (!rc) {
+      ce = mixed_set_state(h->mx, h->mesh, h->U0, h->st, &h->launches);
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+      if (ce != cudaSuccess) rc = fail(SPOC_E_CUDA, "mixed-precision set-up", ce);
+    }
+  }
   if (rc) {
     delete h;
     return rc;
@@ -428,6 +445,16 @@ extern "C" int spoc_set_params(spoc_handle *h, const spoc_params *p) {
   else CK(cudaMemsetAsync(h->z0, 0, sizeof(double) * n, h->st), "zero z0");
   if (p->fc) CK(copy_in(h, h->fc, p->fc, p->ld, cudaMemcpyHostToDevice), "upload fc");
   else CK(cudaMemsetAsync(h->fc, 0, sizeof(double) * n, h->st), "zero fc");
+  if (h->mx) {
+    bool zero = true;
+    for (const double *w : {p->w0, p->z0})
+      if (w)
+        for (int e = 0; e < h->ne && zero; ++e)
+          for (int i = 0; i < h->nm && zero; ++i) zero = w[(size_t)e * p->ld + i] == 0.0;
+    CK(mixed_set_params(h->mx, h->op, h->hb, h->fc, h->w0, h->z0, zero, h->mu0, h->mb0, h->g0,
+                        h->hh0, h->st),
+       "mixed-precision parameters");
+  }
   CK(cudaStreamSynchronize(h->st), "synchronize");
   h->have_params = true;
   return SPOC_OK;
@@ -471,12 +498,14 @@ extern "C" int spoc_set_state(spoc_handle *h, int ld, const double *u, const dou
   CK(copy_in(h, h->U0[0], u, ld, cudaMemcpyHostToDevice), "upload u");
   CK(copy_in(h, h->U0[1], v, ld, cudaMemcpyHostToDevice), "upload v");
   CK(copy_in(h, h->U0[2], hh, ld, cudaMemcpyHostToDevice), "upload h");
+  if (h->mx) CK(mixed_set_state(h->mx, h->mesh, h->U0, h->st, &h->launches), "mixed state");
   CK(cudaStreamSynchronize(h->st), "synchronize");
   return SPOC_OK;
 }
 
 extern "C" int spoc_get_state(spoc_handle *h, int ld, double *u, double *v, double *hh) {
   if (!h || !u || !v || !hh || ld < (h ? h->nm : 1)) return fail(SPOC_E_ARG, "bad argument");
+  if (h->mx) CK(mixed_get_state(h->mx, h->U0, h->st, &h->launches), "mixed state");
   CK(copy_out(h, u, h->U0[0], ld, cudaMemcpyDeviceToHost), "download u");
   CK(copy_out(h, v, h->U0[1], ld, cudaMemcpyDeviceToHost), "download v");
   CK(copy_out(h, hh, h->U0[2], ld, cudaMemcpyDeviceToHost), "download h");
@@ -485,7 +514,9 @@ extern "C" int spoc_get_state(spoc_handle *h, int ld, double *u, double *v, doub
 }
 
 namespace {
-int enqueue_steps(spoc_handle *h, double dt, int nsteps) {
+// RK4 steps of the FP64 kernels on U0 (also used by the adjoint, which stays
+// FP64 whatever the handle's precision).
+int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps) {
   StageArgs sa{};
   sa.dt = dt;
   sa.dt6 = dt / 6.0;  // dt / 6.d0 (src/shwwnl.f:277)
@@ -505,6 +536,14 @@ int enqueue_steps(spoc_handle *h, double dt, int nsteps) {
   }
   return SPOC_OK;
 }
+
+int enqueue_steps(spoc_handle *h, double dt, int nsteps) {
+  if (h->mx) {
+    CK(mixed_steps(h->mx, h->mesh, dt, nsteps, h->flag, h->st, &h->launches), "mixed RK4 steps");
+    return SPOC_OK;
+  }
+  return enqueue_steps_fp64(h, dt, nsteps);
+}
 }  // namespace
 
 extern "C" int spoc_rk4_steps(spoc_handle *h, double dt, int nsteps) {
@@ -523,8 +562,10 @@ extern "C" int spoc_rk4_steps_host(spoc_handle *h, int ld, double *u, double *v,
   CK(copy_in(h, h->U0[0], u, ld, cudaMemcpyHostToDevice), "upload u");
   CK(copy_in(h, h->U0[1], v, ld, cudaMemcpyHostToDevice), "upload v");
   CK(copy_in(h, h->U0[2], hh, ld, cudaMemcpyHostToDevice), "upload h");
+  if (h->mx) CK(mixed_set_state(h->mx, h->mesh, h->U0, h->st, &h->launches), "mixed state");
   int rc = enqueue_steps(h, dt, nsteps);
   if (rc) return rc;
+  if (h->mx) CK(mixed_get_state(h->mx, h->U0, h->st, &h->launches), "mixed state");
   CK(copy_out(h, u, h->U0[0], ld, cudaMemcpyDeviceToHost), "download u");
   CK(copy_out(h, v, h->U0[1], ld, cudaMemcpyDeviceToHost), "download v");
   CK(copy_out(h, hh, h->U0[2], ld, cudaMemcpyDeviceToHost), "download h");
@@ -533,6 +574,7 @@ extern "C" int spoc_rk4_steps_host(spoc_handle *h, int ld, double *u, double *v,
 
 extern "C" int spoc_energy(spoc_handle *h, double *ke, double *pe, double *mass) {
   if (!h || !ke || !pe || !mass) return fail(SPOC_E_ARG, "null argument");
+  if (h->mx) CK(mixed_get_state(h->mx, h->U0, h->st, &h->launches), "mixed state");
   CK(launch_energy(h->op, h->mesh, h->U0[0], h->U0[1], h->U0[2], h->hb, h->g0, h->eterms,
                    h->escal, h->st, h->sms, &h->launches),
      "launch energy");
@@ -588,6 +630,27 @@ extern "C" int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *k
                                 int *nkinds) {
   if (!h || nsteps < 1 || !kernel_ms || !nkinds) return fail(SPOC_E_ARG, "bad argument");
   if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  if (h->mx) {
+    // per-kernel time of the first stage of each step, scaled to the 4 stages
+    const int nk = mixed_kernels_per_rhs(h->mx);
+    cudaEvent_t ev[4];
+    for (int i = 0; i < 4; ++i) CK(cudaEventCreate(&ev[i]), "event");
+    for (int k = 0; k < nk; ++k) kernel_ms[k] = 0.0;
+    cudaError_t ce = cudaSuccess;
+    for (int it = 0; it < nsteps && ce == cudaSuccess; ++it) {
+      ce = mixed_steps(h->mx, h->mesh, dt, 1, h->flag, h->st, &h->launches, ev);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[nk]);
+      for (int k = 0; k < nk && ce == cudaSuccess; ++k) {
+        float ms = 0.f;
+        ce = cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        kernel_ms[k] += 4.0 * ms;
+      }
+    }
+    for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+    *nkinds = nk;
+    if (ce != cudaSuccess) return fail(SPOC_E_CUDA, "profile", ce);
+    return check_flag(h);
+  }
   const int nk = h->variant == SPOC_LIN ? 1 : 3;
   cudaEvent_t ev[4];
   for (int i = 0; i < 4; ++i) CK(cudaEventCreate(&ev[i]), "event");
@@ -939,7 +1002,7 @@ int advance(spoc_handle *h, AdjCtx *c, double *const x[3], double dt, int nsteps
   if (nsteps <= 0) return SPOC_OK;
   int rc = copy3(h, h->U0, x);
   if (rc) return rc;
-  if ((rc = enqueue_steps(h, dt, nsteps))) return rc;
+  if ((rc = enqueue_steps_fp64(h, dt, nsteps))) return rc;
   c->fwd_steps += nsteps;
   return copy3(h, x, h->U0);
 }

@@ -1,0 +1,1125 @@
+// Mixed-precision form of the RK4 DG shallow-water right-hand side.
+//
+// Basis.  The reference expands each field in phi = P_k1(x) P_k2(y) (mode
+// order of src/mat1.f) and solves with the Cholesky factor U of the mass
+// matrix amm = U^T U (src/shwwnl.f:153-156, DTRSM4 src/dtrsm1.f:47-82).  Here
+// the contractions use psi = U^-T phi, which is orthonormal on the reference
+// triangle.  With c = U a the psi coefficients of a field and b_psi = U^-T b
+// the psi load vector of a load vector b:
+//   * a mass solve a = amm^-1 b becomes c = b_psi (no work);
+//   * cal_b (b += coeff agx^T a, src/calb2.f:3-24) becomes b_psi += coeff GX c
+//     with GX = U^-T agx^T U^-1 (likewise GY);
+//   * spectoxy / xytospec (src/nonlin.f:35-107) become Pp = pi2 U^-1 and
+//     Pp^T diag(wi);
+//   * the face trace of cal_flu (src/calflu.f:6-71) and the lift of tri_f
+//     (src/mat1.f:172-209) become TR_s = pico(.,.,s) U^-1 and TR_s^T;
+//   * the wall solve reduc_gn -> amml solve -> reduc_inv_gn
+//     (src/mat1.f:418-473, amml = R^T amm R with R the map of reduc_inv_gn)
+//     becomes the orthogonal projector onto span(U R).
+// All of these are well conditioned, so FP32 contractions keep FP32 accuracy;
+// in the reference basis the mass solves amplify contraction rounding by up to
+// cond(amm) (2.1e8 at degree 6).  The RK4 state (psi coefficients) and its
+// accumulation stay FP64 (src/shwwnl.f:242-284); the conversions between the
+// bases are FP64.
+//
+// Kernels (one warp per element, lanes over modes, quadrature points or the
+// 3*ngf face points; operators staged in shared memory per persistent block):
+//   kx_vol<VAR>  nonlinear variants, phases A, B and the volume parts of C, D
+//                of calvarnl_*.f (q, quadrature products, F and h volume
+//                terms), writing partial load vectors and the face traces of
+//                q, uh, vh;
+//   kx_tend<VAR> face lifts of phases C, D, wall projections, RK4 update in
+//                FP64, and the face traces of the next stage input;
+//   kx_lin       calvar_lin.f in one kernel.
+// Face values are the central averages of cal_flu, formed from traces that
+// each element writes for its own three sides (no face arrays).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "spoc_mixed.h"
+
+namespace spoc {
+
+namespace {
+
+constexpr int kMxWarps = 8;  // warps (elements in flight) per block
+
+template <int NC_, int Q_, int G_>
+struct MDims {
+  static constexpr int N = (NC_ + 1) * (NC_ + 2) / 2;
+  static constexpr int Q = Q_;
+  static constexpr int G = G_;
+  static constexpr int TG = 3 * G_;
+  static constexpr int TS = TG + 1;  // trace record: TG mean-free traces + the mean
+  static constexpr int R = (N + 31) / 32;
+  // operator image in shared memory (floats)
+  static constexpr int PPT = 0;               // [n*Q + q]  = Pp(q, n)
+  static constexpr int PW = PPT + N * Q;      // [q*N + i]  = Pp(q, i) wi(q)
+  static constexpr int GX = PW + Q * N;       // [k*N + i]  = GX(i, k)
+  static constexpr int GY = GX + N * N;       // [k*N + i]  = GY(i, k)
+  static constexpr int TRT = GY + N * N;      // [n*TG + l] = TR(l, n), l = s*G + j
+  static constexpr int LIFT = TRT + N * TG;   // [l*N + i]  = TR(l, i)
+  static constexpr int PWALL = LIFT + TG * N; // [k*N + i]  = Pwall(i, k)
+  static constexpr int WIF = PWALL + N * N;   // [j] = wif(j)
+  static constexpr int NOPS = (WIF + G + 3) / 4 * 4;
+  // per-warp scratch (floats)
+  static constexpr int S_U = 0, S_V = N, S_H = 2 * N;
+  static constexpr int S_Q = 3 * N;           // qxx, qxy, qyx, qyy
+  static constexpr int S_VEC = 7 * N;         // six combined vectors
+  static constexpr int S_UH = 13 * N, S_VH = 14 * N, S_TMP = 15 * N;
+  static constexpr int S_GL = 16 * N;         // 4 face vectors of TG
+  static constexpr int S_QP = S_GL + 4 * TG;  // 7 quadrature vectors of Q
+  static constexpr int WS = (S_QP + 7 * Q + 3) / 4 * 4;
+  static_assert(TG <= 32, "face points of one element must fit one warp");
+  static_assert(N <= 64 && Q <= 64, "two rows per lane at most");
+};
+
+struct MxArgs {
+  int ne;
+  const float *ops;
+  DevMesh m;
+  const float *tr_in;  // [3][ne][TS] trace records of the stage input (u, v, h)
+  float *tr_out;       // [3][ne][TS] trace records of the next stage input
+  float *y;            // [3][ne][N] stage input (FP32); replaced by the next one
+  float *part;         // [3][ne][N] partial load vectors (u, v, h)
+  float *trq;          // [6][ne][TS] trace records of qxx, qxy, qyx, qyy, uh, vh
+  const float *hbq, *fcq, *w0q, *z0q;  // [ne][Q]; w0q / z0q null when zero
+  float mu0, mb0, g0, hh0;
+  int stage;           // 0..3 RK4 stage; -1: write the tendency to k64
+  double dt, dt6;
+  double *c64, *acc, *k64;  // [3][ne][N] psi coefficients, FP64
+  int *flag;
+};
+
+__device__ __forceinline__ float fma32(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+template <class Dm>
+__device__ void stage_mx_ops(float *s, const float *g) {
+  const float4 *src = reinterpret_cast<const float4 *>(g);
+  float4 *dst = reinterpret_cast<float4 *>(s);
+  for (int i = threadIdx.x; i < Dm::NOPS / 4; i += blockDim.x) dst[i] = src[i];
+}
+
+// The face of side k of element e as element e sees it.
+struct FaceRef {
+  int f, nb, s2;
+  float sig, nx, ny;  // sig = its * 0.5 (the tri_f factor); nx, ny = norm(., f)
+  bool wall;
+};
+
+__device__ __forceinline__ FaceRef face_ref(const DevMesh &m, int e, int k) {
+  FaceRef r;
+  r.f = m.itm[3 * e + k];
+  const int isg = m.its[3 * e + k];
+  const int t1 = m.tseg[2 * r.f], t2 = m.tseg[2 * r.f + 1];
+  r.nb = isg > 0 ? t2 : t1;
+  r.s2 = isg > 0 ? m.ssit[2 * r.f + 1] : m.ssit[2 * r.f];
+  r.wall = t2 < 0;
+  r.sig = isg > 0 ? 0.5f : -0.5f;
+  r.nx = (float)m.norm[2 * r.f];
+  r.ny = (float)m.norm[2 * r.f + 1];
+  return r;
+}
+
+// Trace records.  The weak derivative of a field F on an element,
+// -int F dpsi/dx + sum_faces int psi F* n_x, is a small difference of two large
+// terms when F has a large element mean m (Gauss's theorem makes the mean's two
+// contributions cancel exactly).  In FP32 that cancellation loses up to three
+// digits, so the mean is taken out of both terms: the volume contractions skip
+// the constant mode (psi_0 = const) and the face terms use F* - m.  A trace
+// record of an element holds, for each of its 3 x ngf face points, the trace
+// of F - m, followed by m itself.
+//
+// cal_flu central value minus the own mean, on the face seen from side k,
+// point j of element e: own trace and the neighbour's trace at the mirrored
+// point (src/calflu.f:45-62); a wall face keeps the own trace
+// (src/calflu.f:35-39).
+template <int G>
+__device__ __forceinline__ float face_value(const float *tr, const FaceRef &r, int e, int l, int j) {
+  constexpr int TG = 3 * G, TS = TG + 1;
+  const float own = tr[(size_t)e * TS + l];
+  if (r.wall) return own;
+  const float *nb = tr + (size_t)r.nb * TS;
+  return 0.5f * (own + nb[r.s2 * G + (G - 1 - j)] + (nb[TG] - tr[(size_t)e * TS + TG]));
+}
+
+// Trace record (mean-free traces, then the mean) of up to six fields held in
+// the warp's shared vectors x[f] (psi coefficients); written by lanes 0..TG.
+template <class Dm, int NF>
+__device__ __forceinline__ void write_traces(const float *o, const float *const (&x)[NF], float *out,
+                                             size_t stride, int e) {
+  constexpr int N = Dm::N, TG = Dm::TG, TS = Dm::TS;
+  const int lane = threadIdx.x & 31;
+  if (lane > TG) return;
+  float t[NF];
+  if (lane < TG) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) t[f] = 0.f;
+#pragma unroll 4
+    for (int n = 1; n < N; ++n) {
+      const float p = o[Dm::TRT + n * TG + lane];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) t[f] = fma32(p, x[f][n], t[f]);
+    }
+  } else {
+    const float p0 = o[Dm::TRT];  // psi_0, the constant mode's value
+#pragma unroll
+    for (int f = 0; f < NF; ++f) t[f] = p0 * x[f][0];
+  }
+  const size_t off = (size_t)e * TS + lane;
+#pragma unroll
+  for (int f = 0; f < NF; ++f) out[f * stride + off] = t[f];
+}
+
+// Orthogonal projection of the warp's vector x (shared, length N) onto the
+// wall-compatible subspace; lanes receive rows i = lane + 32 r.
+template <class Dm>
+__device__ __forceinline__ void project_rows(const float *o, const float *x, float (&out)[Dm::R]) {
+  constexpr int N = Dm::N;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int r = 0; r < Dm::R; ++r) {
+    const int i = lane + 32 * r;
+    float a = 0.f;
+    if (i < N) {
+#pragma unroll 4
+      for (int k = 0; k < N; ++k) a = fma32(o[Dm::PWALL + k * N + i], x[k], a);
+    }
+    out[r] = a;
+  }
+}
+
+// Wall solves of a vector tendency (gx, gy) in the psi basis.
+//  no-slip (calvarnl_ns.f:404-421): both components projected;
+//  free-slip / inviscid / linear (wall_solve_rot): normal component
+//  gn = nx gx + ny gy projected, tangential one untouched.
+template <class Dm, bool NOSLIP>
+__device__ void wall_vec(const float *o, float *tmp, float (&gx)[Dm::R], float (&gy)[Dm::R],
+                         float nx, float ny) {
+  constexpr int N = Dm::N;
+  const int lane = threadIdx.x & 31;
+  if (NOSLIP) {
+    float px[Dm::R], py[Dm::R];
+#pragma unroll
+    for (int r = 0; r < Dm::R; ++r)
+      if (lane + 32 * r < N) tmp[lane + 32 * r] = gx[r];
+    __syncwarp();
+    project_rows<Dm>(o, tmp, px);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < Dm::R; ++r)
+      if (lane + 32 * r < N) tmp[lane + 32 * r] = gy[r];
+    __syncwarp();
+    project_rows<Dm>(o, tmp, py);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < Dm::R; ++r) {
+      gx[r] = px[r];
+      gy[r] = py[r];
+    }
+  } else {
+    float gn[Dm::R], pg[Dm::R];
+#pragma unroll
+    for (int r = 0; r < Dm::R; ++r) {
+      gn[r] = nx * gx[r] + ny * gy[r];
+      if (lane + 32 * r < N) tmp[lane + 32 * r] = gn[r];
+    }
+    __syncwarp();
+    project_rows<Dm>(o, tmp, pg);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < Dm::R; ++r) {
+      const float d = pg[r] - gn[r];
+      gx[r] += nx * d;
+      gy[r] += ny * d;
+    }
+  }
+}
+
+// RK4 bookkeeping of src/shwwnl.f:242-284 on one psi coefficient, FP64;
+// returns the next stage input.
+__device__ __forceinline__ double rk4_update(const MxArgs &a, size_t i, double d) {
+  double *c = a.c64 + i, *acc = a.acc + i;
+  const double u0 = *c;
+  switch (a.stage) {
+    case 0: *acc = d; return u0 + a.dt * d * 0.5;
+    case 1: *acc = *acc + 2.0 * d; return u0 + a.dt * d * 0.5;
+    case 2: *acc = *acc + 2.0 * d; return u0 + a.dt * d;
+    default: {
+      const double u1 = u0 + a.dt6 * (*acc + d);
+      *c = u1;
+      return u1;
+    }
+  }
+}
+
+// Finishes an element: non-finite check, RK4 update (or tendency output),
+// next stage input and its traces.  t[3][R] holds the psi tendencies.
+template <class Dm>
+__device__ void finish_element(const MxArgs &a, const float *o, float *w, int e,
+                               float (&t)[3][Dm::R]) {
+  constexpr int N = Dm::N;
+  const int lane = threadIdx.x & 31;
+  const size_t fn = (size_t)a.ne * N;
+  bool bad = false;
+#pragma unroll
+  for (int f = 0; f < 3; ++f)
+#pragma unroll
+    for (int r = 0; r < Dm::R; ++r) {
+      const int i = lane + 32 * r;
+      if (i >= N) continue;
+      const float d = t[f][r];
+      bad |= !isfinite(d);
+      const size_t gi = f * fn + (size_t)e * N + i;
+      if (a.stage < 0) {
+        a.k64[gi] = (double)d;
+      } else {
+        const double yn = rk4_update(a, gi, (double)d);
+        const float y32 = (float)yn;
+        a.y[gi] = y32;
+        w[f * N + i] = y32;
+      }
+    }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flag, 1);
+  if (a.stage < 0) return;
+  __syncwarp();
+  const float *const x[3] = {w, w + N, w + 2 * N};
+  write_traces<Dm, 3>(o, x, a.tr_out, (size_t)a.ne * Dm::TS, e);
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Nonlinear variants: volume kernel (calvarnl_fs.f:88-332 and the volume terms
+// of :341-544).
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(32 * kMxWarps) kx_vol(const MxArgs a) {
+  constexpr int N = Dm::N, Q = Dm::Q, G = Dm::G, TG = Dm::TG, R = Dm::R;
+  extern __shared__ __align__(16) float sm[];
+  float *o = sm;
+  stage_mx_ops<Dm>(o, a.ops);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float *w = sm + Dm::NOPS + wib * Dm::WS;
+  float *su = w + Dm::S_U, *sv = w + Dm::S_V, *sh = w + Dm::S_H, *sq = w + Dm::S_Q;
+  float *vec = w + Dm::S_VEC, *suh = w + Dm::S_UH, *svh = w + Dm::S_VH, *tmp = w + Dm::S_TMP;
+  float *gl = w + Dm::S_GL, *qp = w + Dm::S_QP;
+  const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
+  const int stride = gridDim.x * kMxWarps;
+  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+    const double *vp = a.m.vect + 5 * (size_t)e;
+    const float ax = (float)vp[0], bx = (float)vp[1], ay = (float)vp[2], by = (float)vp[3],
+                di = (float)vp[4];
+    for (int i = lane; i < N; i += 32) {
+      const size_t gi = (size_t)e * N + i;
+      su[i] = a.y[gi];
+      sv[i] = a.y[fn + gi];
+      sh[i] = a.y[2 * fn + gi];
+    }
+    // face values of u and v, as lift inputs of the four q components
+    if (lane < TG) {
+      const int k = lane / G, j = lane - k * G;
+      const FaceRef r = face_ref(a.m, e, k);
+      const float fu = face_value<G>(a.tr_in, r, e, lane, j);
+      const float fv = face_value<G>(a.tr_in + tn, r, e, lane, j);
+      const float s = r.sig * di * o[Dm::WIF + (r.sig > 0.f ? j : G - 1 - j)];
+      gl[lane] = s * r.nx * fu;
+      gl[TG + lane] = s * r.ny * fu;
+      gl[2 * TG + lane] = s * r.nx * fv;
+      gl[3 * TG + lane] = s * r.ny * fv;
+    }
+    __syncwarp();
+    // u, v, h + hb at the quadrature points (spectoxy)
+    for (int q = lane; q < Q; q += 32) {
+      float U = 0.f, V = 0.f, H = 0.f;
+#pragma unroll 4
+      for (int n = 0; n < N; ++n) {
+        const float p = o[Dm::PPT + n * Q + q];
+        U = fma32(p, su[n], U);
+        V = fma32(p, sv[n], V);
+        H = fma32(p, sh[n], H);
+      }
+      qp[q] = U;
+      qp[Q + q] = V;
+      qp[2 * Q + q] = H + a.hbq[(size_t)e * Q + q];
+    }
+    // q = weak gradients of u, v (calvarnl_fs.f:115-164): cal_b with coeff -1,
+    // geometry, then tri_f of the traces; the mass solve is the identity
+    float qv[4][R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      float gxu = 0.f, gyu = 0.f, gxv = 0.f, gyv = 0.f;
+      float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
+      if (i < N) {
+#pragma unroll 4
+        for (int k = 1; k < N; ++k) {  // constant mode: see the trace records
+          const float cx = o[Dm::GX + k * N + i], cy = o[Dm::GY + k * N + i];
+          gxu = fma32(cx, su[k], gxu);
+          gyu = fma32(cy, su[k], gyu);
+          gxv = fma32(cx, sv[k], gxv);
+          gyv = fma32(cy, sv[k], gyv);
+        }
+#pragma unroll
+        for (int l = 0; l < TG; ++l) {
+          const float L = o[Dm::LIFT + l * N + i];
+          l0 = fma32(L, gl[l], l0);
+          l1 = fma32(L, gl[TG + l], l1);
+          l2 = fma32(L, gl[2 * TG + l], l2);
+          l3 = fma32(L, gl[3 * TG + l], l3);
+        }
+      }
+      qv[0][r] = (ay * gyu - by * gxu) * di + l0;
+      qv[1][r] = (bx * gxu - ax * gyu) * di + l1;
+      qv[2][r] = (ay * gyv - by * gxv) * di + l2;
+      qv[3][r] = (bx * gxv - ax * gyv) * di + l3;
+    }
+    if (VAR == SPOC_FS && a.m.bdl[e]) {
+      // calvarnl_fs.f:165-205: of the rotated tensor only the tangential-normal
+      // component gtn is solved in the wall sub-basis
+      const float nx = (float)a.m.normt[2 * (size_t)e], ny = (float)a.m.normt[2 * (size_t)e + 1];
+      float gtn[R], pg[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        gtn[r] = nx * ny * qv[0][r] - nx * nx * qv[2][r] + ny * ny * qv[1][r] - nx * ny * qv[3][r];
+        if (lane + 32 * r < N) tmp[lane + 32 * r] = gtn[r];
+      }
+      __syncwarp();
+      project_rows<Dm>(o, tmp, pg);
+      __syncwarp();
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const float d = pg[r] - gtn[r];
+        qv[0][r] += d * nx * ny;
+        qv[2][r] -= d * nx * nx;
+        qv[1][r] += d * ny * ny;
+        qv[3][r] -= d * nx * ny;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      if (i < N)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) sq[c * N + i] = qv[c][r];
+    }
+    __syncwarp();
+    // quadrature-point products (calvarnl_fs.f:243-332); xytospec is linear,
+    // so the four projections of -adu + w1, -adv + z1, uh, vh take combined
+    // integrands
+    for (int q = lane; q < Q; q += 32) {
+      float gxx = 0.f, gxy = 0.f, gyx = 0.f, gyy = 0.f;
+#pragma unroll 4
+      for (int n = 0; n < N; ++n) {
+        const float p = o[Dm::PPT + n * Q + q];
+        gxx = fma32(p, sq[n], gxx);
+        gxy = fma32(p, sq[N + n], gxy);
+        gyx = fma32(p, sq[2 * N + n], gyx);
+        gyy = fma32(p, sq[3 * N + n], gyy);
+      }
+      const float fc = a.fcq[(size_t)e * Q + q];
+      gxy -= fc;
+      gyx += fc;
+      const float U = qp[q], V = qp[Q + q], H = qp[2 * Q + q];
+      float wk = -a.mb0 * U, zk = -a.mb0 * V;
+      if (a.w0q) {
+        wk += a.w0q[(size_t)e * Q + q];
+        zk += a.z0q[(size_t)e * Q + q];
+      }
+      qp[3 * Q + q] = wk / H - (U * gxx + V * gxy);
+      qp[4 * Q + q] = zk / H - (U * gyx + V * gyy);
+      qp[5 * Q + q] = U * H;
+      qp[6 * Q + q] = V * H;
+    }
+    __syncwarp();
+    float bxr[R], byr[R], uh[R], vh[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+      if (i < N) {
+#pragma unroll 4
+        for (int q = 0; q < Q; ++q) {
+          const float p = o[Dm::PW + q * N + i];
+          s0 = fma32(p, qp[3 * Q + q], s0);
+          s1 = fma32(p, qp[4 * Q + q], s1);
+          s2 = fma32(p, qp[5 * Q + q], s2);
+          s3 = fma32(p, qp[6 * Q + q], s3);
+        }
+      }
+      bxr[r] = s0;
+      byr[r] = s1;
+      uh[r] = s2;
+      vh[r] = s3;
+    }
+    if (a.m.bdl[e]) {
+      // uh, vh wall solves (calvarnl_fs.f:333-340, calvarnl_ns.f:249-265)
+      const float nx = (float)a.m.normt[2 * (size_t)e], ny = (float)a.m.normt[2 * (size_t)e + 1];
+      wall_vec<Dm, VAR == SPOC_NS>(o, tmp, uh, vh, nx, ny);
+    }
+    // combined vectors of the cal_b chains: F = mu0 q - g0 h (phase C) and
+    // uh, vh (phase D)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      if (i >= N) continue;
+      const float hh = sh[i];
+      const float fxx = a.mu0 * sq[i] - a.g0 * hh, fxy = a.mu0 * sq[N + i];
+      const float fyx = a.mu0 * sq[2 * N + i], fyy = a.mu0 * sq[3 * N + i] - a.g0 * hh;
+      vec[i] = di * (bx * fxy - by * fxx);
+      vec[N + i] = di * (ay * fxx - ax * fxy);
+      vec[2 * N + i] = di * (bx * fyy - by * fyx);
+      vec[3 * N + i] = di * (ay * fyx - ax * fyy);
+      vec[4 * N + i] = di * (by * uh[r] - bx * vh[r]);
+      vec[5 * N + i] = di * (ax * vh[r] - ay * uh[r]);
+      suh[i] = uh[r];
+      svh[i] = vh[r];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      if (i >= N) continue;
+      float gx = bxr[r], gy = byr[r], hp = 0.f;
+#pragma unroll 4
+      for (int k = 1; k < N; ++k) {  // constant mode: see the trace records
+        const float cx = o[Dm::GX + k * N + i], cy = o[Dm::GY + k * N + i];
+        gx = fma32(cx, vec[k], gx);
+        gx = fma32(cy, vec[N + k], gx);
+        gy = fma32(cx, vec[2 * N + k], gy);
+        gy = fma32(cy, vec[3 * N + k], gy);
+        hp = fma32(cx, vec[4 * N + k], hp);
+        hp = fma32(cy, vec[5 * N + k], hp);
+      }
+      const size_t gi = (size_t)e * N + i;
+      a.part[gi] = gx;
+      a.part[fn + gi] = gy;
+      a.part[2 * fn + gi] = hp;
+    }
+    // trace records of q and uh, vh for the face terms of phases C and D
+    {
+      const float *const x[6] = {sq, sq + N, sq + 2 * N, sq + 3 * N, suh, svh};
+      write_traces<Dm, 6>(o, x, a.trq, tn, e);
+    }
+    __syncwarp();
+  }
+}
+
+// Nonlinear variants: face lifts of phases C and D (calvarnl_fs.f:350-544),
+// wall solves, RK4 update.
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(32 * kMxWarps) kx_tend(const MxArgs a) {
+  constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, R = Dm::R;
+  extern __shared__ __align__(16) float sm[];
+  float *o = sm;
+  stage_mx_ops<Dm>(o, a.ops);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float *w = sm + Dm::NOPS + wib * Dm::WS;
+  float *gl = w + Dm::S_GL, *tmp = w + Dm::S_TMP;
+  const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
+  const int stride = gridDim.x * kMxWarps;
+  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+    const float di = (float)a.m.vect[5 * (size_t)e + 4];
+    if (lane < TG) {
+      const int k = lane / G, j = lane - k * G;
+      const FaceRef r = face_ref(a.m, e, k);
+      const float fqxx = face_value<G>(a.trq, r, e, lane, j);
+      const float fqxy = face_value<G>(a.trq + tn, r, e, lane, j);
+      const float fqyx = face_value<G>(a.trq + 2 * tn, r, e, lane, j);
+      const float fqyy = face_value<G>(a.trq + 3 * tn, r, e, lane, j);
+      const float fuh = face_value<G>(a.trq + 4 * tn, r, e, lane, j);
+      const float fvh = face_value<G>(a.trq + 5 * tn, r, e, lane, j);
+      const float fh = face_value<G>(a.tr_in + 2 * tn, r, e, lane, j);
+      const float Fxx = a.mu0 * fqxx - a.g0 * fh, Fxy = a.mu0 * fqxy;
+      const float Fyx = a.mu0 * fqyx, Fyy = a.mu0 * fqyy - a.g0 * fh;
+      const float s = r.sig * di * o[Dm::WIF + (r.sig > 0.f ? j : G - 1 - j)];
+      gl[lane] = s * (r.nx * Fxx + r.ny * Fxy);
+      gl[TG + lane] = s * (r.nx * Fyx + r.ny * Fyy);
+      gl[2 * TG + lane] = -s * (r.nx * fuh + r.ny * fvh);
+    }
+    __syncwarp();
+    float t[3][R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      float gx = 0.f, gy = 0.f, hh = 0.f;
+      if (i < N) {
+        const size_t gi = (size_t)e * N + i;
+        gx = a.part[gi];
+        gy = a.part[fn + gi];
+        hh = a.part[2 * fn + gi];
+#pragma unroll
+        for (int l = 0; l < TG; ++l) {
+          const float L = o[Dm::LIFT + l * N + i];
+          gx = fma32(L, gl[l], gx);
+          gy = fma32(L, gl[TG + l], gy);
+          hh = fma32(L, gl[2 * TG + l], hh);
+        }
+      }
+      t[0][r] = gx;
+      t[1][r] = gy;
+      t[2][r] = hh;
+    }
+    if (a.m.bdl[e]) {
+      const float nx = (float)a.m.normt[2 * (size_t)e], ny = (float)a.m.normt[2 * (size_t)e + 1];
+      wall_vec<Dm, VAR == SPOC_NS>(o, tmp, t[0], t[1], nx, ny);
+    }
+    finish_element<Dm>(a, o, w, e, t);
+  }
+}
+
+// Linear variant (calvar_lin.f:7-287) in one kernel.
+template <class Dm>
+__global__ void __launch_bounds__(32 * kMxWarps) kx_lin(const MxArgs a) {
+  constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, R = Dm::R;
+  extern __shared__ __align__(16) float sm[];
+  float *o = sm;
+  stage_mx_ops<Dm>(o, a.ops);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float *w = sm + Dm::NOPS + wib * Dm::WS;
+  float *su = w + Dm::S_U, *sv = w + Dm::S_V, *sh = w + Dm::S_H;
+  float *gl = w + Dm::S_GL, *tmp = w + Dm::S_TMP;
+  const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
+  const int stride = gridDim.x * kMxWarps;
+  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+    const double *vp = a.m.vect + 5 * (size_t)e;
+    const float ax = (float)vp[0], bx = (float)vp[1], ay = (float)vp[2], by = (float)vp[3],
+                di = (float)vp[4];
+    for (int i = lane; i < N; i += 32) {
+      const size_t gi = (size_t)e * N + i;
+      su[i] = a.y[gi];
+      sv[i] = a.y[fn + gi];
+      sh[i] = a.y[2 * fn + gi];
+    }
+    if (lane < TG) {
+      const int k = lane / G, j = lane - k * G;
+      const FaceRef r = face_ref(a.m, e, k);
+      const float fu = face_value<G>(a.tr_in, r, e, lane, j);
+      const float fv = face_value<G>(a.tr_in + tn, r, e, lane, j);
+      const float fh = face_value<G>(a.tr_in + 2 * tn, r, e, lane, j);
+      const float s = r.sig * di * o[Dm::WIF + (r.sig > 0.f ? j : G - 1 - j)];
+      const float fxx = -a.g0 * fh;
+      gl[lane] = s * r.nx * fxx;
+      gl[TG + lane] = s * r.ny * fxx;
+      gl[2 * TG + lane] = -s * a.hh0 * (r.nx * fu + r.ny * fv);
+    }
+    __syncwarp();
+    float t[3][R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      float gxh = 0.f, gyh = 0.f, gxu = 0.f, gyu = 0.f, gxv = 0.f, gyv = 0.f;
+      float l0 = 0.f, l1 = 0.f, l2 = 0.f;
+      if (i < N) {
+#pragma unroll 4
+        for (int k = 1; k < N; ++k) {  // constant mode: see the trace records
+          const float cx = o[Dm::GX + k * N + i], cy = o[Dm::GY + k * N + i];
+          gxh = fma32(cx, sh[k], gxh);
+          gyh = fma32(cy, sh[k], gyh);
+          gxu = fma32(cx, su[k], gxu);
+          gyu = fma32(cy, su[k], gyu);
+          gxv = fma32(cx, sv[k], gxv);
+          gyv = fma32(cy, sv[k], gyv);
+        }
+#pragma unroll
+        for (int l = 0; l < TG; ++l) {
+          const float L = o[Dm::LIFT + l * N + i];
+          l0 = fma32(L, gl[l], l0);
+          l1 = fma32(L, gl[TG + l], l1);
+          l2 = fma32(L, gl[2 * TG + l], l2);
+        }
+      }
+      // fxx = fyy = -g0 h: gx = cal_b(agx, fxx, -by di) + cal_b(agy, fxx, ay di) + lift
+      t[0][r] = -a.g0 * di * (ay * gyh - by * gxh) + l0;
+      t[1][r] = -a.g0 * di * (bx * gxh - ax * gyh) + l1;
+      t[2][r] = a.hh0 * di * (by * gxu - ay * gyu - bx * gxv + ax * gyv) + l2;
+    }
+    if (a.m.bdl[e]) {
+      const float nx = (float)a.m.normt[2 * (size_t)e], ny = (float)a.m.normt[2 * (size_t)e + 1];
+      wall_vec<Dm, false>(o, tmp, t[0], t[1], nx, ny);
+    }
+    __syncwarp();
+    finish_element<Dm>(a, o, w, e, t);
+  }
+}
+
+// Stage input and its traces from the FP64 psi state.
+template <class Dm>
+__global__ void __launch_bounds__(32 * kMxWarps) kx_prep(const MxArgs a) {
+  constexpr int N = Dm::N;
+  extern __shared__ __align__(16) float sm[];
+  float *o = sm;
+  stage_mx_ops<Dm>(o, a.ops);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float *w = sm + Dm::NOPS + wib * Dm::WS;
+  const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
+  const int stride = gridDim.x * kMxWarps;
+  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+    for (int f = 0; f < 3; ++f)
+      for (int i = lane; i < N; i += 32) {
+        const size_t gi = f * fn + (size_t)e * N + i;
+        const float v = (float)a.c64[gi];
+        a.y[gi] = v;
+        w[f * N + i] = v;
+      }
+    __syncwarp();
+    const float *const x[3] = {w, w + N, w + 2 * N};
+    write_traces<Dm, 3>(o, x, a.tr_out, tn, e);
+    __syncwarp();
+  }
+}
+
+// FP64 basis changes: out = T x per element with T upper triangular (row-major).
+__global__ void kx_upper(int ne, int n, const double *T, const double *x, double *out) {
+  const size_t total = (size_t)ne * n;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = t / n;
+    const int i = (int)(t - e * n);
+    const double *xe = x + e * n;
+    double s = 0.0;
+    for (int k = i; k < n; ++k) s += T[i * n + k] * xe[k];
+    out[t] = s;
+  }
+}
+
+// Values of a reference-basis field at the quadrature points (spectoxy), FP64
+// sum, stored as FP32: out[e*ng + q] = sum_n pi2(q, n) x[e*nm + n].
+__global__ void kx_quad(int ne, int nm, int ng, const double *p2, const double *x, float *out) {
+  const size_t total = (size_t)ne * ng;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = t / ng;
+    const int q = (int)(t - e * ng);
+    double s = 0.0;
+    for (int n = 0; n < nm; ++n) s += p2[(size_t)n * ng + q] * x[e * nm + n];
+    out[t] = (float)s;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct MixedCtx {
+  int variant = 0, nc = 0, N = 0, Q = 0, G = 0, ne = 0, sms = 148;
+  int cur = 0;  // which trace buffer holds the traces of the current stage input
+  bool w0z0 = false;
+  float mu0 = 0, mb0 = 0, g0 = 0, hh0 = 0;
+  std::vector<void *> allocs;
+  float *ops = nullptr;
+  double *U = nullptr, *Ui = nullptr;
+  double *c64 = nullptr, *acc = nullptr, *k64 = nullptr, *cin = nullptr;
+  float *y = nullptr, *tr[2]{}, *part = nullptr, *trq = nullptr;
+  float *hbq = nullptr, *fcq = nullptr, *w0q = nullptr, *z0q = nullptr;
+  template <class T>
+  cudaError_t alloc(T **p, size_t n) {
+    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
+    if (e == cudaSuccess) allocs.push_back((void *)*p);
+    return e;
+  }
+  ~MixedCtx() {
+    for (void *p : allocs) cudaFree(p);
+  }
+};
+
+namespace {
+
+// Host construction of the psi-basis operators, FP64.
+struct PsiOps {
+  int N, Q, G;
+  std::vector<double> U, Ui, Pp, GX, GY, TR, PWALL;
+};
+
+bool build_psi(const spoc_tables *t, PsiOps &p, std::string *err) {
+  const int nc = t->nc, N = t->nm, Q = t->ng, G = t->ngf, NR = N - nc - 1;
+  const int lm = t->ld_mat, lq = t->ld_pi2, lp1 = t->ld_pico1, lp2 = t->ld_pico2;
+  auto MAT = [&](const double *a, int i, int j) { return a[(size_t)j * lm + i]; };  // a(i,j)
+  p.N = N;
+  p.Q = Q;
+  p.G = G;
+  p.U.assign(N * N, 0.0);
+  p.Ui.assign(N * N, 0.0);
+  for (int i = 0; i < N; ++i)
+    for (int k = i; k < N; ++k) p.U[i * N + k] = MAT(t->amm, i, k);
+  // U^-1 by back substitution, column by column
+  for (int c = 0; c < N; ++c)
+    for (int i = N - 1; i >= 0; --i) {
+      double s = i == c ? 1.0 : 0.0;
+      for (int k = i + 1; k < N; ++k) s -= p.U[i * N + k] * p.Ui[k * N + c];
+      p.Ui[i * N + c] = s / p.U[i * N + i];
+    }
+  p.Pp.assign(Q * N, 0.0);
+  for (int q = 0; q < Q; ++q)
+    for (int n = 0; n < N; ++n) {
+      double s = 0.0;
+      for (int m = 0; m <= n; ++m) s += t->pi2[(size_t)m * lq + q] * p.Ui[m * N + n];
+      p.Pp[q * N + n] = s;
+    }
+  // GX = U^-T A U^-1 with A(i, j) = agx(j, i): cal_b adds coeff * sum_j agx(j,i) a_j
+  auto conj = [&](const double *ag, std::vector<double> &out) {
+    std::vector<double> tmp(N * N, 0.0);
+    for (int i = 0; i < N; ++i)
+      for (int n = 0; n < N; ++n) {
+        double s = 0.0;
+        for (int j = 0; j <= n; ++j) s += MAT(ag, j, i) * p.Ui[j * N + n];
+        tmp[i * N + n] = s;
+      }
+    out.assign(N * N, 0.0);
+    for (int m = 0; m < N; ++m)
+      for (int n = 0; n < N; ++n) {
+        double s = 0.0;
+        for (int i = 0; i <= m; ++i) s += p.Ui[i * N + m] * tmp[i * N + n];
+        out[m * N + n] = s;
+      }
+  };
+  conj(t->agx, p.GX);
+  conj(t->agy, p.GY);
+  p.TR.assign(3 * G * N, 0.0);
+  for (int s = 0; s < 3; ++s)
+    for (int j = 0; j < G; ++j)
+      for (int n = 0; n < N; ++n) {
+        double acc = 0.0;
+        for (int m = 0; m <= n; ++m)
+          acc += t->pico[((size_t)s * lp2 + m) * lp1 + j] * p.Ui[m * N + n];
+        p.TR[(s * G + j) * N + n] = acc;
+      }
+  // wall sub-basis: R = matrix of reduc_inv_gn (src/mat1.f:445-473), columns
+  // mapped to psi and orthonormalised (modified Gram-Schmidt, two passes)
+  std::vector<double> R(N * NR, 0.0);
+  for (int j = 0; j <= nc - 1; ++j) {
+    const int c1 = t->cip[2 * j], c2 = t->cip[2 * j + 1];
+    for (int l = 0; l <= nc - j - 1; ++l) {
+      const int r = c2 + l;
+      if (r < 0 || r >= NR || c1 < 0 || c1 + l + 1 >= N) {
+        if (err) *err = "cip table inconsistent with nc";
+        return false;
+      }
+      R[c1 * NR + r] = (l % 2 == 0) ? 1.0 : -1.0;
+      R[(c1 + l + 1) * NR + r] = 1.0;
+    }
+  }
+  std::vector<double> B(N * NR, 0.0);  // U R
+  for (int i = 0; i < N; ++i)
+    for (int r = 0; r < NR; ++r) {
+      double s = 0.0;
+      for (int k = i; k < N; ++k) s += p.U[i * N + k] * R[k * NR + r];
+      B[i * NR + r] = s;
+    }
+  for (int r = 0; r < NR; ++r) {
+    for (int pass = 0; pass < 2; ++pass)
+      for (int r2 = 0; r2 < r; ++r2) {
+        double d = 0.0;
+        for (int i = 0; i < N; ++i) d += B[i * NR + r] * B[i * NR + r2];
+        for (int i = 0; i < N; ++i) B[i * NR + r] -= d * B[i * NR + r2];
+      }
+    double nrm = 0.0;
+    for (int i = 0; i < N; ++i) nrm += B[i * NR + r] * B[i * NR + r];
+    nrm = std::sqrt(nrm);
+    if (!(nrm > 0.0)) {
+      if (err) *err = "wall sub-basis is rank deficient";
+      return false;
+    }
+    for (int i = 0; i < N; ++i) B[i * NR + r] /= nrm;
+  }
+  p.PWALL.assign(N * N, 0.0);
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < N; ++k) {
+      double s = 0.0;
+      for (int r = 0; r < NR; ++r) s += B[i * NR + r] * B[k * NR + r];
+      p.PWALL[i * N + k] = s;
+    }
+  return true;
+}
+
+template <class Dm>
+std::vector<float> ops_image(const PsiOps &p, const spoc_tables *t) {
+  constexpr int N = Dm::N, Q = Dm::Q, G = Dm::G, TG = Dm::TG;
+  std::vector<float> o(Dm::NOPS, 0.f);
+  for (int n = 0; n < N; ++n)
+    for (int q = 0; q < Q; ++q) o[Dm::PPT + n * Q + q] = (float)p.Pp[q * N + n];
+  for (int q = 0; q < Q; ++q)
+    for (int i = 0; i < N; ++i) o[Dm::PW + q * N + i] = (float)(p.Pp[q * N + i] * t->wi[q]);
+  for (int k = 0; k < N; ++k)
+    for (int i = 0; i < N; ++i) {
+      o[Dm::GX + k * N + i] = (float)p.GX[i * N + k];
+      o[Dm::GY + k * N + i] = (float)p.GY[i * N + k];
+      o[Dm::PWALL + k * N + i] = (float)p.PWALL[i * N + k];
+    }
+  for (int n = 0; n < N; ++n)
+    for (int l = 0; l < TG; ++l) {
+      o[Dm::TRT + n * TG + l] = (float)p.TR[l * N + n];
+      o[Dm::LIFT + l * N + n] = (float)p.TR[l * N + n];
+    }
+  for (int j = 0; j < G; ++j) o[Dm::WIF + j] = (float)t->wif[j];
+  return o;
+}
+
+// Persistent grid: as many blocks as stay resident (occupancy x SMs), or
+// fewer when the elements run out.  Cached per kernel.
+using MxKernel = void (*)(MxArgs);
+int grid_for(MxKernel kernel, size_t smem, int sms, int ne) {
+  struct Entry {
+    MxKernel k;
+    int per_sm;
+  };
+  static std::vector<Entry> cache;
+  int per_sm = 0;
+  for (const Entry &x : cache)
+    if (x.k == kernel) per_sm = x.per_sm;
+  if (!per_sm) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * kMxWarps, smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    cache.push_back({kernel, per_sm});
+  }
+  const int need = (ne + kMxWarps - 1) / kMxWarps;
+  const int cap = sms * per_sm;
+  return need < cap ? need : cap;
+}
+
+template <class Dm>
+constexpr size_t mx_smem() {
+  return sizeof(float) * (Dm::NOPS + (size_t)kMxWarps * Dm::WS);
+}
+
+// Launches of one right-hand side (stage >= 0: with the RK4 update).
+template <class Dm>
+cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *launches,
+                      cudaEvent_t *ev) {
+  constexpr size_t smem = mx_smem<Dm>();
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], st);
+  };
+  if (c->variant == SPOC_LIN) {
+    const int g = grid_for(kx_lin<Dm>, smem, c->sms, c->ne);
+    mark(0);
+    kx_lin<Dm><<<g, 32 * kMxWarps, smem, st>>>(a);
+    mark(1);
+    if (launches) *launches += 1;
+    return cudaGetLastError();
+  }
+  auto go = [&](MxKernel kv, MxKernel kt) {
+    const int gv = grid_for(kv, smem, c->sms, c->ne);
+    const int gt = grid_for(kt, smem, c->sms, c->ne);
+    mark(0);
+    kv<<<gv, 32 * kMxWarps, smem, st>>>(a);
+    mark(1);
+    kt<<<gt, 32 * kMxWarps, smem, st>>>(a);
+    mark(2);
+    if (launches) *launches += 2;
+  };
+  if (c->variant == SPOC_FS) go(kx_vol<Dm, SPOC_FS>, kx_tend<Dm, SPOC_FS>);
+  else if (c->variant == SPOC_NS) go(kx_vol<Dm, SPOC_NS>, kx_tend<Dm, SPOC_NS>);
+  else go(kx_vol<Dm, SPOC_INV>, kx_tend<Dm, SPOC_INV>);
+  return cudaGetLastError();
+}
+
+template <class Dm>
+cudaError_t run_prep(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *launches) {
+  constexpr size_t smem = mx_smem<Dm>();
+  const int g = grid_for(kx_prep<Dm>, smem, c->sms, c->ne);
+  kx_prep<Dm><<<g, 32 * kMxWarps, smem, st>>>(a);
+  if (launches) *launches += 1;
+  return cudaGetLastError();
+}
+
+// Dispatch over the tabulated (nc, ng, ngf) combinations.
+template <class F>
+bool with_dims(int nc, int ng, int ngf, F &&f) {
+  if (nc == 3 && ng == 12 && ngf == 4) return f(MDims<3, 12, 4>{}), true;
+  if (nc == 4 && ng == 25 && ngf == 5) return f(MDims<4, 25, 5>{}), true;
+  if (nc == 5 && ng == 27 && ngf == 6) return f(MDims<5, 27, 6>{}), true;
+  if (nc == 6 && ng == 33 && ngf == 7) return f(MDims<6, 33, 7>{}), true;
+  if (nc == 7 && ng == 42 && ngf == 9) return f(MDims<7, 42, 9>{}), true;
+  return false;
+}
+
+MxArgs base_args(MixedCtx *c, const DevMesh &m) {
+  MxArgs a{};
+  a.ne = c->ne;
+  a.ops = c->ops;
+  a.m = m;
+  a.y = c->y;
+  a.part = c->part;
+  a.trq = c->trq;
+  a.hbq = c->hbq;
+  a.fcq = c->fcq;
+  a.w0q = c->w0z0 ? nullptr : c->w0q;
+  a.z0q = c->w0z0 ? nullptr : c->z0q;
+  a.mu0 = c->mu0;
+  a.mb0 = c->mb0;
+  a.g0 = c->g0;
+  a.hh0 = c->hh0;
+  a.c64 = c->c64;
+  a.acc = c->acc;
+  a.k64 = c->k64;
+  return a;
+}
+
+int blocks_for(size_t n) {
+  const size_t b = (n + 255) / 256;
+  return (int)(b < 4096 ? (b ? b : 1) : 4096);
+}
+
+}  // namespace
+
+bool mixed_available(int nc, int ng, int ngf) {
+  return with_dims(nc, ng, ngf, [](auto) {});
+}
+
+int mixed_kernels_per_rhs(const MixedCtx *c) { return c->variant == SPOC_LIN ? 1 : 2; }
+
+int mixed_create(MixedCtx **out, const spoc_tables *t, int variant, int ne, int sms,
+                 std::string *err) {
+  *out = nullptr;
+  if (!mixed_available(t->nc, t->ng, t->ngf)) {
+    if (err) *err = "mixed precision is built for (nc, ng, ngf) = (3,12,4), (4,25,5), (5,27,6), (6,33,7), (7,42,9)";
+    return SPOC_E_UNSUPPORTED;
+  }
+  PsiOps p;
+  if (!build_psi(t, p, err)) return SPOC_E_MATRIX;
+  MixedCtx *c = new (std::nothrow) MixedCtx();
+  if (!c) return SPOC_E_NOMEM;
+  c->variant = variant;
+  c->nc = t->nc;
+  c->N = p.N;
+  c->Q = p.Q;
+  c->G = p.G;
+  c->ne = ne;
+  c->sms = sms;
+  std::vector<float> img;
+  with_dims(t->nc, t->ng, t->ngf, [&](auto d) {
+    using Dm = decltype(d);
+    img = ops_image<Dm>(p, t);
+  });
+  const size_t fn = (size_t)ne * p.N, tn = (size_t)ne * (3 * p.G + 1), qn = (size_t)ne * p.Q;
+  cudaError_t ce = c->alloc(&c->ops, img.size());
+  if (ce == cudaSuccess) ce = cudaMemcpy(c->ops, img.data(), sizeof(float) * img.size(), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = c->alloc(&c->U, p.U.size());
+  if (ce == cudaSuccess) ce = cudaMemcpy(c->U, p.U.data(), sizeof(double) * p.U.size(), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = c->alloc(&c->Ui, p.Ui.size());
+  if (ce == cudaSuccess) ce = cudaMemcpy(c->Ui, p.Ui.data(), sizeof(double) * p.Ui.size(), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = c->alloc(&c->c64, 3 * fn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->acc, 3 * fn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->k64, 3 * fn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->cin, 3 * fn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->y, 3 * fn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->tr[0], 3 * tn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->tr[1], 3 * tn);
+  if (ce == cudaSuccess && variant != SPOC_LIN) ce = c->alloc(&c->part, 3 * fn);
+  if (ce == cudaSuccess && variant != SPOC_LIN) ce = c->alloc(&c->trq, 6 * tn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->hbq, qn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->fcq, qn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->w0q, qn);
+  if (ce == cudaSuccess) ce = c->alloc(&c->z0q, qn);
+  if (ce == cudaSuccess) ce = cudaMemset(c->c64, 0, sizeof(double) * 3 * fn);
+  if (ce != cudaSuccess) {
+    if (err) *err = std::string("mixed-precision device set-up: ") + cudaGetErrorString(ce);
+    delete c;
+    return ce == cudaErrorMemoryAllocation ? SPOC_E_NOMEM : SPOC_E_CUDA;
+  }
+  *out = c;
+  return SPOC_OK;
+}
+
+void mixed_destroy(MixedCtx *c) { delete c; }
+
+cudaError_t mixed_set_params(MixedCtx *c, const DevOps &op, const double *hb, const double *fc,
+                             const double *w0, const double *z0, bool w0z0_zero, double mu0,
+                             double mb0, double g0, double hh0, cudaStream_t st) {
+  c->mu0 = (float)mu0;
+  c->mb0 = (float)mb0;
+  c->g0 = (float)g0;
+  c->hh0 = (float)hh0;
+  c->w0z0 = w0z0_zero;
+  const int b = blocks_for((size_t)c->ne * c->Q);
+  kx_quad<<<b, 256, 0, st>>>(c->ne, c->N, c->Q, op.p2, hb, c->hbq);
+  kx_quad<<<b, 256, 0, st>>>(c->ne, c->N, c->Q, op.p2, fc, c->fcq);
+  kx_quad<<<b, 256, 0, st>>>(c->ne, c->N, c->Q, op.p2, w0, c->w0q);
+  kx_quad<<<b, 256, 0, st>>>(c->ne, c->N, c->Q, op.p2, z0, c->z0q);
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_set_state(MixedCtx *c, const DevMesh &m, const double *const phi[3],
+                            cudaStream_t st, long long *launches) {
+  const size_t fn = (size_t)c->ne * c->N;
+  const int b = blocks_for(fn);
+  for (int f = 0; f < 3; ++f) kx_upper<<<b, 256, 0, st>>>(c->ne, c->N, c->U, phi[f], c->c64 + f * fn);
+  if (launches) *launches += 3;
+  MxArgs a = base_args(c, m);
+  c->cur = 0;
+  a.tr_out = c->tr[0];
+  cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) return ce;
+  with_dims(c->nc, c->Q, c->G, [&](auto d) { ce = run_prep<decltype(d)>(c, a, st, launches); });
+  return ce;
+}
+
+cudaError_t mixed_get_state(MixedCtx *c, double *const phi[3], cudaStream_t st, long long *launches) {
+  const size_t fn = (size_t)c->ne * c->N;
+  const int b = blocks_for(fn);
+  for (int f = 0; f < 3; ++f) kx_upper<<<b, 256, 0, st>>>(c->ne, c->N, c->Ui, c->c64 + f * fn, phi[f]);
+  if (launches) *launches += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_steps(MixedCtx *c, const DevMesh &m, double dt, int nsteps, int *flag,
+                        cudaStream_t st, long long *launches, cudaEvent_t *ev) {
+  MxArgs a = base_args(c, m);
+  a.dt = dt;
+  a.dt6 = dt / 6.0;
+  a.flag = flag;
+  cudaError_t ce = cudaSuccess;
+  for (int it = 0; it < nsteps && ce == cudaSuccess; ++it)
+    for (int s = 0; s < 4 && ce == cudaSuccess; ++s) {
+      a.stage = s;
+      a.tr_in = c->tr[c->cur];
+      a.tr_out = c->tr[c->cur ^ 1];
+      cudaEvent_t *e = (ev && it == nsteps - 1 && s == 0) ? ev : nullptr;
+      with_dims(c->nc, c->Q, c->G, [&](auto d) { ce = run_stage<decltype(d)>(c, a, st, launches, e); });
+      c->cur ^= 1;
+    }
+  return ce;
+}
+
+cudaError_t mixed_rhs(MixedCtx *c, const DevMesh &m, const double *const in[3],
+                      double *const out[3], int *flag, cudaStream_t st, long long *launches) {
+  // the resident state is kept: the input goes through cin and the stage
+  // buffers, which the next mixed_steps call rebuilds from c64
+  const size_t fn = (size_t)c->ne * c->N;
+  const int b = blocks_for(fn);
+  for (int f = 0; f < 3; ++f) kx_upper<<<b, 256, 0, st>>>(c->ne, c->N, c->U, in[f], c->cin + f * fn);
+  if (launches) *launches += 3;
+  MxArgs a = base_args(c, m);
+  a.c64 = c->cin;
+  a.flag = flag;
+  a.tr_out = c->tr[c->cur ^ 1];
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess)
+    with_dims(c->nc, c->Q, c->G, [&](auto d) { ce = run_prep<decltype(d)>(c, a, st, launches); });
+  a.stage = -1;
+  a.tr_in = c->tr[c->cur ^ 1];
+  a.tr_out = nullptr;
+  if (ce == cudaSuccess)
+    with_dims(c->nc, c->Q, c->G, [&](auto d) { ce = run_stage<decltype(d)>(c, a, st, launches, nullptr); });
+  for (int f = 0; f < 3 && ce == cudaSuccess; ++f) {
+    kx_upper<<<b, 256, 0, st>>>(c->ne, c->N, c->Ui, c->k64 + f * fn, out[f]);
+    ce = cudaGetLastError();
+  }
+  if (launches) *launches += 3;
+  // restore the stage input of the resident state
+  a = base_args(c, m);
+  a.tr_out = c->tr[c->cur];
+  if (ce == cudaSuccess)
+    with_dims(c->nc, c->Q, c->G, [&](auto d) { ce = run_prep<decltype(d)>(c, a, st, launches); });
+  return ce;
+}
+
+}  // namespace spoc
