@@ -46,6 +46,101 @@ def workload_desc(cfg, ne, nm):
             f"f0={cfg.f0}, beta={cfg.beta}, mu0={cfg.mu0}, mb0={cfg.mb0}, H={cfg.depth}, ic={cfg.ic}")
 
 
+def model_counts_mixed(cfg, ne):
+    """Per-kernel algorithmic FP32 flops and compulsory HBM bytes of one
+    mixed-precision RHS (kx_vol, kx_tend; kx_lin for the linear variant).
+
+    Flops: the multiply-adds the kernels issue (2 flops each).  Bytes: own
+    element reads and writes (state FP32 / FP64, partial load vectors, trace
+    records of 3*ngf + 1 floats; a neighbour's record counted once more).
+    """
+    N, Q, G = cfg.nm, cfg.ng, cfg.ngf
+    TG, TS = 3 * G, 3 * G + 1
+    rk4_bytes = 3 * N * (8 + 8 + 8 + 4)  # c64 read, acc read+write, y write
+    if cfg.variant == "lin":
+        macs = 6 * N * (N - 1) + 3 * TG * N + 3 * TG * (N - 1)
+        return {"kx_lin": (2.0 * ne * macs, ne * (3 * N * 4 + 2 * 3 * TS * 4 + rk4_bytes + 3 * TS * 4))}
+    vol = 4 * N * (N - 1) + 4 * TG * N + 3 * Q * N + 4 * Q * N + 4 * Q * N + 6 * N * (N - 1) + 6 * TG * (N - 1)
+    tend = 3 * TG * N + 3 * TG * (N - 1)
+    return {
+        "kx_vol": (2.0 * ne * vol, ne * (3 * N * 4 + 2 * 2 * TS * 4 + 2 * Q * 4 + 3 * N * 4 + 6 * TS * 4)),
+        "kx_tend": (2.0 * ne * tend, ne * (3 * N * 4 + 2 * 7 * TS * 4 + rk4_bytes + 3 * TS * 4)),
+    }
+
+
+def mnorm_factory(p):
+    det = p.mesh.det
+    A = p.T.ammo.T
+
+    def mnorm(x):
+        return float(np.sqrt(np.sum(det * np.einsum("ei,ij,ej->e", x, A, x))))
+    return mnorm
+
+
+def timed_steps(torch, stream, flush, s, dt, nsteps):
+    """ms per RK4 step over nsteps single-step calls, L2 flushed before each."""
+    out = []
+    for _ in range(nsteps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            a.record(stream)
+        s.rk4_steps(dt, 1)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        b.synchronize()
+        out.append(a.elapsed_time(b))
+    return sum(out) / nsteps
+
+
+def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, tsteps=10):
+    """Mixed-precision form against plain FP64 on one configuration: ms per
+    step of both, relative L2 errors of eta, u, v after `steps` steps, energy
+    drift of both runs, and the roofline of the dominant mixed kernel."""
+    cfg = W.CONFIGS[name]
+    p = W.build_problem(cfg)
+    mnorm = mnorm_factory(p)
+    dof = 3.0 * p.T.nm * p.mesh.ne
+    res, states, drift = {}, {}, {}
+    for prec in ("fp64", "mixed"):
+        s = W.make_solver(p, prec)
+        s.set_stream(stream.cuda_stream)
+        s.set_state(p.u, p.v, p.h)
+        s.rk4_steps(p.dt, 3)
+        res[prec] = timed_steps(torch, stream, flush, s, p.dt, tsteps)
+        s.set_state(p.u, p.v, p.h)
+        e0 = s.energy()
+        s.rk4_steps(p.dt, steps)
+        e1 = s.energy()
+        states[prec] = s.get_state()
+        drift[prec] = ((e1[0] + e1[1]) - (e0[0] + e0[1])) / (e0[0] + e0[1])
+        if prec == "mixed":
+            s.set_state(p.u, p.v, p.h)
+            kms = s.profile_rk4(p.dt, 2)
+        s.close()
+    errs = {f: mnorm(states["mixed"][i] - states["fp64"][i]) / mnorm(states["fp64"][i])
+            for i, f in enumerate(("u", "v", "eta"))}
+    counts = model_counts_mixed(cfg, p.mesh.ne)
+    per_launch = {n: float(kms[i]) / 8 for i, n in enumerate(counts)}
+    dom = max(per_launch, key=per_launch.get)
+    fl, by = counts[dom]
+    dur = per_launch[dom] * 1e-3
+    fp32 = api.fp64_peak(2)
+    return {
+        "config": f"{name}: {p.mesh.ne} triangles, degree {cfg.nc} (nm={p.T.nm}), dt={p.dt}",
+        "fp64_ms_per_step": res["fp64"], "mixed_ms_per_step": res["mixed"],
+        "fp64_value": dof / (res["fp64"] * 1e-3), "mixed_value": dof / (res["mixed"] * 1e-3),
+        "speedup": res["fp64"] / res["mixed"],
+        "steps_compared": steps, "rel_l2_error_vs_fp64": errs,
+        "energy_drift": drift, "energy_drift_difference": drift["mixed"] - drift["fp64"],
+        "kernel_ms_per_launch": per_launch,
+        "roofline": {"kernel": dom, "bound": "fp32", "achieved": fl / dur / 1e12, "peak": fp32,
+                     "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp32,
+                     "hbm_gbs": by / dur / 1e9,
+                     "peak_source": "measured live: spoc_fp64_peak mode 2 (FP32 FMA chains)"},
+    }
+
+
 def model_counts(cfg, ne, nf):
     """Per-kernel algorithmic FP64 flops and compulsory HBM bytes of one RHS.
 
@@ -222,8 +317,10 @@ def main():
     ap.add_argument("--config", default="c2_fs_p6")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma"],
-                    help="fp64: bit-exact reference order (headline); fp64_fma: fused multiply-adds")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma", "mixed"],
+                    help="fp64: bit-exact reference order (headline); fp64_fma: fused "
+                         "multiply-adds; mixed: FP32 contractions, FP64 state")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -317,7 +414,7 @@ def main():
     s.set_state(p.u, p.v, p.h)
     prof_steps = 2
     kms = s.profile_rk4(p.dt, prof_steps)
-    counts = model_counts(cfg, ne, p.mesh.nf)
+    counts = model_counts(cfg, ne, p.mesh.nf) if args.precision != "mixed" else model_counts_mixed(cfg, ne)
     names = list(counts)
     per_launch_ms = {n: float(kms[i]) / (4 * prof_steps) for i, n in enumerate(names)}
     dom = max(per_launch_ms, key=per_launch_ms.get)
@@ -338,46 +435,44 @@ def main():
     roof = {"kernel": dom, "bound": "hbm", "achieved": by / dur / 1e9, "peak": hbm_peak,
             "unit": "GB/s", "frac": by / dur / 1e9 / hbm_peak, "traffic": traffic,
             "peak_source": hbm_src, "algorithmic_bytes_per_launch": by}
-    roof_fp64 = {"kernel": dom, "bound": "fp64", "achieved": fl / dur / 1e12,
-                 "peak": fp64_fma, "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp64_fma,
-                 "peak_mul_add": fp64_mul_add, "frac_of_mul_add": fl / dur / 1e12 / fp64_mul_add,
-                 "algorithmic_flops_per_launch": fl,
-                 "peak_source": "measured live: spoc_fp64_peak (DFMA chains, 148 SMs)"}
+    if args.precision == "mixed":
+        fp32 = api.fp64_peak(2)
+        roof_fp64 = {"kernel": dom, "bound": "fp32", "achieved": fl / dur / 1e12, "peak": fp32,
+                     "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp32,
+                     "algorithmic_flops_per_launch": fl,
+                     "peak_source": "measured live: spoc_fp64_peak mode 2 (FP32 FMA chains)"}
+    else:
+        roof_fp64 = {"kernel": dom, "bound": "fp64", "achieved": fl / dur / 1e12,
+                     "peak": fp64_fma, "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp64_fma,
+                     "peak_mul_add": fp64_mul_add, "frac_of_mul_add": fl / dur / 1e12 / fp64_mul_add,
+                     "algorithmic_flops_per_launch": fl,
+                     "peak_source": "measured live: spoc_fp64_peak (DFMA chains, 148 SMs)"}
 
-    # the other precision mode on the same workload, and its distance from the
-    # bit-exact result after the timed steps
-    other = "fp64_fma" if args.precision == "fp64" else "fp64"
-    s2 = W.make_solver(p, other)
-    s2.set_stream(stream.cuda_stream)
-    s2.set_state(p.u, p.v, p.h)
-    s2.rk4_steps(p.dt, args.warmup)
-    o_times = []
-    for _ in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            flush.zero_()
-            a.record(stream)
-        s2.rk4_steps(p.dt, 1)
-        with torch.cuda.stream(stream):
-            b.record(stream)
-        b.synchronize()
-        o_times.append(a.elapsed_time(b))
+    # the other precision modes on the same workload, and their distance from
+    # the headline run after 100 steps
+    mnorm = mnorm_factory(p)
     s.set_state(p.u, p.v, p.h)
-    s2.set_state(p.u, p.v, p.h)
     s.rk4_steps(p.dt, 100)
-    s2.rk4_steps(p.dt, 100)
-    sa_, sb_ = s.get_state(), s2.get_state()
-    det = p.mesh.det
-    A = p.T.ammo.T
+    ref_state = s.get_state()
+    others = []
+    for other in [x for x in ("fp64", "fp64_fma", "mixed") if x != args.precision]:
+        s2 = W.make_solver(p, other)
+        s2.set_stream(stream.cuda_stream)
+        s2.set_state(p.u, p.v, p.h)
+        s2.rk4_steps(p.dt, args.warmup)
+        ms = timed_steps(torch, stream, flush, s2, p.dt, args.steps)
+        s2.set_state(p.u, p.v, p.h)
+        s2.rk4_steps(p.dt, 100)
+        st2 = s2.get_state()
+        s2.close()
+        others.append({"precision": other, "value": dof / (ms * 1e-3), "ms_per_step": ms,
+                       "rel_l2_diff_after_100_steps": {
+                           f: mnorm(st2[i] - ref_state[i]) / mnorm(ref_state[i])
+                           for i, f in enumerate(("u", "v", "eta"))}})
 
-    def mnorm(x):
-        return float(np.sqrt(np.sum(det * np.einsum("ei,ij,ej->e", x, A, x))))
-
-    diff = max(mnorm(x - y) / mnorm(x) for x, y in zip(sa_, sb_))
-    s2.close()
-    other_line = {"precision": other, "value": dof * args.steps / (sum(o_times) * 1e-3),
-                  "ms_per_step": sum(o_times) / args.steps,
-                  "rel_l2_diff_vs_other_after_100_steps": diff}
+    mixed = None
+    if world == 1 and not args.no_mixed:
+        mixed = mixed_measure(torch, stream, flush, W, api)
 
     adjoint = None
     if world == 1 and not args.no_adjoint:
@@ -388,19 +483,22 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision != "mixed" else "f32 contractions / f64 state",
+            "data": "synthetic",
             "config": {"workload": workload_desc(cfg, ne, nm), "ne": ne, "nm": nm, "dt": p.dt,
-                       "precision": ("fp64, reference operation order (bit-exact to the CPU oracle)"
-                                     if args.precision == "fp64" else
-                                     "fp64 with fused multiply-adds (not bit-exact)"),
+                       "precision": {"fp64": "fp64, reference operation order (bit-exact to the CPU oracle)",
+                                     "fp64_fma": "fp64 with fused multiply-adds (not bit-exact)",
+                                     "mixed": "FP32 contractions in the orthonormal basis, FP64 RK4 state"}[args.precision],
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "kernel_ms_per_launch": per_launch_ms,
             "roofline": roof,
-            "roofline_fp64": roof_fp64,
-            "other_precision": other_line,
+            ("roofline_fp32" if args.precision == "mixed" else "roofline_fp64"): roof_fp64,
+            "other_precisions": others,
+            "mixed_c3": mixed,
             "adjoint": adjoint,
             "clocks": clocks,
         }

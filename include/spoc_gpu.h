@@ -138,8 +138,9 @@ long long spoc_kernel_launches(spoc_handle *h);
  * 0 q-phase, 1 nonlinear volume, 2 tendency+RK4; linear: 0), *nkinds the
  * number of kinds. */
 int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms, int *nkinds);
-/* Measured FP64 throughput of this GPU in TFLOP/s (2 flops per multiply-add);
- * mode 0: fused multiply-add, mode 1: separately rounded multiply and add. */
+/* Measured throughput of this GPU in TFLOP/s (2 flops per multiply-add);
+ * mode 0: FP64 fused multiply-add, mode 1: FP64 separately rounded multiply
+ * and add, mode 2: FP32 fused multiply-add. */
 int spoc_fp64_peak(int mode, double *tflops);
 /* Energy diagnostic that allocates nothing.  No counterpart in the reference
  * (it computes what src/energy.f:3-96 computes, like spoc_energy).  For

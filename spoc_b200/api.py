@@ -213,7 +213,8 @@ class Tables:
 
 
 def fp64_peak(mode: int = 0) -> float:
-    """Measured FP64 TFLOP/s of the current GPU (0: FMA, 1: mul + add)."""
+    """Measured TFLOP/s of the current GPU (0: FP64 FMA, 1: FP64 mul + add,
+    2: FP32 FMA)."""
     t = C.c_double()
     _check(load_library().spoc_fp64_peak(mode, C.byref(t)), "fp64_peak")
     return t.value

@@ -686,7 +686,7 @@ extern "C" int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *k
 }
 
 extern "C" int spoc_fp64_peak(int mode, double *tflops) {
-  if (!tflops || (mode != 0 && mode != 1)) return fail(SPOC_E_ARG, "bad argument");
+  if (!tflops || mode < 0 || mode > 2) return fail(SPOC_E_ARG, "bad argument");
   int dev = 0, sms = 0;
   CK(cudaGetDevice(&dev), "device");
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");

@@ -698,14 +698,30 @@ __global__ void __launch_bounds__(256) k_fp64_peak(double *out, int iters, doubl
   for (int i = 0; i < 8; ++i) s += x[i];
   if (s == 12345.678) out[0] = s;  // keeps the loop live
 }
+// FP32 fused multiply-add chains (the arithmetic of the mixed-precision kernels).
+__global__ void __launch_bounds__(256) k_fp32_peak(double *out, int iters, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x[i] = threadIdx.x * 1e-3f + i;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = __fmaf_rn(x[i], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += x[i];
+  if (s == 12345.678f) out[0] = s;  // keeps the loop live
+}
 }  // namespace
 
 cudaError_t launch_fp64_peak(int mode, int sms, int iters, double *out, cudaStream_t st) {
   const int grid = sms * 8;
   if (mode == 0)
     k_fp64_peak<0><<<grid, 256, 0, st>>>(out, iters, 0.999999, 1e-9);
-  else
+  else if (mode == 1)
     k_fp64_peak<1><<<grid, 256, 0, st>>>(out, iters, 0.999999, 1e-9);
+  else
+    k_fp32_peak<<<grid, 256, 0, st>>>(out, iters, 0.999999f, 1e-9f);
   return cudaGetLastError();
 }
 }  // namespace spoc

@@ -134,7 +134,8 @@ cudaError_t launch_rhs_fast_fma(int variant, const DevOps &op, const DevMesh &m,
                                 const RhsBuffers &b, const StageArgs &sa, cudaStream_t st, int sms,
                                 long long *launches, cudaEvent_t *ev = nullptr);
 
-// 8 independent chains of `iters` FP64 operations per thread, sms*8 blocks of 256
+// 8 independent chains of `iters` multiply-adds per thread, sms*8 blocks of 256;
+// mode 0 FP64 fused, 1 FP64 separately rounded, 2 FP32 fused
 cudaError_t launch_fp64_peak(int mode, int sms, int iters, double *out, cudaStream_t st);
 
 }  // namespace spoc

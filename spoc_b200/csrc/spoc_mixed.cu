@@ -55,6 +55,9 @@ struct MDims {
   static constexpr int TG = 3 * G_;
   static constexpr int TS = TG + 1;  // trace record: TG mean-free traces + the mean
   static constexpr int R = (N + 31) / 32;
+  // resident blocks per SM the register budget is sized for (shared memory
+  // allows about 4 blocks of 8 warps at degree <= 6 and 3 at degree 7)
+  static constexpr int MINB = R == 1 ? 4 : 2;
   // operator image in shared memory (floats)
   static constexpr int PPT = 0;               // [n*Q + q]  = Pp(q, n)
   static constexpr int PW = PPT + N * Q;      // [q*N + i]  = Pp(q, i) wi(q)
@@ -295,7 +298,7 @@ __device__ void finish_element(const MxArgs &a, const float *o, float *w, int e,
 // Nonlinear variants: volume kernel (calvarnl_fs.f:88-332 and the volume terms
 // of :341-544).
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(32 * kMxWarps) kx_vol(const MxArgs a) {
+__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_vol(const MxArgs a) {
   constexpr int N = Dm::N, Q = Dm::Q, G = Dm::G, TG = Dm::TG, R = Dm::R;
   extern __shared__ __align__(16) float sm[];
   float *o = sm;
@@ -510,7 +513,7 @@ __global__ void __launch_bounds__(32 * kMxWarps) kx_vol(const MxArgs a) {
 // Nonlinear variants: face lifts of phases C and D (calvarnl_fs.f:350-544),
 // wall solves, RK4 update.
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(32 * kMxWarps) kx_tend(const MxArgs a) {
+__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_tend(const MxArgs a) {
   constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, R = Dm::R;
   extern __shared__ __align__(16) float sm[];
   float *o = sm;
@@ -573,7 +576,7 @@ __global__ void __launch_bounds__(32 * kMxWarps) kx_tend(const MxArgs a) {
 
 // Linear variant (calvar_lin.f:7-287) in one kernel.
 template <class Dm>
-__global__ void __launch_bounds__(32 * kMxWarps) kx_lin(const MxArgs a) {
+__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_lin(const MxArgs a) {
   constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, R = Dm::R;
   extern __shared__ __align__(16) float sm[];
   float *o = sm;
@@ -649,7 +652,7 @@ __global__ void __launch_bounds__(32 * kMxWarps) kx_lin(const MxArgs a) {
 
 // Stage input and its traces from the FP64 psi state.
 template <class Dm>
-__global__ void __launch_bounds__(32 * kMxWarps) kx_prep(const MxArgs a) {
+__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_prep(const MxArgs a) {
   constexpr int N = Dm::N;
   extern __shared__ __align__(16) float sm[];
   float *o = sm;
