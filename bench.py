@@ -136,7 +136,7 @@ def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, ts
         "kernel_ms_per_launch": per_launch,
         "roofline": {"kernel": dom, "bound": "fp32", "achieved": fl / dur / 1e12, "peak": fp32,
                      "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp32,
-                     "hbm_gbs": by / dur / 1e9,
+                     "hbm_gbs": by / dur / 1e9, "traffic": NCU_TRAFFIC.get(f"{name}:{dom}"),
                      "peak_source": "measured live: spoc_fp64_peak mode 2 (FP32 FMA chains)"},
     }
 
@@ -152,12 +152,20 @@ def model_counts(cfg, ne, nf):
     N, Q, G = cfg.nm, cfg.ng, cfg.ngf
     if cfg.variant == "lin":
         macs = ne * (6 * N * N + 3 * N * N + 4 * 3 * N * G) + nf * 3 * 2 * N * G
-        return {"k_lin": (2.0 * macs, 8.0 * ne * N * (3 + 9))}
+        return {"kf_lin": (2.0 * macs, 8.0 * ne * N * (3 + 9))}
     return {
-        "k_qphase": (2.0 * (ne * (8 * N * N + 12 * N * G) + nf * 2 * 2 * N * G), 8.0 * ne * N * (2 + 4)),
-        "k_nlvol": (2.0 * ne * (2 * N * N + 17 * Q * N), 8.0 * ne * N * (11 + 8)),
-        "k_tend": (2.0 * (ne * (15 * N * N + 18 * N * G) + nf * 6 * 2 * N * G), 8.0 * ne * N * (8 + 12)),
+        "kf_qphase": (2.0 * (ne * (8 * N * N + 12 * N * G) + nf * 2 * 2 * N * G), 8.0 * ne * N * (2 + 4)),
+        "kf_nlvol": (2.0 * ne * (2 * N * N + 17 * Q * N), 8.0 * ne * N * (11 + 8)),
+        "kf_tend": (2.0 * (ne * (15 * N * N + 18 * N * G) + nf * 6 * 2 * N * G), 8.0 * ne * N * (8 + 12)),
     }
+
+
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel on
+# the workload: profiles/kf_kernels_c2_fs_p6.md, profiles/kx_kernels_c3_inv_p7.md
+NCU_TRAFFIC = {
+    "c2_fs_p6:kf_qphase": 19441408, "c2_fs_p6:kf_nlvol": 104103936, "c2_fs_p6:kf_tend": 108311040,
+    "c3_inv_p7:kx_vol": 251344384, "c3_inv_p7:kx_tend": 468087552,
+}
 
 
 def sample_clocks_start(out: Path):
@@ -428,10 +436,7 @@ def main():
         hbm_src = "measured"
     except Exception:
         hbm_peak, hbm_src = 6650.0, "fallback"
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get(f"{cfg.name}:{dom}")
+    traffic = NCU_TRAFFIC.get(f"{cfg.name}:{dom}")
     roof = {"kernel": dom, "bound": "hbm", "achieved": by / dur / 1e9, "peak": hbm_peak,
             "unit": "GB/s", "frac": by / dur / 1e9 / hbm_peak, "traffic": traffic,
             "peak_source": hbm_src, "algorithmic_bytes_per_launch": by}

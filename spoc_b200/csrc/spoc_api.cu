@@ -1107,8 +1107,21 @@ long long binom(int n, int k) {
 // snapshot buffers available (binomial checkpointing).  lam enters as the
 // adjoint of the state at i1 and leaves as the adjoint of the state at i0,
 // observation forcing included.
+// Split of a reversal of l steps with free_snaps checkpoints (revolve's
+// binomial rule): the first k steps are reversed after the last l - k, whose
+// starting state goes into a checkpoint.
+int split_steps(int l, int free_snaps) {
+  int r = 1;
+  while (binom(free_snaps + r, free_snaps) < l) ++r;
+  const long long right = binom(free_snaps - 1 + r, free_snaps - 1);
+  return (int)std::max<long long>(1, l - std::min<long long>(right, l - 1));
+}
+
+// Reverse steps i0..i1-1 from the state `base` at step i0.  With `filled`,
+// the checkpoints of the rightmost chain already hold their states (taken by
+// the forward sweep of spoc_bwd_window).
 int reverse(spoc_handle *h, AdjCtx *c, int i0, int i1, double *const base[3], int free_snaps,
-            double *const lam[3], double dt) {
+            double *const lam[3], double dt, bool filled) {
   int rc;
   const int l = i1 - i0;
   if (l <= 0) return SPOC_OK;
@@ -1123,17 +1136,16 @@ int reverse(spoc_handle *h, AdjCtx *c, int i0, int i1, double *const base[3], in
     }
     return SPOC_OK;
   }
-  int r = 1;
-  while (binom(free_snaps + r, free_snaps) < l) ++r;
-  long long right = binom(free_snaps - 1 + r, free_snaps - 1);
-  int k = (int)std::max<long long>(1, l - std::min<long long>(right, l - 1));
+  const int k = split_steps(l, free_snaps);
   double *slot[3];
   double *snap = c->snaps[free_snaps - 1];
   for (int f = 0; f < 3; ++f) slot[f] = snap + f * c->n;
-  if ((rc = copy3(h, slot, base))) return rc;
-  if ((rc = advance(h, c, slot, dt, k))) return rc;
-  if ((rc = reverse(h, c, i0 + k, i1, slot, free_snaps - 1, lam, dt))) return rc;
-  return reverse(h, c, i0, i0 + k, base, free_snaps, lam, dt);
+  if (!filled) {
+    if ((rc = copy3(h, slot, base))) return rc;
+    if ((rc = advance(h, c, slot, dt, k))) return rc;
+  }
+  if ((rc = reverse(h, c, i0 + k, i1, slot, free_snaps - 1, lam, dt, filled))) return rc;
+  return reverse(h, c, i0, i0 + k, base, free_snaps, lam, dt, false);
 }
 
 int host_to_dev3(spoc_handle *h, double *const dst[3], int ld, const double *a, const double *b,
@@ -1216,7 +1228,7 @@ extern "C" int spoc_adj_steps(spoc_handle *h, int ld, const double *u0, const do
   if (!rc) rc = host_to_dev3(h, lam, ld, bu, bv, bh);
   std::vector<int> saved;
   saved.swap(c->steps);  // no observation forcing inside this call
-  if (!rc) rc = reverse(h, c, 0, nsteps, x, 0, lam, dt);
+  if (!rc) rc = reverse(h, c, 0, nsteps, x, 0, lam, dt, false);
   c->steps.swap(saved);
   if (!rc) rc = dev_to_host3(h, bu, bv, bh, ld, lam);
   return rc ? rc : check_flag(h);
@@ -1309,15 +1321,42 @@ extern "C" int spoc_bwd_window(spoc_handle *h, int ld, const double *u0, const d
     if (e != cudaSuccess) return fail(SPOC_E_NOMEM, "checkpoint buffers", e);
     c->snaps.push_back(p);
   }
-  // forward sweep: cost and residuals at the observation times
-  rc = spoc_fwd_window(h, ld, u0, v0, h0, dt, nsteps, cost);
-  if (rc) return rc;
-  double *const *x0 = c->V[4], *const *lam = c->V[5];
+  // forward sweep: cost and residuals at the observation times, and the
+  // checkpoints of the rightmost chain of the reversal (slot f-1 for the
+  // level with f free checkpoints)
+  std::vector<int> pos;
+  for (int i0 = 0, f = snaps; nsteps - i0 > 1 && f > 0; --f) {
+    i0 += split_steps(nsteps - i0, f);
+    pos.push_back(i0);
+  }
+  double *const *x0 = c->V[4], *const *lam = c->V[5], *const *x = c->V[3];
   rc = host_to_dev3(h, x0, ld, u0, v0, h0);
+  if (!rc) rc = copy3(h, x, x0);
+  double J = 0.0;
+  int t = obs_index(c, 0);
+  if (!rc && t >= 0) rc = obs_eval(h, c, t, x, &J);
+  size_t lv = 0;
+  for (int i = 0; i < nsteps && !rc;) {
+    int next = nsteps;
+    for (int st : c->steps)
+      if (st > i && st < next) next = st;
+    if (lv < pos.size() && pos[lv] < next) next = pos[lv];
+    rc = advance(h, c, x, dt, next - i);
+    i = next;
+    if (!rc && lv < pos.size() && pos[lv] == i) {
+      double *slot[3];
+      for (int f = 0; f < 3; ++f) slot[f] = c->snaps[snaps - 1 - lv] + f * c->n;
+      rc = copy3(h, slot, x);
+      ++lv;
+    }
+    t = obs_index(c, i);
+    if (!rc && t >= 0) rc = obs_eval(h, c, t, x, &J);
+  }
+  *cost = J;
   if (!rc) rc = zero3(h, lam);
-  int t = obs_index(c, nsteps);
+  t = obs_index(c, nsteps);
   if (!rc && t >= 0) rc = obs_force(h, c, t, lam);
-  if (!rc) rc = reverse(h, c, 0, nsteps, x0, snaps, lam, dt);
+  if (!rc) rc = reverse(h, c, 0, nsteps, x0, snaps, lam, dt, true);
   if (!rc) rc = dev_to_host3(h, gu, gv, gh, ld, lam);
   return rc ? rc : check_flag(h);
 }
