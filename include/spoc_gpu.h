@@ -138,6 +138,13 @@ long long spoc_kernel_launches(spoc_handle *h);
  * 0 q-phase, 1 nonlinear volume, 2 tendency+RK4; linear: 0), *nkinds the
  * number of kinds. */
 int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms, int *nkinds);
+/* Self-test of the tcgen05 TF32 tensor-core path the mixed kernels use (no
+ * reference counterpart): D (128 x n) = A (128 x K) B^T (B: n x K), row-major
+ * host arrays, as one TF32 product (split 0) or the three-term hi/lo split
+ * (split 1), onto dinit (128 x n) when not null.  (kpad, n) in {(8, 16),
+ * (32, 32), (40, 48), (48, 144)}, K <= kpad. */
+int spoc_tc_selftest(int K, int kpad, int n, int split, const float *A, const float *B,
+                     const float *dinit, float *D);
 /* Measured throughput of this GPU in TFLOP/s (2 flops per multiply-add);
  * mode 0: FP64 fused multiply-add, mode 1: FP64 separately rounded multiply
  * and add, mode 2: FP32 fused multiply-add. */

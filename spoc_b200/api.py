@@ -220,6 +220,22 @@ def fp64_peak(mode: int = 0) -> float:
     return t.value
 
 
+def tc_selftest(A, B, kpad: int, split: int, dinit=None):
+    """D = dinit + A B^T on the tensor cores (tcgen05, TF32; split 1 = 3xTF32)."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    n = B.shape[0]
+    D = np.zeros((128, n), np.float32)
+    fp = C.POINTER(C.c_float)
+    di = None if dinit is None else np.ascontiguousarray(dinit, dtype=np.float32)
+    lib = load_library()
+    lib.spoc_tc_selftest.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, fp, fp, fp, fp]
+    _check(lib.spoc_tc_selftest(A.shape[1], kpad, n, split, A.ctypes.data_as(fp), B.ctypes.data_as(fp),
+                                None if di is None else di.ctypes.data_as(fp), D.ctypes.data_as(fp)),
+           "tc_selftest")
+    return D
+
+
 def build_tables(nc: int, ng: int, ngf: int) -> Tables:
     """Quadrature, basis tables, operators and Cholesky factors for degree nc."""
     lib = load_library()
