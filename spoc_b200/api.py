@@ -369,8 +369,9 @@ class Solver:
             pass
 
     def set_kernel_path(self, path: str) -> None:
-        """'auto', 'generic' (runtime-sized kernels) or 'templated' (compile-time sized)."""
-        code = {"auto": 0, "generic": 1, "templated": 2}[path]
+        """'auto', 'generic' (runtime-sized kernels), 'templated' (compile-time
+        sized) or, for the mixed precision, 'tensor' (tcgen05 volume kernel)."""
+        code = {"auto": 0, "generic": 1, "templated": 2, "tensor": 3}[path]
         _check(self.lib.spoc_set_kernel_path(self._h, code), "set_kernel_path")
 
     def set_stream(self, stream_ptr: int) -> None:

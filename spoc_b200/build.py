@@ -27,11 +27,11 @@ NVCC_FLAGS = [
     "-Xptxas", "-v",
 ]
 SOURCES = ["spoc_kernels.cu", "spoc_fast.cu", "spoc_api.cu", "spoc_noalloc.cu", "spoc_adjoint.cu",
-           "spoc_mixed.cu", "spoc_tc_selftest.cu"]
+           "spoc_mixed.cu", "spoc_mixed_tc.cu", "spoc_tc_selftest.cu"]
 # spoc_fast.cu is compiled a second time with fused multiply-adds
 VARIANT_SOURCES = [("spoc_fast.cu", "spoc_fast_fma", ["-DSPOC_FMA=1"])]
 HOST_SOURCES = ["spoc_host.cpp"]
-HEADERS = ["spoc_device.cuh", "spoc_kernels.h", "spoc_mixed.h", "spoc_tc.cuh"]
+HEADERS = ["spoc_device.cuh", "spoc_kernels.h", "spoc_mixed.h", "spoc_tc.cuh", "spoc_mixed_dev.cuh"]
 
 
 def _nvcc() -> str:

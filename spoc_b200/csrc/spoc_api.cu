@@ -283,6 +283,7 @@ int check_flag(spoc_handle *h) {
   CK(cudaStreamSynchronize(h->st), "synchronize");
   if (flag) {
     CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->st), "clear flag");
+    if (flag & 2) return fail(SPOC_E_CUDA, "tensor-core wait limit reached");
     return fail(SPOC_E_NONFINITE, "non-finite tendency detected");
   }
   return SPOC_OK;
@@ -416,7 +417,11 @@ extern "C" void spoc_destroy(spoc_handle *h) {
 }
 
 extern "C" int spoc_set_kernel_path(spoc_handle *h, int path) {
-  if (!h || path < SPOC_PATH_AUTO || path > SPOC_PATH_TEMPLATED) return fail(SPOC_E_ARG, "bad argument");
+  if (!h || path < SPOC_PATH_AUTO || path > SPOC_PATH_TENSOR) return fail(SPOC_E_ARG, "bad argument");
+  if (path == SPOC_PATH_TENSOR && (!h->mx || !mixed_set_tensor(h->mx, true)))
+    return fail(SPOC_E_UNSUPPORTED, "tensor-core kernels: SPOC_MIXED, nonlinear variants, tabulated (nc, ng, ngf)");
+  if (h->mx && (path == SPOC_PATH_TEMPLATED || path == SPOC_PATH_GENERIC)) mixed_set_tensor(h->mx, false);
+  if (h->mx && path == SPOC_PATH_AUTO) mixed_set_tensor(h->mx, true);
   if (path == SPOC_PATH_TEMPLATED && !fast_available(h->nc, h->ng, h->ngf))
     return fail(SPOC_E_UNSUPPORTED, "no compile-time-sized kernels for this (nc, ng, ngf)");
   h->path = path;

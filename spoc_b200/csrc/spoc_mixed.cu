@@ -40,114 +40,12 @@
 #include <vector>
 
 #include "spoc_mixed.h"
+#include "spoc_mixed_dev.cuh"
 
 namespace spoc {
+using namespace mx;
 
 namespace {
-
-constexpr int kMxWarps = 8;  // warps (elements in flight) per block
-
-template <int NC_, int Q_, int G_>
-struct MDims {
-  static constexpr int N = (NC_ + 1) * (NC_ + 2) / 2;
-  static constexpr int Q = Q_;
-  static constexpr int G = G_;
-  static constexpr int TG = 3 * G_;
-  static constexpr int TS = TG + 1;  // trace record: TG mean-free traces + the mean
-  static constexpr int R = (N + 31) / 32;
-  // resident blocks per SM the register budget is sized for (shared memory
-  // allows about 4 blocks of 8 warps at degree <= 6 and 3 at degree 7)
-  static constexpr int MINB = R == 1 ? 4 : 2;
-  // operator image in shared memory (floats)
-  static constexpr int PPT = 0;               // [n*Q + q]  = Pp(q, n)
-  static constexpr int PW = PPT + N * Q;      // [q*N + i]  = Pp(q, i) wi(q)
-  static constexpr int GX = PW + Q * N;       // [k*N + i]  = GX(i, k)
-  static constexpr int GY = GX + N * N;       // [k*N + i]  = GY(i, k)
-  static constexpr int TRT = GY + N * N;      // [n*TG + l] = TR(l, n), l = s*G + j
-  static constexpr int LIFT = TRT + N * TG;   // [l*N + i]  = TR(l, i)
-  static constexpr int PWALL = LIFT + TG * N; // [k*N + i]  = Pwall(i, k)
-  static constexpr int WIF = PWALL + N * N;   // [j] = wif(j)
-  static constexpr int NOPS = (WIF + G + 3) / 4 * 4;
-  // per-warp scratch (floats)
-  static constexpr int S_U = 0, S_V = N, S_H = 2 * N;
-  static constexpr int S_Q = 3 * N;           // qxx, qxy, qyx, qyy
-  static constexpr int S_VEC = 7 * N;         // six combined vectors
-  static constexpr int S_UH = 13 * N, S_VH = 14 * N, S_TMP = 15 * N;
-  static constexpr int S_GL = 16 * N;         // 4 face vectors of TG
-  static constexpr int S_QP = S_GL + 4 * TG;  // 7 quadrature vectors of Q
-  static constexpr int WS = (S_QP + 7 * Q + 3) / 4 * 4;
-  static_assert(TG <= 32, "face points of one element must fit one warp");
-  static_assert(N <= 64 && Q <= 64, "two rows per lane at most");
-};
-
-struct MxArgs {
-  int ne;
-  const float *ops;
-  DevMesh m;
-  const float *tr_in;  // [3][ne][TS] trace records of the stage input (u, v, h)
-  float *tr_out;       // [3][ne][TS] trace records of the next stage input
-  float *y;            // [3][ne][N] stage input (FP32); replaced by the next one
-  float *part;         // [3][ne][N] partial load vectors (u, v, h)
-  float *trq;          // [6][ne][TS] trace records of qxx, qxy, qyx, qyy, uh, vh
-  const float *hbq, *fcq, *w0q, *z0q;  // [ne][Q]; w0q / z0q null when zero
-  float mu0, mb0, g0, hh0;
-  int stage;           // 0..3 RK4 stage; -1: write the tendency to k64
-  double dt, dt6;
-  double *c64, *acc, *k64;  // [3][ne][N] psi coefficients, FP64
-  int *flag;
-};
-
-__device__ __forceinline__ float fma32(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-
-template <class Dm>
-__device__ void stage_mx_ops(float *s, const float *g) {
-  const float4 *src = reinterpret_cast<const float4 *>(g);
-  float4 *dst = reinterpret_cast<float4 *>(s);
-  for (int i = threadIdx.x; i < Dm::NOPS / 4; i += blockDim.x) dst[i] = src[i];
-}
-
-// The face of side k of element e as element e sees it.
-struct FaceRef {
-  int f, nb, s2;
-  float sig, nx, ny;  // sig = its * 0.5 (the tri_f factor); nx, ny = norm(., f)
-  bool wall;
-};
-
-__device__ __forceinline__ FaceRef face_ref(const DevMesh &m, int e, int k) {
-  FaceRef r;
-  r.f = m.itm[3 * e + k];
-  const int isg = m.its[3 * e + k];
-  const int t1 = m.tseg[2 * r.f], t2 = m.tseg[2 * r.f + 1];
-  r.nb = isg > 0 ? t2 : t1;
-  r.s2 = isg > 0 ? m.ssit[2 * r.f + 1] : m.ssit[2 * r.f];
-  r.wall = t2 < 0;
-  r.sig = isg > 0 ? 0.5f : -0.5f;
-  r.nx = (float)m.norm[2 * r.f];
-  r.ny = (float)m.norm[2 * r.f + 1];
-  return r;
-}
-
-// Trace records.  The weak derivative of a field F on an element,
-// -int F dpsi/dx + sum_faces int psi F* n_x, is a small difference of two large
-// terms when F has a large element mean m (Gauss's theorem makes the mean's two
-// contributions cancel exactly).  In FP32 that cancellation loses up to three
-// digits, so the mean is taken out of both terms: the volume contractions skip
-// the constant mode (psi_0 = const) and the face terms use F* - m.  A trace
-// record of an element holds, for each of its 3 x ngf face points, the trace
-// of F - m, followed by m itself.
-//
-// cal_flu central value minus the own mean, on the face seen from side k,
-// point j of element e: own trace and the neighbour's trace at the mirrored
-// point (src/calflu.f:45-62); a wall face keeps the own trace
-// (src/calflu.f:35-39).
-template <int G>
-__device__ __forceinline__ float face_value(const float *tr, const FaceRef &r, int e, int l, int j) {
-  constexpr int TG = 3 * G, TS = TG + 1;
-  const float own = tr[(size_t)e * TS + l];
-  if (r.wall) return own;
-  const float *nb = tr + (size_t)r.nb * TS;
-  return 0.5f * (own + nb[r.s2 * G + (G - 1 - j)] + (nb[TG] - tr[(size_t)e * TS + TG]));
-}
 
 // Trace record (mean-free traces, then the mean) of up to six fields held in
 // the warp's shared vectors x[f] (psi coefficients); written by lanes 0..TG.
@@ -719,6 +617,9 @@ struct MixedCtx {
   double *c64 = nullptr, *acc = nullptr, *k64 = nullptr, *cin = nullptr;
   float *y = nullptr, *tr[2]{}, *part = nullptr, *trq = nullptr;
   float *hbq = nullptr, *fcq = nullptr, *w0q = nullptr, *z0q = nullptr;
+  float *tcimg = nullptr;  // operator image of the tensor-core volume kernel
+  bool tc = false;         // nonlinear volume work on the tensor cores
+  float psi0 = 0.f, wif[10]{};
   template <class T>
   cudaError_t alloc(T **p, size_t n) {
     cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
@@ -732,11 +633,7 @@ struct MixedCtx {
 
 namespace {
 
-// Host construction of the psi-basis operators, FP64.
-struct PsiOps {
-  int N, Q, G;
-  std::vector<double> U, Ui, Pp, GX, GY, TR, PWALL;
-};
+// Host construction of the psi-basis operators, FP64 (PsiOps: spoc_mixed_dev.cuh).
 
 bool build_psi(const spoc_tables *t, PsiOps &p, std::string *err) {
   const int nc = t->nc, N = t->nm, Q = t->ng, G = t->ngf, NR = N - nc - 1;
@@ -908,11 +805,17 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
     if (launches) *launches += 1;
     return cudaGetLastError();
   }
+  cudaError_t tce = cudaSuccess;
   auto go = [&](MxKernel kv, MxKernel kt) {
     const int gv = grid_for(kv, smem, c->sms, c->ne);
     const int gt = grid_for(kt, smem, c->sms, c->ne);
     mark(0);
-    kv<<<gv, 32 * kMxWarps, smem, st>>>(a);
+    if (c->tc) {
+      tce = mixed_tc_vol(c->variant, c->nc, c->Q, c->G, a, c->tcimg, c->sms, st);
+      if (tce != cudaSuccess) return;
+    } else {
+      kv<<<gv, 32 * kMxWarps, smem, st>>>(a);
+    }
     mark(1);
     kt<<<gt, 32 * kMxWarps, smem, st>>>(a);
     mark(2);
@@ -921,6 +824,7 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
   if (c->variant == SPOC_FS) go(kx_vol<Dm, SPOC_FS>, kx_tend<Dm, SPOC_FS>);
   else if (c->variant == SPOC_NS) go(kx_vol<Dm, SPOC_NS>, kx_tend<Dm, SPOC_NS>);
   else go(kx_vol<Dm, SPOC_INV>, kx_tend<Dm, SPOC_INV>);
+  if (tce != cudaSuccess) return tce;
   return cudaGetLastError();
 }
 
@@ -963,6 +867,8 @@ MxArgs base_args(MixedCtx *c, const DevMesh &m) {
   a.c64 = c->c64;
   a.acc = c->acc;
   a.k64 = c->k64;
+  a.psi0 = c->psi0;
+  for (int j = 0; j < 10; ++j) a.wif[j] = c->wif[j];
   return a;
 }
 
@@ -978,6 +884,14 @@ bool mixed_available(int nc, int ng, int ngf) {
 }
 
 int mixed_kernels_per_rhs(const MixedCtx *c) { return c->variant == SPOC_LIN ? 1 : 2; }
+
+bool mixed_set_tensor(MixedCtx *c, bool on) {
+  if (on && !c->tcimg) return false;
+  c->tc = on;
+  return true;
+}
+
+bool mixed_uses_tensor(const MixedCtx *c) { return c->tc; }
 
 int mixed_create(MixedCtx **out, const spoc_tables *t, int variant, int ne, int sms,
                  std::string *err) {
@@ -1002,9 +916,18 @@ int mixed_create(MixedCtx **out, const spoc_tables *t, int variant, int ne, int 
     using Dm = decltype(d);
     img = ops_image<Dm>(p, t);
   });
+  c->psi0 = (float)p.TR[0];  // trace of the constant mode: its value
+  for (int j = 0; j < t->ngf && j < 10; ++j) c->wif[j] = (float)t->wif[j];
+  std::vector<float> tcimg;
+  if (variant != SPOC_LIN && mixed_tc_available(t->nc, t->ng, t->ngf))
+    tcimg = mixed_tc_image(t->nc, t->ng, t->ngf, p, t->wi);
   const size_t fn = (size_t)ne * p.N, tn = (size_t)ne * (3 * p.G + 1), qn = (size_t)ne * p.Q;
   cudaError_t ce = c->alloc(&c->ops, img.size());
   if (ce == cudaSuccess) ce = cudaMemcpy(c->ops, img.data(), sizeof(float) * img.size(), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess && !tcimg.empty()) ce = c->alloc(&c->tcimg, tcimg.size());
+  if (ce == cudaSuccess && !tcimg.empty())
+    ce = cudaMemcpy(c->tcimg, tcimg.data(), sizeof(float) * tcimg.size(), cudaMemcpyHostToDevice);
+  c->tc = !tcimg.empty();
   if (ce == cudaSuccess) ce = c->alloc(&c->U, p.U.size());
   if (ce == cudaSuccess) ce = cudaMemcpy(c->U, p.U.data(), sizeof(double) * p.U.size(), cudaMemcpyHostToDevice);
   if (ce == cudaSuccess) ce = c->alloc(&c->Ui, p.Ui.size());

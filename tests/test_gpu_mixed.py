@@ -15,6 +15,16 @@ from spoc_b200 import api
 from spoc_b200 import workloads as W
 
 NAMES = ["c1_lin_p3", "c2_fs_p6", "c3_inv_p7", "c4_ns_p4"]
+# 'templated': FP32 pipes; 'tensor': tcgen05 volume kernel (nonlinear variants)
+PATHS = ["templated", "tensor"]
+
+
+def mixed(p, path="tensor"):
+    s = W.make_solver(p, "mixed")
+    if path == "tensor" and p.cfg.variant == "lin":
+        pytest.skip("the linear variant has no tensor-core kernel")
+    s.set_kernel_path(path)
+    return s
 
 
 def rel(T, M, a, b):
@@ -29,8 +39,9 @@ def tables(p):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("name", NAMES)
-def test_rhs_matches_fp64(name):
+def test_rhs_matches_fp64(name, path):
     """The initial states are in geostrophic balance, where the u, v
     tendencies are small residuals of large cancelling terms; the comparison
     uses an unbalanced state (u reversed)."""
@@ -38,7 +49,7 @@ def test_rhs_matches_fp64(name):
     OT, OM = tables(p)
     x = (-p.u, -p.v, p.h)
     ref = W.make_solver(p, "fp64").cal_var(*x)
-    mx = W.make_solver(p, "mixed").cal_var(*x)
+    mx = mixed(p, path).cal_var(*x)
     for a, b, tol in zip(mx, ref, (1e-4, 1e-4, 1e-5)):
         if O.mass_norm(OT, OM, b) == 0.0:
             assert np.abs(a).max() == 0.0
@@ -57,13 +68,14 @@ def test_state_round_trip(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["c1_lin_p3", "c2_fs_p6", "c3_inv_p7", "c4_ns_p4"])
-def test_rk4_steps_match_fp64(name):
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("name", NAMES)
+def test_rk4_steps_match_fp64(name, path):
     p = W.build_problem(W.small(W.CONFIGS[name], 8))
     OT, OM = tables(p)
     out = []
     for prec in ("fp64", "mixed"):
-        s = W.make_solver(p, prec)
+        s = W.make_solver(p, prec) if prec == "fp64" else mixed(p, path)
         s.set_state(p.u, p.v, p.h)
         s.rk4_steps(p.dt, 100)
         out.append(s.get_state())
@@ -102,10 +114,11 @@ def test_cal_var_keeps_the_resident_state():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("name", NAMES)
-def test_mass_conserved(name):
+def test_mass_conserved(name, path):
     p = W.build_problem(W.small(W.CONFIGS[name], 8))
-    s = W.make_solver(p, "mixed")
+    s = mixed(p, path)
     s.set_state(p.u, p.v, p.h)
     m0 = s.energy()[2]
     s.rk4_steps(p.dt, 50)
@@ -136,4 +149,32 @@ def test_untabulated_degree_is_rejected():
     T2 = api.build_tables(3, 25, 5)  # degree 3 with the degree-4 rules: not instantiated
     with pytest.raises(api.SpocError) as ei:
         api.Solver(T2, p.mesh, "lin", "mixed")
+    assert ei.value.code == 7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c2_fs_p6", "c3_inv_p7", "c4_ns_p4"])
+def test_tensor_and_fp32_pipes_agree(name):
+    """The tcgen05 kernel (three-term TF32 split) and the FP32-FMA kernel
+    compute the same right-hand side to FP32 rounding; mesh of 2 x 12 x 12
+    elements spans several 128-element tiles and a partial last tile."""
+    p = W.build_problem(W.small(W.CONFIGS[name], 12))
+    OT, OM = tables(p)
+    x = (-p.u, -p.v, p.h)
+    a = mixed(p, "templated").cal_var(*x)
+    b = mixed(p, "tensor").cal_var(*x)
+    ref = W.make_solver(p, "fp64").cal_var(*x)
+    for f in range(3):
+        # the two FP32 results differ from each other by no more than each
+        # differs from FP64
+        d = rel(OT, OM, a[f], b[f])
+        assert d <= 2.0 * max(rel(OT, OM, a[f], ref[f]), rel(OT, OM, b[f], ref[f])) + 1e-7, (f, d)
+
+
+@pytest.mark.gpu
+def test_tensor_path_refused_for_fp64():
+    p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 4))
+    s = W.make_solver(p, "fp64")
+    with pytest.raises(api.SpocError) as ei:
+        s.set_kernel_path("tensor")
     assert ei.value.code == 7
