@@ -72,6 +72,7 @@ struct TcDims {
 };
 
 constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr int kTcThreads = 256;  // two threads per element of the 128-element tile
 
 // Two A buffers, one mbarrier each, one commit per group; a buffer is
 // rewritten, or the accumulators of its group read, only after waiting for
@@ -104,7 +105,7 @@ __device__ __forceinline__ void sync_for_mma() {
 
 // this thread's row of A buffer b (kpad columns): four values at column k
 template <class T>
-__device__ __forceinline__ void put4(float *sm, int b, int kpad, int k, float x0, float x1,
+__device__ __forceinline__ void put4(float *sm, int b, int kpad, int row, int k, float x0, float x1,
                                      float x2, float x3) {
   float4 h, l;
   tc::split_tf32(x0, h.x, l.x);
@@ -112,14 +113,14 @@ __device__ __forceinline__ void put4(float *sm, int b, int kpad, int k, float x0
   tc::split_tf32(x2, h.z, l.z);
   tc::split_tf32(x3, h.w, l.w);
   float *hi = sm + T::O_A + b * T::ABUF;
-  const uint32_t o = tc::kmaj_off(threadIdx.x, k, kpad) / 4;
+  const uint32_t o = tc::kmaj_off(row, k, kpad) / 4;
   *reinterpret_cast<float4 *>(hi + o) = h;
   *reinterpret_cast<float4 *>(hi + 128 * T::KA + o) = l;
 }
 template <class T>
-__device__ __forceinline__ void put8(float *sm, int b, int kpad, int k, const float (&x)[8]) {
-  put4<T>(sm, b, kpad, k, x[0], x[1], x[2], x[3]);
-  put4<T>(sm, b, kpad, k + 4, x[4], x[5], x[6], x[7]);
+__device__ __forceinline__ void put8(float *sm, int b, int kpad, int row, int k, const float (&x)[8]) {
+  put4<T>(sm, b, kpad, row, k, x[0], x[1], x[2], x[3]);
+  put4<T>(sm, b, kpad, row, k + 4, x[4], x[5], x[6], x[7]);
 }
 
 // MMA group (issued by thread 0): D[dcol .. dcol+n) (+)= A(b) B^T with B the
@@ -144,17 +145,20 @@ __device__ __forceinline__ void issue(float *sm, uint32_t tm, int b, int kpad, i
 }
 
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__restrict__ img) {
+__global__ void __launch_bounds__(kTcThreads, 1) kt_vol(const MxArgs a, const float *__restrict__ img) {
   using T = TcDims<Dm>;
   constexpr int N = Dm::N, Q = Dm::Q, G = Dm::G, TG = Dm::TG, TS = Dm::TS;
   constexpr int W = T::W, WQ = T::WQ, WT = T::WT, KN = T::KN, KQ = T::KQ, KT = T::KT;
   constexpr int BK = T::O_BK, BKT = T::L_BK;
   extern __shared__ __align__(1024) float sm[];
-  const int t = threadIdx.x, warp = t >> 5;
+  // two threads per element: thread t owns row t % 128 (its TMEM lane) and
+  // the 8-column chunks of parity t / 128
+  const int t = threadIdx.x, warp = t >> 5, row = t & 127, half = t >> 7;
+  auto own = [&](int c) { return ((c >> 3) & 1) == half; };
   {
     const float4 *src = reinterpret_cast<const float4 *>(img);
     float4 *dst = reinterpret_cast<float4 *>(sm);
-    for (int i = t; i < T::IMG / 4; i += 128) dst[i] = src[i];
+    for (int i = t; i < T::IMG / 4; i += kTcThreads) dst[i] = src[i];
   }
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + T::O_A + 2 * T::ABUF);
   uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 2);
@@ -166,17 +170,16 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
   }
   sync_for_mma();
   const uint32_t tm = *slot;
-  const uint32_t lrow = (uint32_t)(warp * 32) << 16;
+  const uint32_t lrow = (uint32_t)((warp & 3) * 32) << 16;
   Pipe p{mbar, {0u, 0u}, {0u, 0u}, a.flag};
   const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * TS;
-  auto ld8 = [&](int col, float (&v)[8]) {
-    tc::tmem_ld8(tm + lrow + (uint32_t)col, v);
-    tc::tmem_wait_ld();
-  };
+  // TMEM loads are issued in batches and completed with one wait
+  auto ld = [&](int col, float (&v)[8]) { tc::tmem_ld8(tm + lrow + (uint32_t)col, v); };
+  auto ldw = [&]() { tc::tmem_wait_ld(); };
   auto st8 = [&](int col, const float (&v)[8]) { tc::tmem_st8(tm + lrow + (uint32_t)col, v); };
 
   for (int tile = blockIdx.x; tile * 128 < a.ne; tile += gridDim.x) {
-    const int e = tile * 128 + t;
+    const int e = tile * 128 + row;
     const bool valid = e < a.ne;
     float ax = 0.f, bx = 0.f, ay = 0.f, by = 0.f, di = 0.f, wnx = 0.f, wny = 0.f;
     bool wall = false;
@@ -194,46 +197,55 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
 #pragma unroll
       for (int k = 0; k < 3; ++k) fr[k] = face_ref(a.m, e, k);
     }
-    auto Y = [&](int f, int k) -> float {
-      return (valid && k < N) ? a.y[f * fn + (size_t)e * N + k] : 0.f;
+    const float *yrow = a.y + (size_t)(valid ? e : 0) * N;
+    auto Y8 = [&](int f, int c, float (&v)[8]) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = (valid && c + j < N) ? __ldg(yrow + f * fn + c + j) : 0.f;
     };
 
     // ---- 1. u, v -> [GXm; GYm; Pp], h -> Pp
+#pragma unroll 1
+    for (int f = 0; f < 3; ++f) {
+      const int b = f == 1 ? 1 : 0;
+      p.wait(b);
+      for (int c = 0; c < KN; c += 8)
+        if (own(c)) {
+          float v[8];
+          Y8(f, c, v);
+          put8<T>(sm, b, KN, row, c, v);
+        }
+      sync_for_mma();
+      if (f < 2)
+        issue<T>(sm, tm, b, KN, BK, BKT, T::R_GX, 2 * W + WQ, f == 0 ? T::C_U : T::C_V, false);
+      else
+        issue<T>(sm, tm, b, KN, BK, BKT, T::R_PP, WQ, T::C_H, false);
+      p.commit(b);
+    }
     p.wait(0);
-    for (int k = 0; k < KN; k += 4) put4<T>(sm, 0, KN, k, Y(0, k), Y(0, k + 1), Y(0, k + 2), Y(0, k + 3));
-    sync_for_mma();
-    issue<T>(sm, tm, 0, KN, BK, BKT, T::R_GX, 2 * W + WQ, T::C_U, false);
-    p.commit(0);
     p.wait(1);
-    for (int k = 0; k < KN; k += 4) put4<T>(sm, 1, KN, k, Y(1, k), Y(1, k + 1), Y(1, k + 2), Y(1, k + 3));
-    sync_for_mma();
-    issue<T>(sm, tm, 1, KN, BK, BKT, T::R_GX, 2 * W + WQ, T::C_V, false);
-    p.commit(1);
-    p.wait(0);
-    for (int k = 0; k < KN; k += 4) put4<T>(sm, 0, KN, k, Y(2, k), Y(2, k + 1), Y(2, k + 2), Y(2, k + 3));
-    sync_for_mma();
-    issue<T>(sm, tm, 0, KN, BK, BKT, T::R_PP, WQ, T::C_H, false);
-    p.commit(0);
-    p.wait(1);
-    p.wait(0);
 
     // ---- 2. q: geometry on the volume parts (calvarnl_fs.f:115-164), in place
-    for (int c = 0; c < W; c += 8) {
+    for (int c = 0; c < W; c += 8)
+      if (own(c)) {
+        float gxu[8], gyu[8], gxv[8], gyv[8], r[8];
+        ld(T::C_U + c, gxu);
+        ld(T::C_U + W + c, gyu);
+        ld(T::C_V + c, gxv);
+        ld(T::C_V + W + c, gyv);
+        ldw();
 #pragma unroll
-      for (int f = 0; f < 2; ++f) {
-        const int base = f == 0 ? T::C_U : T::C_V;
-        float gx[8], gy[8], q0[8], q1[8];
-        ld8(base + c, gx);
-        ld8(base + W + c, gy);
+        for (int j = 0; j < 8; ++j) r[j] = (ay * gyu[j] - by * gxu[j]) * di;
+        st8(T::C_U + c, r);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          q0[j] = (ay * gy[j] - by * gx[j]) * di;
-          q1[j] = (bx * gx[j] - ax * gy[j]) * di;
-        }
-        st8(base + c, q0);
-        st8(base + W + c, q1);
+        for (int j = 0; j < 8; ++j) r[j] = (bx * gxu[j] - ax * gyu[j]) * di;
+        st8(T::C_U + W + c, r);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) r[j] = (ay * gyv[j] - by * gxv[j]) * di;
+        st8(T::C_V + c, r);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) r[j] = (bx * gxv[j] - ax * gyv[j]) * di;
+        st8(T::C_V + W + c, r);
       }
-    }
     tc::tmem_wait_st();
     // lifts of the u (then v) face values, accumulated onto the volume parts
 #pragma unroll 1
@@ -241,25 +253,26 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
       p.wait(0);
       p.wait(1);
       const float *tr = a.tr_in + f * tn;
-      for (int k4 = 0; k4 < KT; k4 += 4) {
-        float x[4], z[4];
+      for (int c = 0; c < KT; c += 8)
+        if (own(c)) {
+          float x[8], z[8];
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          const int l = k4 + jj;
-          x[jj] = 0.f;
-          z[jj] = 0.f;
-          if (valid && l < TG) {
-            const int side = l / G, j = l - side * G;
-            const FaceRef &r = fr[side];
-            const float fv = face_value<G>(tr, r, e, l, j);
-            const float s = r.sig * di * a.wif[r.sig > 0.f ? j : G - 1 - j];
-            x[jj] = s * r.nx * fv;
-            z[jj] = s * r.ny * fv;
+          for (int jj = 0; jj < 8; ++jj) {
+            const int l = c + jj;
+            x[jj] = 0.f;
+            z[jj] = 0.f;
+            if (valid && l < TG) {
+              const int side = l / G, j = l - side * G;
+              const FaceRef &r = fr[side];
+              const float fv = face_value<G>(tr, r, e, l, j);
+              const float s = r.sig * di * a.wif[r.sig > 0.f ? j : G - 1 - j];
+              x[jj] = s * r.nx * fv;
+              z[jj] = s * r.ny * fv;
+            }
           }
+          put8<T>(sm, 0, KT, row, c, x);
+          put8<T>(sm, 1, KT, row, c, z);
         }
-        put4<T>(sm, 0, KT, k4, x[0], x[1], x[2], x[3]);
-        put4<T>(sm, 1, KT, k4, z[0], z[1], z[2], z[3]);
-      }
       sync_for_mma();
       const int base = f == 0 ? T::C_U : T::C_V;
       issue<T>(sm, tm, 0, KT, T::O_BL, T::L_BL, 0, W, base, true);
@@ -271,43 +284,47 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
     p.wait(1);
     if (VAR == SPOC_FS && __syncthreads_or(wall)) {
       // calvarnl_fs.f:165-205: gtn = n.(grad u) t projected onto the wall sub-basis
-      for (int c = 0; c < KN; c += 8) {
-        float qa[8], qb[8], qc[8], qd[8], g[8];
-        ld8(T::C_U + c, qa);
-        ld8(T::C_U + W + c, qb);
-        ld8(T::C_V + c, qc);
-        ld8(T::C_V + W + c, qd);
+      for (int c = 0; c < KN; c += 8)
+        if (own(c)) {
+          float qa[8], qb[8], qc[8], qd[8], g[8];
+          ld(T::C_U + c, qa);
+          ld(T::C_U + W + c, qb);
+          ld(T::C_V + c, qc);
+          ld(T::C_V + W + c, qd);
+          ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          g[j] = wall ? wnx * wny * qa[j] - wnx * wnx * qc[j] + wny * wny * qb[j] - wnx * wny * qd[j]
-                      : 0.f;
-        put8<T>(sm, 0, KN, c, g);
-      }
+          for (int j = 0; j < 8; ++j)
+            g[j] = wall ? wnx * wny * qa[j] - wnx * wnx * qc[j] + wny * wny * qb[j] - wnx * wny * qd[j]
+                        : 0.f;
+          put8<T>(sm, 0, KN, row, c, g);
+        }
       sync_for_mma();
       issue<T>(sm, tm, 0, KN, BK, BKT, T::R_PW, W, T::S, false);
       p.commit(0);
       p.wait(0);
-      for (int c = 0; c < W; c += 8) {
-        float qa[8], qb[8], qc[8], qd[8], pg[8];
-        ld8(T::C_U + c, qa);
-        ld8(T::C_U + W + c, qb);
-        ld8(T::C_V + c, qc);
-        ld8(T::C_V + W + c, qd);
-        ld8(T::S + c, pg);
+      for (int c = 0; c < W; c += 8)
+        if (own(c)) {
+          float qa[8], qb[8], qc[8], qd[8], pg[8];
+          ld(T::C_U + c, qa);
+          ld(T::C_U + W + c, qb);
+          ld(T::C_V + c, qc);
+          ld(T::C_V + W + c, qd);
+          ld(T::S + c, pg);
+          ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const float g = wnx * wny * qa[j] - wnx * wnx * qc[j] + wny * wny * qb[j] - wnx * wny * qd[j];
-          const float d = wall ? pg[j] - g : 0.f;
-          qa[j] += d * wnx * wny;
-          qc[j] -= d * wnx * wnx;
-          qb[j] += d * wny * wny;
-          qd[j] -= d * wnx * wny;
+          for (int j = 0; j < 8; ++j) {
+            const float g = wnx * wny * qa[j] - wnx * wnx * qc[j] + wny * wny * qb[j] - wnx * wny * qd[j];
+            const float d = wall ? pg[j] - g : 0.f;
+            qa[j] += d * wnx * wny;
+            qc[j] -= d * wnx * wnx;
+            qb[j] += d * wny * wny;
+            qd[j] -= d * wnx * wny;
+          }
+          st8(T::C_U + c, qa);
+          st8(T::C_U + W + c, qb);
+          st8(T::C_V + c, qc);
+          st8(T::C_V + W + c, qd);
         }
-        st8(T::C_U + c, qa);
-        st8(T::C_U + W + c, qb);
-        st8(T::C_V + c, qc);
-        st8(T::C_V + W + c, qd);
-      }
       tc::tmem_wait_st();
     }
 
@@ -317,64 +334,71 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
       // pr 0: (Fxx, Fxy) -> gx;  pr 1: (Fyx, Fyy) -> gy
       const int qa = pr == 0 ? T::C_U : T::C_V;
       p.wait(0);
-      for (int c = 0; c < KN; c += 8) {
-        float q[8], f[8];
-        ld8(qa + c, q);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) f[j] = a.mu0 * q[j] - (pr == 0 ? a.g0 * Y(2, c + j) : 0.f);
-        put8<T>(sm, 0, KN, c, f);
-      }
       p.wait(1);
-      for (int c = 0; c < KN; c += 8) {
-        float q[8], f[8];
-        ld8(qa + W + c, q);
+      for (int c = 0; c < KN; c += 8)
+        if (own(c)) {
+          float q0[8], q1[8], h[8], f0[8], f1[8];
+          ld(qa + c, q0);
+          ld(qa + W + c, q1);
+          Y8(2, c, h);
+          ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) f[j] = a.mu0 * q[j] - (pr == 1 ? a.g0 * Y(2, c + j) : 0.f);
-        put8<T>(sm, 1, KN, c, f);
-      }
+          for (int j = 0; j < 8; ++j) {
+            f0[j] = a.mu0 * q0[j] - (pr == 0 ? a.g0 * h[j] : 0.f);
+            f1[j] = a.mu0 * q1[j] - (pr == 1 ? a.g0 * h[j] : 0.f);
+          }
+          put8<T>(sm, 0, KN, row, c, f0);
+          put8<T>(sm, 1, KN, row, c, f1);
+        }
       sync_for_mma();
       issue<T>(sm, tm, 0, KN, BK, BKT, T::R_GX, 2 * W, T::S, false);
       p.commit(0);
       p.wait(0);
       float acc[W];
 #pragma unroll
-      for (int c = 0; c < W; c += 8) {
-        float gx[8], gy[8];
-        ld8(T::S + c, gx);
-        ld8(T::S + W + c, gy);
+      for (int c = 0; c < W; c += 8)
+        if (own(c)) {
+          float gx[8], gy[8];
+          ld(T::S + c, gx);
+          ld(T::S + W + c, gy);
+          ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[c + j] = di * (ay * gy[j] - by * gx[j]);
-      }
+          for (int j = 0; j < 8; ++j) acc[c + j] = di * (ay * gy[j] - by * gx[j]);
+        }
       sync_for_mma();
       issue<T>(sm, tm, 1, KN, BK, BKT, T::R_GX, 2 * W, T::S, false);
       p.commit(1);
       p.wait(1);
 #pragma unroll
-      for (int c = 0; c < W; c += 8) {
-        float gx[8], gy[8];
-        ld8(T::S + c, gx);
-        ld8(T::S + W + c, gy);
+      for (int c = 0; c < W; c += 8)
+        if (own(c)) {
+          float gx[8], gy[8];
+          ld(T::S + c, gx);
+          ld(T::S + W + c, gy);
+          ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const float v = acc[c + j] + di * (bx * gx[j] - ax * gy[j]);
-          if (valid && c + j < N) a.part[pr * fn + (size_t)e * N + c + j] = v;
+          for (int j = 0; j < 8; ++j) {
+            const float v = acc[c + j] + di * (bx * gx[j] - ax * gy[j]);
+            if (valid && c + j < N) a.part[pr * fn + (size_t)e * N + c + j] = v;
+          }
         }
-      }
     }
 
     // ---- 4. trace records of q (mean-free traces, then the mean)
 #pragma unroll 1
     for (int pr = 0; pr < 2; ++pr) {
       const int qa = pr == 0 ? T::C_U : T::C_V;
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        p.wait(b);
-        for (int c = 0; c < KN; c += 8) {
-          float q[8];
-          ld8(qa + b * W + c, q);
-          put8<T>(sm, b, KN, c, q);
+      p.wait(0);
+      p.wait(1);
+      for (int c = 0; c < KN; c += 8)
+        if (own(c)) {
+          float q0[8], q1[8];
+          ld(qa + c, q0);
+          ld(qa + W + c, q1);
+          ldw();
+          put8<T>(sm, 0, KN, row, c, q0);
+          put8<T>(sm, 1, KN, row, c, q1);
         }
-      }
       sync_for_mma();
       issue<T>(sm, tm, 0, KN, BK, BKT, T::R_TR, WT, T::S + (2 * pr) * WT, false);
       p.commit(0);
@@ -383,20 +407,27 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
     }
     p.wait(0);
     p.wait(1);
-#pragma unroll 1
-    for (int f = 0; f < 4; ++f) {
-      const int qcol = (f < 2 ? T::C_U : T::C_V) + (f & 1) * W;
-      float q0[8];
-      ld8(qcol, q0);
-      float *rec = a.trq + f * tn + (size_t)(valid ? e : 0) * TS;
-      for (int c = 0; c < WT; c += 8) {
-        float v[8];
-        ld8(T::S + f * WT + c, v);
+    {
+      float m[4][8];
+      ld(T::C_U, m[0]);
+      ld(T::C_U + W, m[1]);
+      ld(T::C_V, m[2]);
+      ld(T::C_V + W, m[3]);
+      ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (valid && c + j < TG) rec[c + j] = v[j];
+      for (int f = 0; f < 4; ++f) {
+        float *rec = a.trq + f * tn + (size_t)(valid ? e : 0) * TS;
+        for (int c = 0; c < WT; c += 8)
+          if (own(c)) {
+            float v[8];
+            ld(T::S + f * WT + c, v);
+            ldw();
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              if (valid && c + j < TG) rec[c + j] = v[j];
+          }
+        if (valid && half == 0) rec[TG] = a.psi0 * m[f][0];
       }
-      if (valid) rec[TG] = a.psi0 * q0[0];
     }
 
     // ---- 5. phase B: q at the quadrature points, products, projections
@@ -404,17 +435,16 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
     for (int pr = 0; pr < 2; ++pr) {
       const int qa = pr == 0 ? T::C_U : T::C_V;
       p.wait(0);
-      for (int c = 0; c < KN; c += 8) {
-        float q[8];
-        ld8(qa + c, q);
-        put8<T>(sm, 0, KN, c, q);
-      }
       p.wait(1);
-      for (int c = 0; c < KN; c += 8) {
-        float q[8];
-        ld8(qa + W + c, q);
-        put8<T>(sm, 1, KN, c, q);
-      }
+      for (int c = 0; c < KN; c += 8)
+        if (own(c)) {
+          float q0[8], q1[8];
+          ld(qa + c, q0);
+          ld(qa + W + c, q1);
+          ldw();
+          put8<T>(sm, 0, KN, row, c, q0);
+          put8<T>(sm, 1, KN, row, c, q1);
+        }
       sync_for_mma();
       issue<T>(sm, tm, 0, KN, BK, BKT, T::R_PP, WQ, T::S, false);
       p.commit(0);
@@ -423,34 +453,38 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
       p.wait(0);
       p.wait(1);
       // integrand: pr 0: wk/H - (U Gxx + V (Gxy - fc)); pr 1: zk/H - (U (Gyx + fc) + V Gyy)
-      const int b = pr;  // buffer for the integrand
-      for (int c = 0; c < KQ; c += 8) {
-        float U[8], V[8], H[8], G1[8], G2[8], r[8];
-        ld8(T::C_U + 2 * W + c, U);
-        ld8(T::C_V + 2 * W + c, V);
-        ld8(T::C_H + c, H);
-        ld8(T::S + c, G1);
-        ld8(T::S + WQ + c, G2);
+      const int b = pr;
+      for (int c = 0; c < KQ; c += 8)
+        if (own(c)) {
+          float U[8], V[8], H[8], G1[8], G2[8], r[8];
+          ld(T::C_U + 2 * W + c, U);
+          ld(T::C_V + 2 * W + c, V);
+          ld(T::C_H + c, H);
+          ld(T::S + c, G1);
+          ld(T::S + WQ + c, G2);
+          float hb[8], fc[8], w[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int q = c + j;
-          r[j] = 0.f;
-          if (valid && q < Q) {
-            const size_t qi = (size_t)e * Q + q;
-            const float hq = H[j] + a.hbq[qi], fc = a.fcq[qi];
-            if (pr == 0) {
-              float wk = -a.mb0 * U[j];
-              if (a.w0q) wk += a.w0q[qi];
-              r[j] = wk / hq - (U[j] * G1[j] + V[j] * (G2[j] - fc));
-            } else {
-              float zk = -a.mb0 * V[j];
-              if (a.z0q) zk += a.z0q[qi];
-              r[j] = zk / hq - (U[j] * (G1[j] + fc) + V[j] * G2[j]);
-            }
+          for (int j = 0; j < 8; ++j) {
+            const int q = c + j;
+            const bool in = valid && q < Q;
+            const size_t qi = (size_t)(valid ? e : 0) * Q + (q < Q ? q : 0);
+            hb[j] = in ? __ldg(a.hbq + qi) : 1.f;
+            fc[j] = in ? __ldg(a.fcq + qi) : 0.f;
+            const float *wz = pr == 0 ? a.w0q : a.z0q;
+            w[j] = (in && wz) ? __ldg(wz + qi) : 0.f;
           }
+          ldw();
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float hq = H[j] + hb[j];
+            if (pr == 0)
+              r[j] = (w[j] - a.mb0 * U[j]) / hq - (U[j] * G1[j] + V[j] * (G2[j] - fc[j]));
+            else
+              r[j] = (w[j] - a.mb0 * V[j]) / hq - (U[j] * (G1[j] + fc[j]) + V[j] * G2[j]);
+            if (!(valid && c + j < Q)) r[j] = 0.f;
+          }
+          put8<T>(sm, b, KQ, row, c, r);
         }
-        put8<T>(sm, b, KQ, c, r);
-      }
       sync_for_mma();
       // load vector of -adu + w1 -> S + 2 WQ; of -adv + z1 -> C_U (q_xx consumed)
       issue<T>(sm, tm, b, KQ, T::O_BP, T::L_BP, 0, W, pr == 0 ? T::S + 2 * WQ : T::C_U, false);
@@ -459,21 +493,28 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
     // uh, vh integrands (U H, V H)
     p.wait(0);
     p.wait(1);
-    for (int c = 0; c < KQ; c += 8) {
-      float U[8], V[8], H[8], ru[8], rv[8];
-      ld8(T::C_U + 2 * W + c, U);
-      ld8(T::C_V + 2 * W + c, V);
-      ld8(T::C_H + c, H);
+    for (int c = 0; c < KQ; c += 8)
+      if (own(c)) {
+        float U[8], V[8], H[8], ru[8], rv[8], hb[8];
+        ld(T::C_U + 2 * W + c, U);
+        ld(T::C_V + 2 * W + c, V);
+        ld(T::C_H + c, H);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int q = c + j;
-        const float hq = (valid && q < Q) ? H[j] + a.hbq[(size_t)e * Q + q] : 0.f;
-        ru[j] = (valid && q < Q) ? U[j] * hq : 0.f;
-        rv[j] = (valid && q < Q) ? V[j] * hq : 0.f;
+        for (int j = 0; j < 8; ++j) {
+          const int q = c + j;
+          hb[j] = (valid && q < Q) ? __ldg(a.hbq + (size_t)e * Q + q) : 0.f;
+        }
+        ldw();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const bool in = valid && c + j < Q;
+          const float hq = H[j] + hb[j];
+          ru[j] = in ? U[j] * hq : 0.f;
+          rv[j] = in ? V[j] * hq : 0.f;
+        }
+        put8<T>(sm, 0, KQ, row, c, ru);
+        put8<T>(sm, 1, KQ, row, c, rv);
       }
-      put8<T>(sm, 0, KQ, c, ru);
-      put8<T>(sm, 1, KQ, c, rv);
-    }
     sync_for_mma();
     issue<T>(sm, tm, 0, KQ, T::O_BP, T::L_BP, 0, W, T::C_U + W, false);  // uh
     p.commit(0);
@@ -482,38 +523,42 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
     p.wait(0);
     p.wait(1);
     // partial load vectors of u, v: projection + phase C volume terms
-    for (int c = 0; c < W; c += 8) {
-      float gx[8], gy[8];
-      ld8(T::S + 2 * WQ + c, gx);
-      ld8(T::C_U + c, gy);
+    for (int c = 0; c < W; c += 8)
+      if (own(c)) {
+        float gx[8], gy[8];
+        ld(T::S + 2 * WQ + c, gx);
+        ld(T::C_U + c, gy);
+        ldw();
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (valid && c + j < N) {
-          const size_t gi = (size_t)e * N + c + j;
-          a.part[gi] += gx[j];
-          a.part[fn + gi] += gy[j];
-        }
-    }
+        for (int j = 0; j < 8; ++j)
+          if (valid && c + j < N) {
+            const size_t gi = (size_t)e * N + c + j;
+            a.part[gi] += gx[j];
+            a.part[fn + gi] += gy[j];
+          }
+      }
 
     // ---- 6. uh, vh: wall solves (calvarnl_fs.f:333-340, calvarnl_ns.f:249-265)
     if (__syncthreads_or(wall)) {
-      for (int c = 0; c < KN; c += 8) {
-        float uh[8], vh[8], g0v[8], g1v[8];
-        ld8(T::C_U + W + c, uh);
-        ld8(T::C_V + c, vh);
+      for (int c = 0; c < KN; c += 8)
+        if (own(c)) {
+          float uh[8], vh[8], g0v[8], g1v[8];
+          ld(T::C_U + W + c, uh);
+          ld(T::C_V + c, vh);
+          ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (VAR == SPOC_NS) {
-            g0v[j] = wall ? uh[j] : 0.f;
-            g1v[j] = wall ? vh[j] : 0.f;
-          } else {
-            g0v[j] = wall ? wnx * uh[j] + wny * vh[j] : 0.f;
-            g1v[j] = 0.f;
+          for (int j = 0; j < 8; ++j) {
+            if (VAR == SPOC_NS) {
+              g0v[j] = wall ? uh[j] : 0.f;
+              g1v[j] = wall ? vh[j] : 0.f;
+            } else {
+              g0v[j] = wall ? wnx * uh[j] + wny * vh[j] : 0.f;
+              g1v[j] = 0.f;
+            }
           }
+          put8<T>(sm, 0, KN, row, c, g0v);
+          if (VAR == SPOC_NS) put8<T>(sm, 1, KN, row, c, g1v);
         }
-        put8<T>(sm, 0, KN, c, g0v);
-        if (VAR == SPOC_NS) put8<T>(sm, 1, KN, c, g1v);
-      }
       sync_for_mma();
       issue<T>(sm, tm, 0, KN, BK, BKT, T::R_PW, W, T::S, false);
       p.commit(0);
@@ -523,45 +568,49 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
       }
       p.wait(0);
       p.wait(1);
-      for (int c = 0; c < W; c += 8) {
-        float uh[8], vh[8], p0[8], p1[8];
-        ld8(T::C_U + W + c, uh);
-        ld8(T::C_V + c, vh);
-        ld8(T::S + c, p0);
-        if (VAR == SPOC_NS) ld8(T::S + W + c, p1);
+      for (int c = 0; c < W; c += 8)
+        if (own(c)) {
+          float uh[8], vh[8], p0[8], p1[8];
+          ld(T::C_U + W + c, uh);
+          ld(T::C_V + c, vh);
+          ld(T::S + c, p0);
+          if (VAR == SPOC_NS) ld(T::S + W + c, p1);
+          ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (VAR == SPOC_NS) {
-            if (wall) {
-              uh[j] = p0[j];
-              vh[j] = p1[j];
+          for (int j = 0; j < 8; ++j) {
+            if (VAR == SPOC_NS) {
+              if (wall) {
+                uh[j] = p0[j];
+                vh[j] = p1[j];
+              }
+            } else {
+              const float d = wall ? p0[j] - (wnx * uh[j] + wny * vh[j]) : 0.f;
+              uh[j] += wnx * d;
+              vh[j] += wny * d;
             }
-          } else {
-            const float d = wall ? p0[j] - (wnx * uh[j] + wny * vh[j]) : 0.f;
-            uh[j] += wnx * d;
-            vh[j] += wny * d;
           }
+          st8(T::C_U + W + c, uh);
+          st8(T::C_V + c, vh);
         }
-        st8(T::C_U + W + c, uh);
-        st8(T::C_V + c, vh);
-      }
       tc::tmem_wait_st();
     }
-    // h volume terms (phase D): GXm (di (by uh - bx vh)) + GYm (di (ax vh - ay uh))
+    // h volume terms (phase D)
     p.wait(0);
     p.wait(1);
-    for (int c = 0; c < KN; c += 8) {
-      float uh[8], vh[8], hx[8], hy[8];
-      ld8(T::C_U + W + c, uh);
-      ld8(T::C_V + c, vh);
+    for (int c = 0; c < KN; c += 8)
+      if (own(c)) {
+        float uh[8], vh[8], hx[8], hy[8];
+        ld(T::C_U + W + c, uh);
+        ld(T::C_V + c, vh);
+        ldw();
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        hx[j] = di * (by * uh[j] - bx * vh[j]);
-        hy[j] = di * (ax * vh[j] - ay * uh[j]);
+        for (int j = 0; j < 8; ++j) {
+          hx[j] = di * (by * uh[j] - bx * vh[j]);
+          hy[j] = di * (ax * vh[j] - ay * uh[j]);
+        }
+        put8<T>(sm, 0, KN, row, c, hx);
+        put8<T>(sm, 1, KN, row, c, hy);
       }
-      put8<T>(sm, 0, KN, c, hx);
-      put8<T>(sm, 1, KN, c, hy);
-    }
     sync_for_mma();
     issue<T>(sm, tm, 0, KN, BK, BKT, T::R_GX, W, T::S + W, false);
     issue<T>(sm, tm, 1, KN, BK, BKT, T::R_GY, W, T::S + W, true);
@@ -569,21 +618,20 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
     p.commit(1);
     p.wait(0);
     p.wait(1);
-    for (int c = 0; c < W; c += 8) {
-      float hp[8];
-      ld8(T::S + W + c, hp);
+    // h partial load vector, and the A rows of uh, vh for their traces
+    for (int c = 0; c < KN; c += 8)
+      if (own(c)) {
+        float hp[8], uh[8], vh[8];
+        ld(T::S + W + c, hp);
+        ld(T::C_U + W + c, uh);
+        ld(T::C_V + c, vh);
+        ldw();
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (valid && c + j < N) a.part[2 * fn + (size_t)e * N + c + j] = hp[j];
-    }
-    // trace records of uh, vh
-    for (int c = 0; c < KN; c += 8) {
-      float uh[8], vh[8];
-      ld8(T::C_U + W + c, uh);
-      ld8(T::C_V + c, vh);
-      put8<T>(sm, 0, KN, c, uh);
-      put8<T>(sm, 1, KN, c, vh);
-    }
+        for (int j = 0; j < 8; ++j)
+          if (valid && c + j < N) a.part[2 * fn + (size_t)e * N + c + j] = hp[j];
+        put8<T>(sm, 0, KN, row, c, uh);
+        put8<T>(sm, 1, KN, row, c, vh);
+      }
     sync_for_mma();
     issue<T>(sm, tm, 0, KN, BK, BKT, T::R_TR, WT, T::S + 2 * W, false);
     p.commit(0);
@@ -591,22 +639,28 @@ __global__ void __launch_bounds__(128, 1) kt_vol(const MxArgs a, const float *__
     p.commit(1);
     p.wait(0);
     p.wait(1);
-#pragma unroll 1
-    for (int f = 0; f < 2; ++f) {
-      float m0[8];
-      ld8(f == 0 ? T::C_U + W : T::C_V, m0);
-      float *rec = a.trq + (4 + f) * tn + (size_t)(valid ? e : 0) * TS;
-      for (int c = 0; c < WT; c += 8) {
-        float v[8];
-        ld8(T::S + 2 * W + f * WT + c, v);
+    {
+      float m0[8], m1[8];
+      ld(T::C_U + W, m0);
+      ld(T::C_V, m1);
+      ldw();
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (valid && c + j < TG) rec[c + j] = v[j];
+      for (int f = 0; f < 2; ++f) {
+        float *rec = a.trq + (4 + f) * tn + (size_t)(valid ? e : 0) * TS;
+        for (int c = 0; c < WT; c += 8)
+          if (own(c)) {
+            float v[8];
+            ld(T::S + 2 * W + f * WT + c, v);
+            ldw();
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              if (valid && c + j < TG) rec[c + j] = v[j];
+          }
+        if (valid && half == 0) rec[TG] = a.psi0 * (f == 0 ? m0[0] : m1[0]);
       }
-      if (valid) rec[TG] = a.psi0 * m0[0];
     }
-    // the next tile's first A writes wait on the buffers; TMEM reads above
-    // completed (tcgen05.wait::ld) before any later MMA is issued
+    // the next tile waits on the A buffers before rewriting them; every TMEM
+    // read above completed (tcgen05.wait::ld) before the next MMA issue
   }
   p.wait(0);
   p.wait(1);
@@ -690,7 +744,7 @@ cudaError_t mixed_tc_vol(int variant, int nc, int ng, int ngf, const MxArgs &a, 
       if (ce != cudaSuccess) return;
       const int tiles = (a.ne + 127) / 128;
       const int grid = tiles < sms ? tiles : sms;
-      kern<<<grid, 128, T::SMEM, st>>>(a, img);
+      kern<<<grid, kTcThreads, T::SMEM, st>>>(a, img);
       ce = cudaGetLastError();
     };
     if (variant == SPOC_FS) go(kt_vol<Dm, SPOC_FS>);
