@@ -94,34 +94,42 @@ def timed_steps(torch, stream, flush, s, dt, nsteps):
 
 
 def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, tsteps=10):
-    """Mixed-precision form against plain FP64 on one configuration: ms per
-    step of both, relative L2 errors of eta, u, v after `steps` steps, energy
-    drift of both runs, and the roofline of the dominant mixed kernel."""
+    """Mixed-precision form against plain FP64 on one configuration, with the
+    volume work on the FP32 pipes (the default) and on the tensor cores: ms
+    per step, relative L2 errors of u, v, eta after `steps` steps, energy
+    drift of every run, and the roofline of the dominant mixed kernel."""
     cfg = W.CONFIGS[name]
     p = W.build_problem(cfg)
     mnorm = mnorm_factory(p)
     dof = 3.0 * p.T.nm * p.mesh.ne
-    res, states, drift = {}, {}, {}
-    for prec in ("fp64", "mixed"):
+    runs = [("fp64", "fp64", "auto"), ("mixed", "mixed", "templated"), ("mixed_tensor", "mixed", "tensor")]
+    res, states, drift, kms = {}, {}, {}, {}
+    for key, prec, path in runs:
         s = W.make_solver(p, prec)
+        s.set_kernel_path(path)
         s.set_stream(stream.cuda_stream)
         s.set_state(p.u, p.v, p.h)
         s.rk4_steps(p.dt, 3)
-        res[prec] = timed_steps(torch, stream, flush, s, p.dt, tsteps)
+        res[key] = timed_steps(torch, stream, flush, s, p.dt, tsteps)
         s.set_state(p.u, p.v, p.h)
         e0 = s.energy()
         s.rk4_steps(p.dt, steps)
         e1 = s.energy()
-        states[prec] = s.get_state()
-        drift[prec] = ((e1[0] + e1[1]) - (e0[0] + e0[1])) / (e0[0] + e0[1])
+        states[key] = s.get_state()
+        drift[key] = ((e1[0] + e1[1]) - (e0[0] + e0[1])) / (e0[0] + e0[1])
         if prec == "mixed":
             s.set_state(p.u, p.v, p.h)
-            kms = s.profile_rk4(p.dt, 2)
+            kms[key] = s.profile_rk4(p.dt, 2)
         s.close()
-    errs = {f: mnorm(states["mixed"][i] - states["fp64"][i]) / mnorm(states["fp64"][i])
-            for i, f in enumerate(("u", "v", "eta"))}
+
+    def errs(key):
+        return {f: mnorm(states[key][i] - states["fp64"][i]) / mnorm(states["fp64"][i])
+                for i, f in enumerate(("u", "v", "eta"))}
+
     counts = model_counts_mixed(cfg, p.mesh.ne)
-    per_launch = {n: float(kms[i]) / 8 for i, n in enumerate(counts)}
+    per_launch = {n: float(kms["mixed"][i]) / 8 for i, n in enumerate(counts)}
+    tcounts = {("kt_vol" if k == "kx_vol" else k): v for k, v in counts.items()}
+    per_launch_tc = {n: float(kms["mixed_tensor"][i]) / 8 for i, n in enumerate(tcounts)}
     dom = max(per_launch, key=per_launch.get)
     fl, by = counts[dom]
     dur = per_launch[dom] * 1e-3
@@ -131,13 +139,22 @@ def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, ts
         "fp64_ms_per_step": res["fp64"], "mixed_ms_per_step": res["mixed"],
         "fp64_value": dof / (res["fp64"] * 1e-3), "mixed_value": dof / (res["mixed"] * 1e-3),
         "speedup": res["fp64"] / res["mixed"],
-        "steps_compared": steps, "rel_l2_error_vs_fp64": errs,
-        "energy_drift": drift, "energy_drift_difference": drift["mixed"] - drift["fp64"],
+        "steps_compared": steps, "rel_l2_error_vs_fp64": errs("mixed"),
+        "energy_drift": {"fp64": drift["fp64"], "mixed": drift["mixed"]},
+        "energy_drift_difference": drift["mixed"] - drift["fp64"],
         "kernel_ms_per_launch": per_launch,
         "roofline": {"kernel": dom, "bound": "fp32", "achieved": fl / dur / 1e12, "peak": fp32,
                      "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp32,
                      "hbm_gbs": by / dur / 1e9, "traffic": NCU_TRAFFIC.get(f"{name}:{dom}"),
                      "peak_source": "measured live: spoc_fp64_peak mode 2 (FP32 FMA chains)"},
+        "tensor_core_path": {
+            "volume_kernel": "kt_vol: tcgen05 TF32 MMAs (3-term split), accumulators in TMEM",
+            "ms_per_step": res["mixed_tensor"], "value": dof / (res["mixed_tensor"] * 1e-3),
+            "speedup": res["fp64"] / res["mixed_tensor"],
+            "rel_l2_error_vs_fp64": errs("mixed_tensor"),
+            "energy_drift": drift["mixed_tensor"],
+            "kernel_ms_per_launch": per_launch_tc,
+            "traffic_kt_vol": NCU_TRAFFIC.get(f"{name}:kt_vol")},
     }
 
 
@@ -165,6 +182,7 @@ def model_counts(cfg, ne, nf):
 NCU_TRAFFIC = {
     "c2_fs_p6:kf_qphase": 19441408, "c2_fs_p6:kf_nlvol": 104103936, "c2_fs_p6:kf_tend": 108311040,
     "c3_inv_p7:kx_vol": 251344384, "c3_inv_p7:kx_tend": 468087552,
+    "c3_inv_p7:kt_vol": 250172160,
 }
 
 

@@ -104,8 +104,9 @@ void spoc_destroy(spoc_handle *h);
 #define SPOC_PATH_GENERIC 1
 #define SPOC_PATH_TEMPLATED 2
 #define SPOC_PATH_TENSOR 3 /* SPOC_MIXED only: nonlinear volume work on the tcgen05 tensor
-                              cores (the default of SPOC_PATH_AUTO for SPOC_MIXED when built for
-                              (nc, ng, ngf)); SPOC_PATH_TEMPLATED keeps it on the FP32 pipes */
+                              cores (three-term TF32 products); SPOC_PATH_AUTO and
+                              SPOC_PATH_TEMPLATED keep it on the FP32 pipes, which are more
+                              accurate (FP32 fused multiply-adds) */
 int spoc_set_kernel_path(spoc_handle *h, int path);
 /* Use an external cudaStream_t (0 = the handle's own stream). */
 int spoc_set_stream(spoc_handle *h, void *stream);

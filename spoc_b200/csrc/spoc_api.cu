@@ -421,7 +421,7 @@ extern "C" int spoc_set_kernel_path(spoc_handle *h, int path) {
   if (path == SPOC_PATH_TENSOR && (!h->mx || !mixed_set_tensor(h->mx, true)))
     return fail(SPOC_E_UNSUPPORTED, "tensor-core kernels: SPOC_MIXED, nonlinear variants, tabulated (nc, ng, ngf)");
   if (h->mx && (path == SPOC_PATH_TEMPLATED || path == SPOC_PATH_GENERIC)) mixed_set_tensor(h->mx, false);
-  if (h->mx && path == SPOC_PATH_AUTO) mixed_set_tensor(h->mx, true);
+  if (h->mx && path == SPOC_PATH_AUTO) mixed_default_path(h->mx);
   if (path == SPOC_PATH_TEMPLATED && !fast_available(h->nc, h->ng, h->ngf))
     return fail(SPOC_E_UNSUPPORTED, "no compile-time-sized kernels for this (nc, ng, ngf)");
   h->path = path;

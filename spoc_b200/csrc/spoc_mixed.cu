@@ -891,6 +891,8 @@ bool mixed_set_tensor(MixedCtx *c, bool on) {
   return true;
 }
 
+void mixed_default_path(MixedCtx *c) { c->tc = false; }
+
 bool mixed_uses_tensor(const MixedCtx *c) { return c->tc; }
 
 int mixed_create(MixedCtx **out, const spoc_tables *t, int variant, int ne, int sms,
@@ -927,7 +929,11 @@ int mixed_create(MixedCtx **out, const spoc_tables *t, int variant, int ne, int 
   if (ce == cudaSuccess && !tcimg.empty()) ce = c->alloc(&c->tcimg, tcimg.size());
   if (ce == cudaSuccess && !tcimg.empty())
     ce = cudaMemcpy(c->tcimg, tcimg.data(), sizeof(float) * tcimg.size(), cudaMemcpyHostToDevice);
-  c->tc = !tcimg.empty();
+  // default kernel family: the FP32 pipes.  The tensor-core kernel is faster
+  // at degree 7 but its three-term TF32 products are less accurate than FP32
+  // multiply-adds (C3, 1000 steps: 1.0e-5 against 2.0e-6 relative eta
+  // error), so it is chosen explicitly with SPOC_PATH_TENSOR.
+  c->tc = false;
   if (ce == cudaSuccess) ce = c->alloc(&c->U, p.U.size());
   if (ce == cudaSuccess) ce = cudaMemcpy(c->U, p.U.data(), sizeof(double) * p.U.size(), cudaMemcpyHostToDevice);
   if (ce == cudaSuccess) ce = c->alloc(&c->Ui, p.Ui.size());

@@ -54,10 +54,11 @@ cudaError_t mixed_rhs(MixedCtx *c, const DevMesh &m, const double *const in[3],
 // Kernels per right-hand side (1 linear, 2 nonlinear).
 int mixed_kernels_per_rhs(const MixedCtx *c);
 
-// Nonlinear volume kernel on the tensor cores (tcgen05, default when built
-// for the dimensions) or on the FP32 pipes; false if the tensor-core kernel
-// is not available.
+// Nonlinear volume kernel on the tensor cores (tcgen05) or on the FP32 pipes;
+// false if the tensor-core kernel is not available.
 bool mixed_set_tensor(MixedCtx *c, bool on);
+// back to the default family (FP32 pipes)
+void mixed_default_path(MixedCtx *c);
 bool mixed_uses_tensor(const MixedCtx *c);
 
 }  // namespace spoc

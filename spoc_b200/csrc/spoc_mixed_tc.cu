@@ -253,6 +253,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) kt_vol(const MxArgs a, const fl
       p.wait(0);
       p.wait(1);
       const float *tr = a.tr_in + f * tn;
+      // unrolled: the face of each point is known at compile time, so the
+      // face references stay in registers
+#pragma unroll
       for (int c = 0; c < KT; c += 8)
         if (own(c)) {
           float x[8], z[8];
