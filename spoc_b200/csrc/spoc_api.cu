@@ -858,6 +858,7 @@ struct AdjCtx {
          *aq = nullptr, *lx = nullptr, *ly = nullptr, *lh = nullptr, *lq = nullptr;
   // RK4 step work: states x, s2, s3, s4 (3 fields each), tendencies, vectors
   double *S[4][3] = {}, *K[4][3] = {}, *V[6][3] = {};
+  double *qs[3] = {};  // q of the forward stages 1-3 of the step being reversed
   // observations
   int nobs = 0, ntimes = 0, nel = 0;
   int *d_elem = nullptr, *d_el_list = nullptr, *d_el_start = nullptr, *d_obs_of = nullptr;
@@ -906,7 +907,7 @@ int adj_init(spoc_handle *h, AdjCtx *c) {
   auto A = [&](double **p, size_t k) {
     if (e == cudaSuccess) e = h->alloc(p, k);
   };
-  A(&c->qb, 4 * n); A(&c->qd, 4 * n); A(&c->tgx0, n); A(&c->tgy0, n); A(&c->tuh, n);
+  A(&c->qb, 4 * n); A(&c->qd, 4 * n); A(&c->qs[0], 4 * n); A(&c->qs[1], 4 * n); A(&c->qs[2], 4 * n); A(&c->tgx0, n); A(&c->tgy0, n); A(&c->tuh, n);
   A(&c->tvh, n); A(&c->tf, 4 * n); A(&c->agx0, n); A(&c->agy0, n); A(&c->auh, n);
   A(&c->avh, n); A(&c->af, 4 * n); A(&c->aq, 4 * n); A(&c->lx, ls); A(&c->ly, ls);
   A(&c->lh, ls); A(&c->lq, 4 * ls);
@@ -933,6 +934,18 @@ int fwd_rhs(spoc_handle *h, double *const s[3], double *const k[3]) {
 }
 
 // tangent-linear tendency: out = J(s) d
+// q of the base state s into q: the compile-time-sized kernel where there
+// is one (bit-identical), else the generic one
+int base_q(spoc_handle *h, double *const s[3], double *q) {
+  cudaError_t e = cudaErrorNotSupported;
+  if (h->path != SPOC_PATH_GENERIC && fast_available(h->nc, h->ng, h->ngf))
+    e = launch_qphase_fast(h->variant, h->op, h->mesh, s[0], s[1], q, h->st, h->sms);
+  if (e == cudaErrorNotSupported)
+    e = launch_qphase(h->variant, h->op, h->mesh, s[0], s[1], q, h->st, h->sms);
+  CK(e, "base q");
+  return SPOC_OK;
+}
+
 int tlm_rhs(spoc_handle *h, AdjCtx *c, double *const s[3], double *const d[3],
             double *const out[3]) {
   StageArgs sa{};
@@ -944,8 +957,9 @@ int tlm_rhs(spoc_handle *h, AdjCtx *c, double *const s[3], double *const d[3],
     CK(launch_lin(h->op, h->mesh, la, sa, h->st, h->sms), "tlm linear");
     return SPOC_OK;
   }
-  CK(launch_qphase(h->variant, h->op, h->mesh, s[0], s[1], c->qb, h->st, h->sms), "tlm base q");
-  CK(launch_qphase(h->variant, h->op, h->mesh, d[0], d[1], c->qd, h->st, h->sms), "tlm q");
+  int rq = base_q(h, s, c->qb);
+  if (!rq) rq = base_q(h, d, c->qd);  // the q-phase is linear: same kernel on the perturbation
+  if (rq) return rq;
   TlmArgs ta{s[0], s[1], s[2], h->hb, h->w0, h->z0, h->fc, c->qb, d[0], d[1], d[2], c->qd,
              c->tgx0, c->tgy0, c->tuh, c->tvh, c->tf, h->mu0, h->mb0, h->g0};
   CK(launch_nlvol_tlm(h->variant, h->op, h->mesh, ta, h->st, h->sms), "tlm nlvol");
@@ -955,16 +969,23 @@ int tlm_rhs(spoc_handle *h, AdjCtx *c, double *const s[3], double *const d[3],
 }
 
 // adjoint tendency: out = J(s)^T b
+// Adjoint of one right-hand side at base state s; qbase: the base state's q
+// when already computed (by the forward stages), else null.
 int adj_rhs(spoc_handle *h, AdjCtx *c, double *const s[3], double *const b[3],
-            double *const out[3]) {
+            double *const out[3], const double *qbase = nullptr) {
   if (h->variant == SPOC_LIN) {
     AdjLinArgs la{b[0], b[1], b[2], out[0], out[1], out[2], c->lx, c->ly, c->lh, h->g0, h->hh0};
     CK(launch_adj_lin(h->op, h->mesh, la, h->st, h->sms), "adjoint linear");
     return SPOC_OK;
   }
-  CK(launch_qphase(h->variant, h->op, h->mesh, s[0], s[1], c->qb, h->st, h->sms), "adjoint base q");
+  const double *qb = qbase;
+  if (!qb) {
+    const int rc = base_q(h, s, c->qb);
+    if (rc) return rc;
+    qb = c->qb;
+  }
   AdjTendArgs ta{b[0], b[1], b[2], c->agx0, c->agy0, c->af, c->auh, c->avh, c->lx, c->ly, c->lh};
-  AdjNlArgs na{s[0], s[1], s[2], h->hb, h->w0, h->z0, h->fc, c->qb, c->af, c->agx0, c->agy0,
+  AdjNlArgs na{s[0], s[1], s[2], h->hb, h->w0, h->z0, h->fc, qb, c->af, c->agx0, c->agy0,
                c->auh, c->avh, out[0], out[1], out[2], c->aq, h->mu0, h->mb0, h->g0};
   AdjQArgs qa{c->aq, out[0], out[1], c->lq};
   CK(launch_adj_nl(h->variant, h->op, h->mesh, ta, na, qa, h->st, h->sms), "adjoint");
@@ -991,14 +1012,19 @@ int zero3(spoc_handle *h, double *const x[3]) {
 }
 
 // Stage states of the RK4 step from x (S[0] = x given): S[1..3], K[0..2].
+// Forward stages of one RK4 step from S[0]; the q of each evaluated stage
+// (left in the handle's q buffer by the forward right-hand side) is kept for
+// the adjoint right-hand sides.
 int stages(spoc_handle *h, AdjCtx *c, double dt) {
   int rc;
-  if ((rc = fwd_rhs(h, c->S[0], c->K[0]))) return rc;
-  if ((rc = axpy3(h, c->S[0], 0.5 * dt, c->K[0], c->S[1]))) return rc;
-  if ((rc = fwd_rhs(h, c->S[1], c->K[1]))) return rc;
-  if ((rc = axpy3(h, c->S[0], 0.5 * dt, c->K[1], c->S[2]))) return rc;
-  if ((rc = fwd_rhs(h, c->S[2], c->K[2]))) return rc;
-  return axpy3(h, c->S[0], dt, c->K[2], c->S[3]);
+  const size_t qbytes = sizeof(double) * 4 * c->n;
+  for (int i = 0; i < 3; ++i) {
+    if ((rc = fwd_rhs(h, c->S[i], c->K[i]))) return rc;
+    if (h->variant != SPOC_LIN)
+      CK(cudaMemcpyAsync(c->qs[i], h->q, qbytes, cudaMemcpyDeviceToDevice, h->st), "keep q");
+    if ((rc = axpy3(h, c->S[0], i == 2 ? dt : 0.5 * dt, c->K[i], c->S[i + 1]))) return rc;
+  }
+  return SPOC_OK;
 }
 
 // Advance a state by nsteps forward RK4 steps in place (the handle's RK4
@@ -1032,16 +1058,17 @@ int adj_step(spoc_handle *h, AdjCtx *c, double *const x[3], double *const lam[3]
   double *const *L = lam;
   double *const *kb = c->V[0], *const *sb = c->V[1], *const *acc = c->V[2];
   if ((rc = axpby3(h, dt / 6.0, L, 0.0, L, kb))) return rc;
+  const bool nl = h->variant != SPOC_LIN;
   if ((rc = adj_rhs(h, c, c->S[3], kb, sb))) return rc;
   if ((rc = copy3(h, acc, sb))) return rc;
   if ((rc = axpby3(h, dt, sb, dt / 3.0, L, kb))) return rc;
-  if ((rc = adj_rhs(h, c, c->S[2], kb, sb))) return rc;
+  if ((rc = adj_rhs(h, c, c->S[2], kb, sb, nl ? c->qs[2] : nullptr))) return rc;
   if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
   if ((rc = axpby3(h, 0.5 * dt, sb, dt / 3.0, L, kb))) return rc;
-  if ((rc = adj_rhs(h, c, c->S[1], kb, sb))) return rc;
+  if ((rc = adj_rhs(h, c, c->S[1], kb, sb, nl ? c->qs[1] : nullptr))) return rc;
   if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
   if ((rc = axpby3(h, 0.5 * dt, sb, dt / 6.0, L, kb))) return rc;
-  if ((rc = adj_rhs(h, c, c->S[0], kb, sb))) return rc;
+  if ((rc = adj_rhs(h, c, c->S[0], kb, sb, nl ? c->qs[0] : nullptr))) return rc;
   if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
   if ((rc = axpy3(h, L, 1.0, acc, L))) return rc;
   c->adj_steps += 1;

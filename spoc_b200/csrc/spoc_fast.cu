@@ -1052,6 +1052,25 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   return cudaGetLastError();
 }
 
+// The q-phase alone (the base state's q of the tangent-linear and adjoint
+// right-hand sides).
+template <class Dm, int VAR>
+cudaError_t run_q(const DevOps &op, const DevMesh &m, const double *su, const double *sv, double *q,
+                  cudaStream_t st, int sms) {
+  static int wq = 0, gq = 0, ne_cached = -1;
+  static size_t sq = 0;
+  if (ne_cached != m.ne) {
+    wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
+    sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
+    cudaError_t e = prepare(kf_qphase<Dm, VAR>, sq);
+    if (e != cudaSuccess) return e;
+    gq = resident_grid(kf_qphase<Dm, VAR>, 32 * wq, sq, sms, m.ne, wq);
+    ne_cached = m.ne;
+  }
+  kf_qphase<Dm, VAR><<<gq, 32 * wq, sq, st>>>(op, m, su, sv, q);
+  return cudaGetLastError();
+}
+
 template <class Dm>
 cudaError_t run_lin(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
                     cudaStream_t st, int sms, cudaEvent_t *ev) {
@@ -1098,6 +1117,28 @@ bool FAST_AVAILABLE(int nc, int ng, int ngf) {
          (nc == 5 && ng == 27 && ngf == 6) || (nc == 6 && ng == 33 && ngf == 7) ||
          (nc == 7 && ng == 42 && ngf == 9);
 }
+
+#if !SPOC_FMA
+cudaError_t launch_qphase_fast(int variant, const DevOps &op, const DevMesh &m, const double *su,
+                               const double *sv, double *q, cudaStream_t st, int sms) {
+  const int nc = op.nc, ng = op.ng, ngf = op.ngf;
+  auto go = [&](auto d) -> cudaError_t {
+    using Dm = decltype(d);
+    switch (variant) {
+      case kFS: return run_q<Dm, kFS>(op, m, su, sv, q, st, sms);
+      case kNS: return run_q<Dm, kNS>(op, m, su, sv, q, st, sms);
+      case kINV: return run_q<Dm, kINV>(op, m, su, sv, q, st, sms);
+      default: return cudaErrorNotSupported;
+    }
+  };
+  if (nc == 3 && ng == 12 && ngf == 4) return go(Dims<3, 12, 4>{});
+  if (nc == 4 && ng == 25 && ngf == 5) return go(Dims<4, 25, 5>{});
+  if (nc == 5 && ng == 27 && ngf == 6) return go(Dims<5, 27, 6>{});
+  if (nc == 6 && ng == 33 && ngf == 7) return go(Dims<6, 33, 7>{});
+  if (nc == 7 && ng == 42 && ngf == 9) return go(Dims<7, 42, 9>{});
+  return cudaErrorNotSupported;
+}
+#endif
 
 cudaError_t LAUNCH_FAST(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
                         const StageArgs &sa, cudaStream_t st, int sms, long long *launches,

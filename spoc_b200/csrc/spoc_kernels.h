@@ -128,6 +128,11 @@ cudaError_t launch_rhs_fast(int variant, const DevOps &op, const DevMesh &m, con
                             const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
                             cudaEvent_t *ev = nullptr);
 
+// The compile-time-sized q-phase alone (nonlinear variants, tabulated sizes;
+// cudaErrorNotSupported otherwise); bit-identical to launch_qphase.
+cudaError_t launch_qphase_fast(int variant, const DevOps &op, const DevMesh &m, const double *su,
+                               const double *sv, double *q, cudaStream_t st, int sms);
+
 // The same kernels with fused multiply-adds (spoc_fast.cu built with SPOC_FMA=1).
 bool fast_available_fma(int nc, int ng, int ngf);
 cudaError_t launch_rhs_fast_fma(int variant, const DevOps &op, const DevMesh &m,
