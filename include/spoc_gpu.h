@@ -142,6 +142,25 @@ long long spoc_kernel_launches(spoc_handle *h);
  * 0 q-phase, 1 nonlinear volume, 2 tendency+RK4; linear: 0), *nkinds the
  * number of kinds. */
 int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms, int *nkinds);
+/* ---- ensemble of basins (no reference counterpart: the reference runs one
+ * basin per process).  Members are SPOC_MIXED handles of the free-slip variant
+ * (degree 3-6, tabulated rules), each with its own mesh, parameters, state and
+ * time step, set through the handle API.  spoc_ensemble_steps advances every
+ * member by nsteps RK4 steps with one cooperative launch per RK4 stage for
+ * all members together (replayed from a CUDA graph when use_graph != 0 and
+ * capture succeeds); the members' states are then read with spoc_get_state.
+ * Work layout: blocks_per_sm resident blocks per SM (1 .. max), dealt to the
+ * members in proportion to ne nm^2 (weight 0) or ne nm (weight 1);
+ * spoc_ensemble_configure sets it, spoc_ensemble_info reports it (graph: 1
+ * when steps run from a graph; member_blocks: blocks per member, or null). */
+typedef struct spoc_ensemble spoc_ensemble;
+int spoc_ensemble_create(int nmem, spoc_handle *const *members, spoc_ensemble **out);
+void spoc_ensemble_destroy(spoc_ensemble *e);
+int spoc_ensemble_configure(spoc_ensemble *e, int blocks_per_sm, int weight);
+int spoc_ensemble_info(spoc_ensemble *e, int *blocks_per_sm, int *max_blocks_per_sm, int *weight,
+                       int *blocks, int *graph, int *member_blocks);
+int spoc_ensemble_steps(spoc_ensemble *e, const double *dt, int nsteps, int use_graph);
+
 /* Self-test of the tcgen05 TF32 tensor-core path the mixed kernels use (no
  * reference counterpart): D (128 x n) = A (128 x K) B^T (B: n x K), row-major
  * host arrays, as one TF32 product (split 0) or the three-term hi/lo split

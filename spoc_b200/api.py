@@ -90,6 +90,12 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     sig = {
         "spoc_create": (C.c_int, [C.POINTER(_Tables), C.POINTER(_Mesh), C.c_int, C.c_int, C.POINTER(vp)]),
         "spoc_destroy": (None, [vp]),
+        "spoc_ensemble_create": (C.c_int, [C.c_int, C.POINTER(vp), C.POINTER(vp)]),
+        "spoc_ensemble_destroy": (None, [vp]),
+        "spoc_ensemble_configure": (C.c_int, [vp, C.c_int, C.c_int]),
+        "spoc_ensemble_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "spoc_ensemble_steps": (C.c_int, [vp, _DP, C.c_int, C.c_int]),
         "spoc_set_stream": (C.c_int, [vp, vp]),
         "spoc_set_kernel_path": (C.c_int, [vp, C.c_int]),
         "spoc_set_params": (C.c_int, [vp, C.POINTER(_Params)]),
@@ -497,3 +503,60 @@ class Solver:
     @property
     def launches(self) -> int:
         return int(self.lib.spoc_kernel_launches(self._h))
+
+
+class Ensemble:
+    """Members (Solver handles of precision 'mixed', free-slip, degree 3-6)
+    stepped together: one cooperative launch per RK4 stage for all members.
+    States, parameters and meshes stay in the members; each has its own dt."""
+
+    def __init__(self, members):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m._h.value for m in self.members])
+        self._e = C.c_void_p()
+        _check(self.lib.spoc_ensemble_create(len(self.members), arr, C.byref(self._e)), "ensemble_create")
+
+    def close(self) -> None:
+        if self._e:
+            self.lib.spoc_ensemble_destroy(self._e)
+            self._e = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def configure(self, blocks_per_sm: int, weight: int) -> None:
+        _check(self.lib.spoc_ensemble_configure(self._e, blocks_per_sm, weight), "ensemble_configure")
+
+    def info(self) -> dict:
+        v = [C.c_int() for _ in range(5)]
+        mb = (C.c_int * len(self.members))()
+        _check(self.lib.spoc_ensemble_info(self._e, *map(C.byref, v), mb), "ensemble_info")
+        return {"blocks_per_sm": v[0].value, "max_blocks_per_sm": v[1].value, "weight": v[2].value,
+                "blocks": v[3].value, "graph": bool(v[4].value), "member_blocks": list(mb)}
+
+    def steps(self, dts, nsteps: int, graph: bool = True) -> None:
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        _check(self.lib.spoc_ensemble_steps(self._e, _d(d), nsteps, int(graph)), "ensemble_steps")
+
+    def autotune(self, dts, nsteps: int = 3) -> dict:
+        """Times every layout (resident blocks per SM x work weight) over
+        nsteps steps after one warm-up step and keeps the fastest.  Advances
+        the members' states: set them again afterwards."""
+        import time
+        best, table = None, []
+        for bps in range(1, self.info()["max_blocks_per_sm"] + 1):
+            for weight in (0, 1):
+                self.configure(bps, weight)
+                self.steps(dts, 1)
+                t = time.perf_counter()
+                self.steps(dts, nsteps)
+                ms = (time.perf_counter() - t) * 1e3 / nsteps
+                table.append({"blocks_per_sm": bps, "weight": weight, "ms_per_step": ms})
+                if best is None or ms < best["ms_per_step"]:
+                    best = table[-1]
+        self.configure(best["blocks_per_sm"], best["weight"])
+        return {"best": best, "tried": table}

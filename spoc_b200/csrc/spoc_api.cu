@@ -1401,3 +1401,76 @@ extern "C" int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long 
   c->fwd_steps = c->adj_steps = 0;
   return SPOC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Ensemble (no reference counterpart: the reference runs one basin per process)
+
+struct spoc_ensemble {
+  std::vector<spoc_handle *> mem;
+  MixedEns *ens = nullptr;
+  ~spoc_ensemble() {
+    if (ens) mixed_ens_destroy(ens);
+  }
+};
+
+extern "C" int spoc_ensemble_create(int nmem, spoc_handle *const *members, spoc_ensemble **out) {
+  if (!out || nmem < 1 || !members) return fail(SPOC_E_ARG, "bad argument");
+  *out = nullptr;
+  std::vector<MixedCtx *> ctx;
+  std::vector<DevMesh> mesh;
+  std::vector<int *> flags;
+  for (int i = 0; i < nmem; ++i) {
+    spoc_handle *h = members[i];
+    if (!h || !h->mx || h->variant != SPOC_FS || !h->have_params)
+      return fail(SPOC_E_UNSUPPORTED,
+                  "ensemble members: SPOC_MIXED handles of the free-slip variant with parameters set");
+    if (mixed_uses_tensor(h->mx))
+      return fail(SPOC_E_UNSUPPORTED, "ensemble members run the FP32-pipe kernels");
+    CK(cudaStreamSynchronize(h->st), "synchronize member");
+    ctx.push_back(h->mx);
+    mesh.push_back(h->mesh);
+    flags.push_back(h->flag);
+  }
+  spoc_ensemble *e = new (std::nothrow) spoc_ensemble();
+  if (!e) return fail(SPOC_E_NOMEM, "host allocation");
+  e->mem.assign(members, members + nmem);
+  std::string err;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int rc = mixed_ens_create(&e->ens, ctx.data(), mesh.data(), flags.data(), nmem, sms, &err);
+  if (rc) {
+    delete e;
+    return fail(rc, err.c_str());
+  }
+  *out = e;
+  return SPOC_OK;
+}
+
+extern "C" void spoc_ensemble_destroy(spoc_ensemble *e) { delete e; }
+
+extern "C" int spoc_ensemble_configure(spoc_ensemble *e, int blocks_per_sm, int weight) {
+  if (!e) return fail(SPOC_E_ARG, "null ensemble");
+  const int rc = mixed_ens_configure(e->ens, blocks_per_sm, weight);
+  return rc ? fail(rc, "ensemble layout") : SPOC_OK;
+}
+
+extern "C" int spoc_ensemble_info(spoc_ensemble *e, int *blocks_per_sm, int *max_blocks_per_sm,
+                                  int *weight, int *blocks, int *graph, int *member_blocks) {
+  if (!e || !blocks_per_sm || !max_blocks_per_sm || !weight || !blocks || !graph)
+    return fail(SPOC_E_ARG, "null argument");
+  mixed_ens_info(e->ens, blocks_per_sm, max_blocks_per_sm, weight, blocks, graph);
+  if (member_blocks)
+    for (size_t i = 0; i < e->mem.size(); ++i) member_blocks[i] = mixed_ens_member_blocks(e->ens, (int)i);
+  return SPOC_OK;
+}
+
+extern "C" int spoc_ensemble_steps(spoc_ensemble *e, const double *dt, int nsteps, int use_graph) {
+  if (!e || !dt || nsteps < 0) return fail(SPOC_E_ARG, "bad argument");
+  CK(mixed_ens_steps(e->ens, dt, nsteps, use_graph != 0), "ensemble steps");
+  for (spoc_handle *h : e->mem) {
+    const int rc = check_flag(h);
+    if (rc) return rc;
+  }
+  return SPOC_OK;
+}

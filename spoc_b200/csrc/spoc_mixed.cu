@@ -33,8 +33,10 @@
 //   kx_lin       calvar_lin.f in one kernel.
 // Face values are the central averages of cal_flu, formed from traces that
 // each element writes for its own three sides (no face arrays).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -195,21 +197,20 @@ __device__ void finish_element(const MxArgs &a, const float *o, float *w, int e,
 // ---------------------------------------------------------------------------
 // Nonlinear variants: volume kernel (calvarnl_fs.f:88-332 and the volume terms
 // of :341-544).
+// Body shared by kx_vol and the ensemble kernel: block blk of nblk working
+// on the elements of one member; the operators are already in sm.
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_vol(const MxArgs a) {
+__device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, int nblk) {
   constexpr int N = Dm::N, Q = Dm::Q, G = Dm::G, TG = Dm::TG, R = Dm::R;
-  extern __shared__ __align__(16) float sm[];
   float *o = sm;
-  stage_mx_ops<Dm>(o, a.ops);
-  __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   float *w = sm + Dm::NOPS + wib * Dm::WS;
   float *su = w + Dm::S_U, *sv = w + Dm::S_V, *sh = w + Dm::S_H, *sq = w + Dm::S_Q;
   float *vec = w + Dm::S_VEC, *suh = w + Dm::S_UH, *svh = w + Dm::S_VH, *tmp = w + Dm::S_TMP;
   float *gl = w + Dm::S_GL, *qp = w + Dm::S_QP;
   const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
-  const int stride = gridDim.x * kMxWarps;
-  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+  const int stride = nblk * kMxWarps;
+  for (int e = blk * kMxWarps + wib; e < a.ne; e += stride) {
     const double *vp = a.m.vect + 5 * (size_t)e;
     const float ax = (float)vp[0], bx = (float)vp[1], ay = (float)vp[2], by = (float)vp[3],
                 di = (float)vp[4];
@@ -408,21 +409,26 @@ __global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_vol(const MxArgs a
   }
 }
 
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_vol(const MxArgs a) {
+  extern __shared__ __align__(16) float sm[];
+  stage_mx_ops<Dm>(sm, a.ops);
+  __syncthreads();
+  vol_body<Dm, VAR>(a, sm, blockIdx.x, gridDim.x);
+}
+
 // Nonlinear variants: face lifts of phases C and D (calvarnl_fs.f:350-544),
 // wall solves, RK4 update.
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_tend(const MxArgs a) {
+__device__ __forceinline__ void tend_body(const MxArgs &a, float *sm, int blk, int nblk) {
   constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, R = Dm::R;
-  extern __shared__ __align__(16) float sm[];
   float *o = sm;
-  stage_mx_ops<Dm>(o, a.ops);
-  __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   float *w = sm + Dm::NOPS + wib * Dm::WS;
   float *gl = w + Dm::S_GL, *tmp = w + Dm::S_TMP;
   const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
-  const int stride = gridDim.x * kMxWarps;
-  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+  const int stride = nblk * kMxWarps;
+  for (int e = blk * kMxWarps + wib; e < a.ne; e += stride) {
     const float di = (float)a.m.vect[5 * (size_t)e + 4];
     if (lane < TG) {
       const int k = lane / G, j = lane - k * G;
@@ -470,6 +476,14 @@ __global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_tend(const MxArgs 
     }
     finish_element<Dm>(a, o, w, e, t);
   }
+}
+
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_tend(const MxArgs a) {
+  extern __shared__ __align__(16) float sm[];
+  stage_mx_ops<Dm>(sm, a.ops);
+  __syncthreads();
+  tend_body<Dm, VAR>(a, sm, blockIdx.x, gridDim.x);
 }
 
 // Linear variant (calvar_lin.f:7-287) in one kernel.
@@ -1051,6 +1065,254 @@ cudaError_t mixed_rhs(MixedCtx *c, const DevMesh &m, const double *const in[3],
   a.tr_out = c->tr[c->cur];
   if (ce == cudaSuccess)
     with_dims(c->nc, c->Q, c->G, [&](auto d) { ce = run_prep<decltype(d)>(c, a, st, launches); });
+  return ce;
+}
+
+
+// ---------------------------------------------------------------------------
+// Ensemble: members with their own meshes, degrees 3-6 and time steps advance
+// together, one cooperative launch per RK4 stage for all of them.  Blocks are
+// dealt to members in proportion to their work; a block stages its member's
+// operators once, runs the volume phase on the member's elements, waits for
+// the whole grid (the face terms of the tendency phase read neighbour trace
+// records), then runs the tendency phase.  All members are free-slip
+// (calvarnl_fs.f) and use the FP32-pipe kernels.
+
+struct EnsMember {
+  MxArgs a;        // stage, tr_in and tr_out are set per launch
+  float *tr[2];
+  int nc, first_block, nblocks;
+};
+
+namespace {
+
+template <class F>
+__device__ __forceinline__ void ens_dims(int nc, F &&f) {
+  switch (nc) {
+    case 3: f(MDims<3, 12, 4>{}); break;
+    case 4: f(MDims<4, 25, 5>{}); break;
+    case 5: f(MDims<5, 27, 6>{}); break;
+    default: f(MDims<6, 33, 7>{}); break;
+  }
+}
+
+constexpr int kEnsMinBlocks = 4;  // degrees 3-6: one row per lane, 64 registers
+
+__global__ void __launch_bounds__(32 * kMxWarps, kEnsMinBlocks)
+    kx_ens_stage(const EnsMember *__restrict__ mem, const int *__restrict__ blk_member, int stage,
+                 int cur) {
+  extern __shared__ __align__(16) float sm[];
+  const EnsMember &em = mem[blk_member[blockIdx.x]];
+  MxArgs a = em.a;
+  a.stage = stage;
+  a.tr_in = em.tr[cur];
+  a.tr_out = em.tr[cur ^ 1];
+  const int lb = blockIdx.x - em.first_block, nb = em.nblocks;
+  ens_dims(em.nc, [&](auto d) { stage_mx_ops<decltype(d)>(sm, a.ops); });
+  __syncthreads();
+  ens_dims(em.nc, [&](auto d) { vol_body<decltype(d), SPOC_FS>(a, sm, lb, nb); });
+  cooperative_groups::this_grid().sync();
+  ens_dims(em.nc, [&](auto d) { tend_body<decltype(d), SPOC_FS>(a, sm, lb, nb); });
+}
+
+size_t ens_smem() { return mx_smem<MDims<6, 33, 7>>(); }
+
+}  // namespace
+
+struct MixedEns {
+  std::vector<MixedCtx *> mem;
+  std::vector<DevMesh> mesh;
+  std::vector<int *> flag;
+  std::vector<double> dt;
+  std::vector<int> nb;  // blocks of each member under the current layout
+  int sms = 148, bps = 0, weight = 0, nblk = 0, max_bps = 1;
+  EnsMember *d_mem = nullptr;
+  int *d_blk = nullptr;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool graph_ok = true;
+  ~MixedEns() {
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaFree(d_mem);
+    cudaFree(d_blk);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace {
+
+// Blocks per member in proportion to its work (weight 0: ne nm^2, 1: ne nm),
+// at least one each.
+int ens_layout(MixedEns *e) {
+  const int n = (int)e->mem.size();
+  const int total = e->bps * e->sms;
+  if (total < n) return SPOC_E_UNSUPPORTED;
+  std::vector<double> w(n);
+  double sw = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double N = e->mem[i]->N;
+    w[i] = (double)e->mem[i]->ne * (e->weight == 0 ? N * N : N);
+    sw += w[i];
+  }
+  std::vector<int> nb(n, 1);
+  int left = total - n;
+  for (int i = 0; i < n; ++i) {
+    const int extra = (int)std::floor(left * w[i] / sw);
+    nb[i] += extra;
+  }
+  int used = 0;
+  for (int v : nb) used += v;
+  for (int i = 0; used < total; i = (i + 1) % n, ++used) ++nb[i];  // remainder
+  e->nb = nb;
+  std::vector<EnsMember> hm(n);
+  std::vector<int> blk;
+  for (int i = 0; i < n; ++i) {
+    MixedCtx *c = e->mem[i];
+    EnsMember &m = hm[i];
+    m.a = base_args(c, e->mesh[i]);
+    m.a.dt = e->dt[i];
+    m.a.dt6 = e->dt[i] / 6.0;
+    m.a.flag = e->flag[i];
+    m.tr[0] = c->tr[0];
+    m.tr[1] = c->tr[1];
+    m.nc = c->nc;
+    m.first_block = (int)blk.size();
+    m.nblocks = nb[i];
+    for (int b = 0; b < nb[i]; ++b) blk.push_back(i);
+  }
+  e->nblk = (int)blk.size();
+  cudaFree(e->d_mem);
+  cudaFree(e->d_blk);
+  e->d_mem = nullptr;
+  e->d_blk = nullptr;
+  cudaError_t ce = cudaMalloc(&e->d_mem, sizeof(EnsMember) * n);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_blk, sizeof(int) * blk.size());
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(e->d_mem, hm.data(), sizeof(EnsMember) * n, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(e->d_blk, blk.data(), sizeof(int) * blk.size(), cudaMemcpyHostToDevice);
+  if (e->exec) {
+    cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+  }
+  return ce == cudaSuccess ? SPOC_OK : SPOC_E_CUDA;
+}
+
+cudaError_t ens_launch_step(MixedEns *e, int cur0) {
+  const size_t smem = ens_smem();
+  for (int s = 0; s < 4; ++s) {
+    int stage = s, cur = (cur0 + s) & 1;
+    void *args[] = {(void *)&e->d_mem, (void *)&e->d_blk, (void *)&stage, (void *)&cur};
+    cudaError_t ce = cudaLaunchCooperativeKernel((const void *)kx_ens_stage, dim3(e->nblk),
+                                                 dim3(32 * kMxWarps), args, smem, e->st);
+    if (ce != cudaSuccess) return ce;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+int mixed_ens_create(MixedEns **out, MixedCtx *const *ctx, const DevMesh *meshes,
+                     int *const *flags, int n, int sms, std::string *err) {
+  *out = nullptr;
+  for (int i = 0; i < n; ++i)
+    if (ctx[i]->variant != SPOC_FS || ctx[i]->nc < 3 || ctx[i]->nc > 6) {
+      if (err) *err = "ensemble members: free-slip variant, degree 3-6, mixed precision";
+      return SPOC_E_UNSUPPORTED;
+    }
+  int coop = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (!coop) {
+    if (err) *err = "device has no cooperative launch";
+    return SPOC_E_UNSUPPORTED;
+  }
+  MixedEns *e = new (std::nothrow) MixedEns();
+  if (!e) return SPOC_E_NOMEM;
+  e->mem.assign(ctx, ctx + n);
+  e->mesh.assign(meshes, meshes + n);
+  e->flag.assign(flags, flags + n);
+  e->dt.assign(n, 0.0);
+  e->sms = sms;
+  const size_t smem = ens_smem();
+  cudaError_t ce = cudaFuncSetAttribute(kx_ens_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem);
+  int occ = 0;
+  if (ce == cudaSuccess)
+    ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kx_ens_stage, 32 * kMxWarps, smem);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
+  if (ce != cudaSuccess || occ < 1) {
+    if (err) *err = std::string("ensemble set-up: ") + cudaGetErrorString(ce);
+    delete e;
+    return SPOC_E_CUDA;
+  }
+  e->max_bps = occ;
+  e->bps = occ;
+  const int rc = ens_layout(e);
+  if (rc) {
+    if (err) *err = "ensemble: more members than resident blocks";
+    delete e;
+    return rc;
+  }
+  *out = e;
+  return SPOC_OK;
+}
+
+void mixed_ens_destroy(MixedEns *e) { delete e; }
+
+int mixed_ens_configure(MixedEns *e, int bps, int weight) {
+  if (bps < 1 || bps > e->max_bps || weight < 0 || weight > 1) return SPOC_E_ARG;
+  e->bps = bps;
+  e->weight = weight;
+  return ens_layout(e);
+}
+
+void mixed_ens_info(const MixedEns *e, int *bps, int *max_bps, int *weight, int *blocks,
+                    int *graph) {
+  *bps = e->bps;
+  *max_bps = e->max_bps;
+  *weight = e->weight;
+  *blocks = e->nblk;
+  *graph = e->exec != nullptr;
+}
+
+int mixed_ens_member_blocks(const MixedEns *e, int i) {
+  return (i >= 0 && i < (int)e->nb.size()) ? e->nb[i] : -1;
+}
+
+cudaError_t mixed_ens_steps(MixedEns *e, const double *dt, int nsteps, bool use_graph) {
+  bool changed = false;
+  for (size_t i = 0; i < e->mem.size(); ++i)
+    if (e->dt[i] != dt[i]) {
+      e->dt[i] = dt[i];
+      changed = true;
+    }
+  if (changed && ens_layout(e)) return cudaErrorMemoryAllocation;
+  // members step in lockstep from the trace buffer their state set-up filled
+  const int cur0 = e->mem[0]->cur;
+  for (MixedCtx *c : e->mem)
+    if (c->cur != cur0) return cudaErrorInvalidValue;
+  cudaError_t ce = cudaSuccess;
+  if (use_graph && e->graph_ok && !e->exec) {
+    cudaGraph_t g = nullptr;
+    ce = cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      const cudaError_t le = ens_launch_step(e, cur0);
+      ce = cudaStreamEndCapture(e->st, &g);
+      if (le != cudaSuccess) ce = le;
+    }
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      e->graph_ok = false;  // fall back to direct launches
+      e->exec = nullptr;
+      cudaGetLastError();
+      ce = cudaSuccess;
+    }
+  }
+  for (int it = 0; it < nsteps && ce == cudaSuccess; ++it)
+    ce = (use_graph && e->exec) ? cudaGraphLaunch(e->exec, e->st) : ens_launch_step(e, cur0);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
   return ce;
 }
 

@@ -61,4 +61,18 @@ bool mixed_set_tensor(MixedCtx *c, bool on);
 void mixed_default_path(MixedCtx *c);
 bool mixed_uses_tensor(const MixedCtx *c);
 
+// Ensemble of members (mixed precision, free-slip, degree 3-6) stepped
+// together: one cooperative launch per RK4 stage for all members, optionally
+// replayed from a CUDA graph.  Blocks are dealt to members in proportion to
+// their work: weight 0 ne nm^2, 1 ne nm; bps resident blocks per SM.
+struct MixedEns;
+int mixed_ens_create(MixedEns **out, MixedCtx *const *ctx, const DevMesh *meshes,
+                     int *const *flags, int n, int sms, std::string *err);
+void mixed_ens_destroy(MixedEns *e);
+int mixed_ens_configure(MixedEns *e, int bps, int weight);
+void mixed_ens_info(const MixedEns *e, int *bps, int *max_bps, int *weight, int *blocks,
+                    int *graph);
+int mixed_ens_member_blocks(const MixedEns *e, int i);
+cudaError_t mixed_ens_steps(MixedEns *e, const double *dt, int nsteps, bool use_graph);
+
 }  // namespace spoc

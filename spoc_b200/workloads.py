@@ -282,3 +282,133 @@ def random_observations(p: Problem, nobs: int, seed: int):
     py = rng.uniform(-0.5 * L, 0.5 * L, nobs)
     elem, xi, eta = locate(p.mesh, px, py)
     return elem, basis_at(p.cfg.nc, xi, eta), px, py
+
+
+# ---------------------------------------------------------------------------
+# Ensemble configuration C5: members on adapt.f-style refined meshes
+# ---------------------------------------------------------------------------
+
+def refine(inn: np.ndarray, x: np.ndarray, y: np.ndarray, marked: np.ndarray):
+    """One level of red refinement with green closure (src/adapt.f:532-997).
+
+    Marked triangles are split into four by their edge midpoints; a triangle
+    with two or three split edges is marked too (until none is left), and a
+    triangle with one split edge is bisected from the opposite vertex to the
+    midpoint, so the result is conforming and neighbouring levels differ by
+    at most one.  Vertex order (counter-clockwise) is kept.  inn is 0-based
+    here; returns (inn, x, y)."""
+    inn = np.asarray(inn)
+    marked = np.array(marked, dtype=bool)
+    ne = inn.shape[0]
+    edges = [(0, 1), (1, 2), (2, 0)]
+    key = lambda a, b: (a, b) if a < b else (b, a)
+    while True:
+        split = set()
+        for t in np.nonzero(marked)[0]:
+            for a, b in edges:
+                split.add(key(inn[t, a], inn[t, b]))
+        grow = []
+        for t in np.nonzero(~marked)[0]:
+            c = sum(key(inn[t, a], inn[t, b]) in split for a, b in edges)
+            if c >= 2:
+                grow.append(t)
+        if not grow:
+            break
+        marked[grow] = True
+    xs, ys = list(x), list(y)
+    mid = {}
+
+    def m(a, b):
+        k = key(a, b)
+        if k not in mid:
+            mid[k] = len(xs)
+            xs.append(0.5 * (x[a] + x[b]))
+            ys.append(0.5 * (y[a] + y[b]))
+        return mid[k]
+
+    out = []
+    for t in range(ne):
+        a, b, c = (int(v) for v in inn[t])
+        if marked[t]:
+            ab, bc, ca = m(a, b), m(b, c), m(c, a)
+            out += [(a, ab, ca), (ab, b, bc), (ca, bc, c), (ab, bc, ca)]
+            continue
+        s = [key(p, q) in split for p, q in ((a, b), (b, c), (c, a))]
+        if s[0]:
+            k = m(a, b)
+            out += [(a, k, c), (k, b, c)]
+        elif s[1]:
+            k = m(b, c)
+            out += [(a, b, k), (a, k, c)]
+        elif s[2]:
+            k = m(c, a)
+            out += [(a, b, k), (k, b, c)]
+        else:
+            out.append((a, b, c))
+    return np.array(out, dtype=np.int32), np.array(xs), np.array(ys)
+
+
+@dataclass
+class Member:
+    cfg: Config
+    center: tuple
+    radius: float
+    levels: int
+    amplitude: float
+
+
+def ensemble_members(count: int = 64, seed: int = 5) -> list:
+    """Seeded members of configuration C5: degree 3-6, free-slip, a Gaussian
+    eta bump of random centre, amplitude and width, and a mesh refined
+    around it (1-3 levels on a 48, 64 or 80 square base, 4k-40k triangles)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    tables = {3: (12, 4), 4: (25, 5), 5: (27, 6), 6: (33, 7)}
+    out = []
+    for i in range(count):
+        nc = int(rng.integers(3, 7))
+        ng, ngf = tables[nc]
+        n = int(rng.choice([48, 64, 80]))
+        cfg = Config(f"c5_member{i:02d}", "fs", nc, ng, ngf, n, beta=2.0e-11, mu0=100.0,
+                     mb0=1.0e-3, ic="bump", steps=500, seed=100 + i)
+        L = cfg.length
+        center = (float(rng.uniform(-0.2, 0.2) * L), float(rng.uniform(-0.2, 0.2) * L))
+        out.append(Member(cfg, center, float(rng.uniform(0.1, 0.2) * L), int(rng.integers(1, 4)),
+                          float(rng.uniform(0.5, 2.0))))
+    return out
+
+
+def amr_mesh(mb: Member):
+    """Square basin (rmal split) refined `levels` times around the bump, the
+    refinement radius shrinking by 0.7 per level; the refined region stays
+    away from the walls, whose elements keep the base mesh's layout."""
+    nn, inn, x, y = square_mesh(mb.cfg.n, mb.cfg.length)
+    inn = inn - 1
+    r = mb.radius
+    for _ in range(mb.levels):
+        cx = x[inn].mean(axis=1)
+        cy = y[inn].mean(axis=1)
+        marked = (cx - mb.center[0]) ** 2 + (cy - mb.center[1]) ** 2 < r * r
+        inn, x, y = refine(inn, x, y, marked)
+        r *= 0.7
+    return x.size, (inn + 1).astype(np.int32), x, y
+
+
+def build_member(mb: Member) -> Problem:
+    cfg = mb.cfg
+    T = api.build_tables(cfg.nc, cfg.ng, cfg.ngf)
+    nn, inn, x, y = amr_mesh(mb)
+    mesh = api.build_mesh(inn, x, y, cfg.nc, cfg.f0, cfg.beta)
+    px, py = api.projection_points(mesh, T)
+    w = 0.5 * mb.radius
+    eta = mb.amplitude * np.exp(-((px - mb.center[0]) ** 2 + (py - mb.center[1]) ** 2) / w ** 2)
+    ex = eta * (-2.0 * (px - mb.center[0]) / w ** 2)
+    ey = eta * (-2.0 * (py - mb.center[1]) / w ** 2)
+    f = cfg.f0 + cfg.beta * py
+    h = api.project(T, eta)
+    u = api.project(T, -cfg.g0 / f * ey)
+    v = api.project(T, cfg.g0 / f * ex)
+    hb = np.zeros((mesh.ne, T.nm))
+    hb[:, 0] = cfg.depth
+    z = np.zeros((mesh.ne, T.nm))
+    dt = cfl_dt(cfg.nc, mesh, cfg.g0, cfg.depth)
+    return Problem(cfg, T, mesh, u, v, h, hb, mesh.fc, z, z.copy(), dt)
