@@ -150,7 +150,8 @@ int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms, i
  * all members together (replayed from a CUDA graph when use_graph != 0 and
  * capture succeeds); the members' states are then read with spoc_get_state.
  * Work layout: blocks_per_sm resident blocks per SM (1 .. max), dealt to the
- * members in proportion to ne nm^2 (weight 0) or ne nm (weight 1);
+ * members in proportion to their work modelled as ne nm^p, p = 2, 1, 0.5, 0
+ * for weight 0, 1, 2, 3;
  * spoc_ensemble_configure sets it, spoc_ensemble_info reports it (graph: 1
  * when steps run from a graph; member_blocks: blocks per member, or null). */
 typedef struct spoc_ensemble spoc_ensemble;

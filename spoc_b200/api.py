@@ -543,13 +543,14 @@ class Ensemble:
         _check(self.lib.spoc_ensemble_steps(self._e, _d(d), nsteps, int(graph)), "ensemble_steps")
 
     def autotune(self, dts, nsteps: int = 3) -> dict:
-        """Times every layout (resident blocks per SM x work weight) over
+        """Times every layout (resident blocks per SM x work model ne nm^p,
+        p = 2, 1, 0.5, 0) over
         nsteps steps after one warm-up step and keeps the fastest.  Advances
         the members' states: set them again afterwards."""
         import time
         best, table = None, []
         for bps in range(1, self.info()["max_blocks_per_sm"] + 1):
-            for weight in (0, 1):
+            for weight in (0, 1, 2, 3):
                 self.configure(bps, weight)
                 self.steps(dts, 1)
                 t = time.perf_counter()

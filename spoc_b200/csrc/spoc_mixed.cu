@@ -1141,8 +1141,8 @@ struct MixedEns {
 
 namespace {
 
-// Blocks per member in proportion to its work (weight 0: ne nm^2, 1: ne nm),
-// at least one each.
+// Blocks per member in proportion to its work, modelled as ne nm^p with
+// p = 2, 1, 0.5, 0 for weight 0..3; at least one block each.
 int ens_layout(MixedEns *e) {
   const int n = (int)e->mem.size();
   const int total = e->bps * e->sms;
@@ -1151,7 +1151,8 @@ int ens_layout(MixedEns *e) {
   double sw = 0.0;
   for (int i = 0; i < n; ++i) {
     const double N = e->mem[i]->N;
-    w[i] = (double)e->mem[i]->ne * (e->weight == 0 ? N * N : N);
+    static const double expo[4] = {2.0, 1.0, 0.5, 0.0};
+    w[i] = (double)e->mem[i]->ne * std::pow(N, expo[e->weight]);
     sw += w[i];
   }
   std::vector<int> nb(n, 1);
@@ -1261,7 +1262,7 @@ int mixed_ens_create(MixedEns **out, MixedCtx *const *ctx, const DevMesh *meshes
 void mixed_ens_destroy(MixedEns *e) { delete e; }
 
 int mixed_ens_configure(MixedEns *e, int bps, int weight) {
-  if (bps < 1 || bps > e->max_bps || weight < 0 || weight > 1) return SPOC_E_ARG;
+  if (bps < 1 || bps > e->max_bps || weight < 0 || weight > 3) return SPOC_E_ARG;
   e->bps = bps;
   e->weight = weight;
   return ens_layout(e);

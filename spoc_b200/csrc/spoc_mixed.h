@@ -64,7 +64,8 @@ bool mixed_uses_tensor(const MixedCtx *c);
 // Ensemble of members (mixed precision, free-slip, degree 3-6) stepped
 // together: one cooperative launch per RK4 stage for all members, optionally
 // replayed from a CUDA graph.  Blocks are dealt to members in proportion to
-// their work: weight 0 ne nm^2, 1 ne nm; bps resident blocks per SM.
+// their work, modelled as ne nm^p with p = 2, 1, 0.5, 0 for weight 0..3;
+// bps resident blocks per SM.
 struct MixedEns;
 int mixed_ens_create(MixedEns **out, MixedCtx *const *ctx, const DevMesh *meshes,
                      int *const *flags, int n, int sms, std::string *err);

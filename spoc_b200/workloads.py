@@ -393,9 +393,15 @@ def amr_mesh(mb: Member):
     return x.size, (inn + 1).astype(np.int32), x, y
 
 
+_TABLES = {}
+
+
 def build_member(mb: Member) -> Problem:
     cfg = mb.cfg
-    T = api.build_tables(cfg.nc, cfg.ng, cfg.ngf)
+    key = (cfg.nc, cfg.ng, cfg.ngf)
+    if key not in _TABLES:
+        _TABLES[key] = api.build_tables(*key)
+    T = _TABLES[key]
     nn, inn, x, y = amr_mesh(mb)
     mesh = api.build_mesh(inn, x, y, cfg.nc, cfg.f0, cfg.beta)
     px, py = api.projection_points(mesh, T)
