@@ -158,14 +158,15 @@ def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, ts
     }
 
 
-def ensemble_measure(torch, stream, W, api, count=64, steps=500):
+def ensemble_measure(torch, stream, W, api, replicas, rank=0, world=1, count=64, steps=500):
     """Configuration C5: 64 free-slip members of degree 3-6 on their own
     refined meshes (4k-40k triangles), mixed precision, stepped together (one
     cooperative launch per RK4 stage, CUDA graph); the layout is picked by
     the autotuner.  Reports the aggregate DOF-updates/s over `steps` steps and
     each member's relative L2 eta error against its own FP64 run."""
     t0 = time.perf_counter()
-    ps = [W.build_member(m) for m in W.ensemble_members(count, seed=5)]
+    allm = W.ensemble_members(count, seed=5)
+    ps = [W.build_member(allm[i]) for i in replicas.member_share(count, rank, world)]
     build_s = time.perf_counter() - t0
     dts = [p.dt for p in ps]
     mem = []
@@ -189,6 +190,8 @@ def ensemble_measure(torch, stream, W, api, count=64, steps=500):
     ms = a.elapsed_time(b)
     info = ens.info()
     dof = sum(3.0 * p.T.nm * p.mesh.ne for p in ps)
+    # members split across GPUs (replicas): all ranks' work over the slowest time
+    ms_all, units = replicas.reduce_throughput(ms, dof * steps, world, "cuda")
     errs = []
     for p, s in zip(ps, mem):
         f = W.make_solver(p, "fp64")
@@ -201,13 +204,19 @@ def ensemble_measure(torch, stream, W, api, count=64, steps=500):
     ens.close()
     for s in mem:
         s.close()
+    if world > 1:
+        import torch.distributed as dist
+        gathered = [None] * world
+        dist.all_gather_object(gathered, errs)
+        errs = [e for g in gathered for e in g]
     ne = np.array([p.mesh.ne for p in ps])
     mb = np.array(info["member_blocks"])
     return {
-        "config": f"c5: {count} calvarnl_fs members, degree 3-6, {int(ne.min())}-{int(ne.max())} "
-                  f"triangles (refined meshes, {int(ne.sum())} in all), own dt each, {steps} steps",
-        "value": dof * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
-        "dof_per_step": dof,
+        "config": f"c5: {count} calvarnl_fs members, degree 3-6, refined meshes, own dt each, "
+                  f"{steps} steps; this rank: {len(ps)} members, {int(ne.min())}-{int(ne.max())} "
+                  f"triangles ({int(ne.sum())} in all)",
+        "value": units / (ms_all * 1e-3), "unit": UNIT, "ms_per_step": ms_all / steps,
+        "dof_per_step": units / steps, "members_split_over_ranks": world,
         "precision": "mixed (FP32 contractions, FP64 state)",
         "launches_per_step": 4, "graph": info["graph"],
         "autotuner": {"best": tune["best"], "tried": tune["tried"],
@@ -426,7 +435,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from spoc_b200 import api
+    from spoc_b200 import api, replicas
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -468,12 +477,10 @@ def main():
     clocks = sample_clocks_stop(proc, fh, clk_file, local) if rank == 0 else None
     times = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(times))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
     dof = 3.0 * nm * ne
-    value = dof * args.steps * world / (total_ms * 1e-3)
+    # replicas: all ranks' work over the slowest rank's time
+    total_ms, units = replicas.reduce_throughput(total_ms, dof * args.steps, world, "cuda")
+    value = units / (total_ms * 1e-3)
 
     # ---- e2e: host buffers through spoc_rk4_steps_host ----
     pin = [torch.from_numpy(a.copy()).pin_memory() for a in (p.u, p.v, p.h)]
@@ -491,12 +498,8 @@ def main():
         b.record(stream)
         b.synchronize()
         e_times.append(a.elapsed_time(b))
-    e_ms = float(sum(e_times))
-    if world > 1:
-        t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e2e = {"value": dof * e2e_steps * world / (e_ms * 1e-3), "unit": UNIT,
+    e_ms, e_units = replicas.reduce_throughput(float(sum(e_times)), dof * e2e_steps, world, "cuda")
+    e2e = {"value": e_units / (e_ms * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": 3 * ne * nm * 8, "d2h_bytes_per_step": 3 * ne * nm * 8}
 
     # ---- per-kernel timing and roofline of the dominant kernel ----
@@ -560,8 +563,8 @@ def main():
     if world == 1 and not args.no_mixed:
         mixed = mixed_measure(torch, stream, flush, W, api)
     ensemble = None
-    if world == 1 and not args.no_ensemble:
-        ensemble = ensemble_measure(torch, stream, W, api)
+    if not args.no_ensemble:
+        ensemble = ensemble_measure(torch, stream, W, api, replicas, rank, world)
 
     adjoint = None
     if world == 1 and not args.no_adjoint:
