@@ -27,6 +27,29 @@ namespace {
 constexpr int kT = 256;
 constexpr int kWB = kT / kWarp;
 
+// Sizes known at compile time for the tabulated (nc, ng, ngf): the kernels
+// read their sizes from op, so fixing them here lets every loop be unrolled
+// and every index be folded; RtDims keeps the runtime sizes.
+struct RtDims {
+  static constexpr int NC = 0, NG = 0, NGF = 0;
+};
+template <int NC_, int NG_, int NGF_>
+struct FixDims {
+  static constexpr int NC = NC_, NG = NG_, NGF = NGF_;
+};
+template <class D>
+__device__ __forceinline__ DevOps fixed_dims(const DevOps &in) {
+  DevOps o = in;
+  if (D::NC > 0) {
+    o.nc = D::NC;
+    o.nm = (D::NC + 1) * (D::NC + 2) / 2;
+    o.nmr = D::NC * (D::NC + 1) / 2;
+    o.ng = D::NG;
+    o.ngf = D::NGF;
+  }
+  return o;
+}
+
 __device__ __forceinline__ int wg() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 __device__ __forceinline__ int wc() { return (gridDim.x * blockDim.x) >> 5; }
 __device__ __forceinline__ double fmac(double acc, double a, double b) { return __fma_rn(a, b, acc); }
@@ -264,8 +287,9 @@ struct TaSmem {
   double g[3][kMaxModes];
 };
 
-template <int VAR>
-__global__ void __launch_bounds__(kT) k_adj_tend_a(DevOps op, DevMesh m, AdjTendArgs a) {
+template <int VAR, class D = RtDims>
+__global__ void __launch_bounds__(kT) k_adj_tend_a(DevOps op_in, DevMesh m, AdjTendArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
   __shared__ TaSmem sall[kWB];
   __shared__ double smw[kWB][kMaxModes];
   TaSmem &S = sall[threadIdx.x >> 5];
@@ -301,7 +325,9 @@ __global__ void __launch_bounds__(kT) k_adj_tend_a(DevOps op, DevMesh m, AdjTend
   }
 }
 
-__global__ void __launch_bounds__(kT) k_adj_tend_b(DevOps op, DevMesh m, AdjTendArgs a) {
+template <class D = RtDims>
+__global__ void __launch_bounds__(kT) k_adj_tend_b(DevOps op_in, DevMesh m, AdjTendArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
   __shared__ double sall[kWB][3][32];
   double(*S)[32] = sall[threadIdx.x >> 5];
   const int nm = op.nm, ne = m.ne;
@@ -333,8 +359,9 @@ struct NaSmem {
   double sm[kMaxModes];
 };
 
-template <int VAR>
-__global__ void __launch_bounds__(64) k_nlvol_adj(DevOps op, DevMesh m, AdjNlArgs a) {
+template <int VAR, class D = RtDims>
+__global__ void __launch_bounds__(64) k_nlvol_adj(DevOps op_in, DevMesh m, AdjNlArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
   __shared__ NaSmem sall[2];
   NaSmem &S = sall[threadIdx.x >> 5];
   const int nm = op.nm, ng = op.ng, ne = m.ne, l = lane_id();
@@ -434,8 +461,9 @@ __global__ void __launch_bounds__(64) k_nlvol_adj(DevOps op, DevMesh m, AdjNlArg
 // ---------------------------------------------------------------------------
 // adjoint of the q-phase (calvarnl_fs.f:88-226)
 // ---------------------------------------------------------------------------
-template <int VAR>
-__global__ void __launch_bounds__(kT) k_adj_qphase_a(DevOps op, DevMesh m, AdjQArgs a) {
+template <int VAR, class D = RtDims>
+__global__ void __launch_bounds__(kT) k_adj_qphase_a(DevOps op_in, DevMesh m, AdjQArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
   __shared__ double sall[kWB][5][kMaxModes];
   double(*S)[kMaxModes] = sall[threadIdx.x >> 5];
   const int nm = op.nm, ne = m.ne;
@@ -477,7 +505,9 @@ __global__ void __launch_bounds__(kT) k_adj_qphase_a(DevOps op, DevMesh m, AdjQA
   }
 }
 
-__global__ void __launch_bounds__(kT) k_adj_qphase_b(DevOps op, DevMesh m, AdjQArgs a) {
+template <class D = RtDims>
+__global__ void __launch_bounds__(kT) k_adj_qphase_b(DevOps op_in, DevMesh m, AdjQArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
   __shared__ double sall[kWB][4][32];
   double(*S)[32] = sall[threadIdx.x >> 5];
   const int nm = op.nm, ne = m.ne;
@@ -498,7 +528,9 @@ __global__ void __launch_bounds__(kT) k_adj_qphase_b(DevOps op, DevMesh m, AdjQA
 // ---------------------------------------------------------------------------
 // adjoint of the linear variant (calvar_lin.f:7-287)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kT) k_adj_lin_a(DevOps op, DevMesh m, AdjLinArgs a) {
+template <class D = RtDims>
+__global__ void __launch_bounds__(kT) k_adj_lin_a(DevOps op_in, DevMesh m, AdjLinArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
   __shared__ double sall[kWB][3][kMaxModes];
   __shared__ double smw[kWB][kMaxModes];
   double(*S)[kMaxModes] = sall[threadIdx.x >> 5];
@@ -535,7 +567,9 @@ __global__ void __launch_bounds__(kT) k_adj_lin_a(DevOps op, DevMesh m, AdjLinAr
   }
 }
 
-__global__ void __launch_bounds__(kT) k_adj_lin_b(DevOps op, DevMesh m, AdjLinArgs a) {
+template <class D = RtDims>
+__global__ void __launch_bounds__(kT) k_adj_lin_b(DevOps op_in, DevMesh m, AdjLinArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
   __shared__ double sall[kWB][3][32];
   double(*S)[32] = sall[threadIdx.x >> 5];
   const int nm = op.nm, ne = m.ne;
@@ -618,38 +652,63 @@ cudaError_t launch_nlvol_tlm(int variant, const DevOps &op, const DevMesh &m, co
   return cudaGetLastError();
 }
 
+namespace {
+template <class D>
+void adj_nl_kernels(int variant, const DevOps &op, const DevMesh &m, const AdjTendArgs &ta,
+                    const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int g8, int g2) {
+  switch (variant) {
+    case kFS:
+      k_adj_tend_a<kFS, D><<<g8, kT, 0, st>>>(op, m, ta);
+      k_adj_tend_b<D><<<g8, kT, 0, st>>>(op, m, ta);
+      k_nlvol_adj<kFS, D><<<g2, 64, 0, st>>>(op, m, na);
+      k_adj_qphase_a<kFS, D><<<g8, kT, 0, st>>>(op, m, qa);
+      break;
+    case kNS:
+      k_adj_tend_a<kNS, D><<<g8, kT, 0, st>>>(op, m, ta);
+      k_adj_tend_b<D><<<g8, kT, 0, st>>>(op, m, ta);
+      k_nlvol_adj<kNS, D><<<g2, 64, 0, st>>>(op, m, na);
+      k_adj_qphase_a<kNS, D><<<g8, kT, 0, st>>>(op, m, qa);
+      break;
+    default:
+      k_adj_tend_a<kINV, D><<<g8, kT, 0, st>>>(op, m, ta);
+      k_adj_tend_b<D><<<g8, kT, 0, st>>>(op, m, ta);
+      k_nlvol_adj<kINV, D><<<g2, 64, 0, st>>>(op, m, na);
+      k_adj_qphase_a<kINV, D><<<g8, kT, 0, st>>>(op, m, qa);
+      break;
+  }
+  k_adj_qphase_b<D><<<g8, kT, 0, st>>>(op, m, qa);
+}
+
+template <class D>
+void adj_lin_kernels(const DevOps &op, const DevMesh &m, const AdjLinArgs &a, cudaStream_t st, int g) {
+  k_adj_lin_a<D><<<g, kT, 0, st>>>(op, m, a);
+  k_adj_lin_b<D><<<g, kT, 0, st>>>(op, m, a);
+}
+
+template <class F>
+bool with_fixed(const DevOps &op, F &&f) {
+  if (op.nc == 3 && op.ng == 12 && op.ngf == 4) return f(FixDims<3, 12, 4>{}), true;
+  if (op.nc == 4 && op.ng == 25 && op.ngf == 5) return f(FixDims<4, 25, 5>{}), true;
+  if (op.nc == 5 && op.ng == 27 && op.ngf == 6) return f(FixDims<5, 27, 6>{}), true;
+  if (op.nc == 6 && op.ng == 33 && op.ngf == 7) return f(FixDims<6, 33, 7>{}), true;
+  if (op.nc == 7 && op.ng == 42 && op.ngf == 9) return f(FixDims<7, 42, 9>{}), true;
+  return false;
+}
+}  // namespace
+
 cudaError_t launch_adj_nl(int variant, const DevOps &op, const DevMesh &m, const AdjTendArgs &ta,
                           const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int sms) {
   const int g8 = grid_for(m.ne, sms, kWB), g2 = grid_for(m.ne, sms, 2);
-  switch (variant) {
-    case kFS:
-      k_adj_tend_a<kFS><<<g8, kT, 0, st>>>(op, m, ta);
-      k_adj_tend_b<<<g8, kT, 0, st>>>(op, m, ta);
-      k_nlvol_adj<kFS><<<g2, 64, 0, st>>>(op, m, na);
-      k_adj_qphase_a<kFS><<<g8, kT, 0, st>>>(op, m, qa);
-      break;
-    case kNS:
-      k_adj_tend_a<kNS><<<g8, kT, 0, st>>>(op, m, ta);
-      k_adj_tend_b<<<g8, kT, 0, st>>>(op, m, ta);
-      k_nlvol_adj<kNS><<<g2, 64, 0, st>>>(op, m, na);
-      k_adj_qphase_a<kNS><<<g8, kT, 0, st>>>(op, m, qa);
-      break;
-    default:
-      k_adj_tend_a<kINV><<<g8, kT, 0, st>>>(op, m, ta);
-      k_adj_tend_b<<<g8, kT, 0, st>>>(op, m, ta);
-      k_nlvol_adj<kINV><<<g2, 64, 0, st>>>(op, m, na);
-      k_adj_qphase_a<kINV><<<g8, kT, 0, st>>>(op, m, qa);
-      break;
-  }
-  k_adj_qphase_b<<<g8, kT, 0, st>>>(op, m, qa);
+  if (!with_fixed(op, [&](auto d) { adj_nl_kernels<decltype(d)>(variant, op, m, ta, na, qa, st, g8, g2); }))
+    adj_nl_kernels<RtDims>(variant, op, m, ta, na, qa, st, g8, g2);
   return cudaGetLastError();
 }
 
 cudaError_t launch_adj_lin(const DevOps &op, const DevMesh &m, const AdjLinArgs &a,
                            cudaStream_t st, int sms) {
   const int g = grid_for(m.ne, sms, kWB);
-  k_adj_lin_a<<<g, kT, 0, st>>>(op, m, a);
-  k_adj_lin_b<<<g, kT, 0, st>>>(op, m, a);
+  if (!with_fixed(op, [&](auto d) { adj_lin_kernels<decltype(d)>(op, m, a, st, g); }))
+    adj_lin_kernels<RtDims>(op, m, a, st, g);
   return cudaGetLastError();
 }
 
