@@ -18,6 +18,8 @@
 // by dot-product and finite-difference tests, not bit for bit.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "spoc_device.cuh"
 #include "spoc_kernels.h"
 
@@ -48,6 +50,15 @@ __device__ __forceinline__ DevOps fixed_dims(const DevOps &in) {
     o.ngf = D::NGF;
   }
   return o;
+}
+
+// Resident blocks per SM asked of the compiler for the heavier adjoint
+// kernels: with compile-time sizes up to degree 6 a cap of 80 registers
+// costs a few spilled words and raises the resident warps from 16 to 24
+// (these kernels are latency-bound).
+template <class D>
+constexpr int adj_min_blocks() {
+  return D::NC >= 1 && D::NC <= 6 ? 3 : 1;
 }
 
 __device__ __forceinline__ int wg() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
@@ -288,7 +299,7 @@ struct TaSmem {
 };
 
 template <int VAR, class D = RtDims>
-__global__ void __launch_bounds__(kT) k_adj_tend_a(DevOps op_in, DevMesh m, AdjTendArgs a) {
+__global__ void __launch_bounds__(kT, adj_min_blocks<D>()) k_adj_tend_a(DevOps op_in, DevMesh m, AdjTendArgs a) {
   const DevOps op = fixed_dims<D>(op_in);
   __shared__ TaSmem sall[kWB];
   __shared__ double smw[kWB][kMaxModes];
@@ -360,7 +371,7 @@ struct NaSmem {
 };
 
 template <int VAR, class D = RtDims>
-__global__ void __launch_bounds__(64) k_nlvol_adj(DevOps op_in, DevMesh m, AdjNlArgs a) {
+__global__ void __launch_bounds__(64, 4 * adj_min_blocks<D>()) k_nlvol_adj(DevOps op_in, DevMesh m, AdjNlArgs a) {
   const DevOps op = fixed_dims<D>(op_in);
   __shared__ NaSmem sall[2];
   NaSmem &S = sall[threadIdx.x >> 5];
@@ -462,7 +473,7 @@ __global__ void __launch_bounds__(64) k_nlvol_adj(DevOps op_in, DevMesh m, AdjNl
 // adjoint of the q-phase (calvarnl_fs.f:88-226)
 // ---------------------------------------------------------------------------
 template <int VAR, class D = RtDims>
-__global__ void __launch_bounds__(kT) k_adj_qphase_a(DevOps op_in, DevMesh m, AdjQArgs a) {
+__global__ void __launch_bounds__(kT, adj_min_blocks<D>()) k_adj_qphase_a(DevOps op_in, DevMesh m, AdjQArgs a) {
   const DevOps op = fixed_dims<D>(op_in);
   __shared__ double sall[kWB][5][kMaxModes];
   double(*S)[kMaxModes] = sall[threadIdx.x >> 5];
@@ -605,6 +616,29 @@ __global__ void k_axpby(size_t n, double a, const double *x, double b, const dou
     out[i] = fma(a, x[i], b * y[i]);
 }
 
+// Bookkeeping of the adjoint RK4 step after one stage adjoint sbar (3 fields,
+// n values each, one launch): see AdjCombine in spoc_kernels.h.
+__global__ void k_adj_combine(size_t n, AdjCombine c) {
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < 3 * n;
+       j += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(j / n);
+    const size_t i = j - (size_t)f * n;
+    const double L = c.lam[f][i];
+    if (c.mode == AdjCombine::kInit) {
+      c.kb[f][i] = fma(c.a, L, c.b * L);
+      continue;
+    }
+    const double sb = c.sb[f][i];
+    const double acc = c.mode == AdjCombine::kFirst ? sb : fma(1.0, sb, c.acc[f][i]);
+    if (c.mode == AdjCombine::kLast) {
+      c.lam[f][i] = fma(1.0, acc, L);
+      continue;
+    }
+    c.acc[f][i] = acc;
+    c.kb[f][i] = fma(c.a, sb, c.b * L);
+  }
+}
+
 // Observation values: obs o lies in element elem[o] with basis values
 // basis[o*nm + n]; val[o] = sum_n h(elem, n) basis(n).
 __global__ void k_obs_eval(int nobs, int nm, const int *elem, const double *basis, const double *h,
@@ -698,7 +732,8 @@ bool with_fixed(const DevOps &op, F &&f) {
 
 cudaError_t launch_adj_nl(int variant, const DevOps &op, const DevMesh &m, const AdjTendArgs &ta,
                           const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int sms) {
-  const int g8 = grid_for(m.ne, sms, kWB), g2 = grid_for(m.ne, sms, 2);
+  // k_nlvol_adj: 2-warp blocks, up to 12 resident per SM
+  const int g8 = grid_for(m.ne, sms, kWB), g2 = std::min((m.ne + 1) / 2, sms * 24);
   if (!with_fixed(op, [&](auto d) { adj_nl_kernels<decltype(d)>(variant, op, m, ta, na, qa, st, g8, g2); }))
     adj_nl_kernels<RtDims>(variant, op, m, ta, na, qa, st, g8, g2);
   return cudaGetLastError();
@@ -727,6 +762,14 @@ cudaError_t launch_axpby(size_t n, double a, const double *x, double b, const do
   if (blocks > (size_t)sms * 16) blocks = (size_t)sms * 16;
   if (blocks < 1) blocks = 1;
   k_axpby<<<(unsigned)blocks, 256, 0, st>>>(n, a, x, b, y, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_combine(size_t n, const AdjCombine &c, cudaStream_t st, int sms) {
+  size_t blocks = (3 * n + 255) / 256;
+  if (blocks > (size_t)sms * 16) blocks = (size_t)sms * 16;
+  if (blocks < 1) blocks = 1;
+  k_adj_combine<<<(unsigned)blocks, 256, 0, st>>>(n, c);
   return cudaGetLastError();
 }
 

@@ -265,16 +265,19 @@ RhsBuffers rhs_buffers(spoc_handle *h, double *const s[3]) {
   return b;
 }
 
-cudaError_t launch(spoc_handle *h, double *const s[3], const StageArgs &sa, cudaEvent_t *ev) {
+// One FP64 right-hand side or RK4 stage; q (4 ne nm values) receives the
+// nonlinear variants' q-phase output instead of the handle's buffer when given.
+cudaError_t launch(spoc_handle *h, double *const s[3], const StageArgs &sa, cudaEvent_t *ev,
+                   double *q = nullptr) {
   const bool fast = h->path != SPOC_PATH_GENERIC && fast_available(h->nc, h->ng, h->ngf);
+  RhsBuffers b = rhs_buffers(h, s);
+  if (q) b.q = q;
   if (fast && h->precision == SPOC_FP64_FMA)
-    return launch_rhs_fast_fma(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms,
-                               &h->launches, ev);
+    return launch_rhs_fast_fma(h->variant, h->op, h->mesh, b, sa, h->st, h->sms, &h->launches,
+                               ev);
   if (fast)
-    return launch_rhs_fast(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms,
-                           &h->launches, ev);
-  return launch_rhs(h->variant, h->op, h->mesh, rhs_buffers(h, s), sa, h->st, h->sms,
-                    &h->launches, ev);
+    return launch_rhs_fast(h->variant, h->op, h->mesh, b, sa, h->st, h->sms, &h->launches, ev);
+  return launch_rhs(h->variant, h->op, h->mesh, b, sa, h->st, h->sms, &h->launches, ev);
 }
 
 int check_flag(spoc_handle *h) {
@@ -519,20 +522,21 @@ extern "C" int spoc_get_state(spoc_handle *h, int ld, double *u, double *v, doub
 }
 
 namespace {
-// RK4 steps of the FP64 kernels on U0 (also used by the adjoint, which stays
-// FP64 whatever the handle's precision).
-int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps) {
+// RK4 steps of the FP64 kernels on `base` (U0 by default), in place (also
+// used by the adjoint, which stays FP64 whatever the handle's precision).
+int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *base = nullptr) {
+  if (!base) base = h->U0;
   StageArgs sa{};
   sa.dt = dt;
   sa.dt6 = dt / 6.0;  // dt / 6.d0 (src/shwwnl.f:277)
   sa.flag = h->flag;
   for (int c = 0; c < 3; ++c) {
-    sa.base[c] = h->U0[c];
+    sa.base[c] = base[c];
     sa.acc[c] = h->ACC[c];
   }
   for (int it = 0; it < nsteps; ++it) {
     for (int s = 0; s < 4; ++s) {
-      double *const *in = s == 0 ? h->U0 : (s == 2 ? h->SB : h->SA);
+      double *const *in = s == 0 ? base : (s == 2 ? h->SB : h->SA);
       double *const *out = s == 1 ? h->SB : h->SA;
       sa.stage = s;
       for (int c = 0; c < 3; ++c) sa.out[c] = out[c];
@@ -923,16 +927,6 @@ int adj_init(spoc_handle *h, AdjCtx *c) {
   return SPOC_OK;
 }
 
-// forward tendency k = f(s) with the handle's precision and kernel family
-int fwd_rhs(spoc_handle *h, double *const s[3], double *const k[3]) {
-  StageArgs sa{};
-  sa.stage = -1;
-  for (int f = 0; f < 3; ++f) sa.tend[f] = k[f];
-  sa.flag = h->flag;
-  CK(launch(h, s, sa, nullptr), "forward rhs");
-  return SPOC_OK;
-}
-
 // tangent-linear tendency: out = J(s) d
 // q of the base state s into q: the compile-time-sized kernel where there
 // is one (bit-identical), else the generic one
@@ -1011,38 +1005,34 @@ int zero3(spoc_handle *h, double *const x[3]) {
   return SPOC_OK;
 }
 
-// Stage states of the RK4 step from x (S[0] = x given): S[1..3], K[0..2].
-// Forward stages of one RK4 step from S[0]; the q of each evaluated stage
-// (left in the handle's q buffer by the forward right-hand side) is kept for
-// the adjoint right-hand sides.
-int stages(spoc_handle *h, AdjCtx *c, double dt) {
-  int rc;
-  const size_t qbytes = sizeof(double) * 4 * c->n;
+// Stage states S[1..3] of the RK4 step from x, by the forward RK4 stage
+// kernels themselves (so they equal the forward run's stage states bit for
+// bit); the nonlinear variants' q of stages 1-3 lands in qs[0..2] for the
+// adjoint right-hand sides.  K[0] is the stages' accumulator scratch.
+int stages(spoc_handle *h, AdjCtx *c, double *const x[3], double dt) {
+  StageArgs sa{};
+  sa.dt = dt;
+  sa.dt6 = dt / 6.0;
+  sa.flag = h->flag;
+  for (int f = 0; f < 3; ++f) {
+    sa.base[f] = x[f];
+    sa.acc[f] = c->K[0][f];
+  }
+  const bool nl = h->variant != SPOC_LIN;
   for (int i = 0; i < 3; ++i) {
-    if ((rc = fwd_rhs(h, c->S[i], c->K[i]))) return rc;
-    if (h->variant != SPOC_LIN)
-      CK(cudaMemcpyAsync(c->qs[i], h->q, qbytes, cudaMemcpyDeviceToDevice, h->st), "keep q");
-    if ((rc = axpy3(h, c->S[0], i == 2 ? dt : 0.5 * dt, c->K[i], c->S[i + 1]))) return rc;
+    sa.stage = i;
+    for (int f = 0; f < 3; ++f) sa.out[f] = c->S[i + 1][f];
+    CK(launch(h, i == 0 ? x : c->S[i], sa, nullptr, nl ? c->qs[i] : nullptr), "forward stage");
   }
   return SPOC_OK;
 }
 
-// Advance a state by nsteps forward RK4 steps in place (the handle's RK4
-// kernels on its own buffers).
+// Advance a state by nsteps forward RK4 steps in place.
 int advance(spoc_handle *h, AdjCtx *c, double *const x[3], double dt, int nsteps) {
   if (nsteps <= 0) return SPOC_OK;
-  int rc = copy3(h, h->U0, x);
+  int rc = enqueue_steps_fp64(h, dt, nsteps, x);
   if (rc) return rc;
-  if ((rc = enqueue_steps_fp64(h, dt, nsteps))) return rc;
   c->fwd_steps += nsteps;
-  return copy3(h, x, h->U0);
-}
-
-// out = a*x + b*y for the three fields
-int axpby3(spoc_handle *h, double a, double *const x[3], double b, double *const y[3],
-           double *const o[3]) {
-  for (int f = 0; f < 3; ++f)
-    CK(launch_axpby(fsize(h), a, x[f], b, y[f], o[f], h->st, h->sms), "axpby");
   return SPOC_OK;
 }
 
@@ -1053,24 +1043,32 @@ int axpby3(spoc_handle *h, double a, double *const x[3], double b, double *const
 // kbar1 = dt/6 lam + dt/2 s2bar, s1bar = J(s1)^T kbar1, lam += sum sbar.
 int adj_step(spoc_handle *h, AdjCtx *c, double *const x[3], double *const lam[3], double dt) {
   int rc;
-  if ((rc = copy3(h, c->S[0], x))) return rc;
-  if ((rc = stages(h, c, dt))) return rc;
-  double *const *L = lam;
+  if ((rc = stages(h, c, x, dt))) return rc;
   double *const *kb = c->V[0], *const *sb = c->V[1], *const *acc = c->V[2];
-  if ((rc = axpby3(h, dt / 6.0, L, 0.0, L, kb))) return rc;
+  AdjCombine cb{};
+  for (int f = 0; f < 3; ++f) {
+    cb.sb[f] = sb[f];
+    cb.acc[f] = acc[f];
+    cb.lam[f] = lam[f];
+    cb.kb[f] = kb[f];
+  }
+  auto combine = [&](int mode, double a, double b) {
+    cb.mode = mode;
+    cb.a = a;
+    cb.b = b;
+    CK(launch_adj_combine(c->n, cb, h->st, h->sms), "adjoint RK4 bookkeeping");
+    return SPOC_OK;
+  };
   const bool nl = h->variant != SPOC_LIN;
+  if ((rc = combine(AdjCombine::kInit, dt / 6.0, 0.0))) return rc;
   if ((rc = adj_rhs(h, c, c->S[3], kb, sb))) return rc;
-  if ((rc = copy3(h, acc, sb))) return rc;
-  if ((rc = axpby3(h, dt, sb, dt / 3.0, L, kb))) return rc;
+  if ((rc = combine(AdjCombine::kFirst, dt, dt / 3.0))) return rc;
   if ((rc = adj_rhs(h, c, c->S[2], kb, sb, nl ? c->qs[2] : nullptr))) return rc;
-  if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
-  if ((rc = axpby3(h, 0.5 * dt, sb, dt / 3.0, L, kb))) return rc;
+  if ((rc = combine(AdjCombine::kMid, 0.5 * dt, dt / 3.0))) return rc;
   if ((rc = adj_rhs(h, c, c->S[1], kb, sb, nl ? c->qs[1] : nullptr))) return rc;
-  if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
-  if ((rc = axpby3(h, 0.5 * dt, sb, dt / 6.0, L, kb))) return rc;
-  if ((rc = adj_rhs(h, c, c->S[0], kb, sb, nl ? c->qs[0] : nullptr))) return rc;
-  if ((rc = axpy3(h, acc, 1.0, sb, acc))) return rc;
-  if ((rc = axpy3(h, L, 1.0, acc, L))) return rc;
+  if ((rc = combine(AdjCombine::kMid, 0.5 * dt, dt / 6.0))) return rc;
+  if ((rc = adj_rhs(h, c, x, kb, sb, nl ? c->qs[0] : nullptr))) return rc;
+  if ((rc = combine(AdjCombine::kLast, 0.0, 0.0))) return rc;
   c->adj_steps += 1;
   return SPOC_OK;
 }
@@ -1078,10 +1076,9 @@ int adj_step(spoc_handle *h, AdjCtx *c, double *const x[3], double *const lam[3]
 // Tangent-linear RK4 step at x: d <- (dx'/dx) d.
 int tlm_step(spoc_handle *h, AdjCtx *c, double *const x[3], double *const d[3], double dt) {
   int rc;
-  if ((rc = copy3(h, c->S[0], x))) return rc;
-  if ((rc = stages(h, c, dt))) return rc;
+  if ((rc = stages(h, c, x, dt))) return rc;
   double *const *ds = c->V[0], *const *dk = c->V[1], *const *acc = c->V[2];
-  if ((rc = tlm_rhs(h, c, c->S[0], d, dk))) return rc;      // dk1
+  if ((rc = tlm_rhs(h, c, x, d, dk))) return rc;            // dk1
   if ((rc = copy3(h, acc, dk))) return rc;
   if ((rc = axpy3(h, d, 0.5 * dt, dk, ds))) return rc;      // ds2
   if ((rc = tlm_rhs(h, c, c->S[1], ds, dk))) return rc;     // dk2
@@ -1160,9 +1157,13 @@ int reverse(spoc_handle *h, AdjCtx *c, int i0, int i1, double *const base[3], in
   double *const *work = c->V[3];
   if (l == 1 || free_snaps == 0) {
     for (int j = i1 - 1; j >= i0; --j) {
-      if ((rc = copy3(h, work, base))) return rc;
-      if ((rc = advance(h, c, work, dt, j - i0))) return rc;
-      if ((rc = adj_step(h, c, work, lam, dt))) return rc;
+      double *const *x = base;
+      if (j > i0) {
+        if ((rc = copy3(h, work, base))) return rc;
+        if ((rc = advance(h, c, work, dt, j - i0))) return rc;
+        x = work;
+      }
+      if ((rc = adj_step(h, c, x, lam, dt))) return rc;
       const int t = obs_index(c, j);
       if (t >= 0 && (rc = obs_force(h, c, t, lam))) return rc;
     }
@@ -1327,8 +1328,12 @@ extern "C" int spoc_fwd_window(spoc_handle *h, int ld, const double *u0, const d
   double J = 0.0;
   int t = obs_index(c, 0);
   if (!rc && t >= 0) rc = obs_eval(h, c, t, x, &J);
-  for (int i = 1; i <= nsteps && !rc; ++i) {
-    rc = advance(h, c, x, dt, 1);
+  for (int i = 0; i < nsteps && !rc;) {
+    int next = nsteps;
+    for (int st : c->steps)
+      if (st > i && st < next) next = st;
+    rc = advance(h, c, x, dt, next - i);
+    i = next;
     t = obs_index(c, i);
     if (!rc && t >= 0) rc = obs_eval(h, c, t, x, &J);
   }

@@ -115,6 +115,17 @@ cudaError_t launch_axpy(size_t n, const double *x, double c, const double *y, do
                         cudaStream_t st, int sms);
 cudaError_t launch_axpby(size_t n, double a, const double *x, double b, const double *y,
                          double *out, cudaStream_t st, int sms);
+// Adjoint RK4 bookkeeping over the three fields in one launch.  kInit:
+// kb = a lam + b lam.  kFirst: acc = sb, kb = a sb + b lam.  kMid: acc += sb,
+// kb = a sb + b lam.  kLast: lam += acc + sb.
+struct AdjCombine {
+  enum Mode { kInit = 0, kFirst = 1, kMid = 2, kLast = 3 };
+  const double *sb[3];
+  double *acc[3], *lam[3], *kb[3];
+  double a, b;
+  int mode;
+};
+cudaError_t launch_adj_combine(size_t n, const AdjCombine &c, cudaStream_t st, int sms);
 cudaError_t launch_obs_eval(int nobs, int nm, const int *elem, const double *basis,
                             const double *h, double *val, cudaStream_t st);
 cudaError_t launch_obs_adj(int nel, int nm, const int *el_list, const int *el_start,
