@@ -363,18 +363,23 @@ __global__ void __launch_bounds__(kT) k_adj_tend_b(DevOps op_in, DevMesh m, AdjT
 // ---------------------------------------------------------------------------
 // adjoint of the quadrature-point stage (calvarnl_fs.f:243-348)
 // ---------------------------------------------------------------------------
+// Per-warp scratch, sized by the compile-time dimensions when there are
+// some (the maximum sizes would limit the kernel to 16 resident warps per SM).
+template <class D>
 struct NaSmem {
-  double vin[9][kMaxModes];
-  double xb[8][kMaxModes];
-  double qb[9][kMaxQuad];  // quadrature-point adjoints: U V Gxx Gxy Gyx Gyy H Wk Zk
-  double sm[kMaxModes];
+  static constexpr int M = D::NC > 0 ? (D::NC + 1) * (D::NC + 2) / 2 : kMaxModes;
+  static constexpr int Q = D::NC > 0 ? D::NG : kMaxQuad;
+  double vin[9][M];
+  double xb[8][M];
+  double qb[9][Q];  // quadrature-point adjoints: U V Gxx Gxy Gyx Gyy H Wk Zk
+  double sm[M];
 };
 
 template <int VAR, class D = RtDims>
 __global__ void __launch_bounds__(64, 4 * adj_min_blocks<D>()) k_nlvol_adj(DevOps op_in, DevMesh m, AdjNlArgs a) {
   const DevOps op = fixed_dims<D>(op_in);
-  __shared__ NaSmem sall[2];
-  NaSmem &S = sall[threadIdx.x >> 5];
+  __shared__ NaSmem<D> sall[2];
+  NaSmem<D> &S = sall[threadIdx.x >> 5];
   const int nm = op.nm, ng = op.ng, ne = m.ne, l = lane_id();
   const size_t fs = (size_t)ne * nm;
   for (int e = wg(); e < ne; e += wc()) {
