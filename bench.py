@@ -405,6 +405,99 @@ def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
             "checks": "dot-product, central differences (20 directions) and checkpointing invariance in tests/test_gpu_adjoint.py"}
 
 
+def regrid_measure(torch, stream, fp64_mul_add, name="c2_fs_p6", steps=20, reps=10):
+    """Solution-driven regridding of the C2 state after `steps` RK4 steps: the
+    error indicator (cal_conv), refinement of the elements above the 90th
+    percentile of the indicator, the host point location, the device
+    re-projection (interpol) of u, v, eta, verif_rot and checkcfl2.  Kernel
+    times by CUDA events on the handles' stream; the oracle's interpol (one
+    core, walk included) is timed beside it on the same meshes."""
+    from spoc_b200 import api
+    from spoc_b200 import workloads as W
+    cfg = W.CONFIGS[name]
+    p = W.build_problem(cfg)
+    s = W.make_solver(p)
+    s.set_stream(stream.cuda_stream)
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, steps)
+
+    def timed(fn, n=reps):
+        out, ms = None, []
+        for _ in range(n):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return out, float(np.median(ms))
+
+    amax = np.maximum.reduce(s.checkconv())
+    fac1 = float(np.quantile(amax, 0.9))
+    cc, t_conv = timed(lambda: s.cal_conv(fac1, 0.0, 10.0 * fac1))
+    t0 = time.perf_counter()
+    p1, tinter, loc = W.adapt_problem(p, cc["fconv"])
+    t_adapt = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    api.locate_points(p.mesh, p1.mesh, tinter, p.T)
+    t_walk = time.perf_counter() - t0
+    d = api.Solver(p1.T, p1.mesh, cfg.variant)
+    d.set_params(cfg.mu0, cfg.mb0, cfg.g0, p1.hb, p1.fc, p1.w0, p1.z0)
+    d.set_stream(stream.cuda_stream)
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (tinter, *loc)]
+    ptrs = [t.data_ptr() for t in dev]
+    l0 = d.launches
+    d.interpol_from_dev(s, *ptrs)
+    _, t_interp = timed(lambda: d.interpol_from_dev(s, *ptrs))
+    launches = (d.launches - l0) / (reps + 1)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        d.interpol_from(s, tinter, *loc)
+    t_e2e = (time.perf_counter() - t0) / 3 * 1e3
+    _, t_rot = timed(d.verif_rot)
+    (cflmin, dt2), t_cfl2 = timed(lambda: d.cfl2(10, p.dt))
+    nm, ng, ne1 = p.T.nm, p.T.ng, p1.mesh.ne
+    nproj = int((tinter == 0).sum())
+    flops = nproj * (2 * 9.0 * nm * ng + 6.0 * nm * nm)
+    byts = nproj * (ng * 20.0 + 2 * 3 * nm * 8) + (ne1 - nproj) * 2 * 3 * nm * 8
+    # CPU baseline: the oracle's interpol (walk included), one core, same meshes
+    from oracle import oracle as O
+    T = p.T
+    OT = O.Tables(cfg.nc, cfg.ng, cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
+    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, cfg.nc, cfg.f0, cfg.beta)
+    NM = O.Mesh(p1.mesh.inn, p1.mesh.xgr, p1.mesh.ygr, cfg.nc, cfg.f0, cfg.beta)
+    u, v, h = s.get_state()
+    t0 = time.perf_counter()
+    for a in (u, v, h):
+        O.interpol(OT, OM, NM, tinter, a)
+    t_cpu = time.perf_counter() - t0
+    dof = 3.0 * nm * ne1
+    s.close()
+    d.close()
+    return {
+        "config": f"{name}: {p.mesh.ne} -> {ne1} triangles after {steps} RK4 steps; elements with "
+                  f"an indicator above its 90th percentile refined (red + green closure); "
+                  f"{nproj} re-projected, {ne1 - nproj} inherited",
+        "metric": "re-projected DOF per second (interpol of u, v, eta)",
+        "value": dof / (t_interp * 1e-3), "unit": "DOF/s",
+        "interpol_ms": t_interp, "interpol_launches_per_call": launches,
+        "e2e": {"value": dof / (t_e2e * 1e-3), "unit": "DOF/s", "ms": t_e2e,
+                "note": "spoc_interpol with host arrays (point tables uploaded inside)"},
+        "cal_conv_ms": t_conv, "verif_rot_ms": t_rot, "cfl2_ms": t_cfl2,
+        "cfl2": {"cflmin": cflmin, "dt": dt2},
+        "host_refine_s": t_adapt, "host_walk_s": t_walk,
+        "roofline": {"kernel": "k_interpol", "bound": "fp64",
+                     "achieved": flops / (t_interp * 1e-3) / 1e12, "peak": fp64_mul_add,
+                     "unit": "TFLOP/s", "frac": flops / (t_interp * 1e-3) / 1e12 / fp64_mul_add,
+                     "algorithmic_flops_per_call": flops, "algorithmic_bytes_per_call": byts,
+                     "hbm_gbs": byts / (t_interp * 1e-3) / 1e9,
+                     "peak_source": "measured live: spoc_fp64_peak mode 1 (separate DMUL + DADD)"},
+        "cpu_baseline": {"value": dof / t_cpu, "unit": "DOF/s", "cores": 1, "kind": "port",
+                         "sample": "the oracle's interpol of u, v, eta on the same meshes, walk included"},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,6 +509,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-regrid", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma", "mixed"],
                     help="fp64: bit-exact reference order (headline); fp64_fma: fused "
                          "multiply-adds; mixed: FP32 contractions, FP64 state")
@@ -569,6 +663,9 @@ def main():
     adjoint = None
     if world == 1 and not args.no_adjoint:
         adjoint = adjoint_measure(torch, stream)
+    regrid = None
+    if world == 1 and not args.no_regrid:
+        regrid = regrid_measure(torch, stream, fp64_mul_add)
 
     line = None
     if rank == 0:
@@ -593,6 +690,7 @@ def main():
             "mixed_c3": mixed,
             "ensemble_c5": ensemble,
             "adjoint": adjoint,
+            "regrid": regrid,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -134,6 +134,42 @@ int spoc_energy(spoc_handle *h, double *ke, double *pe, double *mass);
 /* CFL time step of src/cfl.f:4-52 on the device (in(3,ne), node coordinates). */
 int spoc_cfl(spoc_handle *h, int nn, const int *in, const double *xgr, const double *ygr,
              double *cflmin, double *dt);
+/* ---- solution-driven regridding (src/adapt.f; the adaptive driver
+ * src/shwwnl_adap.f:375-450) ----
+ * spoc_checkconv: checkconv (src/adapt.f:1260-1334) of the resident u, v, h
+ *   on the device: per element, the largest jump of the trace across its
+ *   interior faces, divided by the field's max |mode 0| (0 when <= 1e-6);
+ *   umax / vmax / hmax are host arrays of ne.
+ * spoc_cal_conv: cal_conv (src/adapt.f:1122-1193): fconv[e] = some field's
+ *   jump > fac1 (refine), fderaff[e] = all three < fac2 (coarsen), host int
+ *   arrays of ne; flags[0] conv, flags[1] deraff, flags[2] timedir; *supmax
+ *   (may be null) the largest jump.
+ * spoc_interpol: interpol (src/adapt.f:1662-1745) on the device: dst's
+ *   resident state becomes src's re-projected onto dst's mesh.  tinter[ne_dst]
+ *   (from spoc_inter_only_new): the src element (1-based) a dst element
+ *   copies, or 0 to project; pt_elem / pt_x / pt_y (ng x ne_dst, from
+ *   spoc_locate_points; may be null when nothing projects) the src element
+ *   and reference coordinates of each quadrature point.  Both handles must
+ *   share the degree and the quadrature rule.
+ * spoc_verif_rot: verif_rot (src/shwwnl_adap.f:481-596) on the resident u, v:
+ *   the mass-matrix load is solved again, in the rotated wall sub-basis on
+ *   wall elements.
+ * spoc_cfl2: checkcfl2 (src/cfl.f:57-140) of the resident state on the
+ *   ngraph-point lattice (the reference uses 10); *dt = dt_in when no
+ *   rounding branch applies. */
+int spoc_checkconv(spoc_handle *h, double *umax, double *vmax, double *hmax);
+int spoc_cal_conv(spoc_handle *h, double fac1, double fac2, double fac3, int *fconv,
+                  int *fderaff, int *flags, double *supmax);
+int spoc_interpol(spoc_handle *dst, spoc_handle *src, const int *tinter, const int *pt_elem,
+                  const double *pt_x, const double *pt_y);
+/* Same with DEVICE arrays, enqueued on dst's stream (after src's stream is
+ * drained when the streams differ); ids outside 1..ne_src are not read and
+ * make the call return SPOC_E_ARG. */
+int spoc_interpol_dev(spoc_handle *dst, spoc_handle *src, const int *tinter, const int *pt_elem,
+                      const double *pt_x, const double *pt_y);
+int spoc_verif_rot(spoc_handle *h);
+int spoc_cfl2(spoc_handle *h, int ngraph, int nn, const int *in, const double *xgr,
+              const double *ygr, double dt_in, double *cflmin, double *dt);
 /* Number of kernels this handle launched so far (telemetry). */
 long long spoc_kernel_launches(spoc_handle *h);
 /* Diagnostics (no reference counterpart): run nsteps RK4 steps like
@@ -278,6 +314,19 @@ int spoc_projection_points(int ne, const int *in, const double *xgr, const doubl
                            const double *xi, const double *yi, double *px, double *py);
 int spoc_project(int nc, int ng, const double *wi, const double *pi2, const double *amm,
                  int ne, const double *vals, double *out, int ld);
+/* Regridding set-up on the host.  inter_only_new (src/adapt.f:1233-1258):
+ * tinter[i] = the old element (1-based) new element i repeats, else 0.
+ * Point location of interpol (src/adapt.f:1690-1718, interlin :1747-1830):
+ * the quadrature points of every new element with tinter == 0 located in the
+ * old mesh (arrays of spoc_build_mesh), the walk continuing from the previous
+ * point's element; pt_elem / pt_x / pt_y are (ng, nenew).  SPOC_E_MESH when a
+ * walk does not end. */
+int spoc_inter_only_new(int ne, int nenew, const int *in, const int *innew, int *tinter);
+int spoc_locate_points(int ne, const int *in, const int *itm, const int *tseg, const int *pseg,
+                       const double *xgr, const double *ygr, int nenew, const int *innew,
+                       const double *xgrnew, const double *ygrnew, const int *tinter, int ng,
+                       const double *xi, const double *yi, int *pt_elem, double *pt_x,
+                       double *pt_y);
 
 #ifdef __cplusplus
 }

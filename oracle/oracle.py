@@ -244,3 +244,91 @@ def mass_norm(T: Tables, M: Mesh, a):
     det = M.vect[:, 0] * M.vect[:, 3] - M.vect[:, 2] * M.vect[:, 1]
     G = T.ammo.T  # numpy [j, i] holds ammo(i, j); symmetric anyway
     return float(np.sqrt(np.sum(det * np.einsum("ei,ij,ej->e", x, G, x))))
+
+
+# ---------------------------------------------------------------------------
+# Regridding (src/adapt.f) and the adaptive driver's CFL (src/cfl.f:57-140)
+# ---------------------------------------------------------------------------
+
+def checkconv(T: Tables, M: Mesh, a):
+    """checkconv of src/adapt.f:1260-1334: normalised trace jump per element."""
+    L = lib()
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    out = np.zeros(M.ne)
+    L.ora_checkconv(C.byref(T.common), M.nf, M.ne, a.shape[1], d(a), i(M.tseg), i(M.ssit), d(out))
+    return out
+
+
+def cal_conv(T: Tables, M: Mesh, u, v, h, fac1, fac2, fac3):
+    """cal_conv of src/adapt.f:1122-1193."""
+    L = lib()
+    u, v, h = (np.ascontiguousarray(x, dtype=np.float64) for x in (u, v, h))
+    fconv = np.zeros(M.ne, np.int32)
+    fderaff = np.zeros(M.ne, np.int32)
+    flags = np.zeros(3, np.int32)
+    mx = [np.zeros(M.ne) for _ in range(3)]
+    sup = C.c_double()
+    L.ora_cal_conv.argtypes = [C.POINTER(Common), C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _IP,
+                               _IP, C.c_double, C.c_double, C.c_double, _IP, _IP, _IP, _DP,
+                               _DP, _DP, _DP]
+    L.ora_cal_conv(C.byref(T.common), M.nf, M.ne, u.shape[1], d(u), d(v), d(h), i(M.tseg),
+                   i(M.ssit), fac1, fac2, fac3, i(fconv), i(fderaff), i(flags), C.byref(sup),
+                   *map(d, mx))
+    return {"fconv": fconv, "fderaff": fderaff, "conv": bool(flags[0]), "deraff": bool(flags[1]),
+            "timedir": bool(flags[2]), "supmax": sup.value, "amax": tuple(mx)}
+
+
+def inter_only_new(inn, innew):
+    """inter_only_new of src/adapt.f:1233-1258 (1-based element tables)."""
+    inn = np.ascontiguousarray(inn, dtype=np.int32)
+    innew = np.ascontiguousarray(innew, dtype=np.int32)
+    out = np.zeros(innew.shape[0], np.int32)
+    lib().ora_inter_only_new(inn.shape[0], innew.shape[0], i(inn), i(innew), i(out))
+    return out
+
+
+def interpol(T: Tables, old: Mesh, new: Mesh, tinter, u):
+    """interpol of src/adapt.f:1662-1745: u (ne_old, ld) onto the new mesh.
+    Returns (unew, loc_elem, loc_x, loc_y); loc_* are (ne_new, ng)."""
+    L = lib()
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    tinter = np.ascontiguousarray(tinter, dtype=np.int32)
+    unew = np.zeros((new.ne, u.shape[1]))
+    le = np.zeros((new.ne, T.ng), np.int32)
+    lx = np.zeros((new.ne, T.ng))
+    ly = np.zeros((new.ne, T.ng))
+    rc = L.ora_interpol(C.byref(T.common), old.ne, i(old.inn), i(old.itm), i(old.tseg),
+                        i(old.pseg), d(old.xgr), d(old.ygr), i(tinter), d(u), u.shape[1],
+                        d(unew), new.ne, d(new.xgr), d(new.ygr), i(new.inn), i(le), d(lx), d(ly))
+    if rc:
+        raise RuntimeError("interlin walk did not end")
+    return unew, le, lx, ly
+
+
+def verif_rot(T: Tables, M: Mesh, u, v):
+    """verif_rot of src/shwwnl_adap.f:481-596 on copies of (u, v)."""
+    u = np.array(u, dtype=np.float64, order="C", copy=True)
+    v = np.array(v, dtype=np.float64, order="C", copy=True)
+    lib().ora_verif_rot(C.byref(T.common), M.ne, u.shape[1], d(u), d(v), d(M.normt), i(M.bdl))
+    return u, v
+
+
+def cal_pgraph(nc, n):
+    nm = (nc + 1) * (nc + 2) // 2
+    out = np.zeros((n, n, nm))
+    lib().ora_cal_pgraph(nc, n, d(out))
+    return out
+
+
+def checkcfl2(nc, M: Mesh, hb, u, v, g0, n=10, dt_in=0.0):
+    """checkcfl2 of src/cfl.f:57-140 on the n-point lattice; returns (cflmin, dt)."""
+    L = lib()
+    pg = cal_pgraph(nc, n)
+    hb, u, v = (np.ascontiguousarray(x, dtype=np.float64) for x in (hb, u, v))
+    L.ora_checkcfl2.restype = C.c_double
+    L.ora_checkcfl2.argtypes = [C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _IP, C.c_double, _DP,
+                                _DP, C.c_int, _DP, C.c_double, _DP]
+    c = C.c_double()
+    dt = L.ora_checkcfl2(nc, M.ne, hb.shape[1], d(hb), d(u), d(v), i(M.inn), g0, d(M.xgr),
+                         d(M.ygr), n, d(pg), dt_in, C.byref(c))
+    return c.value, dt

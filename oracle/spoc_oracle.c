@@ -1270,3 +1270,284 @@ void ora_calh(const ora_common *c, int ne, const double *vals, double *h, int ld
     for (int j = 0; j < nm; j++) VEC(h, i)[j] = b[j];
   }
 }
+
+/* ------------------------------------------------------------------ */
+/* L5: solution-driven regridding and the adaptive driver's CFL        */
+/* ------------------------------------------------------------------ */
+
+/* checkconv: src/adapt.f:1260-1334.  amax(ne): per element, the largest jump
+ * of a0's trace across its interior faces at the ngf edge points, divided by
+ * max |a0(1,i)| (0 when that is <= 1e-6). */
+void ora_checkconv(const ora_common *c, int nf, int ne, int ld, const double *a0,
+                   const int *tseg, const int *ssit, double *amax) {
+  const int nm = c->nm, ngf = c->ngf;
+  double fbdy1[NGFMAX], fbdy2[NGFMAX];
+  for (int i = 1; i <= ne; i++) amax[i - 1] = 0.0;
+  for (int i = 1; i <= nf; i++) {
+    for (int j = 1; j <= ngf; j++) fbdy1[j - 1] = fbdy2[j - 1] = 0.0;
+    const int k1 = I2(tseg, 1, i, 2), k2 = I2(tseg, 2, i, 2);
+    if (k2 > 0) {
+      int cote = I2(ssit, 1, i, 2);
+      for (int i1 = 1; i1 <= nm; i1++)
+        for (int j = 1; j <= ngf; j++)
+          fbdy1[j - 1] = fbdy1[j - 1] + VEC(a0, k1)[i1 - 1] * PICO(c, j, i1, cote);
+      cote = I2(ssit, 2, i, 2);
+      for (int i1 = 1; i1 <= nm; i1++)
+        for (int j = 1; j <= ngf; j++)
+          fbdy2[j - 1] = fbdy2[j - 1] + VEC(a0, k2)[i1 - 1] * PICO(c, ngf - j + 1, i1, cote);
+      for (int j = 1; j <= ngf; j++) {
+        const double dif = fabs(fbdy2[j - 1] - fbdy1[j - 1]);
+        if (amax[k1 - 1] < dif) amax[k1 - 1] = dif;
+        if (amax[k2 - 1] < dif) amax[k2 - 1] = dif;
+      }
+    }
+  }
+  double vmax = fabs(VEC(a0, 1)[0]);
+  for (int i = 2; i <= ne; i++) vmax = fmax(fabs(VEC(a0, i)[0]), vmax);
+  for (int i = 1; i <= ne; i++) amax[i - 1] = vmax > 1.0e-6 ? amax[i - 1] / vmax : 0.0;
+}
+
+/* cal_conv: src/adapt.f:1122-1193.  fconv(i): some field's jump > fac1
+ * (refine); fderaff(i): all three < fac2 (coarsen); flags[0] conv, flags[1]
+ * deraff, flags[2] timedir; *supmax the largest jump. */
+void ora_cal_conv(const ora_common *c, int nf, int ne, int ld, const double *u0,
+                  const double *v0, const double *h0, const int *tseg, const int *ssit,
+                  double fac1, double fac2, double fac3, int *fconv, int *fderaff, int *flags,
+                  double *supmax_out, double *umax, double *vmax, double *hmax) {
+  ora_checkconv(c, nf, ne, ld, u0, tseg, ssit, umax);
+  ora_checkconv(c, nf, ne, ld, v0, tseg, ssit, vmax);
+  ora_checkconv(c, nf, ne, ld, h0, tseg, ssit, hmax);
+  int deraff = 0;
+  double supmax = umax[0];
+  for (int i = 0; i < ne; i++) {
+    fconv[i] = (umax[i] > fac1) || (vmax[i] > fac1) || (hmax[i] > fac1);
+    fderaff[i] = (umax[i] < fac2) && (vmax[i] < fac2) && (hmax[i] < fac2);
+    if (fderaff[i]) deraff = 1;
+    supmax = fmax(supmax, umax[i]);
+    supmax = fmax(supmax, vmax[i]);
+    supmax = fmax(supmax, hmax[i]);
+  }
+  flags[2] = !(supmax > fac3);
+  flags[0] = (supmax > fac1) || deraff;
+  flags[1] = deraff;
+  if (supmax_out) *supmax_out = supmax;
+}
+
+/* inter_only_new: src/adapt.f:1233-1258.  tinter(i) = the old element that
+ * new element i repeats (same three nodes, in order), else 0. */
+void ora_inter_only_new(int ne, int nenew, const int *in, const int *innew, int *tinter) {
+  for (int i = 0; i < nenew; i++) tinter[i] = 0;
+  int tk = 1;
+  for (int i = 1; i <= ne && tk <= nenew; i++) {
+    int k = 0;
+    for (int j = 1; j <= 3; j++)
+      if (I2(in, j, i, 3) == I2(innew, j, tk, 3)) k++;
+    if (k == 3) {
+      tinter[tk - 1] = i;
+      tk++;
+    }
+  }
+}
+
+/* interlin: src/adapt.f:1747-1830.  Walks from element *tk to the element
+ * holding (xdp, ydp) (a point outside the mesh is moved onto the wall edge it
+ * crossed), returning its barycentric coordinates lab(3).  The walk is capped
+ * at maxit moves; returns 0, or -1 when the cap is reached. */
+int ora_interlin(const int *itt, const int *itm, const int *tseg, const int *pseg,
+                 const double *x, const double *y, int *tk_io, double *xdp_io, double *ydp_io,
+                 double *lab, int maxit) {
+  const double eps = 1.0e-9;
+  int tk = *tk_io;
+  double xdp = *xdp_io, ydp = *ydp_io;
+  for (int it = 0; it < maxit; it++) {
+    double x1 = x[I2(itt, 1, tk, 3) - 1], y1 = y[I2(itt, 1, tk, 3) - 1];
+    double x2 = x[I2(itt, 2, tk, 3) - 1], y2 = y[I2(itt, 2, tk, 3) - 1];
+    const double x3 = x[I2(itt, 3, tk, 3) - 1], y3 = y[I2(itt, 3, tk, 3) - 1];
+    const double aire = (x2 - x3) * (y2 - y1) - (x2 - x1) * (y2 - y3);
+    lab[0] = (xdp - x2) * (ydp - y3) - (xdp - x3) * (ydp - y2);
+    lab[1] = (xdp - x3) * (ydp - y1) - (xdp - x1) * (ydp - y3);
+    lab[2] = (xdp - x1) * (ydp - y2) - (xdp - x2) * (ydp - y1);
+    for (int k = 0; k < 3; k++) {
+      lab[k] = lab[k] / aire;
+      if (fabs(lab[k]) < eps) lab[k] = 0.0;
+    }
+    int tk1, ns1 = 0;
+    if (lab[0] >= 0 && lab[1] >= 0 && lab[2] >= 0) {
+      *tk_io = tk;
+      *xdp_io = xdp;
+      *ydp_io = ydp;
+      return 0;
+    }
+    if (lab[0] < 0.0) ns1 = I2(itm, 2, tk, 3);
+    else if (lab[1] < 0.0) ns1 = I2(itm, 3, tk, 3);
+    else ns1 = I2(itm, 1, tk, 3);
+    tk1 = I2(tseg, 1, ns1, 2);
+    if (tk1 == tk) tk1 = I2(tseg, 2, ns1, 2);
+    if (tk1 > 0) {
+      tk = tk1;
+    } else {
+      const int n1 = I2(pseg, 1, ns1, 2), n2 = I2(pseg, 2, ns1, 2);
+      x1 = x[n1 - 1];
+      y1 = y[n1 - 1];
+      x2 = x[n2 - 1];
+      y2 = y[n2 - 1];
+      const double d = (x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2);
+      double pr = (x1 - xdp) * (x1 - x2) + (y1 - ydp) * (y1 - y2);
+      pr = pr / d;
+      xdp = x1 * (1.0 - pr) + x2 * pr;
+      ydp = y1 * (1.0 - pr) + y2 * pr;
+    }
+  }
+  *tk_io = tk;
+  return -1;
+}
+
+/* fsol: src/compare.f:203-219 (the modal expansion of element i at (x, y)) */
+static double fsol_(int nc, double x, double y, const double *b, int ld, int i) {
+  int j = 0;
+  double s = 0.0;
+  for (int kc1 = 0; kc1 <= nc; kc1++)
+    for (int kc2 = 0; kc2 <= nc - kc1; kc2++) {
+      j++;
+      s = s + VEC(b, i)[j - 1] * ora_po(kc1, x) * ora_po(kc2, y);
+    }
+  return s;
+}
+
+/* interpol: src/adapt.f:1662-1745.  unew(ld, nenew) on the new mesh from
+ * u(ld, ne) on the old one: elements with tinter > 0 copy their old element;
+ * the others are the L2 projection of u evaluated at their quadrature points
+ * (located by interlin, the walk continuing from the previous point's
+ * element).  loc_elem / loc_x / loc_y (ng x nenew, may be null) receive the
+ * located element and reference coordinates.  Returns 0, or -1 if a walk hit
+ * its cap. */
+int ora_interpol(const ora_common *c, int ne, const int *in, const int *itm, const int *tseg,
+                 const int *pseg, const double *xgr, const double *ygr, const int *tinter,
+                 const double *u, int ld, double *unew, int nenew, const double *xgrnew,
+                 const double *ygrnew, const int *innew, int *loc_elem, double *loc_x,
+                 double *loc_y) {
+  const int nm = c->nm, ng = c->ng, nc = c->nc;
+  double dia1[NNMAX], mff[NGMAX], b[NNMAX], lab[3];
+  for (int i = 1; i <= nm; i++) dia1[i - 1] = 1.0 / M2(c->amm, c->ldm, i, i);
+  int tk = 1;
+  for (int i = 1; i <= nenew; i++) {
+    if (tinter[i - 1] == 0) {
+      const int i1 = I2(innew, 1, i, 3), i2 = I2(innew, 2, i, 3), i3 = I2(innew, 3, i, 3);
+      const double agx = (xgrnew[i2 - 1] - xgrnew[i1 - 1]) * 0.5;
+      const double bgx = (xgrnew[i3 - 1] - xgrnew[i1 - 1]) * 0.5;
+      const double agy = (ygrnew[i2 - 1] - ygrnew[i1 - 1]) * 0.5;
+      const double bgy = (ygrnew[i3 - 1] - ygrnew[i1 - 1]) * 0.5;
+      const double xof = xgrnew[i1 - 1], yof = ygrnew[i1 - 1];
+      for (int j = 1; j <= ng; j++) {
+        const double y = c->yi[j - 1], x = c->xi[j - 1];
+        double x0 = agx * (x + 1.0) + bgx * (y + 1.0) + xof;
+        double y0 = agy * (x + 1.0) + bgy * (y + 1.0) + yof;
+        if (ora_interlin(in, itm, tseg, pseg, xgr, ygr, &tk, &x0, &y0, lab, 16 * ne + 64))
+          return -1;
+        const double x1 = 2.0 * lab[1] - 1.0, y1 = 2.0 * lab[2] - 1.0;
+        mff[j - 1] = fsol_(nc, x1, y1, u, ld, tk);
+        if (loc_elem) {
+          M2(loc_elem, ng, j, i) = tk;
+          M2(loc_x, ng, j, i) = x1;
+          M2(loc_y, ng, j, i) = y1;
+        }
+      }
+      ora_xytospec(c, b, mff);
+      ora_dtrsm4(nm, c->amm, c->ldm, b, dia1);
+      for (int j = 0; j < nm; j++) VEC(unew, i)[j] = b[j];
+    } else {
+      for (int j = 0; j < nm; j++) VEC(unew, i)[j] = VEC(u, tinter[i - 1])[j];
+    }
+  }
+  return 0;
+}
+
+/* verif_rot: src/shwwnl_adap.f:481-596.  Re-projects (u0, v0) after a regrid:
+ * the mass-matrix load (cal_b with ammo) is solved again, in the rotated
+ * wall-vanishing sub-basis for the normal component on wall elements. */
+void ora_verif_rot(const ora_common *c, int ne, int ld, double *u0, double *v0,
+                   const double *normt, const int *bdl) {
+  const int nm = c->nm, nmr = nm - c->nc - 1;
+  double dia1[NNMAX], dia2[NNMAX];
+  for (int i = 1; i <= nm; i++) dia1[i - 1] = 1.0 / M2(c->amm, c->ldm, i, i);
+  for (int i = 1; i <= nmr; i++) dia2[i - 1] = 1.0 / M2(c->amml, c->ldm, i, i);
+  for (int i = 1; i <= ne; i++) {
+    double gx[NNMAX] = {0}, gy[NNMAX] = {0};
+    ora_cal_b(c, gx, VEC(u0, i), c->ammo, 1.0);
+    ora_cal_b(c, gy, VEC(v0, i), c->ammo, 1.0);
+    if (bdl[i - 1]) {
+      wall_solve_rot(c, gx, gy, I2(normt, 1, i, 2), I2(normt, 2, i, 2), dia1, dia2);
+    } else {
+      solve_amm(c, gx, dia1);
+      solve_amm(c, gy, dia1);
+    }
+    for (int j = 0; j < nm; j++) {
+      VEC(u0, i)[j] = gx[j];
+      VEC(v0, i)[j] = gy[j];
+    }
+  }
+}
+
+/* cal_pgraph: src/visu2.f:4-25.  pgraph(nm, n, n): the basis on the n-point
+ * lattice of the reference triangle, (l, k) with l <= n - k + 1. */
+void ora_cal_pgraph(int nc, int n, double *pgraph) {
+  const int nm = (nc + 1) * (nc + 2) / 2;
+  for (int k = 1; k <= n; k++)
+    for (int l = 1; l <= n - k + 1; l++) {
+      const double y = (double)(2 * k - n - 1) / (double)(n - 1);
+      const double x = (double)(2 * l - n - 1) / (double)(n - 1);
+      int i1 = 0;
+      for (int kc1 = 0; kc1 <= nc; kc1++)
+        for (int kc2 = 0; kc2 <= nc - kc1; kc2++) {
+          i1++;
+          pgraph[((size_t)(k - 1) * n + (l - 1)) * nm + i1 - 1] = ora_po(kc1, x) * ora_po(kc2, y);
+        }
+    }
+}
+
+/* checkcfl2: src/cfl.f:57-140.  Time step from the gravity-wave speed of the
+ * largest depth plus the largest velocity on the lattice of each element.
+ * dt_in is returned unchanged when no branch applies (a NaN bound). */
+double ora_checkcfl2(int nc, int ne, int ld, const double *hb, const double *u,
+                     const double *v, const int *in, double g0, const double *xgr,
+                     const double *ygr, int n, const double *pgraph, double dt_in,
+                     double *cflmin_out) {
+  const int nm = (nc + 1) * (nc + 2) / 2;
+  const double ra = 0.35;
+  double cflmin = 6000.0;
+  for (int i = 1; i <= ne; i++) {
+    double maxdepth = 0.0, maxvel = 0.0;
+    for (int k = 1; k <= n; k++)
+      for (int l = 1; l <= n - k + 1; l++) {
+        double sol0 = 0.0, sol1 = 0.0, sol2 = 0.0;
+        for (int i1 = 1; i1 <= nm; i1++) {
+          const double pp = pgraph[((size_t)(k - 1) * n + (l - 1)) * nm + i1 - 1];
+          sol0 = sol0 + VEC(hb, i)[i1 - 1] * pp;
+          sol1 = sol1 + VEC(u, i)[i1 - 1] * pp;
+          sol2 = sol2 + VEC(v, i)[i1 - 1] * pp;
+        }
+        maxdepth = fmax(maxdepth, sol0);
+        maxvel = fmax(maxvel, sqrt(sol1 * sol1 + sol2 * sol2));
+      }
+    const int i1 = I2(in, 1, i, 3), i2 = I2(in, 2, i, 3), i3 = I2(in, 3, i, 3);
+    double ax = xgr[i2 - 1] - xgr[i1 - 1], ay = ygr[i2 - 1] - ygr[i1 - 1];
+    const double dd1 = sqrt(ax * ax + ay * ay) / (double)nc * ra;
+    ax = xgr[i3 - 1] - xgr[i1 - 1];
+    ay = ygr[i3 - 1] - ygr[i1 - 1];
+    const double dd2 = sqrt(ax * ax + ay * ay) / (double)nc * ra;
+    ax = xgr[i3 - 1] - xgr[i2 - 1];
+    ay = ygr[i3 - 1] - ygr[i2 - 1];
+    const double dd3 = sqrt(ax * ax + ay * ay) / (double)nc * ra;
+    const double cc0 = sqrt(g0 * maxdepth) + maxvel;
+    cflmin = fmin(cflmin, dd1 / cc0);
+    cflmin = fmin(cflmin, dd2 / cc0);
+    cflmin = fmin(cflmin, dd3 / cc0);
+  }
+  if (cflmin_out) *cflmin_out = cflmin;
+  double dt = dt_in;
+  if (cflmin >= 100) dt = (double)(10 * (int)(cflmin / 10));
+  else if (cflmin >= 10 && cflmin < 100) dt = (double)(2 * (int)(cflmin / 2));
+  else if (cflmin < 10 && cflmin >= 1) dt = (double)(int)cflmin;
+  else if (cflmin < 1) dt = (double)((int)(cflmin * 10) / 10);
+  return dt;
+}

@@ -121,6 +121,30 @@ void ora_calh_points(const ora_common *c, int ne, const int *in, const double *x
                      const double *ygr, double *px, double *py);
 void ora_calh(const ora_common *c, int ne, const double *vals, double *h, int ld);
 
+/* ---- L5: regridding (src/adapt.f) and the adaptive driver's CFL ---- */
+void ora_checkconv(const ora_common *c, int nf, int ne, int ld, const double *a0,
+                   const int *tseg, const int *ssit, double *amax);
+void ora_cal_conv(const ora_common *c, int nf, int ne, int ld, const double *u0,
+                  const double *v0, const double *h0, const int *tseg, const int *ssit,
+                  double fac1, double fac2, double fac3, int *fconv, int *fderaff, int *flags,
+                  double *supmax, double *umax, double *vmax, double *hmax);
+void ora_inter_only_new(int ne, int nenew, const int *in, const int *innew, int *tinter);
+int ora_interlin(const int *itt, const int *itm, const int *tseg, const int *pseg,
+                 const double *x, const double *y, int *tk, double *xdp, double *ydp,
+                 double *lab, int maxit);
+int ora_interpol(const ora_common *c, int ne, const int *in, const int *itm, const int *tseg,
+                 const int *pseg, const double *xgr, const double *ygr, const int *tinter,
+                 const double *u, int ld, double *unew, int nenew, const double *xgrnew,
+                 const double *ygrnew, const int *innew, int *loc_elem, double *loc_x,
+                 double *loc_y);
+void ora_verif_rot(const ora_common *c, int ne, int ld, double *u0, double *v0,
+                   const double *normt, const int *bdl);
+void ora_cal_pgraph(int nc, int n, double *pgraph);
+double ora_checkcfl2(int nc, int ne, int ld, const double *hb, const double *u,
+                     const double *v, const int *in, double g0, const double *xgr,
+                     const double *ygr, int n, const double *pgraph, double dt_in,
+                     double *cflmin);
+
 #ifdef __cplusplus
 }
 #endif

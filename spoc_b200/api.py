@@ -108,6 +108,15 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "spoc_energy": (C.c_int, [vp, _DP, _DP, _DP]),
         "spoc_cfl": (C.c_int, [vp, C.c_int, _IP, _DP, _DP, _DP, _DP]),
         "spoc_kernel_launches": (C.c_longlong, [vp]),
+        "spoc_checkconv": (C.c_int, [vp, _DP, _DP, _DP]),
+        "spoc_cal_conv": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, _IP, _IP, _IP, _DP]),
+        "spoc_interpol": (C.c_int, [vp, vp, _IP, _IP, _DP, _DP]),
+        "spoc_interpol_dev": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+        "spoc_verif_rot": (C.c_int, [vp]),
+        "spoc_cfl2": (C.c_int, [vp, C.c_int, C.c_int, _IP, _DP, _DP, C.c_double, _DP, _DP]),
+        "spoc_inter_only_new": (C.c_int, [C.c_int, C.c_int, _IP, _IP, _IP]),
+        "spoc_locate_points": (C.c_int, [C.c_int, _IP, _IP, _IP, _IP, _DP, _DP, C.c_int, _IP, _DP,
+                                         _DP, _IP, C.c_int, _DP, _DP, _IP, _DP, _DP]),
         "spoc_profile_rk4": (C.c_int, [vp, C.c_double, C.c_int, _DP, _IP]),
         "spoc_fp64_peak": (C.c_int, [C.c_int, _DP]),
         "spoc_tlm_rhs": (C.c_int, [vp, C.c_int] + [_DP] * 9),
@@ -328,6 +337,28 @@ def fix_mesh(inn: np.ndarray, nn: int) -> np.ndarray:
     return out
 
 
+def inter_only_new(old: Mesh, new_inn: np.ndarray) -> np.ndarray:
+    """inter_only_new (src/adapt.f:1233-1258): old element each new one repeats, or 0."""
+    new_inn = np.ascontiguousarray(new_inn, dtype=np.int32)
+    out = np.zeros(new_inn.shape[0], np.int32)
+    _check(load_library().spoc_inter_only_new(old.ne, new_inn.shape[0], _i(old.inn), _i(new_inn),
+                                              _i(out)), "inter_only_new")
+    return out
+
+
+def locate_points(old: Mesh, new: Mesh, tinter: np.ndarray, T: Tables):
+    """Point location of interpol (src/adapt.f:1690-1718): (pt_elem, pt_x, pt_y), (ne_new, ng)."""
+    tinter = np.ascontiguousarray(tinter, dtype=np.int32)
+    pe = np.zeros((new.ne, T.ng), np.int32)
+    px = np.zeros((new.ne, T.ng))
+    py = np.zeros((new.ne, T.ng))
+    _check(load_library().spoc_locate_points(
+        old.ne, _i(old.inn), _i(old.itm), _i(old.tseg), _i(old.pseg), _d(old.xgr), _d(old.ygr),
+        new.ne, _i(new.inn), _d(new.xgr), _d(new.ygr), _i(tinter), T.ng, _d(T.xi), _d(T.yi),
+        _i(pe), _d(px), _d(py)), "locate_points")
+    return pe, px, py
+
+
 def projection_points(mesh: Mesh, T: Tables):
     px = np.zeros((mesh.ne, T.ng))
     py = np.zeros((mesh.ne, T.ng))
@@ -430,6 +461,53 @@ class Solver:
         m = self.mesh
         _check(self.lib.spoc_cfl(self._h, m.nn, _i(m.inn), _d(m.xgr), _d(m.ygr), C.byref(c),
                                  C.byref(dt)), "cfl")
+        return c.value, dt.value
+
+    # -- solution-driven regridding (src/adapt.f) --
+    def checkconv(self):
+        """Per-element trace-jump indicators (umax, vmax, hmax) of the resident state."""
+        out = [np.zeros(self.mesh.ne) for _ in range(3)]
+        _check(self.lib.spoc_checkconv(self._h, *map(_d, out)), "checkconv")
+        return tuple(out)
+
+    def cal_conv(self, fac1: float, fac2: float, fac3: float) -> dict:
+        """cal_conv flags of the resident state (src/adapt.f:1122-1193)."""
+        fconv = np.zeros(self.mesh.ne, np.int32)
+        fderaff = np.zeros(self.mesh.ne, np.int32)
+        flags = np.zeros(3, np.int32)
+        sup = C.c_double()
+        _check(self.lib.spoc_cal_conv(self._h, fac1, fac2, fac3, _i(fconv), _i(fderaff), _i(flags),
+                                      C.byref(sup)), "cal_conv")
+        return {"fconv": fconv, "fderaff": fderaff, "conv": bool(flags[0]),
+                "deraff": bool(flags[1]), "timedir": bool(flags[2]), "supmax": sup.value}
+
+    def interpol_from(self, src: "Solver", tinter: np.ndarray, pt_elem=None, pt_x=None,
+                      pt_y=None) -> None:
+        """This handle's state := src's state re-projected onto this mesh (interpol)."""
+        tinter = np.ascontiguousarray(tinter, dtype=np.int32)
+        if pt_elem is None:
+            args = (None, None, None)
+        else:
+            args = (_i(np.ascontiguousarray(pt_elem, dtype=np.int32)),
+                    _d(np.ascontiguousarray(pt_x, dtype=np.float64)),
+                    _d(np.ascontiguousarray(pt_y, dtype=np.float64)))
+        _check(self.lib.spoc_interpol(self._h, src._h, _i(tinter), *args), "interpol")
+
+    def interpol_from_dev(self, src: "Solver", tinter: int, pt_elem: int, pt_x: int,
+                          pt_y: int) -> None:
+        """interpol_from with device pointers (ints), enqueued on this handle's stream."""
+        _check(self.lib.spoc_interpol_dev(self._h, src._h, tinter, pt_elem, pt_x, pt_y),
+               "interpol_dev")
+
+    def verif_rot(self) -> None:
+        _check(self.lib.spoc_verif_rot(self._h), "verif_rot")
+
+    def cfl2(self, ngraph: int = 10, dt_in: float = 0.0):
+        """checkcfl2 (src/cfl.f:57-140) of the resident state: (cflmin, dt)."""
+        c, dt = C.c_double(), C.c_double()
+        m = self.mesh
+        _check(self.lib.spoc_cfl2(self._h, ngraph, m.nn, _i(m.inn), _d(m.xgr), _d(m.ygr), dt_in,
+                                  C.byref(c), C.byref(dt)), "cfl2")
         return c.value, dt.value
 
     def profile_rk4(self, dt: float, nsteps: int):

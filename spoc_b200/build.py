@@ -27,7 +27,7 @@ NVCC_FLAGS = [
     "-Xptxas", "-v",
 ]
 SOURCES = ["spoc_kernels.cu", "spoc_fast.cu", "spoc_api.cu", "spoc_noalloc.cu", "spoc_adjoint.cu",
-           "spoc_mixed.cu", "spoc_mixed_tc.cu", "spoc_tc_selftest.cu"]
+           "spoc_mixed.cu", "spoc_mixed_tc.cu", "spoc_tc_selftest.cu", "spoc_regrid.cu"]
 # spoc_fast.cu is compiled a second time with fused multiply-adds
 VARIANT_SOURCES = [("spoc_fast.cu", "spoc_fast_fma", ["-DSPOC_FMA=1"])]
 HOST_SOURCES = ["spoc_host.cpp"]

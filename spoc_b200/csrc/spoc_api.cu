@@ -100,9 +100,11 @@ int build_ops(spoc_handle *h, const spoc_tables *t) {
   std::vector<double> agx(nm * nm), agy(nm * nm), agxN(nm * nm), agyN(nm * nm), p2(nm * ng),
       p2t(ng * nm), wi(ng), wif(G);
   std::vector<double> picoF(3 * nm * G), picoT(3 * G * nm), uT(nm * nm), uC(nm * nm), dia1(nm);
-  std::vector<double> ulT(nm * nm, 0.0), ulC(nm * nm, 0.0), dia2(nm, 0.0), ammo1(nm);
+  std::vector<double> ulT(nm * nm, 0.0), ulC(nm * nm, 0.0), dia2(nm, 0.0), ammo1(nm),
+      ammoT(nm * nm);
   for (int j = 0; j < nm; ++j)
     for (int i = 0; i < nm; ++i) {
+      ammoT[j * nm + i] = MAT(t->ammo, j, i);
       agx[j * nm + i] = MAT(t->agx, j, i);
       agy[j * nm + i] = MAT(t->agy, j, i);
       agxN[i * nm + j] = MAT(t->agx, j, i);
@@ -182,6 +184,7 @@ int build_ops(spoc_handle *h, const spoc_tables *t) {
   CK(h->upload(&o.inv_a, ia), "upload reduc");
   CK(h->upload(&o.inv_cnt, icnt), "upload reduc");
   CK(h->upload(&o.ammo1, ammo1), "upload ammo");
+  CK(h->upload(&o.ammoT, ammoT), "upload ammo");
   return SPOC_OK;
 }
 
@@ -287,6 +290,7 @@ int check_flag(spoc_handle *h) {
   if (flag) {
     CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->st), "clear flag");
     if (flag & 2) return fail(SPOC_E_CUDA, "tensor-core wait limit reached");
+    if (flag & 4) return fail(SPOC_E_ARG, "interpol: element id out of range");
     return fail(SPOC_E_NONFINITE, "non-finite tendency detected");
   }
   return SPOC_OK;
@@ -412,10 +416,15 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
 
 void adj_forget(spoc_handle *h);
 
+namespace {
+void regrid_forget(spoc_handle *h);
+}
+
 extern "C" void spoc_destroy(spoc_handle *h) {
   if (!h) return;
   if (h->st) cudaStreamSynchronize(h->st);
   adj_forget(h);
+  regrid_forget(h);
   delete h;
 }
 
@@ -1404,6 +1413,243 @@ extern "C" int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long 
   *fwd_steps = c->fwd_steps;
   *adj_steps = c->adj_steps;
   c->fwd_steps = c->adj_steps = 0;
+  return SPOC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Solution-driven regridding (src/adapt.f, src/shwwnl_adap.f:375-450)
+
+namespace {
+
+// Device scratch of the error indicator, allocated on first use.
+struct RegridBufs {
+  RegridScratch s{};
+  bool ready = false;
+};
+std::mutex g_rg_mu;
+std::vector<std::pair<spoc_handle *, RegridBufs *>> g_rg;
+
+RegridBufs *regrid_bufs(spoc_handle *h) {
+  std::lock_guard<std::mutex> lk(g_rg_mu);
+  for (auto &p : g_rg)
+    if (p.first == h) return p.second;
+  RegridBufs *b = new RegridBufs();
+  g_rg.emplace_back(h, b);
+  return b;
+}
+
+void regrid_forget(spoc_handle *h) {
+  std::lock_guard<std::mutex> lk(g_rg_mu);
+  for (size_t i = 0; i < g_rg.size(); ++i)
+    if (g_rg[i].first == h) {
+      delete g_rg[i].second;
+      g_rg.erase(g_rg.begin() + i);
+      return;
+    }
+}
+
+int regrid_init(spoc_handle *h, RegridBufs *b) {
+  if (b->ready) return SPOC_OK;
+  const size_t ne = (size_t)h->ne;
+  cudaError_t e = h->alloc(&b->s.amax_bits, 3 * ne);
+  if (e == cudaSuccess) e = h->alloc(&b->s.small_bits, 4);
+  if (e == cudaSuccess) e = h->alloc(&b->s.amax, 3 * ne);
+  if (e == cudaSuccess) e = h->alloc(&b->s.fconv, ne);
+  if (e == cudaSuccess) e = h->alloc(&b->s.fderaff, ne);
+  if (e == cudaSuccess) e = h->alloc(&b->s.deraff, 1);
+  if (e != cudaSuccess) return fail(SPOC_E_NOMEM, "regrid scratch", e);
+  b->ready = true;
+  return SPOC_OK;
+}
+
+// The resident FP64 state in U0 (a SPOC_MIXED handle keeps it in its own basis).
+int state_to_u0(spoc_handle *h) {
+  if (h->mx) CK(mixed_get_state(h->mx, h->U0, h->st, &h->launches), "mixed state");
+  return SPOC_OK;
+}
+int u0_to_state(spoc_handle *h) {
+  if (h->mx) CK(mixed_set_state(h->mx, h->mesh, h->U0, h->st, &h->launches), "mixed state");
+  return SPOC_OK;
+}
+
+// checkconv of u, v, h and the cal_conv flags on the device; with_flags
+// copies fconv / fderaff too.
+int run_checkconv(spoc_handle *h, double fac1, double fac2, bool with_flags, double *amax3,
+                  int *fconv, int *fderaff, double *sup, int *deraff) {
+  RegridBufs *b = regrid_bufs(h);
+  int rc = regrid_init(h, b);
+  if (!rc) rc = state_to_u0(h);
+  if (rc) return rc;
+  RegridScratch s = b->s;
+  if (!with_flags) s.fconv = s.fderaff = nullptr;
+  CK(launch_checkconv(h->op, h->mesh, h->U0[0], h->U0[1], h->U0[2], fac1, fac2, s, h->st, h->sms,
+                      &h->launches),
+     "checkconv");
+  const size_t ne = (size_t)h->ne;
+  if (amax3)
+    CK(cudaMemcpyAsync(amax3, s.amax, sizeof(double) * 3 * ne, cudaMemcpyDeviceToHost, h->st),
+       "read amax");
+  if (with_flags) {
+    CK(cudaMemcpyAsync(fconv, s.fconv, sizeof(int) * ne, cudaMemcpyDeviceToHost, h->st), "fconv");
+    CK(cudaMemcpyAsync(fderaff, s.fderaff, sizeof(int) * ne, cudaMemcpyDeviceToHost, h->st),
+       "fderaff");
+  }
+  unsigned long long supb = 0;
+  int der = 0;
+  CK(cudaMemcpyAsync(&supb, s.small_bits + 3, sizeof supb, cudaMemcpyDeviceToHost, h->st), "sup");
+  CK(cudaMemcpyAsync(&der, s.deraff, sizeof der, cudaMemcpyDeviceToHost, h->st), "deraff");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  if (sup) std::memcpy(sup, &supb, sizeof supb);
+  if (deraff) *deraff = der;
+  return SPOC_OK;
+}
+
+template <class T>
+cudaError_t upload_tmp(T **d, const T *hsrc, size_t n, cudaStream_t st) {
+  cudaError_t e = cudaMalloc((void **)d, sizeof(T) * (n ? n : 1));
+  if (e == cudaSuccess && n) e = cudaMemcpyAsync(*d, hsrc, sizeof(T) * n, cudaMemcpyHostToDevice, st);
+  return e;
+}
+
+}  // namespace
+
+extern "C" int spoc_checkconv(spoc_handle *h, double *umax, double *vmax, double *hmax) {
+  if (!h || !umax || !vmax || !hmax) return fail(SPOC_E_ARG, "bad argument");
+  std::vector<double> a(3 * (size_t)h->ne);
+  int rc = run_checkconv(h, 0.0, 0.0, false, a.data(), nullptr, nullptr, nullptr, nullptr);
+  if (rc) return rc;
+  const size_t ne = (size_t)h->ne;
+  std::memcpy(umax, a.data(), sizeof(double) * ne);
+  std::memcpy(vmax, a.data() + ne, sizeof(double) * ne);
+  std::memcpy(hmax, a.data() + 2 * ne, sizeof(double) * ne);
+  return SPOC_OK;
+}
+
+extern "C" int spoc_cal_conv(spoc_handle *h, double fac1, double fac2, double fac3, int *fconv,
+                             int *fderaff, int *flags, double *supmax) {
+  if (!h || !fconv || !fderaff || !flags) return fail(SPOC_E_ARG, "bad argument");
+  double sup = 0.0;
+  int der = 0;
+  int rc = run_checkconv(h, fac1, fac2, true, nullptr, fconv, fderaff, &sup, &der);
+  if (rc) return rc;
+  // conv, deraff, timedir (src/adapt.f:1182-1190)
+  flags[0] = (sup > fac1) || der;
+  flags[1] = der;
+  flags[2] = !(sup > fac3);
+  if (supmax) *supmax = sup;
+  return SPOC_OK;
+}
+
+extern "C" int spoc_interpol(spoc_handle *dst, spoc_handle *src, const int *tinter,
+                             const int *pt_elem, const double *pt_x, const double *pt_y) {
+  if (!dst || !src || !tinter) return fail(SPOC_E_ARG, "bad argument");
+  if (dst == src) return fail(SPOC_E_ARG, "interpol needs two handles");
+  if (dst->nc != src->nc || dst->ng != src->ng || dst->nm != src->nm)
+    return fail(SPOC_E_ARG, "the two handles have different degrees or quadrature rules");
+  const int ne = dst->ne, ng = dst->ng;
+  bool project = false;
+  for (int e = 0; e < ne; ++e) {
+    if (tinter[e] < 0 || tinter[e] > src->ne) return fail(SPOC_E_ARG, "tinter out of range");
+    project = project || tinter[e] == 0;
+  }
+  if (project) {
+    if (!pt_elem || !pt_x || !pt_y) return fail(SPOC_E_ARG, "point locations missing");
+    for (int e = 0; e < ne; ++e)
+      if (!tinter[e])
+        for (int q = 0; q < ng; ++q) {
+          const int k = pt_elem[(size_t)e * ng + q];
+          if (k < 1 || k > src->ne) return fail(SPOC_E_ARG, "located element out of range");
+        }
+  }
+  const size_t np = project ? (size_t)ne * ng : 0;
+  int *dt = nullptr, *de = nullptr;
+  double *dx = nullptr, *dy = nullptr;
+  cudaError_t e = upload_tmp(&dt, tinter, (size_t)ne, dst->st);
+  if (e == cudaSuccess) e = upload_tmp(&de, pt_elem, np, dst->st);
+  if (e == cudaSuccess) e = upload_tmp(&dx, pt_x, np, dst->st);
+  if (e == cudaSuccess) e = upload_tmp(&dy, pt_y, np, dst->st);
+  int rc = e == cudaSuccess ? spoc_interpol_dev(dst, src, dt, de, dx, dy)
+                            : fail(SPOC_E_CUDA, "interpol upload", e);
+  cudaStreamSynchronize(dst->st);
+  cudaFree(dt);
+  cudaFree(de);
+  cudaFree(dx);
+  cudaFree(dy);
+  return rc;
+}
+
+extern "C" int spoc_interpol_dev(spoc_handle *dst, spoc_handle *src, const int *tinter,
+                                 const int *pt_elem, const double *pt_x, const double *pt_y) {
+  if (!dst || !src || !tinter) return fail(SPOC_E_ARG, "bad argument");
+  if (dst == src) return fail(SPOC_E_ARG, "interpol needs two handles");
+  if (dst->nc != src->nc || dst->ng != src->ng || dst->nm != src->nm)
+    return fail(SPOC_E_ARG, "the two handles have different degrees or quadrature rules");
+  int rc = state_to_u0(src);
+  if (rc) return rc;
+  if (src->st != dst->st) CK(cudaStreamSynchronize(src->st), "synchronize source");
+  CK(launch_interpol(dst->op, dst->ne, src->ne, tinter, pt_elem, pt_x, pt_y, src->U0, dst->U0,
+                     dst->flag, dst->st, dst->sms, &dst->launches),
+     "interpol");
+  rc = u0_to_state(dst);
+  if (rc) return rc;
+  return check_flag(dst);
+}
+
+extern "C" int spoc_verif_rot(spoc_handle *h) {
+  if (!h) return fail(SPOC_E_ARG, "bad argument");
+  int rc = state_to_u0(h);
+  if (rc) return rc;
+  CK(launch_verif_rot(h->op, h->mesh, h->U0[0], h->U0[1], h->st, h->sms, &h->launches),
+     "verif_rot");
+  rc = u0_to_state(h);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  return SPOC_OK;
+}
+
+extern "C" int spoc_cfl2(spoc_handle *h, int ngraph, int nn, const int *in, const double *xgr,
+                         const double *ygr, double dt_in, double *cflmin, double *dt) {
+  if (!h || !in || !xgr || !ygr || nn < 3 || !cflmin || !dt || ngraph < 2 || ngraph > 64)
+    return fail(SPOC_E_ARG, "bad argument");
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  for (size_t i = 0; i < 3 * (size_t)h->ne; ++i)
+    if (in[i] < 1 || in[i] > nn) return fail(SPOC_E_MESH, "node id out of range");
+  int rc = state_to_u0(h);
+  if (rc) return rc;
+  const size_t np = (size_t)ngraph * (ngraph + 1) / 2;
+  int *din = nullptr;
+  double *dx = nullptr, *dy = nullptr, *pg = nullptr;
+  unsigned long long *bits = nullptr;
+  const double start = 6000.0;  // cflmin=6000.d0 (src/cfl.f:72)
+  unsigned long long sb;
+  std::memcpy(&sb, &start, sizeof sb);
+  cudaError_t e = upload_tmp(&din, in, 3 * (size_t)h->ne, h->st);
+  if (e == cudaSuccess) e = upload_tmp(&dx, xgr, (size_t)nn, h->st);
+  if (e == cudaSuccess) e = upload_tmp(&dy, ygr, (size_t)nn, h->st);
+  if (e == cudaSuccess) e = cudaMalloc(&pg, sizeof(double) * np * h->nm);
+  if (e == cudaSuccess) e = upload_tmp(&bits, &sb, 1, h->st);
+  if (e == cudaSuccess)
+    e = launch_cfl2(h->ne, h->nc, h->nm, ngraph, pg, din, dx, dy, h->hb, h->U0[0], h->U0[1],
+                    h->g0, bits, h->st, h->sms, &h->launches);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&sb, bits, sizeof sb, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(din);
+  cudaFree(dx);
+  cudaFree(dy);
+  cudaFree(pg);
+  cudaFree(bits);
+  if (e != cudaSuccess) return fail(SPOC_E_CUDA, "cfl2", e);
+  double c;
+  std::memcpy(&c, &sb, sizeof c);
+  *cflmin = c;
+  // rounding of src/cfl.f:124-133 (the last branch is an integer division);
+  // dt_in stays when no branch applies
+  double d = dt_in;
+  if (c >= 100) d = (double)(10 * (int)(c / 10));
+  else if (c >= 10 && c < 100) d = (double)(2 * (int)(c / 2));
+  else if (c < 10 && c >= 1) d = (double)((int)c);
+  else if (c < 1) d = (double)((int)(c * 10) / 10);
+  *dt = d;
   return SPOC_OK;
 }
 

@@ -44,6 +44,7 @@ struct DevOps {
   const int *inv_a;     // kind 1: first reduced index; kind 2: reduced source
   const int *inv_cnt;   // kind 1: chain length
   const double *ammo1;  // ammo(j,1), for the mass diagnostic
+  const double *ammoT;  // [j*nm + i] = ammo(j,i)   (cal_b with ammo, verif_rot)
 };
 
 // Mesh pointers with 0-based ids; -1 marks a wall in tseg.

@@ -504,3 +504,127 @@ extern "C" int spoc_project(int nc, int ng, const double *wi, const double *pi2,
   }
   return SPOC_OK;
 }
+
+// inter_only_new (src/adapt.f:1233-1258): tinter[i] = the old element (1-based)
+// that new element i repeats with the same nodes in the same order, else 0.
+// Old elements are matched in order against the new list, as the reference
+// does, so unchanged elements must keep their relative order.
+extern "C" int spoc_inter_only_new(int ne, int nenew, const int *in, const int *innew,
+                                   int *tinter) {
+  if (ne < 1 || nenew < 1 || !in || !innew || !tinter) return SPOC_E_ARG;
+  for (int i = 0; i < nenew; ++i) tinter[i] = 0;
+  int tk = 0;
+  for (int i = 0; i < ne && tk < nenew; ++i) {
+    int k = 0;
+    for (int j = 0; j < 3; ++j)
+      if (in[3 * size_t(i) + j] == innew[3 * size_t(tk) + j]) ++k;
+    if (k == 3) tinter[tk++] = i + 1;
+  }
+  return SPOC_OK;
+}
+
+namespace {
+
+// interlin (src/adapt.f:1747-1830): walk from element *tk (1-based) towards
+// (xdp, ydp) through the faces whose barycentric coordinate is negative; a
+// point pushed out through a wall is moved onto that wall edge.  Barycentric
+// coordinates within 1e-9 of zero count as zero.  At most maxit moves.
+bool interlin(const int *in, const int *itm, const int *tseg, const int *pseg, const double *x,
+              const double *y, int *tk_io, double *xdp_io, double *ydp_io, double lab[3],
+              long maxit) {
+  const double eps = 1.0e-9;
+  int tk = *tk_io;
+  double xdp = *xdp_io, ydp = *ydp_io;
+  for (long it = 0; it < maxit; ++it) {
+    const size_t b = 3 * size_t(tk - 1);
+    double x1 = x[in[b] - 1], y1 = y[in[b] - 1];
+    double x2 = x[in[b + 1] - 1], y2 = y[in[b + 1] - 1];
+    const double x3 = x[in[b + 2] - 1], y3 = y[in[b + 2] - 1];
+    const double aire = (x2 - x3) * (y2 - y1) - (x2 - x1) * (y2 - y3);
+    lab[0] = (xdp - x2) * (ydp - y3) - (xdp - x3) * (ydp - y2);
+    lab[1] = (xdp - x3) * (ydp - y1) - (xdp - x1) * (ydp - y3);
+    lab[2] = (xdp - x1) * (ydp - y2) - (xdp - x2) * (ydp - y1);
+    for (int k = 0; k < 3; ++k) {
+      lab[k] = lab[k] / aire;
+      if (std::fabs(lab[k]) < eps) lab[k] = 0.0;
+    }
+    if (lab[0] >= 0 && lab[1] >= 0 && lab[2] >= 0) {
+      *tk_io = tk;
+      *xdp_io = xdp;
+      *ydp_io = ydp;
+      return true;
+    }
+    // side 2 faces vertex 1, side 3 vertex 2, side 1 vertex 3
+    const int side = lab[0] < 0.0 ? 1 : (lab[1] < 0.0 ? 2 : 0);
+    const int ns1 = itm[b + side];
+    int tk1 = tseg[2 * size_t(ns1 - 1)];
+    if (tk1 == tk) tk1 = tseg[2 * size_t(ns1 - 1) + 1];
+    if (tk1 > 0) {
+      tk = tk1;
+    } else {
+      const int n1 = pseg[2 * size_t(ns1 - 1)], n2 = pseg[2 * size_t(ns1 - 1) + 1];
+      x1 = x[n1 - 1];
+      y1 = y[n1 - 1];
+      x2 = x[n2 - 1];
+      y2 = y[n2 - 1];
+      const double d = (x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2);
+      double pr = (x1 - xdp) * (x1 - x2) + (y1 - ydp) * (y1 - y2);
+      pr = pr / d;
+      xdp = x1 * (1.0 - pr) + x2 * pr;
+      ydp = y1 * (1.0 - pr) + y2 * pr;
+    }
+  }
+  *tk_io = tk;
+  return false;
+}
+
+}  // namespace
+
+// Point location of interpol (src/adapt.f:1690-1718): for every new element
+// with tinter == 0, its quadrature points (the calh map of the new element)
+// are located in the old mesh by interlin, the walk starting from the
+// element the previous point ended in (element 1 first), exactly as the
+// reference's loop runs.  pt_elem (1-based old element) and the reference
+// coordinates pt_x = 2 lab2 - 1, pt_y = 2 lab3 - 1 are (ng, nenew); rows of
+// inherited elements are set to 0.  Old-mesh arrays are those of
+// spoc_build_mesh (1-based, tseg 0 on walls).  Returns SPOC_E_MESH when a
+// walk does not end.
+extern "C" int spoc_locate_points(int ne, const int *in, const int *itm, const int *tseg,
+                                  const int *pseg, const double *xgr, const double *ygr,
+                                  int nenew, const int *innew, const double *xgrnew,
+                                  const double *ygrnew, const int *tinter, int ng,
+                                  const double *xi, const double *yi, int *pt_elem,
+                                  double *pt_x, double *pt_y) {
+  if (ne < 1 || nenew < 1 || ng < 1 || !in || !itm || !tseg || !pseg || !xgr || !ygr ||
+      !innew || !xgrnew || !ygrnew || !tinter || !xi || !yi || !pt_elem || !pt_x || !pt_y)
+    return SPOC_E_ARG;
+  const long maxit = 16L * ne + 64;
+  int tk = 1;
+  double lab[3];
+  for (int i = 0; i < nenew; ++i) {
+    const size_t o = size_t(i) * ng;
+    if (tinter[i] != 0) {
+      for (int j = 0; j < ng; ++j) {
+        pt_elem[o + j] = 0;
+        pt_x[o + j] = pt_y[o + j] = 0.0;
+      }
+      continue;
+    }
+    const int i1 = innew[3 * size_t(i)], i2 = innew[3 * size_t(i) + 1], i3 = innew[3 * size_t(i) + 2];
+    const double agx = (xgrnew[i2 - 1] - xgrnew[i1 - 1]) * 0.5;
+    const double bgx = (xgrnew[i3 - 1] - xgrnew[i1 - 1]) * 0.5;
+    const double agy = (ygrnew[i2 - 1] - ygrnew[i1 - 1]) * 0.5;
+    const double bgy = (ygrnew[i3 - 1] - ygrnew[i1 - 1]) * 0.5;
+    const double xof = xgrnew[i1 - 1], yof = ygrnew[i1 - 1];
+    for (int j = 0; j < ng; ++j) {
+      const double yq = yi[j], xq = xi[j];
+      double x0 = agx * (xq + 1.0) + bgx * (yq + 1.0) + xof;
+      double y0 = agy * (xq + 1.0) + bgy * (yq + 1.0) + yof;
+      if (!interlin(in, itm, tseg, pseg, xgr, ygr, &tk, &x0, &y0, lab, maxit)) return SPOC_E_MESH;
+      pt_elem[o + j] = tk;
+      pt_x[o + j] = 2.0 * lab[1] - 1.0;
+      pt_y[o + j] = 2.0 * lab[2] - 1.0;
+    }
+  }
+  return SPOC_OK;
+}

@@ -115,6 +115,29 @@ cudaError_t launch_axpy(size_t n, const double *x, double c, const double *y, do
                         cudaStream_t st, int sms);
 cudaError_t launch_axpby(size_t n, double a, const double *x, double b, const double *y,
                          double *out, cudaStream_t st, int sms);
+// Regridding (spoc_regrid.cu).  Scratch of the error indicator: amax_bits
+// (3 ne), small_bits (4: mode-0 maxima of u, v, h, then the largest
+// normalised jump), amax (3 ne, normalised), fconv / fderaff (ne, or null),
+// deraff (1).
+struct RegridScratch {
+  unsigned long long *amax_bits, *small_bits;
+  double *amax;
+  int *fconv, *fderaff, *deraff;
+};
+cudaError_t launch_checkconv(const DevOps &op, const DevMesh &m, const double *su,
+                             const double *sv, const double *sh, double fac1, double fac2,
+                             RegridScratch s, cudaStream_t st, int sms, long long *launches);
+cudaError_t launch_interpol(const DevOps &op, int ne_new, int src_ne, const int *tinter,
+                            const int *pel, const double *px, const double *py,
+                            const double *const src[3], double *const dst[3], int *flag,
+                            cudaStream_t st, int sms, long long *launches);
+cudaError_t launch_verif_rot(const DevOps &op, const DevMesh &m, double *u, double *v,
+                             cudaStream_t st, int sms, long long *launches);
+cudaError_t launch_cfl2(int ne, int nc, int nm, int n, double *pg, const int *in,
+                        const double *xg, const double *yg, const double *hb, const double *u,
+                        const double *v, double g0, unsigned long long *out, cudaStream_t st,
+                        int sms, long long *launches);
+
 // Adjoint RK4 bookkeeping over the three fields in one launch.  kInit:
 // kb = a lam + b lam.  kFirst: acc = sb, kb = a sb + b lam.  kMid: acc += sb,
 // kb = a sb + b lam.  kLast: lam += acc + sb.

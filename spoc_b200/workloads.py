@@ -418,3 +418,58 @@ def build_member(mb: Member) -> Problem:
     z = np.zeros((mesh.ne, T.nm))
     dt = cfl_dt(cfg.nc, mesh, cfg.g0, cfg.depth)
     return Problem(cfg, T, mesh, u, v, h, hb, mesh.fc, z, z.copy(), dt)
+
+
+# ---------------------------------------------------------------------------
+# Solution-driven regridding: the refinement branch of the adaptive driver
+# (src/shwwnl_adap.f:375-450)
+# ---------------------------------------------------------------------------
+
+def adapt_problem(p: Problem, marked: np.ndarray):
+    """The refined mesh of p with the marked elements split (red refinement,
+    green closure, corner fix), its pointers, inter_only_new's tinter and the
+    located quadrature points of the elements to re-project.  Bathymetry and
+    wind on the new mesh follow newinter (src/adapt.f:238-265) for a flat
+    bottom and no wind: hb = H in mode 1, w0 = z0 = 0.  Returns
+    (Problem without state, tinter, (pt_elem, pt_x, pt_y))."""
+    cfg, T = p.cfg, p.T
+    ld = p.hb.shape[1]
+    inn, x, y = refine(p.mesh.inn - 1, p.mesh.xgr, p.mesh.ygr, np.asarray(marked, dtype=bool))
+    # unchanged elements first, in their old order, then the new ones: the
+    # order inter_only_new expects (it matches old elements in sequence)
+    old = {tuple(t) for t in (p.mesh.inn - 1).tolist()}
+    keep = np.array([tuple(t) in old for t in inn.tolist()])
+    inn = np.concatenate([inn[keep], inn[~keep]])
+    inn = api.fix_mesh(inn + 1, x.size)
+    mesh = api.build_mesh(inn, x, y, cfg.nc, cfg.f0, cfg.beta, ld)
+    tinter = api.inter_only_new(p.mesh, inn)
+    loc = api.locate_points(p.mesh, mesh, tinter, T)
+    hb = np.zeros((mesh.ne, ld))
+    hb[:, 0] = p.hb[0, 0]
+    z = np.zeros((mesh.ne, ld))
+    dt = cfl_dt(cfg.nc, mesh, cfg.g0, cfg.depth) * cfg.dt_scale
+    return Problem(cfg, T, mesh, None, None, None, hb, mesh.fc, z, z.copy(), dt), tinter, loc
+
+
+def regrid_step(p: Problem, s: api.Solver, fac1: float, fac2: float, fac3: float,
+                precision: str = "fp64", ngraph: int = 10):
+    """One refinement pass of the adaptive driver on the device state of s:
+    cal_conv's indicator (src/adapt.f:1122-1193), refinement of the flagged
+    elements, interpol of u, v, h onto the new mesh (src/adapt.f:1662-1745),
+    verif_rot (src/shwwnl_adap.f:481-596) and checkcfl2's time step
+    (src/cfl.f:57-140).  Coarsening (deraffiner) is not built.  Returns
+    (new problem, new solver, info); the inputs when nothing is flagged."""
+    cc = s.cal_conv(fac1, fac2, fac3)
+    info = {"conv": cc["conv"], "timedir": cc["timedir"], "supmax": cc["supmax"],
+            "flagged": int(cc["fconv"].sum())}
+    if not cc["fconv"].any():
+        return p, s, info
+    p1, tinter, loc = adapt_problem(p, cc["fconv"])
+    s1 = api.Solver(p1.T, p1.mesh, p.cfg.variant, precision)
+    s1.set_params(p.cfg.mu0, p.cfg.mb0, p.cfg.g0, p1.hb, p1.fc, p1.w0, p1.z0)
+    s1.interpol_from(s, tinter, *loc)
+    s1.verif_rot()
+    cflmin, dt = s1.cfl2(ngraph, p.dt)
+    info.update({"ne_old": p.mesh.ne, "ne_new": p1.mesh.ne,
+                 "inherited": int((tinter > 0).sum()), "cflmin": cflmin, "dt_cfl2": dt})
+    return p1, s1, info

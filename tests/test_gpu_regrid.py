@@ -1,0 +1,152 @@
+"""GPU parity of the regridding kernels against the CPU oracle, through the C ABI.
+
+checkconv / cal_conv, interpol, verif_rot and checkcfl2 run every sum in the
+reference order with separately rounded products and take their maxima /
+minima exactly, so they are compared bit for bit (np.array_equal).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from spoc_b200 import api
+from spoc_b200 import workloads as W
+
+NAMES = ["c1_lin_p3", "c2_fs_p6", "c4_ns_p4", "c3_inv_p7"]
+
+
+def setup(name, n=8, frac=0.2, seed=0):
+    cfg = W.small(W.CONFIGS[name], n)
+    p = W.build_problem(cfg)
+    T = p.T
+    OT = O.Tables(cfg.nc, cfg.ng, cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
+    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, cfg.nc, cfg.f0, cfg.beta)
+    return p, OT, OM
+
+
+def stepped(p, n=3):
+    """A state with jumps between elements: a few RK4 steps from the projection."""
+    s = W.make_solver(p)
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, n)
+    return s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_checkconv_and_cal_conv_bitwise(gpu_lib, name):
+    p, OT, OM = setup(name)
+    s = stepped(p)
+    u, v, h = s.get_state()
+    got = s.checkconv()
+    for g, a in zip(got, (u, v, h)):
+        assert np.array_equal(g, O.checkconv(OT, OM, a))
+    amax = np.maximum.reduce(got)
+    fac1 = float(np.quantile(amax, 0.8))
+    fac2 = float(np.quantile(amax, 0.1))
+    cc = s.cal_conv(fac1, fac2, fac1 * 2)
+    ref = O.cal_conv(OT, OM, u, v, h, fac1, fac2, fac1 * 2)
+    assert np.array_equal(cc["fconv"], ref["fconv"]) and np.array_equal(cc["fderaff"], ref["fderaff"])
+    assert cc["supmax"] == ref["supmax"]
+    assert (cc["conv"], cc["deraff"], cc["timedir"]) == (ref["conv"], ref["deraff"], ref["timedir"])
+    assert 0 < cc["fconv"].sum() < p.mesh.ne
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_interpol_bitwise(gpu_lib, name):
+    p, OT, OM = setup(name)
+    s = stepped(p)
+    u, v, h = s.get_state()
+    marked = np.random.default_rng(1).random(p.mesh.ne) < 0.25
+    p1, tinter, loc = W.adapt_problem(p, marked)
+    NM = O.Mesh(p1.mesh.inn, p1.mesh.xgr, p1.mesh.ygr, p.cfg.nc, p.cfg.f0, p.cfg.beta)
+    d = api.Solver(p1.T, p1.mesh, p.cfg.variant)
+    d.set_params(p.cfg.mu0, p.cfg.mb0, p.cfg.g0, p1.hb, p1.fc, p1.w0, p1.z0)
+    d.interpol_from(s, tinter, *loc)
+    got = d.get_state()
+    for g, a in zip(got, (u, v, h)):
+        ref, *_ = O.interpol(OT, OM, NM, tinter, a)
+        assert np.array_equal(g, ref)
+
+
+@pytest.mark.gpu
+def test_interpol_all_inherited_needs_no_points(gpu_lib):
+    p, OT, OM = setup("c2_fs_p6")
+    s = stepped(p)
+    d = W.make_solver(p)
+    d.interpol_from(s, np.arange(1, p.mesh.ne + 1, dtype=np.int32))
+    for g, a in zip(d.get_state(), s.get_state()):
+        assert np.array_equal(g, a)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c2_fs_p6", "c4_ns_p4", "c3_inv_p7"])
+def test_verif_rot_bitwise(gpu_lib, name):
+    p, OT, OM = setup(name)
+    s = stepped(p)
+    u, v, h = s.get_state()
+    s.verif_rot()
+    gu, gv, gh = s.get_state()
+    ru, rv = O.verif_rot(OT, OM, u, v)
+    assert np.array_equal(gu, ru) and np.array_equal(gv, rv) and np.array_equal(gh, h)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("ngraph", [10, 4])
+def test_cfl2_bitwise(gpu_lib, name, ngraph):
+    p, OT, OM = setup(name)
+    s = stepped(p)
+    u, v, h = s.get_state()
+    got = s.cfl2(ngraph, 7.0)
+    ref = O.checkcfl2(p.cfg.nc, OM, p.hb, u, v, p.cfg.g0, ngraph, 7.0)
+    assert got == ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c2_fs_p6", "c4_ns_p4"])
+def test_regrid_step_matches_oracle_pipeline(gpu_lib, name):
+    p, OT, OM = setup(name)
+    s = stepped(p, 5)
+    u, v, h = s.get_state()
+    amax = np.maximum.reduce(s.checkconv())
+    fac1 = float(np.quantile(amax, 0.85))
+    p1, s1, info = W.regrid_step(p, s, fac1, 0.0, 10 * fac1)
+    assert info["flagged"] > 0 and info["ne_new"] > info["ne_old"]
+    NM = O.Mesh(p1.mesh.inn, p1.mesh.xgr, p1.mesh.ygr, p.cfg.nc, p.cfg.f0, p.cfg.beta)
+    tinter = O.inter_only_new(p.mesh.inn, p1.mesh.inn)
+    ru, *_ = O.interpol(OT, OM, NM, tinter, u)
+    rv, *_ = O.interpol(OT, OM, NM, tinter, v)
+    rh, *_ = O.interpol(OT, OM, NM, tinter, h)
+    ru, rv = O.verif_rot(OT, NM, ru, rv)
+    gu, gv, gh = s1.get_state()
+    assert np.array_equal(gu, ru) and np.array_equal(gv, rv) and np.array_equal(gh, rh)
+    cmin, dt = O.checkcfl2(p.cfg.nc, NM, p1.hb, ru, rv, p.cfg.g0, 10, p.dt)
+    assert (info["cflmin"], info["dt_cfl2"]) == (cmin, dt)
+    # the refined run steps on
+    s1.rk4_steps(p1.dt, 3)
+    assert all(np.isfinite(a).all() for a in s1.get_state())
+
+
+@pytest.mark.gpu
+def test_regrid_mixed_handles(gpu_lib):
+    """SPOC_MIXED handles keep their state in their own basis; the regrid moves
+    it through FP64 and back (a round trip through the ill-conditioned basis
+    change, 1e-12 relative here)."""
+    p, OT, OM = setup("c2_fs_p6")
+    s = stepped(p)
+    m = W.make_solver(p, "mixed")
+    m.set_state(*s.get_state())
+    amax = np.maximum.reduce(s.checkconv())
+    cc = s.cal_conv(float(np.quantile(amax, 0.85)), 0.0, 1.0)
+    p1, tinter, loc = W.adapt_problem(p, cc["fconv"])
+    NM = O.Mesh(p1.mesh.inn, p1.mesh.xgr, p1.mesh.ygr, p.cfg.nc, p.cfg.f0, p.cfg.beta)
+    out = []
+    for src, prec in ((s, "fp64"), (m, "mixed")):
+        d = api.Solver(p1.T, p1.mesh, p.cfg.variant, prec)
+        d.set_params(p.cfg.mu0, p.cfg.mb0, p.cfg.g0, p1.hb, p1.fc, p1.w0, p1.z0)
+        d.interpol_from(src, tinter, *loc)
+        d.verif_rot()
+        out.append(d.get_state())
+    for a, b in zip(*out):
+        assert O.mass_norm(OT, NM, a - b) <= 1e-10 * O.mass_norm(OT, NM, a)
