@@ -107,6 +107,61 @@ module spoc_gpu_mod
       type(c_ptr), value :: h
       real(c_double), intent(out) :: ke, pe, mass
     end function
+
+    ! Regridding (src/shwwnl_adap.f:375-450): cal_conv's flags on the device,
+    ! then interpol / verif_rot / checkcfl2 of the state onto a new handle.
+    ! fconv, fderaff are logical*4 arrays in the reference (0 / 1 here).
+    integer(c_int) function spoc_cal_conv(h, fac1, fac2, fac3, fconv, fderaff, flags, supmax) &
+        bind(c, name='spoc_cal_conv')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), value :: fac1, fac2, fac3
+      integer(c_int), intent(out) :: fconv(*), fderaff(*), flags(3)
+      real(c_double), intent(out) :: supmax
+    end function
+
+    integer(c_int) function spoc_inter_only_new(ne, nenew, in, innew, tinter) &
+        bind(c, name='spoc_inter_only_new')
+      import :: c_int
+      integer(c_int), value :: ne, nenew
+      integer(c_int), intent(in) :: in(3,*), innew(3,*)
+      integer(c_int), intent(out) :: tinter(*)
+    end function
+
+    integer(c_int) function spoc_locate_points(ne, in, itm, tseg, pseg, xgr, ygr, nenew, &
+        innew, xgrnew, ygrnew, tinter, ng, xi, yi, pt_elem, pt_x, pt_y) &
+        bind(c, name='spoc_locate_points')
+      import :: c_int, c_double
+      integer(c_int), value :: ne, nenew, ng
+      integer(c_int), intent(in) :: in(3,*), itm(3,*), tseg(2,*), pseg(2,*), innew(3,*), tinter(*)
+      real(c_double), intent(in) :: xgr(*), ygr(*), xgrnew(*), ygrnew(*), xi(*), yi(*)
+      integer(c_int), intent(out) :: pt_elem(ng,*)
+      real(c_double), intent(out) :: pt_x(ng,*), pt_y(ng,*)
+    end function
+
+    integer(c_int) function spoc_interpol(dst, src, tinter, pt_elem, pt_x, pt_y) &
+        bind(c, name='spoc_interpol')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: dst, src
+      integer(c_int), intent(in) :: tinter(*), pt_elem(*)
+      real(c_double), intent(in) :: pt_x(*), pt_y(*)
+    end function
+
+    integer(c_int) function spoc_verif_rot(h) bind(c, name='spoc_verif_rot')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+
+    integer(c_int) function spoc_cfl2(h, ngraph, nn, in, xgr, ygr, dt_in, cflmin, dt) &
+        bind(c, name='spoc_cfl2')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int), value :: ngraph, nn
+      integer(c_int), intent(in) :: in(3,*)
+      real(c_double), intent(in) :: xgr(*), ygr(*)
+      real(c_double), value :: dt_in
+      real(c_double), intent(out) :: cflmin, dt
+    end function
   end interface
 
 contains
