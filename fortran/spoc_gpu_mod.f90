@@ -152,6 +152,17 @@ module spoc_gpu_mod
       type(c_ptr), value :: h
     end function
 
+    ! write_gra's values for all elements: out(5, np, ne) = x, y, u, v, h
+    integer(c_int) function spoc_lattice(h, ngraph, nn, in, xgr, ygr, out) &
+        bind(c, name='spoc_lattice')
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int), value :: ngraph, nn
+      integer(c_int), intent(in) :: in(3,*)
+      real(c_double), intent(in) :: xgr(*), ygr(*)
+      real(c_double), intent(out) :: out(5,*)
+    end function
+
     integer(c_int) function spoc_cfl2(h, ngraph, nn, in, xgr, ygr, dt_in, cflmin, dt) &
         bind(c, name='spoc_cfl2')
       import :: c_int, c_ptr, c_double

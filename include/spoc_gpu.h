@@ -170,6 +170,17 @@ int spoc_interpol_dev(spoc_handle *dst, spoc_handle *src, const int *tinter, con
 int spoc_verif_rot(spoc_handle *h);
 int spoc_cfl2(spoc_handle *h, int ngraph, int nn, const int *in, const double *xgr,
               const double *ygr, double dt_in, double *cflmin, double *dt);
+/* Point evaluation of the resident state (fsol, src/compare.f:203-219):
+ * elem (1-based) and reference coordinates of npts points (host arrays);
+ * out[f * npts + i], f = u, v, h. */
+int spoc_eval_points(spoc_handle *h, int npts, const int *elem, const double *px,
+                     const double *py, double *out);
+/* write_gra's values (src/visu2.f:86-149) on the device: for every element
+ * and every point of the ngraph-point lattice (k outer, l inner) the
+ * physical point and u, v, h: out[(e * np + p) * 5 + c], np = ngraph
+ * (ngraph + 1) / 2, c = x, y, u, v, h. */
+int spoc_lattice(spoc_handle *h, int ngraph, int nn, const int *in, const double *xgr,
+                 const double *ygr, double *out);
 /* Number of kernels this handle launched so far (telemetry). */
 long long spoc_kernel_launches(spoc_handle *h);
 /* Diagnostics (no reference counterpart): run nsteps RK4 steps like
@@ -322,6 +333,13 @@ int spoc_project(int nc, int ng, const double *wi, const double *pi2, const doub
  * point's element; pt_elem / pt_x / pt_y are (ng, nenew).  SPOC_E_MESH when a
  * walk does not end. */
 int spoc_inter_only_new(int ne, int nenew, const int *in, const int *innew, int *tinter);
+/* Sequential point location of compare.f (src/compare.f:118-150): interlin
+ * from *tk (updated) for each point; coordinates summing below 0.5 count as
+ * outside (inside[i] = 0) and restart the walk at reset_tk. */
+int spoc_locate_xy(int ne, const int *in, const int *itm, const int *tseg, const int *pseg,
+                   const double *xgr, const double *ygr, int npts, const double *px,
+                   const double *py, int *tk, int reset_tk, int *elem, double *x1, double *y1,
+                   int *inside);
 int spoc_locate_points(int ne, const int *in, const int *itm, const int *tseg, const int *pseg,
                        const double *xgr, const double *ygr, int nenew, const int *innew,
                        const double *xgrnew, const double *ygrnew, const int *tinter, int ng,

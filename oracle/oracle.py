@@ -332,3 +332,36 @@ def checkcfl2(nc, M: Mesh, hb, u, v, g0, n=10, dt_in=0.0):
     dt = L.ora_checkcfl2(nc, M.ne, hb.shape[1], d(hb), d(u), d(v), i(M.inn), g0, d(M.xgr),
                          d(M.ygr), n, d(pg), dt_in, C.byref(c))
     return c.value, dt
+
+
+def eval_points(nc, u, v, h, elem, px, py):
+    """fsol of u, v, h at points given by element (1-based) and reference coordinates."""
+    u, v, h = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, h))
+    elem = np.ascontiguousarray(elem, dtype=np.int32)
+    px = np.ascontiguousarray(px, dtype=np.float64)
+    py = np.ascontiguousarray(py, dtype=np.float64)
+    out = np.zeros((3, elem.size))
+    lib().ora_eval_points(nc, u.shape[1], d(u), d(v), d(h), elem.size, i(elem), d(px), d(py),
+                          d(out))
+    return out
+
+
+def lattice(nc, M: Mesh, u, v, h, n=10):
+    """write_gra's lattice values: (ne, np, 5) with x, y, u, v, h."""
+    u, v, h = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, h))
+    pg = cal_pgraph(nc, n)
+    out = np.zeros((M.ne, n * (n + 1) // 2, 5))
+    lib().ora_lattice(nc, M.ne, u.shape[1], d(u), d(v), d(h), i(M.inn), d(M.xgr), d(M.ygr), n,
+                      d(pg), d(out))
+    return out
+
+
+def interlin(M: Mesh, tk, x, y):
+    """One interlin walk (src/adapt.f:1747-1830): (tk, x, y, lab)."""
+    t, xx, yy = C.c_int(tk), C.c_double(x), C.c_double(y)
+    lab = np.zeros(3)
+    rc = lib().ora_interlin(i(M.inn), i(M.itm), i(M.tseg), i(M.pseg), d(M.xgr), d(M.ygr),
+                            C.byref(t), C.byref(xx), C.byref(yy), d(lab), 16 * M.ne + 64)
+    if rc:
+        raise RuntimeError("interlin walk did not end")
+    return t.value, xx.value, yy.value, lab

@@ -1551,3 +1551,44 @@ double ora_checkcfl2(int nc, int ne, int ld, const double *hb, const double *u,
   else if (cflmin < 1) dt = (double)((int)(cflmin * 10) / 10);
   return dt;
 }
+
+/* fsol at npts points: out[f * npts + i] for u, v, h (src/compare.f:203-219) */
+void ora_eval_points(int nc, int ld, const double *u, const double *v, const double *h,
+                     int npts, const int *elem, const double *px, const double *py,
+                     double *out) {
+  for (int i = 0; i < npts; i++) {
+    out[i] = fsol_(nc, px[i], py[i], u, ld, elem[i]);
+    out[(size_t)npts + i] = fsol_(nc, px[i], py[i], v, ld, elem[i]);
+    out[2 * (size_t)npts + i] = fsol_(nc, px[i], py[i], h, ld, elem[i]);
+  }
+}
+
+/* write_gra's values (src/visu2.f:86-149): out[(e*np + p)*5 + c], c = x, y,
+ * then the field values of u, v, h at lattice point p (k outer, l inner). */
+void ora_lattice(int nc, int ne, int ld, const double *u, const double *v, const double *h,
+                 const int *in, const double *xgr, const double *ygr, int n,
+                 const double *pgraph, double *out) {
+  const int nm = (nc + 1) * (nc + 2) / 2, np = n * (n + 1) / 2;
+  for (int i = 1; i <= ne; i++) {
+    const int i1 = I2(in, 1, i, 3), i2 = I2(in, 2, i, 3), i3 = I2(in, 3, i, 3);
+    const double ax = (xgr[i2 - 1] - xgr[i1 - 1]) * 0.5, bx = (xgr[i3 - 1] - xgr[i1 - 1]) * 0.5;
+    const double ay = (ygr[i2 - 1] - ygr[i1 - 1]) * 0.5, by = (ygr[i3 - 1] - ygr[i1 - 1]) * 0.5;
+    const double xof = xgr[i1 - 1], yof = ygr[i1 - 1];
+    int p = 0;
+    for (int k = 1; k <= n; k++)
+      for (int l = 1; l <= n - k + 1; l++, p++) {
+        const double y1 = (double)(2 * k - n - 1) / (double)(n - 1);
+        const double x1 = (double)(2 * l - n - 1) / (double)(n - 1);
+        double *o = &out[(((size_t)(i - 1)) * np + p) * 5];
+        o[0] = xof + ax * (x1 + 1.0) + bx * (y1 + 1.0);
+        o[1] = yof + ay * (x1 + 1.0) + by * (y1 + 1.0);
+        const double *fld[3] = {u, v, h};
+        for (int f = 0; f < 3; f++) {
+          double sol = 0.0;
+          for (int j = 1; j <= nm; j++)
+            sol = sol + VEC(fld[f], i)[j - 1] * pgraph[((size_t)(k - 1) * n + (l - 1)) * nm + j - 1];
+          o[2 + f] = sol;
+        }
+      }
+  }
+}

@@ -140,6 +140,12 @@ int ora_interpol(const ora_common *c, int ne, const int *in, const int *itm, con
 void ora_verif_rot(const ora_common *c, int ne, int ld, double *u0, double *v0,
                    const double *normt, const int *bdl);
 void ora_cal_pgraph(int nc, int n, double *pgraph);
+void ora_eval_points(int nc, int ld, const double *u, const double *v, const double *h,
+                     int npts, const int *elem, const double *px, const double *py,
+                     double *out);
+void ora_lattice(int nc, int ne, int ld, const double *u, const double *v, const double *h,
+                 const int *in, const double *xgr, const double *ygr, int n,
+                 const double *pgraph, double *out);
 double ora_checkcfl2(int nc, int ne, int ld, const double *hb, const double *u,
                      const double *v, const int *in, double g0, const double *xgr,
                      const double *ygr, int n, const double *pgraph, double dt_in,

@@ -115,6 +115,10 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "spoc_verif_rot": (C.c_int, [vp]),
         "spoc_cfl2": (C.c_int, [vp, C.c_int, C.c_int, _IP, _DP, _DP, C.c_double, _DP, _DP]),
         "spoc_inter_only_new": (C.c_int, [C.c_int, C.c_int, _IP, _IP, _IP]),
+        "spoc_eval_points": (C.c_int, [vp, C.c_int, _IP, _DP, _DP, _DP]),
+        "spoc_lattice": (C.c_int, [vp, C.c_int, C.c_int, _IP, _DP, _DP, _DP]),
+        "spoc_locate_xy": (C.c_int, [C.c_int, _IP, _IP, _IP, _IP, _DP, _DP, C.c_int, _DP, _DP,
+                                     _IP, C.c_int, _IP, _DP, _DP, _IP]),
         "spoc_locate_points": (C.c_int, [C.c_int, _IP, _IP, _IP, _IP, _DP, _DP, C.c_int, _IP, _DP,
                                          _DP, _IP, C.c_int, _DP, _DP, _IP, _DP, _DP]),
         "spoc_profile_rk4": (C.c_int, [vp, C.c_double, C.c_int, _DP, _IP]),
@@ -346,6 +350,24 @@ def inter_only_new(old: Mesh, new_inn: np.ndarray) -> np.ndarray:
     return out
 
 
+def locate_xy(mesh: Mesh, px, py, tk: int, reset_tk: int):
+    """compare.f's sequential point location (src/compare.f:118-150):
+    (elem, x1, y1, inside, tk after the last point)."""
+    px = np.ascontiguousarray(px, dtype=np.float64)
+    py = np.ascontiguousarray(py, dtype=np.float64)
+    n = px.size
+    elem = np.zeros(n, np.int32)
+    inside = np.zeros(n, np.int32)
+    x1 = np.zeros(n)
+    y1 = np.zeros(n)
+    t = C.c_int(tk)
+    _check(load_library().spoc_locate_xy(mesh.ne, _i(mesh.inn), _i(mesh.itm), _i(mesh.tseg),
+                                         _i(mesh.pseg), _d(mesh.xgr), _d(mesh.ygr), n, _d(px),
+                                         _d(py), C.byref(t), reset_tk, _i(elem), _d(x1), _d(y1),
+                                         _i(inside)), "locate_xy")
+    return elem, x1, y1, inside, t.value
+
+
 def locate_points(old: Mesh, new: Mesh, tinter: np.ndarray, T: Tables):
     """Point location of interpol (src/adapt.f:1690-1718): (pt_elem, pt_x, pt_y), (ne_new, ng)."""
     tinter = np.ascontiguousarray(tinter, dtype=np.int32)
@@ -509,6 +531,24 @@ class Solver:
         _check(self.lib.spoc_cfl2(self._h, ngraph, m.nn, _i(m.inn), _d(m.xgr), _d(m.ygr), dt_in,
                                   C.byref(c), C.byref(dt)), "cfl2")
         return c.value, dt.value
+
+    def eval_points(self, elem, px, py) -> np.ndarray:
+        """fsol of the resident u, v, h at (element, reference coordinates): (3, npts)."""
+        elem = np.ascontiguousarray(elem, dtype=np.int32)
+        px = np.ascontiguousarray(px, dtype=np.float64)
+        py = np.ascontiguousarray(py, dtype=np.float64)
+        out = np.zeros((3, elem.size))
+        _check(self.lib.spoc_eval_points(self._h, elem.size, _i(elem), _d(px), _d(py), _d(out)),
+               "eval_points")
+        return out
+
+    def lattice(self, ngraph: int = 10) -> np.ndarray:
+        """write_gra's lattice values of the resident state: (ne, np, 5) = x, y, u, v, h."""
+        m = self.mesh
+        out = np.zeros((m.ne, ngraph * (ngraph + 1) // 2, 5))
+        _check(self.lib.spoc_lattice(self._h, ngraph, m.nn, _i(m.inn), _d(m.xgr), _d(m.ygr),
+                                     _d(out)), "lattice")
+        return out
 
     def profile_rk4(self, dt: float, nsteps: int):
         """Per-kernel-kind milliseconds over nsteps steps (advances the state)."""

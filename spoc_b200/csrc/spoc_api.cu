@@ -1653,6 +1653,67 @@ extern "C" int spoc_cfl2(spoc_handle *h, int ngraph, int nn, const int *in, cons
   return SPOC_OK;
 }
 
+extern "C" int spoc_eval_points(spoc_handle *h, int npts, const int *elem, const double *px,
+                                const double *py, double *out) {
+  if (!h || npts < 0 || (npts && (!elem || !px || !py || !out)))
+    return fail(SPOC_E_ARG, "bad argument");
+  if (!npts) return SPOC_OK;
+  for (int i = 0; i < npts; ++i)
+    if (elem[i] < 1 || elem[i] > h->ne) return fail(SPOC_E_ARG, "element id out of range");
+  int rc = state_to_u0(h);
+  if (rc) return rc;
+  int *de = nullptr;
+  double *dx = nullptr, *dy = nullptr, *dout = nullptr;
+  const size_t n = (size_t)npts;
+  cudaError_t e = upload_tmp(&de, elem, n, h->st);
+  if (e == cudaSuccess) e = upload_tmp(&dx, px, n, h->st);
+  if (e == cudaSuccess) e = upload_tmp(&dy, py, n, h->st);
+  if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(double) * 3 * n);
+  if (e == cudaSuccess)
+    e = launch_eval_points(h->nc, h->nm, h->ne, npts, de, dx, dy, h->U0, dout, h->flag, h->st,
+                           h->sms, &h->launches);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, dout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(de);
+  cudaFree(dx);
+  cudaFree(dy);
+  cudaFree(dout);
+  if (e != cudaSuccess) return fail(SPOC_E_CUDA, "eval_points", e);
+  return check_flag(h);
+}
+
+extern "C" int spoc_lattice(spoc_handle *h, int ngraph, int nn, const int *in, const double *xgr,
+                            const double *ygr, double *out) {
+  if (!h || !in || !xgr || !ygr || !out || nn < 3 || ngraph < 2 || ngraph > 64)
+    return fail(SPOC_E_ARG, "bad argument");
+  for (size_t i = 0; i < 3 * (size_t)h->ne; ++i)
+    if (in[i] < 1 || in[i] > nn) return fail(SPOC_E_MESH, "node id out of range");
+  int rc = state_to_u0(h);
+  if (rc) return rc;
+  const size_t np = (size_t)ngraph * (ngraph + 1) / 2, tot = 5 * np * h->ne;
+  int *din = nullptr;
+  double *dx = nullptr, *dy = nullptr, *pg = nullptr, *dout = nullptr;
+  cudaError_t e = upload_tmp(&din, in, 3 * (size_t)h->ne, h->st);
+  if (e == cudaSuccess) e = upload_tmp(&dx, xgr, (size_t)nn, h->st);
+  if (e == cudaSuccess) e = upload_tmp(&dy, ygr, (size_t)nn, h->st);
+  if (e == cudaSuccess) e = cudaMalloc(&pg, sizeof(double) * np * h->nm);
+  if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(double) * tot);
+  if (e == cudaSuccess)
+    e = launch_lattice(h->ne, h->nc, h->nm, ngraph, pg, din, dx, dy, h->U0, dout, h->st, h->sms,
+                       &h->launches);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, dout, sizeof(double) * tot, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(din);
+  cudaFree(dx);
+  cudaFree(dy);
+  cudaFree(pg);
+  cudaFree(dout);
+  if (e != cudaSuccess) return fail(SPOC_E_CUDA, "lattice", e);
+  return SPOC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Ensemble (no reference counterpart: the reference runs one basin per process)
 

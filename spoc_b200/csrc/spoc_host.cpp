@@ -628,3 +628,37 @@ extern "C" int spoc_locate_points(int ne, const int *in, const int *itm, const i
   }
   return SPOC_OK;
 }
+
+// Sequential point location of compare.f (src/compare.f:118-150): each point
+// (px[i], py[i]) is located by interlin from the element the previous walk
+// ended in (*tk on entry, updated); a result whose barycentric coordinates sum
+// below 0.5 counts as outside (inside[i] = 0) and the walk restarts from
+// reset_tk.  elem (1-based), x1 = 2 lab2 - 1, y1 = 2 lab3 - 1.
+extern "C" int spoc_locate_xy(int ne, const int *in, const int *itm, const int *tseg,
+                              const int *pseg, const double *xgr, const double *ygr, int npts,
+                              const double *px, const double *py, int *tk, int reset_tk,
+                              int *elem, double *x1, double *y1, int *inside) {
+  if (ne < 1 || npts < 0 || !in || !itm || !tseg || !pseg || !xgr || !ygr || !tk ||
+      (npts && (!px || !py || !elem || !x1 || !y1 || !inside)) || *tk < 1 || *tk > ne ||
+      reset_tk < 1 || reset_tk > ne)
+    return SPOC_E_ARG;
+  const long maxit = 16L * ne + 64;
+  double lab[3];
+  for (int i = 0; i < npts; ++i) {
+    double x = px[i], y = py[i];
+    if (!interlin(in, itm, tseg, pseg, xgr, ygr, tk, &x, &y, lab, maxit)) return SPOC_E_MESH;
+    const double sum = lab[0] + lab[1] + lab[2];
+    if (sum < 0.5) {
+      inside[i] = 0;
+      elem[i] = 0;
+      x1[i] = y1[i] = 0.0;
+      *tk = reset_tk;
+    } else {
+      inside[i] = 1;
+      elem[i] = *tk;
+      x1[i] = 2.0 * lab[1] - 1.0;
+      y1[i] = 2.0 * lab[2] - 1.0;
+    }
+  }
+  return SPOC_OK;
+}

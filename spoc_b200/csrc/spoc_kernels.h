@@ -138,6 +138,14 @@ cudaError_t launch_cfl2(int ne, int nc, int nm, int n, double *pg, const int *in
                         const double *v, double g0, unsigned long long *out, cudaStream_t st,
                         int sms, long long *launches);
 
+cudaError_t launch_eval_points(int nc, int nm, int ne, int npts, const int *elem,
+                               const double *px, const double *py, const double *const f[3],
+                               double *out, int *flag, cudaStream_t st, int sms,
+                               long long *launches);
+cudaError_t launch_lattice(int ne, int nc, int nm, int n, double *pg, const int *in,
+                           const double *xg, const double *yg, const double *const f[3],
+                           double *out, cudaStream_t st, int sms, long long *launches);
+
 // Adjoint RK4 bookkeeping over the three fields in one launch.  kInit:
 // kb = a lam + b lam.  kFirst: acc = sb, kb = a sb + b lam.  kMid: acc += sb,
 // kb = a sb + b lam.  kLast: lam += acc + sb.

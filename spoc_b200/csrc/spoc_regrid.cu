@@ -342,6 +342,102 @@ __global__ void __launch_bounds__(kRT) k_cfl2(int ne, int nc, int nm, int np, co
   }
 }
 
+// ---------------------------------------------------------------------------
+// Point evaluation of the modal fields (fsol, src/compare.f:203-219): one
+// thread per point, the three fields at once; out[f * npts + i].
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRT) k_eval_points(int nc, int nm, int ne, int npts,
+                                                     const int *elem, const double *px,
+                                                     const double *py, const double *su,
+                                                     const double *sv, const double *sh,
+                                                     double *out, int *flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
+    const int k = elem[i];
+    if (k < 1 || k > ne) {
+      atomicOr(flag, 4);
+      continue;
+    }
+    const size_t so = (size_t)(k - 1) * nm;
+    const double x = px[i], y = py[i];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, xa = 1.0, xb = 0.0;
+    int j = 0;
+    for (int kc1 = 0; kc1 <= nc; ++kc1) {
+      if (kc1 == 1) {
+        xb = xa;
+        xa = x;
+      } else if (kc1 >= 2) {
+        const double pn = po_step(kc1, x, xa, xb);
+        xb = xa;
+        xa = pn;
+      }
+      double ya = 1.0, yb = 0.0;
+      for (int kc2 = 0; kc2 <= nc - kc1; ++kc2, ++j) {
+        if (kc2 == 1) {
+          yb = ya;
+          ya = y;
+        } else if (kc2 >= 2) {
+          const double pn = po_step(kc2, y, ya, yb);
+          yb = ya;
+          ya = pn;
+        }
+        s0 = add(s0, mul(mul(su[so + j], xa), ya));
+        s1 = add(s1, mul(mul(sv[so + j], xa), ya));
+        s2 = add(s2, mul(mul(sh[so + j], xa), ya));
+      }
+    }
+    out[i] = s0;
+    out[(size_t)npts + i] = s1;
+    out[2 * (size_t)npts + i] = s2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// write_gra's values (src/visu2.f:86-149): for element e and lattice point p
+// (k outer, l inner), the physical point and the three fields:
+// out[((e * np + p) * 5 + c)], c = x, y, u, v, h.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRT) k_lattice(int ne, int nm, int n, const double *pg,
+                                                 const int *in, const double *xg,
+                                                 const double *yg, const double *su,
+                                                 const double *sv, const double *sh,
+                                                 double *out) {
+  const int np = n * (n + 1) / 2;
+  const size_t total = (size_t)ne * np;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t / np), p = (int)(t - (size_t)e * np);
+    int k = 1, r = p;
+    while (r >= n - k + 1) {
+      r -= n - k + 1;
+      ++k;
+    }
+    const int ll = r + 1;
+    const int i1 = in[3 * e] - 1, i2 = in[3 * e + 1] - 1, i3 = in[3 * e + 2] - 1;
+    const double ax = mul(sub(xg[i2], xg[i1]), 0.5), bx = mul(sub(xg[i3], xg[i1]), 0.5);
+    const double ay = mul(sub(yg[i2], yg[i1]), 0.5), by = mul(sub(yg[i3], yg[i1]), 0.5);
+    const double xof = xg[i1], yof = yg[i1];
+    const double y1 = __ddiv_rn((double)(2 * k - n - 1), (double)(n - 1));
+    const double x1 = __ddiv_rn((double)(2 * ll - n - 1), (double)(n - 1));
+    const double x = add(add(xof, mul(ax, add(x1, 1.0))), mul(bx, add(y1, 1.0)));
+    const double y = add(add(yof, mul(ay, add(x1, 1.0))), mul(by, add(y1, 1.0)));
+    const double *pp = pg + (size_t)p * nm;
+    const size_t o = (size_t)e * nm;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < nm; ++j) {
+      const double w = __ldg(pp + j);
+      s0 = add(s0, mul(su[o + j], w));
+      s1 = add(s1, mul(sv[o + j], w));
+      s2 = add(s2, mul(sh[o + j], w));
+    }
+    double *q = out + t * 5;
+    q[0] = x;
+    q[1] = y;
+    q[2] = s0;
+    q[3] = s1;
+    q[4] = s2;
+  }
+}
+
 int grid_warps(int items, int sms) {
   const int need = (items + kRW - 1) / kRW;
   const int cap = sms * 8;
@@ -392,6 +488,32 @@ cudaError_t launch_cfl2(int ne, int nc, int nm, int n, double *pg, const int *in
   const int np = n * (n + 1) / 2;
   k_pgraph<<<(np + 127) / 128, 128, 0, st>>>(nc, n, pg);
   k_cfl2<<<grid_warps(ne, sms), kRT, 0, st>>>(ne, nc, nm, np, pg, in, xg, yg, hb, u, v, g0, out);
+  *launches += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eval_points(int nc, int nm, int ne, int npts, const int *elem,
+                               const double *px, const double *py, const double *const f[3],
+                               double *out, int *flag, cudaStream_t st, int sms,
+                               long long *launches) {
+  int g = (npts + kRT - 1) / kRT;
+  if (g > sms * 8) g = sms * 8;
+  if (g < 1) g = 1;
+  k_eval_points<<<g, kRT, 0, st>>>(nc, nm, ne, npts, elem, px, py, f[0], f[1], f[2], out, flag);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lattice(int ne, int nc, int nm, int n, double *pg, const int *in,
+                           const double *xg, const double *yg, const double *const f[3],
+                           double *out, cudaStream_t st, int sms, long long *launches) {
+  const int np = n * (n + 1) / 2;
+  k_pgraph<<<(np + 127) / 128, 128, 0, st>>>(nc, n, pg);
+  const size_t total = (size_t)ne * np;
+  size_t g = (total + kRT - 1) / kRT;
+  if (g > (size_t)sms * 16) g = (size_t)sms * 16;
+  if (g < 1) g = 1;
+  k_lattice<<<(unsigned)g, kRT, 0, st>>>(ne, nm, n, pg, in, xg, yg, f[0], f[1], f[2], out);
   *launches += 2;
   return cudaGetLastError();
 }

@@ -53,3 +53,39 @@ def read_state(path: str | Path, nm: int) -> tuple[float, dict]:
             raise ValueError(f"{path}: record {name} is not a multiple of nm={nm}")
         out[name] = a.reshape(-1, nm).astype(np.float64)
     return time, out
+
+
+def fortran_e(v: float, w: int = 10, d: int = 3) -> str:
+    """Fortran Ew.d edit descriptor as gfortran writes it: 0.ddd mantissa,
+    E+ee exponent (three-digit exponents drop the E), right-justified."""
+    import math
+    if math.isnan(v):
+        return "NaN".rjust(w)
+    if math.isinf(v):
+        return ("-Infinity" if v < 0 else "Infinity").rjust(w)
+    neg = math.copysign(1.0, v) < 0
+    if v == 0.0:
+        digits, exp = "0" * d, 0
+    else:
+        s = f"{abs(v):.{d - 1}e}"
+        mant, e = s.split("e")
+        digits = mant.replace(".", "")
+        exp = int(e) + 1
+    body = f"0.{digits}E{exp:+03d}" if abs(exp) <= 99 else f"0.{digits}{exp:+04d}"
+    return (("-" if neg else "") + body).rjust(w)
+
+
+def gra_name(name: str, nper: int) -> str:
+    """write_gra's file name (src/visu2.f:102-110): field letter, output number, '.gra'."""
+    return f"{name}{nper:d}.gra"
+
+
+def write_gra(path: str | Path, lattice: np.ndarray, field: int) -> None:
+    """write_gra (src/visu2.f:86-149): one line 'x y value' per lattice point
+    of every element in format 3(e10.3,1x).  lattice is (ne, np, 5) from
+    Solver.lattice (x, y, u, v, h); field 0, 1, 2 selects u, v, h."""
+    lines = []
+    for el in lattice:
+        for x, y, *vals in el:
+            lines.append(f"{fortran_e(x)} {fortran_e(y)} {fortran_e(vals[field])} ")
+    Path(path).write_text("\n".join(lines) + "\n")

@@ -473,3 +473,46 @@ def regrid_step(p: Problem, s: api.Solver, fac1: float, fac2: float, fac3: float
     info.update({"ne_old": p.mesh.ne, "ne_new": p1.mesh.ne,
                  "inherited": int((tinter > 0).sum()), "cflmin": cflmin, "dt_cfl2": dt})
     return p1, s1, info
+
+
+# ---------------------------------------------------------------------------
+# compare.f: error of a state against the analytic standing wave
+# ---------------------------------------------------------------------------
+
+def compare_standing_wave(p: Problem, s: api.Solver, nx: int, ny: int, lx: float | None = None,
+                          ly: float | None = None):
+    """compare.f (src/compare.f:56-192): the resident state of s evaluated on
+    the (nx-1) x (ny-1) points x0 = lx/2 (2i - nx)/(nx - 1), y0 likewise, each
+    located by interlin's walk on the host and evaluated (fsol) on the device,
+    against u = uc sin(2 pi x0 / lx), v = 0, h = hc cos(2 pi x0 / lx) with
+    c0 = sqrt(10), uc = sin(0.2 pi) g0 / c0, hc = cos(0.2 pi).  Returns the
+    reference's printed norms; the sums run in the reference's point order."""
+    lx = lx or p.cfg.length
+    ly = ly or p.cfg.length
+    g0 = p.cfg.g0
+    c0 = np.sqrt(10.0)
+    pi = 4.0 * np.arctan(1.0)
+    uc = np.sin(0.2 * pi) * g0 / c0
+    hc = np.cos(0.2 * pi) * 1.0
+    m = p.mesh
+    _, _, _, _, tk1 = api.locate_xy(m, np.array([1.0e6]), np.array([1.0e6]), 1, 1)
+    jj, ii = np.meshgrid(np.arange(1, ny), np.arange(1, nx), indexing="ij")
+    x0 = 0.5 * lx * (2.0 * ii.ravel() - nx) / float(nx - 1)
+    y0 = 0.5 * ly * (2.0 * jj.ravel() - ny) / float(ny - 1)
+    elem, x1, y1, inside, _ = api.locate_xy(m, x0, y0, tk1, tk1)
+    k = inside.astype(bool)
+    vals = s.eval_points(elem[k], x1[k], y1[k])
+    ud, vd, hd = vals
+    xs = x0[k]
+    uref = uc * np.sin(2.0 * pi * xs / lx)
+    href = hc * np.cos(2.0 * pi * xs / lx)
+    seq = lambda a: float(np.cumsum(a)[-1]) if a.size else 0.0  # left-to-right sum
+    e1, e2, e3 = seq(np.abs(uref - ud)), seq(np.abs(vd)), seq(np.abs(href - hd))
+    e4, e5, e6 = seq((uref - ud) ** 2), seq(vd ** 2), seq((href - hd) ** 2)
+    k1 = int(k.sum())
+    ps = m.pseg - 1
+    dis = np.sqrt((m.xgr[ps[:, 0]] - m.xgr[ps[:, 1]]) ** 2 + (m.ygr[ps[:, 0]] - m.ygr[ps[:, 1]]) ** 2)
+    return {"outside": int((~k).sum()), "inside": k1, "dx_mean": seq(dis) / float(m.nf),
+            "abs_norm": (e1 / k1, e2 / k1, e3 / k1),
+            "rms_norm": (np.sqrt(e4 / k1), np.sqrt(e5 / k1), np.sqrt(e6 / k1)),
+            "rms_norm_v": float(np.sqrt((e4 + e5) / k1))}

@@ -150,3 +150,47 @@ def test_regrid_mixed_handles(gpu_lib):
         out.append(d.get_state())
     for a, b in zip(*out):
         assert O.mass_norm(OT, NM, a - b) <= 1e-10 * O.mass_norm(OT, NM, a)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_eval_points_and_lattice_bitwise(gpu_lib, name):
+    p, OT, OM = setup(name)
+    s = stepped(p)
+    u, v, h = s.get_state()
+    rng = np.random.default_rng(4)
+    n = 500
+    elem = rng.integers(1, p.mesh.ne + 1, n).astype(np.int32)
+    a = rng.uniform(-1, 1, n)
+    b = rng.uniform(-1, 1, n)
+    px, py = np.minimum(a, -b), np.maximum(b, -1.0)  # inside the reference triangle
+    got = s.eval_points(elem, px, py)
+    assert np.array_equal(got, O.eval_points(p.cfg.nc, u, v, h, elem, px, py))
+    for ng in (10, 5):
+        assert np.array_equal(s.lattice(ng), O.lattice(p.cfg.nc, OM, u, v, h, ng))
+
+
+@pytest.mark.gpu
+def test_compare_standing_wave(gpu_lib):
+    """compare.f's norms: the device evaluation gives the oracle's numbers, and
+    the projection of the analytic wave itself is close to it."""
+    p, OT, OM = setup("c1_lin_p3", n=16)
+    L = p.cfg.length
+    pi = 4.0 * np.arctan(1.0)
+    uc = np.sin(0.2 * pi) * p.cfg.g0 / np.sqrt(10.0)
+    hc = np.cos(0.2 * pi)
+    u, _, _ = O.calh(OT, OM, lambda x, y: uc * np.sin(2 * pi * x / L))
+    hh, _, _ = O.calh(OT, OM, lambda x, y: hc * np.cos(2 * pi * x / L))
+    z = np.zeros_like(u)
+    s = W.make_solver(p)
+    s.set_state(u, z, hh)
+    got = W.compare_standing_wave(p, s, 41, 41)
+
+    class OracleEval:
+        def eval_points(self, elem, px, py):
+            return O.eval_points(p.cfg.nc, u, z, hh, elem, px, py)
+
+    ref = W.compare_standing_wave(p, OracleEval(), 41, 41)
+    assert got == ref
+    assert got["inside"] == 40 * 40 and got["outside"] == 0
+    assert got["rms_norm"][2] < 1e-3 * hc and got["rms_norm"][1] == 0.0

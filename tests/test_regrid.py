@@ -142,3 +142,38 @@ def test_checkcfl2_at_rest_matches_closed_form():
         assert dt == float(int(cmin))
     else:
         assert dt == 0.0  # the reference's integer division
+
+
+def test_fortran_e_format():
+    from spoc_b200.fortran_io import fortran_e
+    cases = {0.0: " 0.000E+00", 1234.5: " 0.123E+04", -1234.5: "-0.123E+04",
+             0.00012345: " 0.123E-03", 9999.6: " 0.100E+05", 1e100: " 0.100+101", 1.0: " 0.100E+01"}
+    for v, s in cases.items():
+        assert fortran_e(v) == s, (v, fortran_e(v))
+
+
+def test_write_gra_layout(tmp_path):
+    from spoc_b200.fortran_io import write_gra, gra_name
+    lat = np.zeros((2, 3, 5))
+    lat[..., 0] = 1.5e5
+    lat[..., 4] = -2.0
+    path = tmp_path / gra_name("h", 12)
+    write_gra(path, lat, 2)
+    lines = path.read_text().splitlines()
+    assert path.name == "h12.gra" and len(lines) == 6
+    assert lines[0] == " 0.150E+06  0.000E+00 -0.200E+01 "
+
+
+def test_host_locate_xy_equals_oracle_walk():
+    p, OT, OM, *_ = setup("c2_fs_p6")
+    rng = np.random.default_rng(3)
+    half = 0.5 * p.cfg.length
+    px = rng.uniform(-half, half, 300)
+    py = rng.uniform(-half, half, 300)
+    elem, x1, y1, inside, tk = api.locate_xy(p.mesh, px, py, 1, 1)
+    t = 1
+    for i in range(px.size):
+        t, _, _, lab = O.interlin(OM, t, px[i], py[i])
+        assert inside[i] == 1 and elem[i] == t
+        assert x1[i] == 2.0 * lab[1] - 1.0 and y1[i] == 2.0 * lab[2] - 1.0
+    assert tk == t
