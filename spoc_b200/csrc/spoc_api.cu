@@ -237,11 +237,18 @@ int build_mesh(spoc_handle *h, const spoc_mesh *m) {
 }
 
 // host (ld, ne) <-> device packed (nm, ne)
+// (ld, ne) caller arrays <-> packed (nm, ne) device fields; packed caller
+// arrays (ld == nm) move as one contiguous copy (a pitched copy of ne rows of
+// nm doubles runs far below the link bandwidth).
 cudaError_t copy_in(spoc_handle *h, double *dst, const double *src, int ld, cudaMemcpyKind k) {
+  if (ld == h->nm)
+    return cudaMemcpyAsync(dst, src, sizeof(double) * h->nm * (size_t)h->ne, k, h->st);
   return cudaMemcpy2DAsync(dst, sizeof(double) * h->nm, src, sizeof(double) * ld,
                            sizeof(double) * h->nm, h->ne, k, h->st);
 }
 cudaError_t copy_out(spoc_handle *h, double *dst, const double *src, int ld, cudaMemcpyKind k) {
+  if (ld == h->nm)
+    return cudaMemcpyAsync(dst, src, sizeof(double) * h->nm * (size_t)h->ne, k, h->st);
   return cudaMemcpy2DAsync(dst, sizeof(double) * ld, src, sizeof(double) * h->nm,
                            sizeof(double) * h->nm, h->ne, k, h->st);
 }

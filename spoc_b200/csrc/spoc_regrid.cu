@@ -52,20 +52,30 @@ __global__ void __launch_bounds__(kRT) k_checkconv(DevOps op, DevMesh m, const d
   const double *a0 = fld == 0 ? su : (fld == 1 ? sv : sh);
   for (int f = gwarp(); f < m.nf; f += nwarps()) {
     const int k1 = m.tseg[2 * f], k2 = m.tseg[2 * f + 1];
-    if (k2 < 0 || fld >= 3) continue;
-    const int c1 = m.ssit[2 * f], c2 = m.ssit[2 * f + 1];
-    const double *p1 = op.picoF + (size_t)c1 * nm * G + j;
-    const double *p2 = op.picoF + (size_t)c2 * nm * G + (G - 1 - j);
-    const double *x1 = a0 + (size_t)k1 * nm, *x2 = a0 + (size_t)k2 * nm;
-    double f1 = 0.0, f2 = 0.0;
-    for (int n = 0; n < nm; ++n) {
-      f1 = add(f1, mul(x1[n], __ldg(p1 + (size_t)n * G)));
-      f2 = add(f2, mul(x2[n], __ldg(p2 + (size_t)n * G)));
+    if (k2 < 0) continue;  // warp-uniform
+    double dif = 0.0;
+    if (fld < 3) {
+      const int c1 = m.ssit[2 * f], c2 = m.ssit[2 * f + 1];
+      const double *p1 = op.picoF + (size_t)c1 * nm * G + j;
+      const double *p2 = op.picoF + (size_t)c2 * nm * G + (G - 1 - j);
+      const double *x1 = a0 + (size_t)k1 * nm, *x2 = a0 + (size_t)k2 * nm;
+      double f1 = 0.0, f2 = 0.0;
+      for (int n = 0; n < nm; ++n) {
+        f1 = add(f1, mul(x1[n], __ldg(p1 + (size_t)n * G)));
+        f2 = add(f2, mul(x2[n], __ldg(p2 + (size_t)n * G)));
+      }
+      dif = fabs(sub(f2, f1));
     }
-    const double dif = fabs(sub(f2, f1));
-    if (dif > 0.0) {  // amax(k) < dif: zero and NaN jumps leave it
-      max_bits(amax + (size_t)fld * ne + k1, dif);
-      max_bits(amax + (size_t)fld * ne + k2, dif);
+    // largest jump of each field over the face's points (max is exact in any
+    // order), then one update per field and element
+    double mx = dif;
+    for (int t = 1; t < G; ++t) {
+      const double v = __shfl_sync(0xffffffffu, dif, l + t < kWarp ? l + t : l);
+      if (j + t < G) mx = fmax(mx, v);
+    }
+    if (fld < 3 && j == 0 && mx > 0.0) {  // amax(k) < dif: zero and NaN jumps leave it
+      max_bits(amax + (size_t)fld * ne + k1, mx);
+      max_bits(amax + (size_t)fld * ne + k2, mx);
     }
   }
 }
