@@ -635,8 +635,10 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
 // ---------------------------------------------------------------------------
 template <class Dm>
 struct BWarp {
+  static constexpr int T = Dm::Q > 32 ? Dm::Q - 32 : 1;  // quadrature points past lane 31
   double vin[9 * Dm::N];
   double wp[8 * Dm::Q];
+  double tail[9 * T];  // values of the nine fields at those points
   double sm[64];
 };
 
@@ -680,29 +682,52 @@ __global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) 
       for (int f = 0; f < 9; ++f) reg_to_sm<Dm>(W.vin + f * N, v9[f]);
     }
     __syncwarp();
-    // spectoxy (src/nonlin.f:62-86) for the nine fields; lanes over points
+    // spectoxy (src/nonlin.f:62-86) for the nine fields; lanes over points.
+    // Points past lane 31 (degree 6: one, degree 7: ten) would cost a second
+    // pass of nine full chains on a few lanes: their (field, point) chains are
+    // spread over the lanes instead, each still summed over n in order.
+    auto products = [&](int qp, const double (&mv)[9]) {
+      const double w = S.wi[qp];
+      W.wp[0 * Q + qp] = mul(w, mul(mv[0], mv[2]));
+      W.wp[1 * Q + qp] = mul(w, mul(mv[1], mv[3]));
+      W.wp[2 * Q + qp] = mul(w, mul(mv[0], mv[4]));
+      W.wp[3 * Q + qp] = mul(w, mul(mv[1], mv[5]));
+      W.wp[4 * Q + qp] = mul(w, mul(mv[0], mv[6]));
+      W.wp[5 * Q + qp] = mul(w, mul(mv[1], mv[6]));
+      W.wp[6 * Q + qp] = mul(w, __ddiv_rn(mv[7], mv[6]));
+      W.wp[7 * Q + qp] = mul(w, __ddiv_rn(mv[8], mv[6]));
+    };
+    if (l < Q) {
+      double mv[9];
 #pragma unroll
-    for (int h = 0; h < RQ; ++h) {
-      const int qp = l + 32 * h;
-      if (qp < Q) {
+      for (int f = 0; f < 9; ++f) mv[f] = 0.0;
+#pragma unroll 4
+      for (int n = 0; n < N; ++n) {
+        const double p = S.p2[n * Q + l];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) mv[f] = macc(mv[f], W.vin[f * N + n], p);
+      }
+      products(l, mv);
+    }
+    if (RQ > 1) {
+      constexpr int T = BWarp<Dm>::T;
+#pragma unroll
+      for (int c0 = 0; c0 < 9 * T; c0 += 32) {
+        const int c = c0 + l;
+        if (c < 9 * T) {
+          const int f = c / T, t = c - f * T;
+          double v = 0.0;
+#pragma unroll 4
+          for (int n = 0; n < N; ++n) v = macc(v, W.vin[f * N + n], S.p2[n * Q + 32 + t]);
+          W.tail[c] = v;
+        }
+      }
+      __syncwarp();
+      if (l < T) {
         double mv[9];
 #pragma unroll
-        for (int f = 0; f < 9; ++f) mv[f] = 0.0;
-#pragma unroll 4
-        for (int n = 0; n < N; ++n) {
-          const double p = S.p2[n * Q + qp];
-#pragma unroll
-          for (int f = 0; f < 9; ++f) mv[f] = macc(mv[f], W.vin[f * N + n], p);
-        }
-        const double w = S.wi[qp];
-        W.wp[0 * Q + qp] = mul(w, mul(mv[0], mv[2]));
-        W.wp[1 * Q + qp] = mul(w, mul(mv[1], mv[3]));
-        W.wp[2 * Q + qp] = mul(w, mul(mv[0], mv[4]));
-        W.wp[3 * Q + qp] = mul(w, mul(mv[1], mv[5]));
-        W.wp[4 * Q + qp] = mul(w, mul(mv[0], mv[6]));
-        W.wp[5 * Q + qp] = mul(w, mul(mv[1], mv[6]));
-        W.wp[6 * Q + qp] = mul(w, __ddiv_rn(mv[7], mv[6]));
-        W.wp[7 * Q + qp] = mul(w, __ddiv_rn(mv[8], mv[6]));
+        for (int f = 0; f < 9; ++f) mv[f] = W.tail[f * T + l];
+        products(32 + l, mv);
       }
     }
     __syncwarp();

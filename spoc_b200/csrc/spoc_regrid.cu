@@ -60,9 +60,10 @@ __global__ void __launch_bounds__(kRT) k_checkconv(DevOps op, DevMesh m, const d
       const double *p2 = op.picoF + (size_t)c2 * nm * G + (G - 1 - j);
       const double *x1 = a0 + (size_t)k1 * nm, *x2 = a0 + (size_t)k2 * nm;
       double f1 = 0.0, f2 = 0.0;
+#pragma unroll 8
       for (int n = 0; n < nm; ++n) {
-        f1 = add(f1, mul(x1[n], __ldg(p1 + (size_t)n * G)));
-        f2 = add(f2, mul(x2[n], __ldg(p2 + (size_t)n * G)));
+        f1 = add(f1, mul(__ldg(x1 + n), __ldg(p1 + (size_t)n * G)));
+        f2 = add(f2, mul(__ldg(x2 + n), __ldg(p2 + (size_t)n * G)));
       }
       dif = fabs(sub(f2, f1));
     }
