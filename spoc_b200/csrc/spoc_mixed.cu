@@ -233,8 +233,10 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       gl[3 * TG + lane] = s * r.ny * fv;
     }
     __syncwarp();
-    // u, v, h + hb at the quadrature points (spectoxy)
-    for (int q = lane; q < Q; q += 32) {
+    // u, v, h + hb at the quadrature points (spectoxy); points past lane 31
+    // run as (field, point) chains spread over the lanes
+    if (lane < Q) {
+      const int q = lane;
       float U = 0.f, V = 0.f, H = 0.f;
 #pragma unroll 4
       for (int n = 0; n < N; ++n) {
@@ -246,6 +248,17 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       qp[q] = U;
       qp[Q + q] = V;
       qp[2 * Q + q] = H + a.hbq[(size_t)e * Q + q];
+    }
+    if (Q > 32) {
+      constexpr int T = Q > 32 ? Q - 32 : 1;
+      for (int c = lane; c < 3 * T; c += 32) {
+        const int f = c / T, q = 32 + c - f * T;
+        const float *x = f == 0 ? su : (f == 1 ? sv : sh);
+        float acc = 0.f;
+#pragma unroll 4
+        for (int n = 0; n < N; ++n) acc = fma32(o[Dm::PPT + n * Q + q], x[n], acc);
+        qp[f * Q + q] = f == 2 ? acc + a.hbq[(size_t)e * Q + q] : acc;
+      }
     }
     // q = weak gradients of u, v (calvarnl_fs.f:115-164): cal_b with coeff -1,
     // geometry, then tri_f of the traces; the mass solve is the identity
@@ -311,16 +324,7 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     // quadrature-point products (calvarnl_fs.f:243-332); xytospec is linear,
     // so the four projections of -adu + w1, -adv + z1, uh, vh take combined
     // integrands
-    for (int q = lane; q < Q; q += 32) {
-      float gxx = 0.f, gxy = 0.f, gyx = 0.f, gyy = 0.f;
-#pragma unroll 4
-      for (int n = 0; n < N; ++n) {
-        const float p = o[Dm::PPT + n * Q + q];
-        gxx = fma32(p, sq[n], gxx);
-        gxy = fma32(p, sq[N + n], gxy);
-        gyx = fma32(p, sq[2 * N + n], gyx);
-        gyy = fma32(p, sq[3 * N + n], gyy);
-      }
+    auto qproducts = [&](int q, float gxx, float gxy, float gyx, float gyy) {
       const float fc = a.fcq[(size_t)e * Q + q];
       gxy -= fc;
       gyx += fc;
@@ -334,6 +338,37 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       qp[4 * Q + q] = zk / H - (U * gyx + V * gyy);
       qp[5 * Q + q] = U * H;
       qp[6 * Q + q] = V * H;
+    };
+    if (lane < Q) {
+      const int q = lane;
+      float gxx = 0.f, gxy = 0.f, gyx = 0.f, gyy = 0.f;
+#pragma unroll 4
+      for (int n = 0; n < N; ++n) {
+        const float p = o[Dm::PPT + n * Q + q];
+        gxx = fma32(p, sq[n], gxx);
+        gxy = fma32(p, sq[N + n], gxy);
+        gyx = fma32(p, sq[2 * N + n], gyx);
+        gyy = fma32(p, sq[3 * N + n], gyy);
+      }
+      qproducts(q, gxx, gxy, gyx, gyy);
+    }
+    if (Q > 32) {
+      // the four gradient values at points past lane 31 as spread chains,
+      // parked in the qp slots their products overwrite
+      constexpr int T = Q > 32 ? Q - 32 : 1;
+      __syncwarp();
+      for (int c = lane; c < 4 * T; c += 32) {
+        const int f = c / T, q = 32 + c - f * T;
+        float acc = 0.f;
+#pragma unroll 4
+        for (int n = 0; n < N; ++n) acc = fma32(o[Dm::PPT + n * Q + q], sq[f * N + n], acc);
+        qp[(3 + f) * Q + q] = acc;
+      }
+      __syncwarp();
+      if (lane < T) {
+        const int q = 32 + lane;
+        qproducts(q, qp[3 * Q + q], qp[4 * Q + q], qp[5 * Q + q], qp[6 * Q + q]);
+      }
     }
     __syncwarp();
     float bxr[R], byr[R], uh[R], vh[R];
