@@ -198,9 +198,12 @@ int spoc_profile_rk4(spoc_handle *h, double dt, int nsteps, double *kernel_ms, i
  * capture succeeds); the members' states are then read with spoc_get_state.
  * Work layout: blocks_per_sm resident blocks per SM (1 .. max), dealt to the
  * members in proportion to their work modelled as ne nm^p, p = 2, 1, 0.5, 0
- * for weight 0, 1, 2, 3;
+ * for weight 0, 1, 2, 3, or measured (weight 4, after spoc_ensemble_balance);
  * spoc_ensemble_configure sets it, spoc_ensemble_info reports it (graph: 1
- * when steps run from a graph; member_blocks: blocks per member, or null). */
+ * when steps run from a graph; member_blocks: blocks per member, or null).
+ * spoc_ensemble_balance runs `rounds` steps (they advance the members) with
+ * per-block cycle counters and after each deals the blocks again in
+ * proportion to every member's measured block cycles (weight 4). */
 typedef struct spoc_ensemble spoc_ensemble;
 int spoc_ensemble_create(int nmem, spoc_handle *const *members, spoc_ensemble **out);
 void spoc_ensemble_destroy(spoc_ensemble *e);
@@ -208,6 +211,7 @@ int spoc_ensemble_configure(spoc_ensemble *e, int blocks_per_sm, int weight);
 int spoc_ensemble_info(spoc_ensemble *e, int *blocks_per_sm, int *max_blocks_per_sm, int *weight,
                        int *blocks, int *graph, int *member_blocks);
 int spoc_ensemble_steps(spoc_ensemble *e, const double *dt, int nsteps, int use_graph);
+int spoc_ensemble_balance(spoc_ensemble *e, const double *dt, int rounds);
 
 /* Self-test of the tcgen05 TF32 tensor-core path the mixed kernels use (no
  * reference counterpart): D (128 x n) = A (128 x K) B^T (B: n x K), row-major

@@ -96,6 +96,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "spoc_ensemble_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "spoc_ensemble_steps": (C.c_int, [vp, _DP, C.c_int, C.c_int]),
+        "spoc_ensemble_balance": (C.c_int, [vp, _DP, C.c_int]),
         "spoc_set_stream": (C.c_int, [vp, vp]),
         "spoc_set_kernel_path": (C.c_int, [vp, C.c_int]),
         "spoc_set_params": (C.c_int, [vp, C.POINTER(_Params)]),
@@ -660,16 +661,26 @@ class Ensemble:
         d = np.ascontiguousarray(dts, dtype=np.float64)
         _check(self.lib.spoc_ensemble_steps(self._e, _d(d), nsteps, int(graph)), "ensemble_steps")
 
+    def balance(self, dts, rounds: int = 2) -> None:
+        """Measured work model (weight 4): `rounds` steps with per-block cycle
+        counters, blocks dealt again after each.  Advances the members."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        _check(self.lib.spoc_ensemble_balance(self._e, _d(d), rounds), "ensemble_balance")
+
     def autotune(self, dts, nsteps: int = 3) -> dict:
-        """Times every layout (resident blocks per SM x work model ne nm^p,
-        p = 2, 1, 0.5, 0) over
-        nsteps steps after one warm-up step and keeps the fastest.  Advances
-        the members' states: set them again afterwards."""
+        """Times every layout (resident blocks per SM x work model: ne nm^p,
+        p = 2, 1, 0.5, 0, or measured block cycles, weight 4) over nsteps
+        steps after one warm-up step and keeps the fastest.  Advances the
+        members' states: set them again afterwards."""
         import time
         best, table = None, []
         for bps in range(1, self.info()["max_blocks_per_sm"] + 1):
-            for weight in (0, 1, 2, 3):
-                self.configure(bps, weight)
+            for weight in (0, 1, 2, 3, 4):
+                if weight == 4:
+                    self.configure(bps, 2)
+                    self.balance(dts, 2)
+                else:
+                    self.configure(bps, weight)
                 self.steps(dts, 1)
                 t = time.perf_counter()
                 self.steps(dts, nsteps)

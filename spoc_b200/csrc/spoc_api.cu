@@ -1784,6 +1784,16 @@ extern "C" int spoc_ensemble_info(spoc_ensemble *e, int *blocks_per_sm, int *max
   return SPOC_OK;
 }
 
+extern "C" int spoc_ensemble_balance(spoc_ensemble *e, const double *dt, int rounds) {
+  if (!e || !dt || rounds < 1) return fail(SPOC_E_ARG, "bad argument");
+  CK(mixed_ens_balance(e->ens, dt, rounds), "ensemble balance");
+  for (spoc_handle *h : e->mem) {
+    const int rc = check_flag(h);
+    if (rc) return rc;
+  }
+  return SPOC_OK;
+}
+
 extern "C" int spoc_ensemble_steps(spoc_ensemble *e, const double *dt, int nsteps, int use_graph) {
   if (!e || !dt || nsteps < 0) return fail(SPOC_E_ARG, "bad argument");
   CK(mixed_ens_steps(e->ens, dt, nsteps, use_graph != 0), "ensemble steps");

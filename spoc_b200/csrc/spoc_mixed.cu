@@ -1133,9 +1133,12 @@ __device__ __forceinline__ void ens_dims(int nc, F &&f) {
 
 constexpr int kEnsMinBlocks = 4;  // degrees 3-6: one row per lane, 64 registers
 
+// bt (null except when balancing): each block adds the SM cycles of its
+// volume phase (operator staging included) and of its tendency phase to
+// bt[2 b] and bt[2 b + 1].
 __global__ void __launch_bounds__(32 * kMxWarps, kEnsMinBlocks)
     kx_ens_stage(const EnsMember *__restrict__ mem, const int *__restrict__ blk_member, int stage,
-                 int cur) {
+                 int cur, unsigned long long *bt) {
   extern __shared__ __align__(16) float sm[];
   const EnsMember &em = mem[blk_member[blockIdx.x]];
   MxArgs a = em.a;
@@ -1143,11 +1146,21 @@ __global__ void __launch_bounds__(32 * kMxWarps, kEnsMinBlocks)
   a.tr_in = em.tr[cur];
   a.tr_out = em.tr[cur ^ 1];
   const int lb = blockIdx.x - em.first_block, nb = em.nblocks;
+  const long long c0 = bt ? clock64() : 0;
   ens_dims(em.nc, [&](auto d) { stage_mx_ops<decltype(d)>(sm, a.ops); });
   __syncthreads();
   ens_dims(em.nc, [&](auto d) { vol_body<decltype(d), SPOC_FS>(a, sm, lb, nb); });
+  if (bt) {
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(bt + 2 * blockIdx.x, (unsigned long long)(clock64() - c0));
+  }
   cooperative_groups::this_grid().sync();
+  const long long c1 = bt ? clock64() : 0;
   ens_dims(em.nc, [&](auto d) { tend_body<decltype(d), SPOC_FS>(a, sm, lb, nb); });
+  if (bt) {
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(bt + 2 * blockIdx.x + 1, (unsigned long long)(clock64() - c1));
+  }
 }
 
 size_t ens_smem() { return mx_smem<MDims<6, 33, 7>>(); }
@@ -1160,9 +1173,11 @@ struct MixedEns {
   std::vector<int *> flag;
   std::vector<double> dt;
   std::vector<int> nb;  // blocks of each member under the current layout
+  std::vector<double> mw;  // measured work per member (weight 4)
   int sms = 148, bps = 0, weight = 0, nblk = 0, max_bps = 1;
   EnsMember *d_mem = nullptr;
   int *d_blk = nullptr;
+  unsigned long long *d_bt = nullptr;  // block cycles while balancing
   cudaStream_t st = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool graph_ok = true;
@@ -1170,6 +1185,7 @@ struct MixedEns {
     if (exec) cudaGraphExecDestroy(exec);
     cudaFree(d_mem);
     cudaFree(d_blk);
+    cudaFree(d_bt);
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -1177,7 +1193,8 @@ struct MixedEns {
 namespace {
 
 // Blocks per member in proportion to its work, modelled as ne nm^p with
-// p = 2, 1, 0.5, 0 for weight 0..3; at least one block each.
+// p = 2, 1, 0.5, 0 for weight 0..3, or measured (weight 4: the member's
+// block cycles of a balancing step); at least one block each.
 int ens_layout(MixedEns *e) {
   const int n = (int)e->mem.size();
   const int total = e->bps * e->sms;
@@ -1187,7 +1204,7 @@ int ens_layout(MixedEns *e) {
   for (int i = 0; i < n; ++i) {
     const double N = e->mem[i]->N;
     static const double expo[4] = {2.0, 1.0, 0.5, 0.0};
-    w[i] = (double)e->mem[i]->ne * std::pow(N, expo[e->weight]);
+    w[i] = e->weight == 4 ? e->mw[i] : (double)e->mem[i]->ne * std::pow(N, expo[e->weight]);
     sw += w[i];
   }
   std::vector<int> nb(n, 1);
@@ -1234,11 +1251,12 @@ int ens_layout(MixedEns *e) {
   return ce == cudaSuccess ? SPOC_OK : SPOC_E_CUDA;
 }
 
-cudaError_t ens_launch_step(MixedEns *e, int cur0) {
+cudaError_t ens_launch_step(MixedEns *e, int cur0, unsigned long long *bt = nullptr) {
   const size_t smem = ens_smem();
   for (int s = 0; s < 4; ++s) {
     int stage = s, cur = (cur0 + s) & 1;
-    void *args[] = {(void *)&e->d_mem, (void *)&e->d_blk, (void *)&stage, (void *)&cur};
+    void *args[] = {(void *)&e->d_mem, (void *)&e->d_blk, (void *)&stage, (void *)&cur,
+                    (void *)&bt};
     cudaError_t ce = cudaLaunchCooperativeKernel((const void *)kx_ens_stage, dim3(e->nblk),
                                                  dim3(32 * kMxWarps), args, smem, e->st);
     if (ce != cudaSuccess) return ce;
@@ -1297,7 +1315,8 @@ int mixed_ens_create(MixedEns **out, MixedCtx *const *ctx, const DevMesh *meshes
 void mixed_ens_destroy(MixedEns *e) { delete e; }
 
 int mixed_ens_configure(MixedEns *e, int bps, int weight) {
-  if (bps < 1 || bps > e->max_bps || weight < 0 || weight > 3) return SPOC_E_ARG;
+  if (bps < 1 || bps > e->max_bps || weight < 0 || weight > 4) return SPOC_E_ARG;
+  if (weight == 4 && e->mw.size() != e->mem.size()) return SPOC_E_ARG;
   e->bps = bps;
   e->weight = weight;
   return ens_layout(e);
@@ -1314,6 +1333,36 @@ void mixed_ens_info(const MixedEns *e, int *bps, int *max_bps, int *weight, int 
 
 int mixed_ens_member_blocks(const MixedEns *e, int i) {
   return (i >= 0 && i < (int)e->nb.size()) ? e->nb[i] : -1;
+}
+
+cudaError_t mixed_ens_balance(MixedEns *e, const double *dt, int rounds) {
+  const int n = (int)e->mem.size();
+  for (int i = 0; i < n; ++i) e->dt[i] = dt[i];
+  const int cur0 = e->mem[0]->cur;
+  for (MixedCtx *c : e->mem)
+    if (c->cur != cur0) return cudaErrorInvalidValue;
+  const size_t cap = 2 * (size_t)e->max_bps * e->sms;
+  cudaError_t ce = cudaSuccess;
+  if (!e->d_bt) ce = cudaMalloc(&e->d_bt, sizeof(unsigned long long) * cap);
+  std::vector<unsigned long long> bt(cap);
+  for (int r = 0; r < rounds && ce == cudaSuccess; ++r) {
+    if (ens_layout(e)) return cudaErrorMemoryAllocation;
+    ce = cudaMemsetAsync(e->d_bt, 0, sizeof(unsigned long long) * 2 * e->nblk, e->st);
+    if (ce == cudaSuccess) ce = ens_launch_step(e, cur0, e->d_bt);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(bt.data(), e->d_bt, sizeof(unsigned long long) * 2 * e->nblk,
+                           cudaMemcpyDeviceToHost, e->st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
+    if (ce != cudaSuccess) break;
+    // a member's work: the cycles of all its blocks in both phases
+    std::vector<double> w(n, 0.0);
+    for (int i = 0, b = 0; i < n; ++i)
+      for (int k = 0; k < e->nb[i]; ++k, ++b) w[i] += (double)bt[2 * b] + (double)bt[2 * b + 1];
+    e->mw = w;
+    e->weight = 4;
+  }
+  if (ce == cudaSuccess && ens_layout(e)) return cudaErrorMemoryAllocation;
+  return ce;
 }
 
 cudaError_t mixed_ens_steps(MixedEns *e, const double *dt, int nsteps, bool use_graph) {

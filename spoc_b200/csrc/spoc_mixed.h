@@ -64,7 +64,8 @@ bool mixed_uses_tensor(const MixedCtx *c);
 // Ensemble of members (mixed precision, free-slip, degree 3-6) stepped
 // together: one cooperative launch per RK4 stage for all members, optionally
 // replayed from a CUDA graph.  Blocks are dealt to members in proportion to
-// their work, modelled as ne nm^p with p = 2, 1, 0.5, 0 for weight 0..3;
+// their work, modelled as ne nm^p with p = 2, 1, 0.5, 0 for weight 0..3, or
+// measured (weight 4, mixed_ens_balance);
 // bps resident blocks per SM.
 struct MixedEns;
 int mixed_ens_create(MixedEns **out, MixedCtx *const *ctx, const DevMesh *meshes,
@@ -75,5 +76,9 @@ void mixed_ens_info(const MixedEns *e, int *bps, int *max_bps, int *weight, int 
                     int *graph);
 int mixed_ens_member_blocks(const MixedEns *e, int i);
 cudaError_t mixed_ens_steps(MixedEns *e, const double *dt, int nsteps, bool use_graph);
+// Measured work model: `rounds` steps (they advance the members), each with
+// per-block cycle counters; after each, blocks are dealt again in proportion
+// to every member's total block cycles (weight 4).
+cudaError_t mixed_ens_balance(MixedEns *e, const double *dt, int rounds);
 
 }  // namespace spoc

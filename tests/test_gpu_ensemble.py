@@ -81,6 +81,27 @@ def test_layouts_and_graph_replay_agree():
 
 
 @pytest.mark.gpu
+def test_measured_balance_keeps_results():
+    """spoc_ensemble_balance's steps (with block cycle counters) and the steps
+    on the re-dealt layout give the same states as plain steps."""
+    ps = small_members()
+    dts = [p.dt for p in ps]
+    ref_mem = [solver(p) for p in ps]
+    api.Ensemble(ref_mem).steps(dts, 4)
+    mem = [solver(p) for p in ps]
+    ens = api.Ensemble(mem)
+    with pytest.raises(api.SpocError):
+        ens.configure(1, 4)  # no measurement yet
+    ens.balance(dts, 2)
+    info = ens.info()
+    assert info["weight"] == 4 and info["blocks"] == sum(info["member_blocks"])
+    ens.steps(dts, 2)
+    for x, y in zip(states(mem), states(ref_mem)):
+        for a, b in zip(x, y):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
 def test_ensemble_error_against_fp64():
     ps = small_members()
     dts = [p.dt for p in ps]
