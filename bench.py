@@ -392,14 +392,19 @@ def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
         b.synchronize()
         return out, a.elapsed_time(b)
 
-    J, t_fwd = timed(lambda: s.fwd_window(x0, p.dt, nsteps))
+    # median of three runs of each window
+    fw = [timed(lambda: s.fwd_window(x0, p.dt, nsteps)) for _ in range(3)]
+    J, t_fwd = fw[0][0], float(np.median([t for _, t in fw]))
     s.adjoint_counters()
-    (J2, g), t_bwd = timed(lambda: s.bwd_window(x0, p.dt, nsteps, snaps))
+    bw = [timed(lambda: s.bwd_window(x0, p.dt, nsteps, snaps)) for _ in range(3)]
+    (J2, g), t_bwd = bw[0][0], float(np.median([t for _, t in bw]))
     nf, na = s.adjoint_counters()
+    nf, na = nf // 3, na // 3
     s.close()
     return {"config": f"c4_ns_p4: {p.mesh.ne} triangles, nm={p.T.nm}, window {nsteps} steps, "
                       f"{snaps} binomial snapshots, {nobs} observation points at steps 50/100/150/200",
             "cost": J, "forward_window_ms": t_fwd, "gradient_ms": t_bwd,
+            "timing": "median of three runs of each window",
             "gradient_over_forward": t_bwd / t_fwd,
             "forward_steps_run_by_gradient": nf, "adjoint_steps": na,
             "checks": "dot-product, central differences (20 directions) and checkpointing invariance in tests/test_gpu_adjoint.py"}
