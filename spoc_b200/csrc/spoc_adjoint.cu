@@ -542,6 +542,425 @@ __global__ void __launch_bounds__(kT) k_adj_qphase_b(DevOps op_in, DevMesh m, Ad
 }
 
 // ---------------------------------------------------------------------------
+// Two elements per warp for the tabulated degrees with nm <= 16 (degrees 3
+// and 4): a 16-lane tile owns an element, one mode (or point) per lane, so
+// the mode loops keep 15 of 16 lanes busy instead of 15 of 32.  Same
+// arithmetic as the kernels above; shuffles and barriers are per tile.
+// ---------------------------------------------------------------------------
+namespace t16 {
+
+constexpr int W = 16;
+__device__ __forceinline__ int lane() { return threadIdx.x & (W - 1); }
+__device__ __forceinline__ unsigned mask() { return 0xffffu << (threadIdx.x & 16); }
+__device__ __forceinline__ void sync() { __syncwarp(mask()); }
+__device__ __forceinline__ double shfl(double x, int k) { return __shfl_sync(mask(), x, k, W); }
+// tile slot of this thread: in the block, in the grid, and the grid's count
+__device__ __forceinline__ int bslot() { return threadIdx.x >> 4; }
+__device__ __forceinline__ int gslot() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 4; }
+__device__ __forceinline__ int nslot() { return (gridDim.x * blockDim.x) >> 4; }
+
+__device__ __forceinline__ double load(const double *__restrict__ g, int n) {
+  const int l = lane();
+  return l < n ? g[l] : 0.0;
+}
+__device__ __forceinline__ void store(double *g, double v, int n) {
+  if (lane() < n) g[lane()] = v;
+}
+
+// DTRSM4 (src/dtrsm1.f:47-82) on the tile, as dtrsm4 in spoc_device.cuh
+__device__ __forceinline__ double dtrsm(double t, int m, const double *__restrict__ uT,
+                                        const double *__restrict__ uC,
+                                        const double *__restrict__ dia, int ld) {
+  const int l = lane();
+  for (int k = 0; k < m; ++k) {
+    if (l == k) t = mul(t, __ldg(dia + k));
+    const double xk = shfl(t, k);
+    if (l > k && l < m) t = sub(t, mul(__ldg(uT + k * ld + l), xk));
+  }
+  for (int k = m - 1; k >= 0; --k) {
+    if (l == k) t = mul(t, __ldg(dia + k));
+    const double bk = shfl(t, k);
+    if (l < k) t = sub(t, mul(bk, __ldg(uC + k * ld + l)));
+  }
+  return t;
+}
+__device__ __forceinline__ double solve_full(const DevOps &op, double b) {
+  return dtrsm(b, op.nm, op.uT, op.uC, op.dia1, op.nm);
+}
+__device__ __forceinline__ double solve_red(const DevOps &op, double b) {
+  return dtrsm(b, op.nmr, op.ulT, op.ulC, op.dia2, op.nm);
+}
+
+// reduc_gn / reduc_inv_gn (src/mat1.f:418-473) through the tile's scratch
+__device__ __forceinline__ double reduc_gn(const DevOps &op, double gn, double *sm) {
+  const int l = lane();
+  store(sm, gn, op.nm);
+  sync();
+  double v = 0.0;
+  if (l < op.nmr) {
+    const double a = sm[__ldg(op.red_k + l)], c = sm[__ldg(op.red_i0 + l)];
+    v = __ldg(op.red_sg + l) > 0 ? add(a, c) : sub(a, c);
+  }
+  sync();
+  return v;
+}
+__device__ __forceinline__ double reduc_inv_gn(const DevOps &op, double gnr, double *sm) {
+  const int l = lane();
+  store(sm, gnr, op.nmr);
+  sync();
+  double v = 0.0;
+  if (l < op.nm) {
+    const int kind = __ldg(op.inv_kind + l);
+    if (kind == 1) {
+      const int a = __ldg(op.inv_a + l), cnt = __ldg(op.inv_cnt + l);
+      for (int ll = 0; ll < cnt; ll += 2) v = add(v, sm[a + ll]);
+      for (int ll = 1; ll < cnt; ll += 2) v = sub(v, sm[a + ll]);
+    } else if (kind == 2) {
+      v = sm[__ldg(op.inv_a + l)];
+    }
+  }
+  sync();
+  return v;
+}
+__device__ __forceinline__ void rot(double &gn, double &gt, double gx, double gy, double dnx,
+                                    double dny) {
+  gn = add(mul(gx, dnx), mul(gy, dny));
+  gt = sub(mul(gx, dny), mul(gy, dnx));
+}
+
+template <int VAR>
+__device__ __forceinline__ void pair_solve(const DevOps &op, const DevMesh &m, int e, double &gx,
+                                           double &gy, double *sm) {
+  if (__ldg(m.bdl + e)) {
+    if (VAR == kNS) {
+      double bu = reduc_gn(op, gx, sm), bv = reduc_gn(op, gy, sm);
+      bu = solve_red(op, bu);
+      bv = solve_red(op, bv);
+      gx = reduc_inv_gn(op, bu, sm);
+      gy = reduc_inv_gn(op, bv, sm);
+    } else {
+      const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+      double gn, gt;
+      rot(gn, gt, gx, gy, dnx, dny);
+      double bu = reduc_gn(op, gn, sm);
+      bu = solve_red(op, bu);
+      gt = solve_full(op, gt);
+      gn = reduc_inv_gn(op, bu, sm);
+      rot(gx, gy, gn, gt, dnx, dny);
+    }
+  } else {
+    gx = solve_full(op, gx);
+    gy = solve_full(op, gy);
+  }
+}
+
+// ans_i = sum_j A(i,j) x_j through AN[j*nm + i] = A(i,j); x in shared memory
+__device__ __forceinline__ double matvecN(const double *AN, const double *x, int nm) {
+  const int l = lane();
+  double s = 0.0;
+  if (l < nm)
+    for (int j = 0; j < nm; ++j) s = fmac(s, __ldg(AN + j * nm + l), x[j]);
+  return s;
+}
+
+// the three side lifts' adjoints (as side_lift_adj)
+__device__ __forceinline__ void side_lift_adj(const DevOps &op, const DevMesh &m, int e,
+                                              const double *g, double coeff, double *L) {
+  const int l = lane(), G = op.ngf, nm = op.nm;
+  if (l < 3 * G) {
+    const int k = l / G, j = l - k * G;
+    const int isg = __ldg(m.its + 3 * e + k);
+    const int j1 = isg > 0 ? j : G - 1 - j;
+    const double sig = isg * coeff * 0.5;
+    const double *p = op.picoF + (size_t)k * nm * G + j1;
+    double s = 0.0;
+    for (int n = 0; n < nm; ++n) s = fmac(s, __ldg(p + n * G), g[n]);
+    L[(3 * (size_t)e + k) * G + j] = sig * __ldg(op.wif + j) * s;
+  }
+}
+
+// face sums of the side-lift adjoints (as face_sums)
+__device__ __forceinline__ void face_sums(const DevOps &op, const DevMesh &m, int e,
+                                          const double *L, double *S) {
+  const int l = lane(), G = op.ngf;
+  if (l < 3 * G) {
+    const int k = l / G, j = l - k * G;
+    const int f = __ldg(m.itm + 3 * e + k);
+    const int t1 = __ldg(m.tseg + 2 * f), t2 = __ldg(m.tseg + 2 * f + 1);
+    double s = L[(3 * (size_t)e + k) * G + j];
+    if (t2 >= 0) {
+      const int nb = (t1 == e) ? t2 : t1;
+      const int kn = (t1 == e) ? __ldg(m.ssit + 2 * f + 1) : __ldg(m.ssit + 2 * f);
+      s += L[(3 * (size_t)nb + kn) * G + j];
+    }
+    S[l] = s;
+  }
+}
+
+// transposed cal_flu (as trace_adj)
+__device__ __forceinline__ double trace_adj(const DevOps &op, const DevMesh &m, int e,
+                                            const double *S, int comp, double scale) {
+  const int l = lane(), G = op.ngf, nm = op.nm;
+  double a = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    const int f = __ldg(m.itm + 3 * e + k);
+    const int t1 = __ldg(m.tseg + 2 * f), t2 = __ldg(m.tseg + 2 * f + 1);
+    const double w = (t2 < 0 ? 1.0 : 0.5) * __ldg(m.norm + 2 * f + comp) * scale;
+    const bool first = (t1 == e);
+    const double *pk = op.picoT + (size_t)k * G * nm;
+    for (int j = 0; j < G; ++j) {
+      const int je = first ? j : G - 1 - j;
+      const double c = w * S[k * G + j];
+      if (l < nm) a = fmac(a, __ldg(pk + (size_t)je * nm + l), c);
+    }
+  }
+  return a;
+}
+
+__device__ __forceinline__ double lin(double c1, double a, double c2, double b) {
+  return fmac(c1 * a, c2, b);
+}
+
+}  // namespace t16
+
+constexpr int kT16 = 256;              // threads per block of the 16-lane-tile kernels
+constexpr int kS16 = kT16 / t16::W;    // element slots per block
+constexpr int kT16N = 128;             // the quadrature-point kernel (static scratch <= 48 KB)
+constexpr int kS16N = kT16N / t16::W;
+
+template <int VAR, class D>
+__global__ void __launch_bounds__(kT16, 3) k16_adj_tend_a(DevOps op_in, DevMesh m, AdjTendArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
+  __shared__ double sg[kS16][3][t16::W];
+  __shared__ double smw[kS16][t16::W];
+  double(*S)[t16::W] = sg[t16::bslot()];
+  double *sm = smw[t16::bslot()];
+  const int nm = op.nm, ne = m.ne;
+  const size_t fs = (size_t)ne * nm;
+  for (int e = t16::gslot(); e < ne; e += t16::nslot()) {
+    const size_t o = (size_t)e * nm;
+    const Geo g = geo(m, e);
+    double gx = t16::load(a.bu + o, nm), gy = t16::load(a.bv + o, nm), b = t16::load(a.bh + o, nm);
+    t16::pair_solve<VAR>(op, m, e, gx, gy, sm);
+    b = t16::solve_full(op, b);
+    t16::store(a.gx0b + o, gx, nm);
+    t16::store(a.gy0b + o, gy, nm);
+    t16::store(S[0], gx, nm);
+    t16::store(S[1], gy, nm);
+    t16::store(S[2], b, nm);
+    t16::sync();
+    const double axg = t16::matvecN(op.agxN, S[0], nm), ayg = t16::matvecN(op.agyN, S[0], nm);
+    const double bxg = t16::matvecN(op.agxN, S[1], nm), byg = t16::matvecN(op.agyN, S[1], nm);
+    const double ah = t16::matvecN(op.agxN, S[2], nm), bh = t16::matvecN(op.agyN, S[2], nm);
+    const double cby = g.by * g.detai, cay = g.ay * g.detai, cbx = g.bx * g.detai, cax = g.ax * g.detai;
+    t16::store(a.fb + o, t16::lin(-cby, axg, cay, ayg), nm);
+    t16::store(a.fb + fs + o, t16::lin(cbx, axg, -cax, ayg), nm);
+    t16::store(a.fb + 2 * fs + o, t16::lin(-cby, bxg, cay, byg), nm);
+    t16::store(a.fb + 3 * fs + o, t16::lin(cbx, bxg, -cax, byg), nm);
+    t16::store(a.uhb + o, t16::lin(cby, ah, -cay, bh), nm);
+    t16::store(a.vhb + o, t16::lin(-cbx, ah, cax, bh), nm);
+    t16::side_lift_adj(op, m, e, S[0], g.detai, a.lx);
+    t16::side_lift_adj(op, m, e, S[1], g.detai, a.ly);
+    t16::side_lift_adj(op, m, e, S[2], -g.detai, a.lh);
+    t16::sync();
+  }
+}
+
+template <class D>
+__global__ void __launch_bounds__(kT16) k16_adj_tend_b(DevOps op_in, DevMesh m, AdjTendArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
+  __shared__ double sall[kS16][3][t16::W];
+  double(*S)[t16::W] = sall[t16::bslot()];
+  const int nm = op.nm, ne = m.ne;
+  const size_t fs = (size_t)ne * nm;
+  for (int e = t16::gslot(); e < ne; e += t16::nslot()) {
+    const size_t o = (size_t)e * nm;
+    t16::face_sums(op, m, e, a.lx, S[0]);
+    t16::face_sums(op, m, e, a.ly, S[1]);
+    t16::face_sums(op, m, e, a.lh, S[2]);
+    t16::sync();
+    t16::store(a.fb + o, t16::load(a.fb + o, nm) + t16::trace_adj(op, m, e, S[0], 0, 1.0), nm);
+    t16::store(a.fb + fs + o, t16::load(a.fb + fs + o, nm) + t16::trace_adj(op, m, e, S[0], 1, 1.0), nm);
+    t16::store(a.fb + 2 * fs + o, t16::load(a.fb + 2 * fs + o, nm) + t16::trace_adj(op, m, e, S[1], 0, 1.0), nm);
+    t16::store(a.fb + 3 * fs + o, t16::load(a.fb + 3 * fs + o, nm) + t16::trace_adj(op, m, e, S[1], 1, 1.0), nm);
+    t16::store(a.uhb + o, t16::load(a.uhb + o, nm) + t16::trace_adj(op, m, e, S[2], 0, 1.0), nm);
+    t16::store(a.vhb + o, t16::load(a.vhb + o, nm) + t16::trace_adj(op, m, e, S[2], 1, 1.0), nm);
+    t16::sync();
+  }
+}
+
+template <class D>
+struct Na16 {
+  static constexpr int M = (D::NC + 1) * (D::NC + 2) / 2, Q = D::NG;
+  double vin[9][M];
+  double xb[8][M];
+  double qb[9][Q];
+  double sm[t16::W];
+};
+
+template <int VAR, class D>
+__global__ void __launch_bounds__(kT16N, 4) k16_nlvol_adj(DevOps op_in, DevMesh m, AdjNlArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
+  __shared__ Na16<D> sall[kS16N];
+  Na16<D> &S = sall[t16::bslot()];
+  const int nm = op.nm, ng = op.ng, ne = m.ne, l = t16::lane();
+  const size_t fs = (size_t)ne * nm;
+  for (int e = t16::gslot(); e < ne; e += t16::nslot()) {
+    const size_t o = (size_t)e * nm;
+    const double uk = t16::load(a.su + o, nm), vk = t16::load(a.sv + o, nm), hh = t16::load(a.sh + o, nm);
+    const double hb = t16::load(a.hb + o, nm), w0 = t16::load(a.w0 + o, nm), z0 = t16::load(a.z0 + o, nm);
+    const double fc = t16::load(a.fc + o, nm);
+    const double q0 = t16::load(a.q + o, nm), q1 = t16::load(a.q + fs + o, nm);
+    const double q2 = t16::load(a.q + 2 * fs + o, nm), q3 = t16::load(a.q + 3 * fs + o, nm);
+    const double f0 = t16::load(a.fb + o, nm), f1 = t16::load(a.fb + fs + o, nm);
+    const double f2 = t16::load(a.fb + 2 * fs + o, nm), f3 = t16::load(a.fb + 3 * fs + o, nm);
+    const double gx0 = t16::load(a.gx0b + o, nm), gy0 = t16::load(a.gy0b + o, nm);
+    double uhb = t16::load(a.uhb + o, nm), vhb = t16::load(a.vhb + o, nm);
+    t16::store(S.vin[0], uk, nm);
+    t16::store(S.vin[1], vk, nm);
+    t16::store(S.vin[2], q0, nm);
+    t16::store(S.vin[3], q1 - fc, nm);
+    t16::store(S.vin[4], q2 + fc, nm);
+    t16::store(S.vin[5], q3, nm);
+    t16::store(S.vin[6], hh + hb, nm);
+    t16::store(S.vin[7], w0 - a.mb0 * uk, nm);
+    t16::store(S.vin[8], z0 - a.mb0 * vk, nm);
+    t16::pair_solve<VAR>(op, m, e, uhb, vhb, S.sm);
+    t16::store(S.xb[0], -gx0, nm);
+    t16::store(S.xb[1], -gx0, nm);
+    t16::store(S.xb[2], -gy0, nm);
+    t16::store(S.xb[3], -gy0, nm);
+    t16::store(S.xb[4], uhb, nm);
+    t16::store(S.xb[5], vhb, nm);
+    t16::store(S.xb[6], gx0, nm);
+    t16::store(S.xb[7], gy0, nm);
+    t16::sync();
+    for (int qp = l; qp < ng; qp += t16::W) {
+      double b[9], pb[8];
+#pragma unroll
+      for (int f = 0; f < 9; ++f) b[f] = 0.0;
+#pragma unroll
+      for (int f = 0; f < 8; ++f) pb[f] = 0.0;
+      for (int n = 0; n < nm; ++n) {
+        const double p = __ldg(op.p2 + (size_t)n * ng + qp);
+#pragma unroll
+        for (int f = 0; f < 9; ++f) b[f] = fmac(b[f], S.vin[f][n], p);
+#pragma unroll
+        for (int f = 0; f < 8; ++f) pb[f] = fmac(pb[f], S.xb[f][n], p);
+      }
+      const double w = __ldg(op.wi + qp), ih = 1.0 / b[6];
+#pragma unroll
+      for (int f = 0; f < 8; ++f) pb[f] *= w;
+      S.qb[0][qp] = pb[0] * b[2] + pb[2] * b[4] + pb[4] * b[6];
+      S.qb[1][qp] = pb[1] * b[3] + pb[3] * b[5] + pb[5] * b[6];
+      S.qb[2][qp] = pb[0] * b[0];
+      S.qb[3][qp] = pb[1] * b[1];
+      S.qb[4][qp] = pb[2] * b[0];
+      S.qb[5][qp] = pb[3] * b[1];
+      S.qb[6][qp] = pb[4] * b[0] + pb[5] * b[1] - (pb[6] * b[7] + pb[7] * b[8]) * ih * ih;
+      S.qb[7][qp] = pb[6] * ih;
+      S.qb[8][qp] = pb[7] * ih;
+    }
+    t16::sync();
+    double M[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) M[f] = 0.0;
+    if (l < nm)
+      for (int qp = 0; qp < ng; ++qp) {
+        const double p = __ldg(op.p2t + (size_t)qp * nm + l);
+#pragma unroll
+        for (int f = 0; f < 9; ++f) M[f] = fmac(M[f], S.qb[f][qp], p);
+      }
+    const double mu0 = a.mu0, g0 = a.g0, mb0 = a.mb0;
+    t16::store(a.ub + o, M[0] - mb0 * M[7], nm);
+    t16::store(a.vb + o, M[1] - mb0 * M[8], nm);
+    t16::store(a.hbo + o, M[6] - g0 * (f0 + f3), nm);
+    t16::store(a.qb + o, M[2] + mu0 * f0, nm);
+    t16::store(a.qb + fs + o, M[3] + mu0 * f1, nm);
+    t16::store(a.qb + 2 * fs + o, M[4] + mu0 * f2, nm);
+    t16::store(a.qb + 3 * fs + o, M[5] + mu0 * f3, nm);
+    t16::sync();
+  }
+}
+
+template <int VAR, class D>
+__global__ void __launch_bounds__(kT16, 3) k16_adj_qphase_a(DevOps op_in, DevMesh m, AdjQArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
+  __shared__ double sall[kS16][5][t16::W];
+  double(*S)[t16::W] = sall[t16::bslot()];
+  const int nm = op.nm, ne = m.ne;
+  const size_t fs = (size_t)ne * nm;
+  for (int e = t16::gslot(); e < ne; e += t16::nslot()) {
+    const size_t o = (size_t)e * nm;
+    const Geo g = geo(m, e);
+    double gxx = t16::load(a.qb + o, nm), gxy = t16::load(a.qb + fs + o, nm);
+    double gyx = t16::load(a.qb + 2 * fs + o, nm), gyy = t16::load(a.qb + 3 * fs + o, nm);
+    if (VAR == kFS && __ldg(m.bdl + e)) {
+      // calvarnl_fs.f:171-204, symmetric
+      const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+      double gnx, gtx, gny, gty, gnn, gnt, gtn, gtt;
+      t16::rot(gnx, gtx, gxx, gyx, dnx, dny);
+      t16::rot(gny, gty, gxy, gyy, dnx, dny);
+      t16::rot(gnn, gnt, gnx, gny, dnx, dny);
+      t16::rot(gtn, gtt, gtx, gty, dnx, dny);
+      double bu = t16::reduc_gn(op, gtn, S[4]);
+      gnn = t16::solve_full(op, gnn);
+      gnt = t16::solve_full(op, gnt);
+      bu = t16::solve_red(op, bu);
+      gtt = t16::solve_full(op, gtt);
+      gtn = t16::reduc_inv_gn(op, bu, S[4]);
+      t16::rot(gnx, gny, gnn, gnt, dnx, dny);
+      t16::rot(gtx, gty, gtn, gtt, dnx, dny);
+      t16::rot(gxx, gyx, gnx, gtx, dnx, dny);
+      t16::rot(gxy, gyy, gny, gty, dnx, dny);
+    } else {
+      gxx = t16::solve_full(op, gxx);
+      gxy = t16::solve_full(op, gxy);
+      gyx = t16::solve_full(op, gyx);
+      gyy = t16::solve_full(op, gyy);
+    }
+    const double d = g.detai;
+    t16::store(S[0], t16::lin(d * g.by, gxx, -d * g.bx, gxy), nm);
+    t16::store(S[1], t16::lin(-d * g.ay, gxx, d * g.ax, gxy), nm);
+    t16::store(S[2], t16::lin(d * g.by, gyx, -d * g.bx, gyy), nm);
+    t16::store(S[3], t16::lin(-d * g.ay, gyx, d * g.ax, gyy), nm);
+    t16::sync();
+    const double uvol = -(t16::matvecN(op.agxN, S[0], nm) + t16::matvecN(op.agyN, S[1], nm));
+    const double vvol = -(t16::matvecN(op.agxN, S[2], nm) + t16::matvecN(op.agyN, S[3], nm));
+    t16::store(a.ub + o, t16::load(a.ub + o, nm) + uvol, nm);
+    t16::store(a.vb + o, t16::load(a.vb + o, nm) + vvol, nm);
+    t16::sync();
+    t16::store(S[0], gxx, nm);
+    t16::store(S[1], gxy, nm);
+    t16::store(S[2], gyx, nm);
+    t16::store(S[3], gyy, nm);
+    t16::sync();
+    for (int c = 0; c < 4; ++c)
+      t16::side_lift_adj(op, m, e, S[c], d, a.lq + (size_t)c * ne * 3 * op.ngf);
+    t16::sync();
+  }
+}
+
+template <class D>
+__global__ void __launch_bounds__(kT16) k16_adj_qphase_b(DevOps op_in, DevMesh m, AdjQArgs a) {
+  const DevOps op = fixed_dims<D>(op_in);
+  __shared__ double sall[kS16][4][t16::W];
+  double(*S)[t16::W] = sall[t16::bslot()];
+  const int nm = op.nm, ne = m.ne;
+  const size_t ls = (size_t)ne * 3 * op.ngf;
+  for (int e = t16::gslot(); e < ne; e += t16::nslot()) {
+    const size_t o = (size_t)e * nm;
+    for (int c = 0; c < 4; ++c) t16::face_sums(op, m, e, a.lq + c * ls, S[c]);
+    t16::sync();
+    const double ut = t16::trace_adj(op, m, e, S[0], 0, 1.0) + t16::trace_adj(op, m, e, S[1], 1, 1.0);
+    const double vt = t16::trace_adj(op, m, e, S[2], 0, 1.0) + t16::trace_adj(op, m, e, S[3], 1, 1.0);
+    t16::store(a.ub + o, t16::load(a.ub + o, nm) + ut, nm);
+    t16::store(a.vb + o, t16::load(a.vb + o, nm) + vt, nm);
+    t16::sync();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // adjoint of the linear variant (calvar_lin.f:7-287)
 // ---------------------------------------------------------------------------
 template <class D = RtDims>
@@ -693,8 +1112,35 @@ cudaError_t launch_nlvol_tlm(int variant, const DevOps &op, const DevMesh &m, co
 
 namespace {
 template <class D>
+constexpr bool tile16() {
+  return D::NC > 0 && (D::NC + 1) * (D::NC + 2) / 2 <= t16::W && 3 * D::NGF <= t16::W;
+}
+
+template <class D, int VAR>
+void adj_nl16(const DevOps &op, const DevMesh &m, const AdjTendArgs &ta, const AdjNlArgs &na,
+              const AdjQArgs &qa, cudaStream_t st, int sms) {
+  int g = (m.ne + kS16 - 1) / kS16;
+  if (g > sms * 8) g = sms * 8;
+  int gn = (m.ne + kS16N - 1) / kS16N;
+  if (gn > sms * 16) gn = sms * 16;
+  k16_adj_tend_a<VAR, D><<<g, kT16, 0, st>>>(op, m, ta);
+  k16_adj_tend_b<D><<<g, kT16, 0, st>>>(op, m, ta);
+  k16_nlvol_adj<VAR, D><<<gn, kT16N, 0, st>>>(op, m, na);
+  k16_adj_qphase_a<VAR, D><<<g, kT16, 0, st>>>(op, m, qa);
+  k16_adj_qphase_b<D><<<g, kT16, 0, st>>>(op, m, qa);
+}
+
+template <class D>
 void adj_nl_kernels(int variant, const DevOps &op, const DevMesh &m, const AdjTendArgs &ta,
-                    const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int g8, int g2) {
+                    const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int g8, int g2,
+                    int sms) {
+  if constexpr (tile16<D>()) {
+    switch (variant) {
+      case kFS: adj_nl16<D, kFS>(op, m, ta, na, qa, st, sms); return;
+      case kNS: adj_nl16<D, kNS>(op, m, ta, na, qa, st, sms); return;
+      default: adj_nl16<D, kINV>(op, m, ta, na, qa, st, sms); return;
+    }
+  }
   switch (variant) {
     case kFS:
       k_adj_tend_a<kFS, D><<<g8, kT, 0, st>>>(op, m, ta);
@@ -739,8 +1185,8 @@ cudaError_t launch_adj_nl(int variant, const DevOps &op, const DevMesh &m, const
                           const AdjNlArgs &na, const AdjQArgs &qa, cudaStream_t st, int sms) {
   // k_nlvol_adj: 2-warp blocks, up to 12 resident per SM
   const int g8 = grid_for(m.ne, sms, kWB), g2 = std::min((m.ne + 1) / 2, sms * 24);
-  if (!with_fixed(op, [&](auto d) { adj_nl_kernels<decltype(d)>(variant, op, m, ta, na, qa, st, g8, g2); }))
-    adj_nl_kernels<RtDims>(variant, op, m, ta, na, qa, st, g8, g2);
+  if (!with_fixed(op, [&](auto d) { adj_nl_kernels<decltype(d)>(variant, op, m, ta, na, qa, st, g8, g2, sms); }))
+    adj_nl_kernels<RtDims>(variant, op, m, ta, na, qa, st, g8, g2, sms);
   return cudaGetLastError();
 }
 

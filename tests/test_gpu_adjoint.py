@@ -16,6 +16,12 @@ from spoc_b200 import workloads as W
 NAMES = ["c4_ns_p4", "c2_fs_p6", "c3_inv_p7", "c1_lin_p3"]
 
 
+def variant_at(name, variant, n=6):
+    """Configuration `name` with another physics variant (same degree and tables)."""
+    import dataclasses
+    return W.build_problem(dataclasses.replace(W.small(W.CONFIGS[name], n), variant=variant))
+
+
 def dot(a, b):
     return sum(float(np.sum(x * y)) for x, y in zip(a, b))
 
@@ -30,6 +36,25 @@ def test_rhs_dot_product(name):
     p = W.build_problem(W.small(W.CONFIGS[name], 6))
     s = W.make_solver(p)
     rng = np.random.default_rng(21)
+    x = (p.u, p.v, p.h)
+    d = rand_like(rng, x)
+    lam = rand_like(rng, x)
+    jd = s.tlm_rhs(x, d)
+    jtl = s.adj_rhs(x, lam)
+    lhs, rhs = dot(jd, lam), dot(d, jtl)
+    scale = sum(float(np.sum(np.abs(a * b))) for a, b in zip(jd, lam))
+    assert abs(lhs - rhs) <= 1e-11 * scale, (lhs, rhs, scale)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c4_ns_p4", "c1_lin_p3"])
+@pytest.mark.parametrize("variant", ["fs", "ns", "inv"])
+def test_rhs_dot_product_low_degrees(name, variant):
+    """Degrees 3 and 4 run the two-elements-per-warp adjoint kernels: every
+    nonlinear variant, wall elements included."""
+    p = variant_at(name, variant)
+    s = W.make_solver(p)
+    rng = np.random.default_rng(22)
     x = (p.u, p.v, p.h)
     d = rand_like(rng, x)
     lam = rand_like(rng, x)
