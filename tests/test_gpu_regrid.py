@@ -194,3 +194,27 @@ def test_compare_standing_wave(gpu_lib):
     assert got == ref
     assert got["inside"] == 40 * 40 and got["outside"] == 0
     assert got["rms_norm"][2] < 1e-3 * hc and got["rms_norm"][1] == 0.0
+
+
+@pytest.mark.gpu
+def test_interpol_dev_rejects_bad_ids(gpu_lib):
+    """Device point tables are not validated on the host: ids outside the
+    source mesh are skipped by the kernel (never read) and the call returns
+    SPOC_E_ARG; the handle stays usable."""
+    import torch
+    p, OT, OM = setup("c2_fs_p6")
+    s = stepped(p)
+    d = W.make_solver(p)
+    ne, ng = p.mesh.ne, p.T.ng
+    tinter = np.zeros(ne, np.int32)
+    tinter[0] = ne + 5                                   # out of range
+    pel = np.full((ne, ng), 1, np.int32)
+    pel[1, 3] = -2                                       # out of range
+    xy = np.full((ne, ng), -0.5)
+    dev = [torch.from_numpy(a).cuda() for a in (tinter, pel, xy, xy.copy())]
+    with pytest.raises(api.SpocError) as ei:
+        d.interpol_from_dev(s, *[t.data_ptr() for t in dev])
+    assert ei.value.code == 1  # SPOC_E_ARG
+    d.interpol_from(s, np.arange(1, ne + 1, dtype=np.int32))
+    for g, a in zip(d.get_state(), s.get_state()):
+        assert np.array_equal(g, a)
