@@ -356,8 +356,20 @@ def cpu_baseline(cfg, p):
         sec = time.perf_counter() - t0
         if sec > 10.0 or k >= 50:
             break
+    # the serial reference: one core, at least one step, about 6 s
+    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    k1, t0 = 0, time.perf_counter()
+    while True:
+        O.rk4(cfg.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, cfg.mu0, cfg.mb0, cfg.g0,
+              p.dt, 1, 1)
+        k1 += 1
+        sec1 = time.perf_counter() - t0
+        if sec1 > 6.0 or k1 >= 20:
+            break
     return {"value": 3.0 * T.nm * p.mesh.ne * k / sec, "unit": UNIT, "cores": threads,
-            "kind": "port", "sample": f"{k} full RK4 steps of the workload, OpenMP over elements"}
+            "kind": "port", "sample": f"{k} full RK4 steps of the workload, OpenMP over elements",
+            "serial": {"value": 3.0 * T.nm * p.mesh.ne * k1 / sec1, "unit": UNIT, "cores": 1,
+                       "sample": f"{k1} full RK4 steps of the workload on one core"}}
 
 
 def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
