@@ -61,7 +61,7 @@ __host__ __device__ constexpr int col_off(int k) { return k * (k + 1) / 2; }
 
 // Operators of the q-phase, tendency and linear kernels.
 template <class Dm>
-struct SOps {
+struct __align__(16) SOps {
   double agx[Dm::N * Dm::N];      // [j*N + i] = agx(j,i)
   double agy[Dm::N * Dm::N];
   double pf[3 * Dm::N * Dm::G];   // [(s*N + n)*G + j] = pico(j,n,s)
@@ -80,7 +80,7 @@ struct SOps {
 
 // Operators of the quadrature-point kernel.
 template <class Dm>
-struct SOpsQ {
+struct __align__(16) SOpsQ {
   double p2[Dm::N * Dm::Q];       // [n*Q + q] = pi2(q,n)
   double p2t[Dm::Q * Dm::N];      // [q*N + n] = pi2(q,n)
   double wi[Dm::Q];
@@ -263,18 +263,31 @@ __device__ __forceinline__ void face_values(const double *pf, const DevMesh &m, 
       const int s1 = __ldg(m.ssit + 2 * f), s2 = __ldg(m.ssit + 2 * f + 1);
       const double *p1 = pf + s1 * N * G + j;
       const double *p2 = pf + s2 * N * G + (G - 1 - j);
+      // the chain over side 1's modes, then side 2's; with an even mode count
+      // the coefficients come in 16-byte pairs (same operations, same order)
+      auto chain = [&](const double *a, const double *p) {
+        if constexpr (N % 2 == 0) {
 #pragma unroll
-      for (int n = 0; n < N; ++n) {
-        const double pv = p1[n * G];
+          for (int n = 0; n < N; n += 2) {
+            const double pv0 = p[n * G], pv1 = p[(n + 1) * G];
 #pragma unroll
-        for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], a1[q * N + n], pv);
-      }
+            for (int q = 0; q < NF; ++q) {
+              const double2 c = *reinterpret_cast<const double2 *>(a + q * N + n);
+              acc[q] = macc(acc[q], c.x, pv0);
+              acc[q] = macc(acc[q], c.y, pv1);
+            }
+          }
+        } else {
 #pragma unroll
-      for (int n = 0; n < N; ++n) {
-        const double pv = p2[n * G];
+          for (int n = 0; n < N; ++n) {
+            const double pv = p[n * G];
 #pragma unroll
-        for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], a2[q * N + n], pv);
-      }
+            for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], a[q * N + n], pv);
+          }
+        }
+      };
+      chain(a1, p1);
+      chain(a2, p2);
 #pragma unroll
       for (int q = 0; q < NF; ++q) acc[q] = mul(0.5, acc[q]);
     }
@@ -293,8 +306,7 @@ __device__ __forceinline__ void matvec2(const double *A, const double *B, const 
   for (int f = 0; f < NF; ++f)
 #pragma unroll
     for (int r = 0; r < R; ++r) ax[f][r] = bx[f][r] = 0.0;
-#pragma unroll
-  for (int j = 0; j < N; ++j) {
+  auto step = [&](int j, const double (&xv)[NF]) {
     double a[R], b[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -303,13 +315,35 @@ __device__ __forceinline__ void matvec2(const double *A, const double *B, const 
       b[r] = (i < N) ? B[j * N + i] : 0.0;
     }
 #pragma unroll
-    for (int f = 0; f < NF; ++f) {
-      const double x = X[f * XS + j];
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        ax[f][r] = macc(ax[f][r], a[r], x);
-        bx[f][r] = macc(bx[f][r], b[r], x);
+        ax[f][r] = macc(ax[f][r], a[r], xv[f]);
+        bx[f][r] = macc(bx[f][r], b[r], xv[f]);
       }
+  };
+  // with an even mode count (XS == N, 16-byte aligned vectors) the inputs
+  // come in 16-byte pairs; the operations and their order are unchanged
+  if constexpr (N % 2 == 0) {
+#pragma unroll
+    for (int j = 0; j < N; j += 2) {
+      double x0[NF], x1[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const double2 c = *reinterpret_cast<const double2 *>(X + f * XS + j);
+        x0[f] = c.x;
+        x1[f] = c.y;
+      }
+      step(j, x0);
+      step(j + 1, x1);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      double x0[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) x0[f] = X[f * XS + j];
+      step(j, x0);
     }
   }
 }
@@ -552,7 +586,7 @@ __device__ __forceinline__ void stage_update(const StageArgs &sa, int fld, int e
 // q-phase (calvarnl_fs.f:88-226)
 // ---------------------------------------------------------------------------
 template <class Dm>
-struct QWarp {
+struct __align__(16) QWarp {
   double own[2 * Dm::N];
   double nb[3 * 2 * Dm::N];
   double fr[2 * 32];
@@ -634,7 +668,7 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
 // nonlinear terms at quadrature points (calvarnl_fs.f:243-348)
 // ---------------------------------------------------------------------------
 template <class Dm>
-struct BWarp {
+struct __align__(16) BWarp {
   static constexpr int T = Dm::Q > 32 ? Dm::Q - 32 : 1;  // quadrature points past lane 31
   double vin[9 * Dm::N];
   double wp[8 * Dm::Q];
@@ -800,7 +834,7 @@ __global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) 
 // tendencies and the RK4 stage update (calvarnl_fs.f:350-544)
 // ---------------------------------------------------------------------------
 template <class Dm>
-struct TWarp {
+struct __align__(16) TWarp {
   double own[6 * Dm::N];       // fxx, fxy, fyx, fyy, uh, vh
   double nb[3 * 6 * Dm::N];
   double fb[6 * 32];           // face values, then fbdxx, fbdxy, fbdyx, fbdyy, fbdx, fbdy
@@ -906,7 +940,7 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
 // linear variant (calvar_lin.f:7-287)
 // ---------------------------------------------------------------------------
 template <class Dm>
-struct LWarp {
+struct __align__(16) LWarp {
   double own[3 * Dm::N];  // fxx = -g0 h, u, v
   double nb[3 * 3 * Dm::N];
   double xs[2 * Dm::N];   // u*hh0, v*hh0
