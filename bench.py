@@ -222,7 +222,8 @@ def ensemble_measure(torch, stream, W, api, replicas, rank=0, world=1, count=64,
         "autotuner": {"best": tune["best"], "tried": tune["tried"],
                       "blocks": info["blocks"],
                       "elements_per_block": {"min": float((ne / mb).min()), "max": float((ne / mb).max())},
-                      "warps_per_block": 8, "elements_per_warp_pass": 1},
+                      "warps_per_block": 8,
+                      "elements_per_warp": {"degree 3-4": 2, "degree 5-6": 1}},
         "eta_rel_l2_error_vs_fp64": {"max": float(max(errs)), "median": float(np.median(errs)),
                                      "members": [float(e) for e in errs]},
         "host_setup_s": build_s,

@@ -49,13 +49,19 @@ using namespace mx;
 
 namespace {
 
+// The lanes of this thread's element (all 32, or its half of the warp).
+template <class Dm>
+__device__ __forceinline__ unsigned lane_mask() {
+  return Dm::LW == 32 ? 0xffffffffu : (0xffffu << (threadIdx.x & 16));
+}
+
 // Trace record (mean-free traces, then the mean) of up to six fields held in
 // the warp's shared vectors x[f] (psi coefficients); written by lanes 0..TG.
 template <class Dm, int NF>
 __device__ __forceinline__ void write_traces(const float *o, const float *const (&x)[NF], float *out,
                                              size_t stride, int e) {
   constexpr int N = Dm::N, TG = Dm::TG, TS = Dm::TS;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (Dm::LW - 1);
   if (lane > TG) return;
   float t[NF];
   if (lane < TG) {
@@ -78,14 +84,14 @@ __device__ __forceinline__ void write_traces(const float *o, const float *const 
 }
 
 // Orthogonal projection of the warp's vector x (shared, length N) onto the
-// wall-compatible subspace; lanes receive rows i = lane + 32 r.
+// wall-compatible subspace; lanes receive rows i = lane + LW r (LW = lanes per element).
 template <class Dm>
 __device__ __forceinline__ void project_rows(const float *o, const float *x, float (&out)[Dm::R]) {
   constexpr int N = Dm::N;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (Dm::LW - 1);
 #pragma unroll
   for (int r = 0; r < Dm::R; ++r) {
-    const int i = lane + 32 * r;
+    const int i = lane + Dm::LW * r;
     float a = 0.f;
     if (i < N) {
 #pragma unroll 4
@@ -103,21 +109,21 @@ template <class Dm, bool NOSLIP>
 __device__ void wall_vec(const float *o, float *tmp, float (&gx)[Dm::R], float (&gy)[Dm::R],
                          float nx, float ny) {
   constexpr int N = Dm::N;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (Dm::LW - 1);
   if (NOSLIP) {
     float px[Dm::R], py[Dm::R];
 #pragma unroll
     for (int r = 0; r < Dm::R; ++r)
-      if (lane + 32 * r < N) tmp[lane + 32 * r] = gx[r];
-    __syncwarp();
+      if (lane + Dm::LW * r < N) tmp[lane + Dm::LW * r] = gx[r];
+    __syncwarp(lane_mask<Dm>());
     project_rows<Dm>(o, tmp, px);
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
 #pragma unroll
     for (int r = 0; r < Dm::R; ++r)
-      if (lane + 32 * r < N) tmp[lane + 32 * r] = gy[r];
-    __syncwarp();
+      if (lane + Dm::LW * r < N) tmp[lane + Dm::LW * r] = gy[r];
+    __syncwarp(lane_mask<Dm>());
     project_rows<Dm>(o, tmp, py);
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
 #pragma unroll
     for (int r = 0; r < Dm::R; ++r) {
       gx[r] = px[r];
@@ -128,11 +134,11 @@ __device__ void wall_vec(const float *o, float *tmp, float (&gx)[Dm::R], float (
 #pragma unroll
     for (int r = 0; r < Dm::R; ++r) {
       gn[r] = nx * gx[r] + ny * gy[r];
-      if (lane + 32 * r < N) tmp[lane + 32 * r] = gn[r];
+      if (lane + Dm::LW * r < N) tmp[lane + Dm::LW * r] = gn[r];
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
     project_rows<Dm>(o, tmp, pg);
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
 #pragma unroll
     for (int r = 0; r < Dm::R; ++r) {
       const float d = pg[r] - gn[r];
@@ -165,14 +171,14 @@ template <class Dm>
 __device__ void finish_element(const MxArgs &a, const float *o, float *w, int e,
                                float (&t)[3][Dm::R]) {
   constexpr int N = Dm::N;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (Dm::LW - 1);
   const size_t fn = (size_t)a.ne * N;
   bool bad = false;
 #pragma unroll
   for (int f = 0; f < 3; ++f)
 #pragma unroll
     for (int r = 0; r < Dm::R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       if (i >= N) continue;
       const float d = t[f][r];
       bad |= !isfinite(d);
@@ -186,12 +192,12 @@ __device__ void finish_element(const MxArgs &a, const float *o, float *w, int e,
         w[f * N + i] = y32;
       }
     }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flag, 1);
+  if (__any_sync(lane_mask<Dm>(), bad) && lane == 0) atomicOr(a.flag, 1);
   if (a.stage < 0) return;
-  __syncwarp();
+  __syncwarp(lane_mask<Dm>());
   const float *const x[3] = {w, w + N, w + 2 * N};
   write_traces<Dm, 3>(o, x, a.tr_out, (size_t)a.ne * Dm::TS, e);
-  __syncwarp();
+  __syncwarp(lane_mask<Dm>());
 }
 
 // ---------------------------------------------------------------------------
@@ -203,18 +209,18 @@ template <class Dm, int VAR>
 __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, int nblk) {
   constexpr int N = Dm::N, Q = Dm::Q, G = Dm::G, TG = Dm::TG, R = Dm::R;
   float *o = sm;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & (Dm::LW - 1), wib = threadIdx.x / Dm::LW;
   float *w = sm + Dm::NOPS + wib * Dm::WS;
   float *su = w + Dm::S_U, *sv = w + Dm::S_V, *sh = w + Dm::S_H, *sq = w + Dm::S_Q;
   float *vec = w + Dm::S_VEC, *suh = w + Dm::S_UH, *svh = w + Dm::S_VH, *tmp = w + Dm::S_TMP;
   float *gl = w + Dm::S_GL, *qp = w + Dm::S_QP;
   const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
-  const int stride = nblk * kMxWarps;
-  for (int e = blk * kMxWarps + wib; e < a.ne; e += stride) {
+  const int stride = nblk * Dm::SLOTS;
+  for (int e = blk * Dm::SLOTS + wib; e < a.ne; e += stride) {
     const double *vp = a.m.vect + 5 * (size_t)e;
     const float ax = (float)vp[0], bx = (float)vp[1], ay = (float)vp[2], by = (float)vp[3],
                 di = (float)vp[4];
-    for (int i = lane; i < N; i += 32) {
+    for (int i = lane; i < N; i += Dm::LW) {
       const size_t gi = (size_t)e * N + i;
       su[i] = a.y[gi];
       sv[i] = a.y[fn + gi];
@@ -232,9 +238,9 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       gl[2 * TG + lane] = s * r.nx * fv;
       gl[3 * TG + lane] = s * r.ny * fv;
     }
-    __syncwarp();
-    // u, v, h + hb at the quadrature points (spectoxy); points past lane 31
-    // run as (field, point) chains spread over the lanes
+    __syncwarp(lane_mask<Dm>());
+    // u, v, h + hb at the quadrature points (spectoxy); points past the
+    // element's last lane run as (field, point) chains spread over the lanes
     if (lane < Q) {
       const int q = lane;
       float U = 0.f, V = 0.f, H = 0.f;
@@ -249,10 +255,10 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       qp[Q + q] = V;
       qp[2 * Q + q] = H + a.hbq[(size_t)e * Q + q];
     }
-    if (Q > 32) {
-      constexpr int T = Q > 32 ? Q - 32 : 1;
-      for (int c = lane; c < 3 * T; c += 32) {
-        const int f = c / T, q = 32 + c - f * T;
+    if (Q > Dm::LW) {
+      constexpr int T = Q > Dm::LW ? Q - Dm::LW : 1;
+      for (int c = lane; c < 3 * T; c += Dm::LW) {
+        const int f = c / T, q = Dm::LW + c - f * T;
         const float *x = f == 0 ? su : (f == 1 ? sv : sh);
         float acc = 0.f;
 #pragma unroll 4
@@ -265,7 +271,7 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     float qv[4][R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       float gxu = 0.f, gyu = 0.f, gxv = 0.f, gyv = 0.f;
       float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
       if (i < N) {
@@ -299,11 +305,11 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         gtn[r] = nx * ny * qv[0][r] - nx * nx * qv[2][r] + ny * ny * qv[1][r] - nx * ny * qv[3][r];
-        if (lane + 32 * r < N) tmp[lane + 32 * r] = gtn[r];
+        if (lane + Dm::LW * r < N) tmp[lane + Dm::LW * r] = gtn[r];
       }
-      __syncwarp();
+      __syncwarp(lane_mask<Dm>());
       project_rows<Dm>(o, tmp, pg);
-      __syncwarp();
+      __syncwarp(lane_mask<Dm>());
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const float d = pg[r] - gtn[r];
@@ -315,12 +321,12 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       if (i < N)
 #pragma unroll
         for (int c = 0; c < 4; ++c) sq[c * N + i] = qv[c][r];
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
     // quadrature-point products (calvarnl_fs.f:243-332); xytospec is linear,
     // so the four projections of -adu + w1, -adv + z1, uh, vh take combined
     // integrands
@@ -352,29 +358,29 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       }
       qproducts(q, gxx, gxy, gyx, gyy);
     }
-    if (Q > 32) {
-      // the four gradient values at points past lane 31 as spread chains,
-      // parked in the qp slots their products overwrite
-      constexpr int T = Q > 32 ? Q - 32 : 1;
-      __syncwarp();
-      for (int c = lane; c < 4 * T; c += 32) {
-        const int f = c / T, q = 32 + c - f * T;
+    if (Q > Dm::LW) {
+      // the four gradient values at points past the last lane as spread
+      // chains, parked in the qp slots their products overwrite
+      constexpr int T = Q > Dm::LW ? Q - Dm::LW : 1;
+      __syncwarp(lane_mask<Dm>());
+      for (int c = lane; c < 4 * T; c += Dm::LW) {
+        const int f = c / T, q = Dm::LW + c - f * T;
         float acc = 0.f;
 #pragma unroll 4
         for (int n = 0; n < N; ++n) acc = fma32(o[Dm::PPT + n * Q + q], sq[f * N + n], acc);
         qp[(3 + f) * Q + q] = acc;
       }
-      __syncwarp();
+      __syncwarp(lane_mask<Dm>());
       if (lane < T) {
-        const int q = 32 + lane;
+        const int q = Dm::LW + lane;
         qproducts(q, qp[3 * Q + q], qp[4 * Q + q], qp[5 * Q + q], qp[6 * Q + q]);
       }
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
     float bxr[R], byr[R], uh[R], vh[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
       if (i < N) {
 #pragma unroll 4
@@ -400,7 +406,7 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     // uh, vh (phase D)
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       if (i >= N) continue;
       const float hh = sh[i];
       const float fxx = a.mu0 * sq[i] - a.g0 * hh, fxy = a.mu0 * sq[N + i];
@@ -414,10 +420,10 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       suh[i] = uh[r];
       svh[i] = vh[r];
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       if (i >= N) continue;
       float gx = bxr[r], gy = byr[r], hp = 0.f;
 #pragma unroll 4
@@ -440,7 +446,7 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       const float *const x[6] = {sq, sq + N, sq + 2 * N, sq + 3 * N, suh, svh};
       write_traces<Dm, 6>(o, x, a.trq, tn, e);
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
   }
 }
 
@@ -458,12 +464,12 @@ template <class Dm, int VAR>
 __device__ __forceinline__ void tend_body(const MxArgs &a, float *sm, int blk, int nblk) {
   constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, R = Dm::R;
   float *o = sm;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & (Dm::LW - 1), wib = threadIdx.x / Dm::LW;
   float *w = sm + Dm::NOPS + wib * Dm::WS;
   float *gl = w + Dm::S_GL, *tmp = w + Dm::S_TMP;
   const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
-  const int stride = nblk * kMxWarps;
-  for (int e = blk * kMxWarps + wib; e < a.ne; e += stride) {
+  const int stride = nblk * Dm::SLOTS;
+  for (int e = blk * Dm::SLOTS + wib; e < a.ne; e += stride) {
     const float di = (float)a.m.vect[5 * (size_t)e + 4];
     if (lane < TG) {
       const int k = lane / G, j = lane - k * G;
@@ -482,11 +488,11 @@ __device__ __forceinline__ void tend_body(const MxArgs &a, float *sm, int blk, i
       gl[TG + lane] = s * (r.nx * Fyx + r.ny * Fyy);
       gl[2 * TG + lane] = -s * (r.nx * fuh + r.ny * fvh);
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
     float t[3][R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       float gx = 0.f, gy = 0.f, hh = 0.f;
       if (i < N) {
         const size_t gi = (size_t)e * N + i;
@@ -529,17 +535,17 @@ __global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_lin(const MxArgs a
   float *o = sm;
   stage_mx_ops<Dm>(o, a.ops);
   __syncthreads();
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & (Dm::LW - 1), wib = threadIdx.x / Dm::LW;
   float *w = sm + Dm::NOPS + wib * Dm::WS;
   float *su = w + Dm::S_U, *sv = w + Dm::S_V, *sh = w + Dm::S_H;
   float *gl = w + Dm::S_GL, *tmp = w + Dm::S_TMP;
   const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
-  const int stride = gridDim.x * kMxWarps;
-  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+  const int stride = gridDim.x * Dm::SLOTS;
+  for (int e = blockIdx.x * Dm::SLOTS + wib; e < a.ne; e += stride) {
     const double *vp = a.m.vect + 5 * (size_t)e;
     const float ax = (float)vp[0], bx = (float)vp[1], ay = (float)vp[2], by = (float)vp[3],
                 di = (float)vp[4];
-    for (int i = lane; i < N; i += 32) {
+    for (int i = lane; i < N; i += Dm::LW) {
       const size_t gi = (size_t)e * N + i;
       su[i] = a.y[gi];
       sv[i] = a.y[fn + gi];
@@ -557,11 +563,11 @@ __global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_lin(const MxArgs a
       gl[TG + lane] = s * r.ny * fxx;
       gl[2 * TG + lane] = -s * a.hh0 * (r.nx * fu + r.ny * fv);
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
     float t[3][R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
+      const int i = lane + Dm::LW * r;
       float gxh = 0.f, gyh = 0.f, gxu = 0.f, gyu = 0.f, gxv = 0.f, gyv = 0.f;
       float l0 = 0.f, l1 = 0.f, l2 = 0.f;
       if (i < N) {
@@ -592,7 +598,7 @@ __global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_lin(const MxArgs a
       const float nx = (float)a.m.normt[2 * (size_t)e], ny = (float)a.m.normt[2 * (size_t)e + 1];
       wall_vec<Dm, false>(o, tmp, t[0], t[1], nx, ny);
     }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
     finish_element<Dm>(a, o, w, e, t);
   }
 }
@@ -605,22 +611,22 @@ __global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_prep(const MxArgs 
   float *o = sm;
   stage_mx_ops<Dm>(o, a.ops);
   __syncthreads();
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & (Dm::LW - 1), wib = threadIdx.x / Dm::LW;
   float *w = sm + Dm::NOPS + wib * Dm::WS;
   const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * Dm::TS;
-  const int stride = gridDim.x * kMxWarps;
-  for (int e = blockIdx.x * kMxWarps + wib; e < a.ne; e += stride) {
+  const int stride = gridDim.x * Dm::SLOTS;
+  for (int e = blockIdx.x * Dm::SLOTS + wib; e < a.ne; e += stride) {
     for (int f = 0; f < 3; ++f)
-      for (int i = lane; i < N; i += 32) {
+      for (int i = lane; i < N; i += Dm::LW) {
         const size_t gi = f * fn + (size_t)e * N + i;
         const float v = (float)a.c64[gi];
         a.y[gi] = v;
         w[f * N + i] = v;
       }
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
     const float *const x[3] = {w, w + N, w + 2 * N};
     write_traces<Dm, 3>(o, x, a.tr_out, tn, e);
-    __syncwarp();
+    __syncwarp(lane_mask<Dm>());
   }
 }
 
@@ -811,7 +817,7 @@ std::vector<float> ops_image(const PsiOps &p, const spoc_tables *t) {
 // Persistent grid: as many blocks as stay resident (occupancy x SMs), or
 // fewer when the elements run out.  Cached per kernel.
 using MxKernel = void (*)(MxArgs);
-int grid_for(MxKernel kernel, size_t smem, int sms, int ne) {
+int grid_for(MxKernel kernel, size_t smem, int sms, int ne, int slots) {
   struct Entry {
     MxKernel k;
     int per_sm;
@@ -828,14 +834,14 @@ int grid_for(MxKernel kernel, size_t smem, int sms, int ne) {
       per_sm = 1;
     cache.push_back({kernel, per_sm});
   }
-  const int need = (ne + kMxWarps - 1) / kMxWarps;
+  const int need = (ne + slots - 1) / slots;
   const int cap = sms * per_sm;
   return need < cap ? need : cap;
 }
 
 template <class Dm>
 constexpr size_t mx_smem() {
-  return sizeof(float) * (Dm::NOPS + (size_t)kMxWarps * Dm::WS);
+  return sizeof(float) * (Dm::NOPS + (size_t)Dm::SLOTS * Dm::WS);
 }
 
 // Launches of one right-hand side (stage >= 0: with the RK4 update).
@@ -847,7 +853,7 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
     if (ev) cudaEventRecord(ev[i], st);
   };
   if (c->variant == SPOC_LIN) {
-    const int g = grid_for(kx_lin<Dm>, smem, c->sms, c->ne);
+    const int g = grid_for(kx_lin<Dm>, smem, c->sms, c->ne, Dm::SLOTS);
     mark(0);
     kx_lin<Dm><<<g, 32 * kMxWarps, smem, st>>>(a);
     mark(1);
@@ -856,8 +862,8 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
   }
   cudaError_t tce = cudaSuccess;
   auto go = [&](MxKernel kv, MxKernel kt) {
-    const int gv = grid_for(kv, smem, c->sms, c->ne);
-    const int gt = grid_for(kt, smem, c->sms, c->ne);
+    const int gv = grid_for(kv, smem, c->sms, c->ne, Dm::SLOTS);
+    const int gt = grid_for(kt, smem, c->sms, c->ne, Dm::SLOTS);
     mark(0);
     if (c->tc) {
       tce = mixed_tc_vol(c->variant, c->nc, c->Q, c->G, a, c->tcimg, c->sms, st);
@@ -880,7 +886,7 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
 template <class Dm>
 cudaError_t run_prep(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *launches) {
   constexpr size_t smem = mx_smem<Dm>();
-  const int g = grid_for(kx_prep<Dm>, smem, c->sms, c->ne);
+  const int g = grid_for(kx_prep<Dm>, smem, c->sms, c->ne, Dm::SLOTS);
   kx_prep<Dm><<<g, 32 * kMxWarps, smem, st>>>(a);
   if (launches) *launches += 1;
   return cudaGetLastError();
@@ -1163,7 +1169,13 @@ __global__ void __launch_bounds__(32 * kMxWarps, kEnsMinBlocks)
   }
 }
 
-size_t ens_smem() { return mx_smem<MDims<6, 33, 7>>(); }
+size_t ens_smem() {
+  const size_t s[4] = {mx_smem<MDims<3, 12, 4>>(), mx_smem<MDims<4, 25, 5>>(),
+                       mx_smem<MDims<5, 27, 6>>(), mx_smem<MDims<6, 33, 7>>()};
+  size_t m = 0;
+  for (size_t v : s) m = v > m ? v : m;
+  return m;
+}
 
 }  // namespace
 

@@ -22,7 +22,11 @@ struct MDims {
   static constexpr int G = G_;
   static constexpr int TG = 3 * G_;
   static constexpr int TS = TG + 1;  // trace record: TG mean-free traces + the mean
-  static constexpr int R = (N + 31) / 32;
+  // lanes per element: 16 when the modes, the trace record and two passes
+  // over the quadrature points fit (degrees 3 and 4: two elements per warp)
+  static constexpr int LW = (N <= 16 && TS <= 16 && Q <= 32) ? 16 : 32;
+  static constexpr int SLOTS = kMxWarps * 32 / LW;  // elements in flight per block
+  static constexpr int R = (N + LW - 1) / LW;
   // resident blocks per SM the register budget is sized for (shared memory
   // allows about 4 blocks of 8 warps at degree <= 6 and 3 at degree 7)
   static constexpr int MINB = R == 1 ? 4 : 2;
@@ -44,7 +48,8 @@ struct MDims {
   static constexpr int S_GL = 16 * N;         // 4 face vectors of TG
   static constexpr int S_QP = S_GL + 4 * TG;  // 7 quadrature vectors of Q
   static constexpr int WS = (S_QP + 7 * Q + 3) / 4 * 4;
-  static_assert(TG <= 32, "face points of one element must fit one warp");
+  static_assert(TS <= LW, "face points of one element must fit its lanes");
+  static_assert(Q <= 2 * LW, "two passes over the quadrature points at most");
   static_assert(N <= 64 && Q <= 64, "two rows per lane at most");
 };
 
