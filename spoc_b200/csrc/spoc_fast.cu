@@ -235,6 +235,44 @@ __device__ __forceinline__ void stage_neighbours(const Sides &sd, double *nb, Fe
   }
 }
 
+// Asynchronous copy of one double from global to shared memory (LDGSTS: no
+// register round trip, the warp keeps computing while the copy is in flight).
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+// Waits for every copy this thread has issued.
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Start the copies of NF fields of element e and of its three neighbours into
+// own[f*N + i] and nb[(k*NF + f)*N + i] (the layouts of load_vec and
+// stage_neighbours); field f is read from fields[f].  The buffers must not be
+// read until cp_async_wait_all() and a __syncwarp().
+template <class Dm, int NF>
+__device__ __forceinline__ void prefetch_element(const double *const (&fields)[NF], int e,
+                                                 const Sides &sd, double *own, double *nb) {
+  const int l = lane_id();
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int r = 0; r < Dm::R; ++r) {
+      const int i = l + 32 * r;
+      if (i < Dm::N) cp_async8(own + f * Dm::N + i, fields[f] + (size_t)e * Dm::N + i);
+    }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int t = sd.nb[k];
+    if (t < 0) continue;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int r = 0; r < Dm::R; ++r) {
+        const int i = l + 32 * r;
+        if (i < Dm::N) cp_async8(nb + (k * NF + f) * Dm::N + i, fields[f] + (size_t)t * Dm::N + i);
+      }
+  }
+}
+
 // Face values of NF fields by the cal_flu chain (src/calflu.f:31-62): lane
 // k*G + j computes point j of the face of side k; fb[f*32 + k*G + j].
 template <class Dm, int NF>
@@ -601,20 +639,27 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
   QWarp<Dm> &W = reinterpret_cast<QWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
   constexpr int N = Dm::N, R = Dm::R;
+  const double *const fields[2] = {su, sv};
+  // the coefficients of the warp's next element are copied into W.own / W.nb
+  // while it works on the current one (the first copy overlaps the staging
+  // of the operators)
+  Sides sd_next;
+  if (warp_global() < m.ne) {
+    sd_next = sides_of(m, warp_global());
+    prefetch_element<Dm, 2>(fields, warp_global(), sd_next, W.own, W.nb);
+  }
   stage_ops(S, op);
   __syncthreads();
   const size_t fs = (size_t)m.ne * N;
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
-    const Sides sd = sides_of(m, e);
+    const Sides sd = sd_next;
+    const int en = e + warp_count();
+    if (en < m.ne) sd_next = sides_of(m, en);
     const Geo g = geo(m, e);
     int isg[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
-    load_vec<Dm>(W.own, su, e);
-    load_vec<Dm>(W.own + N, sv, e);
-    stage_neighbours<Dm, 2>(sd, W.nb, [&](int f, int t, int i) {
-      return (f == 0 ? su : sv)[(size_t)t * N + i];
-    });
+    cp_async_wait_all();
     __syncwarp();
     face_values<Dm, 2>(S.pf, m, sd, W.own, W.nb, W.fr);
     __syncwarp();
@@ -624,7 +669,8 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
     scale_face<Dm>(m, sd, W.fr + 32, W.fb + 96, 1);
     double ax[2][R], bx[2][R];
     matvec2<Dm, 2>(S.agx, S.agy, W.own, N, ax, bx);
-    __syncwarp();
+    __syncwarp();  // W.own / W.nb are free from here on
+    if (en < m.ne) prefetch_element<Dm, 2>(fields, en, sd_next, W.own, W.nb);
     double gq[4][R];  // gxx, gxy, gyx, gyy
 #pragma unroll
     for (int c = 0; c < 2; ++c)
@@ -847,19 +893,27 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
   TWarp<Dm> &W = reinterpret_cast<TWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
   constexpr int N = Dm::N, R = Dm::R;
+  const size_t fs = (size_t)m.ne * N;
+  const double *const src[6] = {a.f, a.f + fs, a.f + 2 * fs, a.f + 3 * fs, a.uh, a.vh};
+  // the coefficients of the warp's next element are copied into W.own / W.nb
+  // while it works on the current one (the first copy overlaps the staging
+  // of the operators)
+  Sides sd_next;
+  if (warp_global() < m.ne) {
+    sd_next = sides_of(m, warp_global());
+    prefetch_element<Dm, 6>(src, warp_global(), sd_next, W.own, W.nb);
+  }
   stage_ops(S, op);
   __syncthreads();
-  const size_t fs = (size_t)m.ne * N;
-  const double *src[6] = {a.f, a.f + fs, a.f + 2 * fs, a.f + 3 * fs, a.uh, a.vh};
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
-    const Sides sd = sides_of(m, e);
+    const Sides sd = sd_next;
+    const int en = e + warp_count();
+    if (en < m.ne) sd_next = sides_of(m, en);
     const Geo g = geo(m, e);
     int isg[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
-#pragma unroll
-    for (int f = 0; f < 6; ++f) load_vec<Dm>(W.own + f * N, src[f], e);
-    stage_neighbours<Dm, 6>(sd, W.nb, [&](int f, int t, int i) { return src[f][(size_t)t * N + i]; });
+    cp_async_wait_all();
     __syncwarp();
     face_values<Dm, 6>(S.pf, m, sd, W.own, W.nb, W.fb);
     __syncwarp();
@@ -887,7 +941,8 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
     axpy<R>(hb, bx[4], -cay);
     axpy<R>(hb, ax[5], -cbx);
     axpy<R>(hb, bx[5], cax);
-    __syncwarp();
+    __syncwarp();  // W.own / W.nb are free from here on
+    if (en < m.ne) prefetch_element<Dm, 6>(src, en, sd_next, W.own, W.nb);
     double t[6][3][R];
     lift_sums<Dm, 6>(S, isg, W.fb, t);
     apply_lift<R>(gx, t[0], isg, g.detai);
