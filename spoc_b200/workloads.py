@@ -17,6 +17,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import api
+from .adapt import AdaptiveMesh
 
 
 @dataclass
@@ -183,6 +184,9 @@ class Problem:
     w0: np.ndarray
     z0: np.ndarray
     dt: float
+    # refinement history of an adapted mesh: (AdaptiveMesh, used, leaf, half)
+    # as adapt_tree leaves it (None: the mesh is its own base mesh)
+    adapt: object = None
 
 
 def build_problem(cfg: Config, ld: int | None = None, tables: api.Tables | None = None) -> Problem:
@@ -421,56 +425,124 @@ def build_member(mb: Member) -> Problem:
 
 
 # ---------------------------------------------------------------------------
-# Solution-driven regridding: the refinement branch of the adaptive driver
-# (src/shwwnl_adap.f:375-450)
+# Solution-driven regridding: the refinement and coarsening pass of the
+# adaptive driver (src/shwwnl_adap.f:375-450, src/adapt.f:5-187)
 # ---------------------------------------------------------------------------
 
 def adapt_problem(p: Problem, marked: np.ndarray):
-    """The refined mesh of p with the marked elements split (red refinement,
-    green closure, corner fix), its pointers, inter_only_new's tinter and the
-    located quadrature points of the elements to re-project.  Bathymetry and
-    wind on the new mesh follow newinter (src/adapt.f:238-265) for a flat
-    bottom and no wind: hb = H in mode 1, w0 = z0 = 0.  Returns
-    (Problem without state, tinter, (pt_elem, pt_x, pt_y))."""
+    """The mesh of p with the marked elements refined (adapt_tree without
+    coarsening): (Problem without state, tinter, (pt_elem, pt_x, pt_y))."""
+    p1, tinter, loc, _ = adapt_tree(p, marked)
+    return p1, tinter, loc
+
+
+def calh2(T: api.Tables, mesh: api.Mesh, tinter: np.ndarray, old: np.ndarray, f, ld: int | None = None):
+    """calh2 (src/adapt.f:303-373): the L2 projection of f(x, y) on the new
+    elements (tinter == 0, by calh's method) and the old coefficients copied
+    on the inherited ones."""
+    ld = ld or old.shape[1]
+    out = np.zeros((mesh.ne, ld))
+    k = tinter > 0
+    out[k] = old[tinter[k] - 1]
+    if (~k).any():
+        px, py = api.projection_points(mesh, T)
+        out[~k] = api.project(T, f(px[~k], py[~k]), ld)
+    return out
+
+
+def _base_adapt(p: Problem):
+    """Refinement history of a mesh that has none: its own elements as the
+    base triangles (mesh vertices are the tree's vertices)."""
+    tree = AdaptiveMesh(p.mesh.inn - 1, p.mesh.xgr, p.mesh.ygr)
+    ne = p.mesh.ne
+    return tree, np.arange(p.mesh.xgr.size), np.arange(ne, dtype=np.int64), np.zeros(ne, np.int8)
+
+
+def _canon(t):
+    """A triangle up to the rotation of its vertices (the corner fix rotates
+    wall elements)."""
+    i = min(range(3), key=lambda j: t[j])
+    return (t[i], t[(i + 1) % 3], t[(i + 2) % 3])
+
+
+def adapt_tree(p: Problem, fconv: np.ndarray, fderaff: np.ndarray | None = None,
+               bathymetry=None):
+    """One pass of the adaptive mesh (src/adapt.f:5-187): coarsening of the
+    nodes whose four children carry fderaff (deraffiner), refinement of the
+    leaves under fconv with the level rules (adapmaille, check_level,
+    protridouble), the new mesh with its unchanged elements first in their
+    old order, inter_only_new's tinter (vertices matched through the tree,
+    since the compaction renumbers them) and the located quadrature points of
+    the other elements.  Depth on the new mesh: calh2 of `bathymetry(x, y)`,
+    or the constant depth of p (newinter, src/adapt.f:238-265); no wind.
+    Returns (Problem without state, tinter, (pt_elem, pt_x, pt_y), info)."""
+    import copy
     cfg, T = p.cfg, p.T
     ld = p.hb.shape[1]
-    inn, x, y = refine(p.mesh.inn - 1, p.mesh.xgr, p.mesh.ygr, np.asarray(marked, dtype=bool))
-    # unchanged elements first, in their old order, then the new ones: the
-    # order inter_only_new expects (it matches old elements in sequence)
-    old = {tuple(t) for t in (p.mesh.inn - 1).tolist()}
-    keep = np.array([tuple(t) in old for t in inn.tolist()])
-    inn = np.concatenate([inn[keep], inn[~keep]])
+    tree0, used0, leaf0, half0 = p.adapt if p.adapt is not None else _base_adapt(p)
+    tree = copy.deepcopy(tree0)
+    fconv = np.asarray(fconv, dtype=bool)
+    fderaff = np.zeros_like(fconv) if fderaff is None else np.asarray(fderaff, dtype=bool)
+    ref, coarse = tree.flags_to_leaves(leaf0, half0, fconv, fderaff)
+    ncoarse = tree.coarsen(coarse)
+    nref = tree.refine(ref)
+    inn, x, y, leaf, half, used = tree.mesh()
+    # unchanged elements first, in their old order (inter_only_new matches
+    # old elements in sequence), then the new ones in tree order
+    old_tree = used0[p.mesh.inn - 1]
+    old_pos = {_canon(tuple(t)): i for i, t in enumerate(old_tree.tolist())}
+    new_tree = used[inn]
+    pos = np.array([old_pos.get(_canon(tuple(t)), -1) for t in new_tree.tolist()])
+    keep = np.nonzero(pos >= 0)[0]
+    keep = keep[np.argsort(pos[keep], kind="stable")]
+    order = np.concatenate([keep, np.nonzero(pos < 0)[0]])
+    inn, leaf, half = inn[order], leaf[order], half[order]
     inn = api.fix_mesh(inn + 1, x.size)
     mesh = api.build_mesh(inn, x, y, cfg.nc, cfg.f0, cfg.beta, ld)
-    tinter = api.inter_only_new(p.mesh, inn)
+    # the old elements in the new vertex numbering (removed vertices: 0)
+    remap = np.full(max(int(used0.max()), int(used.max())) + 1, -1, dtype=np.int64)
+    remap[used] = np.arange(used.size)
+    old_in_new = (remap[old_tree] + 1).astype(np.int32)
+    from types import SimpleNamespace
+    tinter = api.inter_only_new(SimpleNamespace(ne=p.mesh.ne, inn=old_in_new), inn)
     loc = api.locate_points(p.mesh, mesh, tinter, T)
-    hb = np.zeros((mesh.ne, ld))
-    hb[:, 0] = p.hb[0, 0]
+    if bathymetry is None:
+        hb = np.zeros((mesh.ne, ld))
+        hb[:, 0] = p.hb[0, 0]
+    else:
+        hb = calh2(T, mesh, tinter, p.hb, bathymetry, ld)
     z = np.zeros((mesh.ne, ld))
     dt = cfl_dt(cfg.nc, mesh, cfg.g0, cfg.depth) * cfg.dt_scale
-    return Problem(cfg, T, mesh, None, None, None, hb, mesh.fc, z, z.copy(), dt), tinter, loc
+    info = {"refined": nref, "coarsened": ncoarse}
+    p1 = Problem(cfg, T, mesh, None, None, None, hb, mesh.fc, z, z.copy(), dt,
+                 (tree, used, leaf, half))
+    return p1, tinter, loc, info
 
 
 def regrid_step(p: Problem, s: api.Solver, fac1: float, fac2: float, fac3: float,
                 precision: str = "fp64", ngraph: int = 10):
-    """One refinement pass of the adaptive driver on the device state of s:
-    cal_conv's indicator (src/adapt.f:1122-1193), refinement of the flagged
-    elements, interpol of u, v, h onto the new mesh (src/adapt.f:1662-1745),
-    verif_rot (src/shwwnl_adap.f:481-596) and checkcfl2's time step
-    (src/cfl.f:57-140).  Coarsening (deraffiner) is not built.  Returns
-    (new problem, new solver, info); the inputs when nothing is flagged."""
+    """One pass of the adaptive driver on the device state of s
+    (src/adapt.f:5-187): cal_conv's indicator (src/adapt.f:1122-1193),
+    coarsening and refinement of the flagged elements (adapt_tree), interpol
+    of u, v, h onto the new mesh (src/adapt.f:1662-1745), verif_rot
+    (src/shwwnl_adap.f:481-596) and checkcfl2's time step (src/cfl.f:57-140).
+    Returns (new problem, new solver, info); the inputs when the mesh stays
+    as it is."""
     cc = s.cal_conv(fac1, fac2, fac3)
     info = {"conv": cc["conv"], "timedir": cc["timedir"], "supmax": cc["supmax"],
-            "flagged": int(cc["fconv"].sum())}
-    if not cc["fconv"].any():
+            "flagged": int(cc["fconv"].sum()), "flagged_coarsen": int(cc["fderaff"].sum())}
+    if not cc["conv"]:
         return p, s, info
-    p1, tinter, loc = adapt_problem(p, cc["fconv"])
+    p1, tinter, loc, ainfo = adapt_tree(p, cc["fconv"], cc["fderaff"])
+    info.update(ainfo)
+    if ainfo["refined"] == 0 and ainfo["coarsened"] == 0:
+        return p, s, info
     s1 = api.Solver(p1.T, p1.mesh, p.cfg.variant, precision)
     s1.set_params(p.cfg.mu0, p.cfg.mb0, p.cfg.g0, p1.hb, p1.fc, p1.w0, p1.z0)
     s1.interpol_from(s, tinter, *loc)
     s1.verif_rot()
     cflmin, dt = s1.cfl2(ngraph, p.dt)
-    info.update({"ne_old": p.mesh.ne, "ne_new": p1.mesh.ne,
+    info.update({"ne_old": p.mesh.ne, "ne_new": p1.mesh.ne, "tinter": tinter,
                  "inherited": int((tinter > 0).sum()), "cflmin": cflmin, "dt_cfl2": dt})
     return p1, s1, info
 

@@ -129,6 +129,40 @@ def test_regrid_step_matches_oracle_pipeline(gpu_lib, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c2_fs_p6", "c4_ns_p4"])
+def test_regrid_coarsening_matches_oracle_pipeline(gpu_lib, name):
+    """A refined patch flagged calm by cal_conv's fderaff is coarsened
+    (deraffiner through the refinement history) and the device re-projection,
+    verif_rot and checkcfl2 equal the oracle's bit for bit."""
+    p, OT, OM = setup(name)
+    s = stepped(p, 5)
+    amax = np.maximum.reduce(s.checkconv())
+    fac1 = float(np.quantile(amax, 0.85))
+    p1, s1, info = W.regrid_step(p, s, fac1, 0.0, 10 * fac1)
+    assert info["refined"] > 0 and info["coarsened"] == 0
+    s1.rk4_steps(p1.dt, 2)
+    u, v, h = s1.get_state()
+    amax1 = np.maximum.reduce(s1.checkconv())
+    fac2 = float(np.quantile(amax1, 0.97))
+    p2, s2, info2 = W.regrid_step(p1, s1, 1e300, fac2, 1e301)
+    assert info2["refined"] == 0 and info2["coarsened"] > 0 and p2.mesh.ne < p1.mesh.ne
+    M1 = O.Mesh(p1.mesh.inn, p1.mesh.xgr, p1.mesh.ygr, p.cfg.nc, p.cfg.f0, p.cfg.beta)
+    M2 = O.Mesh(p2.mesh.inn, p2.mesh.xgr, p2.mesh.ygr, p.cfg.nc, p.cfg.f0, p.cfg.beta)
+    tinter = info2["tinter"]
+    assert 0 < (tinter > 0).sum() < p2.mesh.ne
+    ru, *_ = O.interpol(OT, M1, M2, tinter, u)
+    rv, *_ = O.interpol(OT, M1, M2, tinter, v)
+    rh, *_ = O.interpol(OT, M1, M2, tinter, h)
+    ru, rv = O.verif_rot(OT, M2, ru, rv)
+    gu, gv, gh = s2.get_state()
+    assert np.array_equal(gu, ru) and np.array_equal(gv, rv) and np.array_equal(gh, rh)
+    cmin, dt = O.checkcfl2(p.cfg.nc, M2, p2.hb, ru, rv, p.cfg.g0, 10, p1.dt)
+    assert (info2["cflmin"], info2["dt_cfl2"]) == (cmin, dt)
+    s2.rk4_steps(p2.dt, 3)
+    assert all(np.isfinite(a).all() for a in s2.get_state())
+
+
+@pytest.mark.gpu
 def test_regrid_mixed_handles(gpu_lib):
     """SPOC_MIXED handles keep their state in their own basis; the regrid moves
     it through FP64 and back (a round trip through the ill-conditioned basis
