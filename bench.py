@@ -13,8 +13,9 @@ DOF-updates/s = 3 * nm * ne * steps / seconds (u, v, eta), whole job.
 `value`: device-resident state, CUDA events around every step on the
 launching stream, L2 flushed (256 MiB write) before every timed step, max
 over ranks.  `e2e`: the host-buffer entry point spoc_rk4_steps_host, one step
-per call with the state copied host->device and back from pinned memory
-inside the timed region.  N > 1 runs independent replicas (one per GPU, no
+per call with pinned host arrays, inside the timed region: the state copied
+host->device, the step, and the new state stored back into the pinned arrays
+by the last stage kernel (mapped host memory) as it computes it.  N > 1 runs independent replicas (one per GPU, no
 collective on the data path): weak scaling.
 
 --impl reference times the CPU restatement of the reference (oracle/,

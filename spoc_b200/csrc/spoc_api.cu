@@ -53,6 +53,9 @@ struct spoc_handle {
   int sms = 148;
   int path = SPOC_PATH_AUTO;
   cudaStream_t own = nullptr, st = nullptr;
+  // second stream and event of spoc_rk4_steps_host (h uploaded beside the q-phase)
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_ev = nullptr, main_ev = nullptr;
   long long launches = 0;
   double mu0 = 0, mb0 = 0, g0 = 9.81, hh0 = 0;
   bool have_params = false;
@@ -85,6 +88,9 @@ struct spoc_handle {
   ~spoc_handle() {
     if (mx) mixed_destroy(mx);
     for (void *p : allocs) cudaFree(p);
+    if (side_ev) cudaEventDestroy(side_ev);
+    if (main_ev) cudaEventDestroy(main_ev);
+    if (side) cudaStreamDestroy(side);
     if (own) cudaStreamDestroy(own);
   }
 };
@@ -240,11 +246,13 @@ int build_mesh(spoc_handle *h, const spoc_mesh *m) {
 // (ld, ne) caller arrays <-> packed (nm, ne) device fields; packed caller
 // arrays (ld == nm) move as one contiguous copy (a pitched copy of ne rows of
 // nm doubles runs far below the link bandwidth).
-cudaError_t copy_in(spoc_handle *h, double *dst, const double *src, int ld, cudaMemcpyKind k) {
+cudaError_t copy_in(spoc_handle *h, double *dst, const double *src, int ld, cudaMemcpyKind k,
+                    cudaStream_t st = nullptr) {
+  if (!st) st = h->st;
   if (ld == h->nm)
-    return cudaMemcpyAsync(dst, src, sizeof(double) * h->nm * (size_t)h->ne, k, h->st);
+    return cudaMemcpyAsync(dst, src, sizeof(double) * h->nm * (size_t)h->ne, k, st);
   return cudaMemcpy2DAsync(dst, sizeof(double) * h->nm, src, sizeof(double) * ld,
-                           sizeof(double) * h->nm, h->ne, k, h->st);
+                           sizeof(double) * h->nm, h->ne, k, st);
 }
 cudaError_t copy_out(spoc_handle *h, double *dst, const double *src, int ld, cudaMemcpyKind k) {
   if (ld == h->nm)
@@ -278,10 +286,11 @@ RhsBuffers rhs_buffers(spoc_handle *h, double *const s[3]) {
 // One FP64 right-hand side or RK4 stage; q (4 ne nm values) receives the
 // nonlinear variants' q-phase output instead of the handle's buffer when given.
 cudaError_t launch(spoc_handle *h, double *const s[3], const StageArgs &sa, cudaEvent_t *ev,
-                   double *q = nullptr) {
+                   double *q = nullptr, cudaEvent_t sh_ready = nullptr) {
   const bool fast = h->path != SPOC_PATH_GENERIC && fast_available(h->nc, h->ng, h->ngf);
   RhsBuffers b = rhs_buffers(h, s);
   if (q) b.q = q;
+  b.sh_ready = sh_ready;
   if (fast && h->precision == SPOC_FP64_FMA)
     return launch_rhs_fast_fma(h->variant, h->op, h->mesh, b, sa, h->st, h->sms, &h->launches,
                                ev);
@@ -538,9 +547,28 @@ extern "C" int spoc_get_state(spoc_handle *h, int ld, double *u, double *v, doub
 }
 
 namespace {
+// Device address of host memory the device can store to directly (pinned,
+// mapped: cudaHostAlloc / cudaMallocHost, or registered); false otherwise.
+bool mapped_host(const double *p, double **dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return false;
+  *dev = static_cast<double *>(a.devicePointer);
+  return true;
+}
+
 // RK4 steps of the FP64 kernels on `base` (U0 by default), in place (also
 // used by the adjoint, which stays FP64 whatever the handle's precision).
-int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *base = nullptr) {
+// host (optional): device addresses of the caller's mapped pinned (ld-strided)
+// arrays; the last stage of the last step stores the new state there too.
+// sh_ready (optional): the first right-hand side's kernels that read h wait
+// for it.
+int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *base = nullptr,
+                       double *const *host = nullptr, int host_ld = 0,
+                       cudaEvent_t sh_ready = nullptr) {
   if (!base) base = h->U0;
   StageArgs sa{};
   sa.dt = dt;
@@ -555,8 +583,14 @@ int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *bas
       double *const *in = s == 0 ? base : (s == 2 ? h->SB : h->SA);
       double *const *out = s == 1 ? h->SB : h->SA;
       sa.stage = s;
-      for (int c = 0; c < 3; ++c) sa.out[c] = out[c];
-      CK(launch(h, in, sa, nullptr), "launch RK4 stage");
+      const bool last = host && it == nsteps - 1 && s == 3;
+      for (int c = 0; c < 3; ++c) {
+        sa.out[c] = out[c];
+        sa.host[c] = last ? host[c] : nullptr;
+      }
+      sa.host_ld = host_ld;
+      CK(launch(h, in, sa, nullptr, nullptr, it == 0 && s == 0 ? sh_ready : nullptr),
+         "launch RK4 stage");
     }
   }
   return SPOC_OK;
@@ -584,16 +618,45 @@ extern "C" int spoc_rk4_steps_host(spoc_handle *h, int ld, double *u, double *v,
   if (!h || !u || !v || !hh || nsteps < 0 || ld < (h ? h->nm : 1))
     return fail(SPOC_E_ARG, "bad argument");
   if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
-  CK(copy_in(h, h->U0[0], u, ld, cudaMemcpyHostToDevice), "upload u");
-  CK(copy_in(h, h->U0[1], v, ld, cudaMemcpyHostToDevice), "upload v");
-  CK(copy_in(h, h->U0[2], hh, ld, cudaMemcpyHostToDevice), "upload h");
+  if (h->mx || nsteps == 0) {
+    CK(copy_in(h, h->U0[0], u, ld, cudaMemcpyHostToDevice), "upload u");
+    CK(copy_in(h, h->U0[1], v, ld, cudaMemcpyHostToDevice), "upload v");
+    CK(copy_in(h, h->U0[2], hh, ld, cudaMemcpyHostToDevice), "upload h");
+  }
   if (h->mx) CK(mixed_set_state(h->mx, h->mesh, h->U0, h->st, &h->launches), "mixed state");
-  int rc = enqueue_steps(h, dt, nsteps);
+  int rc = SPOC_OK;
+  bool direct = false;
+  if (h->mx || nsteps == 0) {
+    rc = enqueue_steps(h, dt, nsteps);
+  } else {
+    // FP64: h is uploaded on a second stream while the first q-phase (which
+    // reads u and v only) runs; into mapped pinned caller arrays the last
+    // stage kernel stores the new state over the link as it computes it (no
+    // separate download)
+    if (!h->side) {
+      CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "stream");
+      CK(cudaEventCreateWithFlags(&h->side_ev, cudaEventDisableTiming), "event");
+      CK(cudaEventCreateWithFlags(&h->main_ev, cudaEventDisableTiming), "event");
+    }
+    // u and v first (the copies share the link), then h behind the q-phase
+    CK(copy_in(h, h->U0[0], u, ld, cudaMemcpyHostToDevice), "upload u");
+    CK(copy_in(h, h->U0[1], v, ld, cudaMemcpyHostToDevice), "upload v");
+    CK(cudaEventRecord(h->main_ev, h->st), "record");  // also orders earlier work on h
+    CK(cudaStreamWaitEvent(h->side, h->main_ev, 0), "wait");
+    CK(copy_in(h, h->U0[2], hh, ld, cudaMemcpyHostToDevice, h->side), "upload h");
+    CK(cudaEventRecord(h->side_ev, h->side), "record");
+    double *dh[3] = {nullptr, nullptr, nullptr};
+    direct = mapped_host(u, &dh[0]) && mapped_host(v, &dh[1]) && mapped_host(hh, &dh[2]);
+    rc = enqueue_steps_fp64(h, dt, nsteps, nullptr, direct ? dh : nullptr, ld, h->side_ev);
+    if (rc) cudaStreamWaitEvent(h->st, h->side_ev, 0);  // leave no copy behind the stream
+  }
   if (rc) return rc;
-  if (h->mx) CK(mixed_get_state(h->mx, h->U0, h->st, &h->launches), "mixed state");
-  CK(copy_out(h, u, h->U0[0], ld, cudaMemcpyDeviceToHost), "download u");
-  CK(copy_out(h, v, h->U0[1], ld, cudaMemcpyDeviceToHost), "download v");
-  CK(copy_out(h, hh, h->U0[2], ld, cudaMemcpyDeviceToHost), "download h");
+  if (!direct) {
+    if (h->mx) CK(mixed_get_state(h->mx, h->U0, h->st, &h->launches), "mixed state");
+    CK(copy_out(h, u, h->U0[0], ld, cudaMemcpyDeviceToHost), "download u");
+    CK(copy_out(h, v, h->U0[1], ld, cudaMemcpyDeviceToHost), "download v");
+    CK(copy_out(h, hh, h->U0[2], ld, cudaMemcpyDeviceToHost), "download h");
+  }
   return check_flag(h);
 }
 

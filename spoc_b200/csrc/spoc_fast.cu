@@ -615,7 +615,9 @@ __device__ __forceinline__ void stage_update(const StageArgs &sa, int fld, int e
       sa.acc[fld][i] = add(sa.acc[fld][i], mul(2.0, dd));
       sa.out[fld][i] = add(u0, mul(sa.dt, dd));
     } else {
-      sa.base[fld][i] = add(u0, mul(sa.dt6, add(sa.acc[fld][i], dd)));
+      const double nv = add(u0, mul(sa.dt6, add(sa.acc[fld][i], dd)));
+      sa.base[fld][i] = nv;
+      if (sa.host[fld]) sa.host[fld][(size_t)e * sa.host_ld + n] = nv;
     }
   }
 }
@@ -1158,6 +1160,7 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   }
   mark(0);
   kf_qphase<Dm, VAR><<<gq, 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
+  if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
   mark(1);
   kf_nlvol<Dm, VAR><<<gb, 32 * wb, sb, st>>>(op, m, na);
   mark(2);
@@ -1199,6 +1202,7 @@ cudaError_t run_lin(const DevOps &op, const DevMesh &m, const RhsBuffers &b, con
     ne_cached = m.ne;
   }
   LinArgs la{b.su, b.sv, b.sh, b.g0, b.hh0};
+  if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
   if (ev) cudaEventRecord(ev[0], st);
   kf_lin<Dm><<<grid, 32 * w, sm, st>>>(op, m, la, sa);
   if (ev) cudaEventRecord(ev[1], st);

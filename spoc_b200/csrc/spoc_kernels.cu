@@ -136,7 +136,9 @@ __device__ __forceinline__ void stage_update(const StageArgs &sa, int fld, int e
       sa.acc[fld][i] = add(sa.acc[fld][i], mul(2.0, dd));
       sa.out[fld][i] = add(u0, mul(sa.dt, dd));
     } else {
-      sa.base[fld][i] = add(u0, mul(sa.dt6, add(sa.acc[fld][i], dd)));
+      const double nv = add(u0, mul(sa.dt6, add(sa.acc[fld][i], dd)));
+      sa.base[fld][i] = nv;
+      if (sa.host[fld]) sa.host[fld][(size_t)e * sa.host_ld + n] = nv;
     }
   }
 }
@@ -580,6 +582,7 @@ cudaError_t launch_rhs(int variant, const DevOps &op, const DevMesh &m, const Rh
   };
   if (variant == kLIN) {
     LinArgs la{b.su, b.sv, b.sh, b.g0, b.hh0};
+    if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
     mark(0);
     k_lin<<<grid, kThreads, 0, st>>>(op, m, la, sa);
     mark(1);
@@ -594,6 +597,7 @@ cudaError_t launch_rhs(int variant, const DevOps &op, const DevMesh &m, const Rh
     case kFS:
       mark(0);
       k_qphase<kFS><<<grid, kThreads, 0, st>>>(op, m, b.su, b.sv, b.q);
+      if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
       mark(1);
       k_nlvol<kFS><<<gridnl, kThreadsNl, 0, st>>>(op, m, na);
       mark(2);
@@ -603,6 +607,7 @@ cudaError_t launch_rhs(int variant, const DevOps &op, const DevMesh &m, const Rh
     case kNS:
       mark(0);
       k_qphase<kNS><<<grid, kThreads, 0, st>>>(op, m, b.su, b.sv, b.q);
+      if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
       mark(1);
       k_nlvol<kNS><<<gridnl, kThreadsNl, 0, st>>>(op, m, na);
       mark(2);
@@ -612,6 +617,7 @@ cudaError_t launch_rhs(int variant, const DevOps &op, const DevMesh &m, const Rh
     default:
       mark(0);
       k_qphase<kINV><<<grid, kThreads, 0, st>>>(op, m, b.su, b.sv, b.q);
+      if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
       mark(1);
       k_nlvol<kINV><<<gridnl, kThreadsNl, 0, st>>>(op, m, na);
       mark(2);

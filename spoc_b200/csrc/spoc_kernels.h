@@ -18,6 +18,10 @@ struct StageArgs {
   double *acc[3];   // du1 + 2 du2 + 2 du3
   double *tend[3];  // tendency output when stage < 0
   int *flag;        // set non-zero on a non-finite tendency
+  // stage 3 only, optional: the new state is also stored to these
+  // (ld-strided) arrays, mapped pinned host memory of the caller
+  double *host[3];
+  int host_ld;
 };
 
 struct NlArgs {
@@ -83,6 +87,9 @@ struct RhsBuffers {
   const double *hb, *w0, *z0, *fc;     // time-constant fields
   double *q, *f, *gx0, *gy0, *uh, *vh; // nonlinear intermediates
   double mu0, mb0, g0, hh0;
+  // optional: recorded when sh is in place (the kernels that read sh wait
+  // for it; the q-phase, which reads only su and sv, does not)
+  cudaEvent_t sh_ready = nullptr;
 };
 
 cudaError_t launch_rhs(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,

@@ -101,6 +101,36 @@ def test_rk4_host_entry_matches_resident(gpu_lib):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ld", [28, 45])
+@pytest.mark.parametrize("path", ["templated", "generic"])
+def test_rk4_host_entry_pinned_buffers(gpu_lib, ld, path):
+    """Mapped pinned caller arrays take the direct path (the last stage stores
+    the new state into them); the result is the resident run's, bit for bit,
+    and the rows past nm of an ld-strided array are left alone."""
+    import torch
+    p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 8), ld=ld)
+    s = W.make_solver(p)
+    s.set_kernel_path(path)
+    pin = [torch.from_numpy(a.copy()).pin_memory() for a in (p.u, p.v, p.h)]
+    host = [t.numpy() for t in pin]
+    for a in host:
+        a[:, p.T.nm:] = 7.0
+    s.rk4_steps_host(*host, p.dt, 3)
+    s2 = W.make_solver(p)
+    s2.set_kernel_path(path)
+    s2.set_state(p.u, p.v, p.h)
+    s2.rk4_steps(p.dt, 3)
+    assert_bitwise(host, s2.get_state(ld), p.T.nm)
+    assert all((a[:, p.T.nm:] == 7.0).all() for a in host)
+    # the handle's resident state is the new state as well
+    assert_bitwise(s.get_state(ld), s2.get_state(ld), p.T.nm)
+    # zero steps: the arrays come back unchanged
+    before = [a.copy() for a in host]
+    s.rk4_steps_host(*host, p.dt, 0)
+    assert all(np.array_equal(a, b) for a, b in zip(host, before))
+
+
+@pytest.mark.gpu
 def test_c1_full_1000_steps_bitwise(gpu_lib):
     """Configuration C1 as specified: 2048 triangles, p3, 1000 RK4 steps at the cfl.f step."""
     p = W.build_problem(W.CONFIGS["c1_lin_p3"])
