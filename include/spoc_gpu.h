@@ -126,7 +126,10 @@ int spoc_set_state(spoc_handle *h, int ld, const double *u, const double *v, con
 int spoc_get_state(spoc_handle *h, int ld, double *u, double *v, double *hh);
 /* nsteps classical RK4 steps on the resident state (src/shwwnl.f:233-286). */
 int spoc_rk4_steps(spoc_handle *h, double dt, int nsteps);
-/* H2D of (u,v,hh), nsteps RK4 steps, D2H back: the host-buffer entry point. */
+/* H2D of (u,v,hh), nsteps RK4 steps, D2H back: the host-buffer entry point.
+   With FP64 handles and mapped pinned arrays (cudaHostAlloc, cudaMallocHost,
+   registered memory) the last stage kernel stores the new state into the
+   arrays directly; only the rows' first nm values are written. */
 int spoc_rk4_steps_host(spoc_handle *h, int ld, double *u, double *v, double *hh, double dt,
                         int nsteps);
 /* Kinetic/potential energy and mass of the resident state (src/energy.f:3-96). */
