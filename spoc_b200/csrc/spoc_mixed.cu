@@ -55,6 +55,44 @@ __device__ __forceinline__ unsigned lane_mask() {
   return Dm::LW == 32 ? 0xffffffffu : (0xffffu << (threadIdx.x & 16));
 }
 
+// f(k, v) for k = k0..L-1 in order, v[c] = x[c][k] for NX shared vectors of
+// length L.  The entries are read W = 4 or 2 at a time (16- or 8-byte
+// broadcast loads) when W divides L; every x[c] must then be W-aligned.  The
+// arithmetic f does, and its order, do not depend on W.
+template <int L, int NX, class F>
+__device__ __forceinline__ void sweep(int k0, const float *const (&x)[NX], F &&f) {
+  constexpr int W = L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : 1);
+  const int kp = (k0 + W - 1) / W * W;
+  for (int k = k0; k < kp && k < L; ++k) {
+    float v[NX];
+#pragma unroll
+    for (int c = 0; c < NX; ++c) v[c] = x[c][k];
+    f(k, v);
+  }
+#pragma unroll 1
+  for (int k = kp; k < L; k += W) {
+    float v[W][NX];
+#pragma unroll
+    for (int c = 0; c < NX; ++c) {
+      if constexpr (W == 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(x[c] + k);
+        v[0][c] = t.x;
+        v[1][c] = t.y;
+        v[2][c] = t.z;
+        v[3][c] = t.w;
+      } else if constexpr (W == 2) {
+        const float2 t = *reinterpret_cast<const float2 *>(x[c] + k);
+        v[0][c] = t.x;
+        v[1][c] = t.y;
+      } else {
+        v[0][c] = x[c][k];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < W; ++j) f(k + j, v[j]);
+  }
+}
+
 // Trace record (mean-free traces, then the mean) of up to six fields held in
 // the warp's shared vectors x[f] (psi coefficients); written by lanes 0..TG.
 template <class Dm, int NF>
@@ -244,13 +282,13 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     if (lane < Q) {
       const int q = lane;
       float U = 0.f, V = 0.f, H = 0.f;
-#pragma unroll 4
-      for (int n = 0; n < N; ++n) {
+      const float *const x3[3] = {su, sv, sh};
+      sweep<N, 3>(0, x3, [&](int n, const float (&v)[3]) {
         const float p = o[Dm::PPT + n * Q + q];
-        U = fma32(p, su[n], U);
-        V = fma32(p, sv[n], V);
-        H = fma32(p, sh[n], H);
-      }
+        U = fma32(p, v[0], U);
+        V = fma32(p, v[1], V);
+        H = fma32(p, v[2], H);
+      });
       qp[q] = U;
       qp[Q + q] = V;
       qp[2 * Q + q] = H + a.hbq[(size_t)e * Q + q];
@@ -259,10 +297,11 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       constexpr int T = Q > Dm::LW ? Q - Dm::LW : 1;
       for (int c = lane; c < 3 * T; c += Dm::LW) {
         const int f = c / T, q = Dm::LW + c - f * T;
-        const float *x = f == 0 ? su : (f == 1 ? sv : sh);
+        const float *const x1[1] = {f == 0 ? su : (f == 1 ? sv : sh)};
         float acc = 0.f;
-#pragma unroll 4
-        for (int n = 0; n < N; ++n) acc = fma32(o[Dm::PPT + n * Q + q], x[n], acc);
+        sweep<N, 1>(0, x1, [&](int n, const float (&v)[1]) {
+          acc = fma32(o[Dm::PPT + n * Q + q], v[0], acc);
+        });
         qp[f * Q + q] = f == 2 ? acc + a.hbq[(size_t)e * Q + q] : acc;
       }
     }
@@ -275,14 +314,14 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       float gxu = 0.f, gyu = 0.f, gxv = 0.f, gyv = 0.f;
       float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
       if (i < N) {
-#pragma unroll 4
-        for (int k = 1; k < N; ++k) {  // constant mode: see the trace records
+        const float *const x2[2] = {su, sv};
+        sweep<N, 2>(1, x2, [&](int k, const float (&v)[2]) {  // constant mode: see the trace records
           const float cx = o[Dm::GX + k * N + i], cy = o[Dm::GY + k * N + i];
-          gxu = fma32(cx, su[k], gxu);
-          gyu = fma32(cy, su[k], gyu);
-          gxv = fma32(cx, sv[k], gxv);
-          gyv = fma32(cy, sv[k], gyv);
-        }
+          gxu = fma32(cx, v[0], gxu);
+          gyu = fma32(cy, v[0], gyu);
+          gxv = fma32(cx, v[1], gxv);
+          gyv = fma32(cy, v[1], gyv);
+        });
 #pragma unroll
         for (int l = 0; l < TG; ++l) {
           const float L = o[Dm::LIFT + l * N + i];
@@ -348,14 +387,14 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     if (lane < Q) {
       const int q = lane;
       float gxx = 0.f, gxy = 0.f, gyx = 0.f, gyy = 0.f;
-#pragma unroll 4
-      for (int n = 0; n < N; ++n) {
+      const float *const x4[4] = {sq, sq + N, sq + 2 * N, sq + 3 * N};
+      sweep<N, 4>(0, x4, [&](int n, const float (&v)[4]) {
         const float p = o[Dm::PPT + n * Q + q];
-        gxx = fma32(p, sq[n], gxx);
-        gxy = fma32(p, sq[N + n], gxy);
-        gyx = fma32(p, sq[2 * N + n], gyx);
-        gyy = fma32(p, sq[3 * N + n], gyy);
-      }
+        gxx = fma32(p, v[0], gxx);
+        gxy = fma32(p, v[1], gxy);
+        gyx = fma32(p, v[2], gyx);
+        gyy = fma32(p, v[3], gyy);
+      });
       qproducts(q, gxx, gxy, gyx, gyy);
     }
     if (Q > Dm::LW) {
@@ -366,8 +405,10 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       for (int c = lane; c < 4 * T; c += Dm::LW) {
         const int f = c / T, q = Dm::LW + c - f * T;
         float acc = 0.f;
-#pragma unroll 4
-        for (int n = 0; n < N; ++n) acc = fma32(o[Dm::PPT + n * Q + q], sq[f * N + n], acc);
+        const float *const x1[1] = {sq + f * N};
+        sweep<N, 1>(0, x1, [&](int n, const float (&v)[1]) {
+          acc = fma32(o[Dm::PPT + n * Q + q], v[0], acc);
+        });
         qp[(3 + f) * Q + q] = acc;
       }
       __syncwarp(lane_mask<Dm>());
@@ -383,14 +424,14 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       const int i = lane + Dm::LW * r;
       float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
       if (i < N) {
-#pragma unroll 4
-        for (int q = 0; q < Q; ++q) {
+        const float *const x4[4] = {qp + 3 * Q, qp + 4 * Q, qp + 5 * Q, qp + 6 * Q};
+        sweep<Q, 4>(0, x4, [&](int q, const float (&v)[4]) {
           const float p = o[Dm::PW + q * N + i];
-          s0 = fma32(p, qp[3 * Q + q], s0);
-          s1 = fma32(p, qp[4 * Q + q], s1);
-          s2 = fma32(p, qp[5 * Q + q], s2);
-          s3 = fma32(p, qp[6 * Q + q], s3);
-        }
+          s0 = fma32(p, v[0], s0);
+          s1 = fma32(p, v[1], s1);
+          s2 = fma32(p, v[2], s2);
+          s3 = fma32(p, v[3], s3);
+        });
       }
       bxr[r] = s0;
       byr[r] = s1;
@@ -426,16 +467,16 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       const int i = lane + Dm::LW * r;
       if (i >= N) continue;
       float gx = bxr[r], gy = byr[r], hp = 0.f;
-#pragma unroll 4
-      for (int k = 1; k < N; ++k) {  // constant mode: see the trace records
+      const float *const x6[6] = {vec, vec + N, vec + 2 * N, vec + 3 * N, vec + 4 * N, vec + 5 * N};
+      sweep<N, 6>(1, x6, [&](int k, const float (&v)[6]) {  // constant mode: see the trace records
         const float cx = o[Dm::GX + k * N + i], cy = o[Dm::GY + k * N + i];
-        gx = fma32(cx, vec[k], gx);
-        gx = fma32(cy, vec[N + k], gx);
-        gy = fma32(cx, vec[2 * N + k], gy);
-        gy = fma32(cy, vec[3 * N + k], gy);
-        hp = fma32(cx, vec[4 * N + k], hp);
-        hp = fma32(cy, vec[5 * N + k], hp);
-      }
+        gx = fma32(cx, v[0], gx);
+        gx = fma32(cy, v[1], gx);
+        gy = fma32(cx, v[2], gy);
+        gy = fma32(cy, v[3], gy);
+        hp = fma32(cx, v[4], hp);
+        hp = fma32(cy, v[5], hp);
+      });
       const size_t gi = (size_t)e * N + i;
       a.part[gi] = gx;
       a.part[fn + gi] = gy;
