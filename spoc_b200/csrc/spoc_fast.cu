@@ -645,8 +645,10 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
   // the coefficients of the warp's next element are copied into W.own / W.nb
   // while it works on the current one (the first copy overlaps the staging
   // of the operators)
-  Sides sd_next;
-  if (warp_global() < m.ne) {
+  // (one row per lane only: at two rows the registers are not there)
+  constexpr bool PF = Dm::R == 1;
+  Sides sd_next{};
+  if (PF && warp_global() < m.ne) {
     sd_next = sides_of(m, warp_global());
     prefetch_element<Dm, 2>(fields, warp_global(), sd_next, W.own, W.nb);
   }
@@ -654,14 +656,20 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
   __syncthreads();
   const size_t fs = (size_t)m.ne * N;
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
-    const Sides sd = sd_next;
+    const Sides sd = PF ? sd_next : sides_of(m, e);
     const int en = e + warp_count();
-    if (en < m.ne) sd_next = sides_of(m, en);
+    if (PF && en < m.ne) sd_next = sides_of(m, en);
     const Geo g = geo(m, e);
     int isg[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
-    cp_async_wait_all();
+    if constexpr (PF) {
+      cp_async_wait_all();
+    } else {
+      load_vec<Dm>(W.own, su, e);
+      load_vec<Dm>(W.own + N, sv, e);
+      stage_neighbours<Dm, 2>(sd, W.nb, [&](int f, int t, int i) { return fields[f][(size_t)t * N + i]; });
+    }
     __syncwarp();
     face_values<Dm, 2>(S.pf, m, sd, W.own, W.nb, W.fr);
     __syncwarp();
@@ -672,7 +680,7 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
     double ax[2][R], bx[2][R];
     matvec2<Dm, 2>(S.agx, S.agy, W.own, N, ax, bx);
     __syncwarp();  // W.own / W.nb are free from here on
-    if (en < m.ne) prefetch_element<Dm, 2>(fields, en, sd_next, W.own, W.nb);
+    if (PF && en < m.ne) prefetch_element<Dm, 2>(fields, en, sd_next, W.own, W.nb);
     double gq[4][R];  // gxx, gxy, gyx, gyy
 #pragma unroll
     for (int c = 0; c < 2; ++c)
@@ -900,22 +908,30 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
   // the coefficients of the warp's next element are copied into W.own / W.nb
   // while it works on the current one (the first copy overlaps the staging
   // of the operators)
-  Sides sd_next;
-  if (warp_global() < m.ne) {
+  // (one row per lane only: at two rows the registers are not there)
+  constexpr bool PF = Dm::R == 1;
+  Sides sd_next{};
+  if (PF && warp_global() < m.ne) {
     sd_next = sides_of(m, warp_global());
     prefetch_element<Dm, 6>(src, warp_global(), sd_next, W.own, W.nb);
   }
   stage_ops(S, op);
   __syncthreads();
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
-    const Sides sd = sd_next;
+    const Sides sd = PF ? sd_next : sides_of(m, e);
     const int en = e + warp_count();
-    if (en < m.ne) sd_next = sides_of(m, en);
+    if (PF && en < m.ne) sd_next = sides_of(m, en);
     const Geo g = geo(m, e);
     int isg[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
-    cp_async_wait_all();
+    if constexpr (PF) {
+      cp_async_wait_all();
+    } else {
+#pragma unroll
+      for (int f = 0; f < 6; ++f) load_vec<Dm>(W.own + f * N, src[f], e);
+      stage_neighbours<Dm, 6>(sd, W.nb, [&](int f, int t, int i) { return src[f][(size_t)t * N + i]; });
+    }
     __syncwarp();
     face_values<Dm, 6>(S.pf, m, sd, W.own, W.nb, W.fb);
     __syncwarp();
@@ -944,7 +960,7 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
     axpy<R>(hb, ax[5], -cbx);
     axpy<R>(hb, bx[5], cax);
     __syncwarp();  // W.own / W.nb are free from here on
-    if (en < m.ne) prefetch_element<Dm, 6>(src, en, sd_next, W.own, W.nb);
+    if (PF && en < m.ne) prefetch_element<Dm, 6>(src, en, sd_next, W.own, W.nb);
     double t[6][3][R];
     lift_sums<Dm, 6>(S, isg, W.fb, t);
     apply_lift<R>(gx, t[0], isg, g.detai);
