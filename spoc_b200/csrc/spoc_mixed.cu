@@ -307,9 +307,15 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     }
     // q = weak gradients of u, v (calvarnl_fs.f:115-164): cal_b with coeff -1,
     // geometry, then tri_f of the traces; the mass solve is the identity
+    // Rows past the last lane (degree 7: 4 of 36) would cost every row loop a
+    // second pass with a few lanes busy: their (output, row) chains are spread
+    // over the lanes instead, each summed in the same order.
+    constexpr int RL = R == 2 ? 1 : R;  // rows computed lane by lane
+    constexpr int T2 = R == 2 ? N - Dm::LW : 1;
+    static_assert(R == 1 || (8 * T2 <= 4 * Q && 4 * T2 <= N && 3 * T2 <= Dm::LW), "row tail");
     float qv[4][R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < RL; ++r) {
       const int i = lane + Dm::LW * r;
       float gxu = 0.f, gyu = 0.f, gxv = 0.f, gyv = 0.f;
       float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
@@ -335,6 +341,36 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       qv[1][r] = (bx * gxu - ax * gyu) * di + l1;
       qv[2][r] = (ay * gyv - by * gxv) * di + l2;
       qv[3][r] = (bx * gxv - ax * gyv) * di + l3;
+    }
+    if constexpr (R == 2) {
+      // chains c = out * T2 + t: out 0-3 the cal_b sums, 4-7 the lift sums of
+      // row LW + t, parked in the free qp slots of the products
+      float *cs = qp + 3 * Q;
+      for (int c = lane; c < 8 * T2; c += Dm::LW) {
+        const int out = c / T2, i = Dm::LW + c - out * T2;
+        float acc = 0.f;
+        if (out < 4) {
+          const int op = (out & 1) ? Dm::GY : Dm::GX;
+          const float *const x1[1] = {out < 2 ? su : sv};
+          sweep<N, 1>(1, x1, [&](int k, const float (&v)[1]) { acc = fma32(o[op + k * N + i], v[0], acc); });
+        } else {
+          const float *g = gl + (out - 4) * TG;
+#pragma unroll 9
+          for (int l = 0; l < TG; ++l) acc = fma32(o[Dm::LIFT + l * N + i], g[l], acc);
+        }
+        cs[c] = acc;
+      }
+      __syncwarp(lane_mask<Dm>());
+      const bool own = lane < T2;
+      const float gxu = own ? cs[lane] : 0.f, gyu = own ? cs[T2 + lane] : 0.f;
+      const float gxv = own ? cs[2 * T2 + lane] : 0.f, gyv = own ? cs[3 * T2 + lane] : 0.f;
+      const float l0 = own ? cs[4 * T2 + lane] : 0.f, l1 = own ? cs[5 * T2 + lane] : 0.f;
+      const float l2 = own ? cs[6 * T2 + lane] : 0.f, l3 = own ? cs[7 * T2 + lane] : 0.f;
+      qv[0][R - 1] = (ay * gyu - by * gxu) * di + l0;
+      qv[1][R - 1] = (bx * gxu - ax * gyu) * di + l1;
+      qv[2][R - 1] = (ay * gyv - by * gxv) * di + l2;
+      qv[3][R - 1] = (bx * gxv - ax * gyv) * di + l3;
+      __syncwarp(lane_mask<Dm>());
     }
     if (VAR == SPOC_FS && a.m.bdl[e]) {
       // calvarnl_fs.f:165-205: of the rotated tensor only the tangential-normal
@@ -420,7 +456,7 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     __syncwarp(lane_mask<Dm>());
     float bxr[R], byr[R], uh[R], vh[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < RL; ++r) {
       const int i = lane + Dm::LW * r;
       float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
       if (i < N) {
@@ -437,6 +473,23 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       byr[r] = s1;
       uh[r] = s2;
       vh[r] = s3;
+    }
+    if constexpr (R == 2) {
+      // the 4 T2 projections of the rows past the last lane as spread chains
+      for (int c = lane; c < 4 * T2; c += Dm::LW) {
+        const int out = c / T2, i = Dm::LW + c - out * T2;
+        float acc = 0.f;
+        const float *const x1[1] = {qp + (3 + out) * Q};
+        sweep<Q, 1>(0, x1, [&](int q, const float (&v)[1]) { acc = fma32(o[Dm::PW + q * N + i], v[0], acc); });
+        tmp[c] = acc;
+      }
+      __syncwarp(lane_mask<Dm>());
+      const bool own = lane < T2;
+      bxr[R - 1] = own ? tmp[lane] : 0.f;
+      byr[R - 1] = own ? tmp[T2 + lane] : 0.f;
+      uh[R - 1] = own ? tmp[2 * T2 + lane] : 0.f;
+      vh[R - 1] = own ? tmp[3 * T2 + lane] : 0.f;
+      __syncwarp(lane_mask<Dm>());
     }
     if (a.m.bdl[e]) {
       // uh, vh wall solves (calvarnl_fs.f:333-340, calvarnl_ns.f:249-265)
@@ -463,7 +516,7 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
     }
     __syncwarp(lane_mask<Dm>());
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < RL; ++r) {
       const int i = lane + Dm::LW * r;
       if (i >= N) continue;
       float gx = bxr[r], gy = byr[r], hp = 0.f;
@@ -481,6 +534,23 @@ __device__ __forceinline__ void vol_body(const MxArgs &a, float *sm, int blk, in
       a.part[gi] = gx;
       a.part[fn + gi] = gy;
       a.part[2 * fn + gi] = hp;
+    }
+    if constexpr (R == 2) {
+      // gx, gy, hp of the rows past the last lane: chains c = out * T2 + t,
+      // started from row LW + t's bxr / byr (held by lane t)
+      const int out = lane / T2, t = lane - out * T2;
+      const float b0 = __shfl_sync(lane_mask<Dm>(), bxr[R - 1], t);
+      const float b1 = __shfl_sync(lane_mask<Dm>(), byr[R - 1], t);
+      if (lane < 3 * T2) {
+        const int i = Dm::LW + t;
+        float acc = out == 0 ? b0 : (out == 1 ? b1 : 0.f);
+        const float *const x2[2] = {vec + 2 * out * N, vec + (2 * out + 1) * N};
+        sweep<N, 2>(1, x2, [&](int k, const float (&v)[2]) {
+          acc = fma32(o[Dm::GX + k * N + i], v[0], acc);
+          acc = fma32(o[Dm::GY + k * N + i], v[1], acc);
+        });
+        a.part[out * fn + (size_t)e * N + i] = acc;
+      }
     }
     // trace records of q and uh, vh for the face terms of phases C and D
     {
