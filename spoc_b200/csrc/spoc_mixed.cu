@@ -601,8 +601,9 @@ __device__ __forceinline__ void tend_body(const MxArgs &a, float *sm, int blk, i
     }
     __syncwarp(lane_mask<Dm>());
     float t[3][R];
+    constexpr int RL = R == 2 ? 1 : R;  // rows computed lane by lane
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < RL; ++r) {
       const int i = lane + Dm::LW * r;
       float gx = 0.f, gy = 0.f, hh = 0.f;
       if (i < N) {
@@ -622,6 +623,28 @@ __device__ __forceinline__ void tend_body(const MxArgs &a, float *sm, int blk, i
       t[1][r] = gy;
       t[2][r] = hh;
     }
+    if constexpr (R == 2) {
+      // rows past the last lane (degree 7: 4 of 36): the lift sums of row
+      // LW + t as chains on lanes out * T2 + t, in the same order, then
+      // gathered to lane t
+      constexpr int T2 = N - Dm::LW;
+      static_assert(3 * T2 <= Dm::LW, "row tail");
+      const int out = lane / T2, tt = lane - out * T2;
+      float acc = 0.f;
+      if (lane < 3 * T2) {
+        const int i = Dm::LW + tt;
+        acc = a.part[out * fn + (size_t)e * N + i];
+        const float *g = gl + out * TG;
+#pragma unroll 9
+        for (int l = 0; l < TG; ++l) acc = fma32(o[Dm::LIFT + l * N + i], g[l], acc);
+      }
+      const bool own = lane < T2;
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        const float v = __shfl_sync(lane_mask<Dm>(), acc, f * T2 + tt);
+        t[f][R - 1] = own ? v : 0.f;
+      }
+    }
     if (a.m.bdl[e]) {
       const float nx = (float)a.m.normt[2 * (size_t)e], ny = (float)a.m.normt[2 * (size_t)e + 1];
       wall_vec<Dm, VAR == SPOC_NS>(o, tmp, t[0], t[1], nx, ny);
@@ -640,7 +663,7 @@ __global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_tend(const MxArgs 
 
 // Linear variant (calvar_lin.f:7-287) in one kernel.
 template <class Dm>
-__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB) kx_lin(const MxArgs a) {
+__global__ void __launch_bounds__(32 * kMxWarps, Dm::MINB_LIN) kx_lin(const MxArgs a) {
   constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, R = Dm::R;
   extern __shared__ __align__(16) float sm[];
   float *o = sm;

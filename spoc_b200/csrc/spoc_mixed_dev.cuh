@@ -28,8 +28,10 @@ struct MDims {
   static constexpr int SLOTS = kMxWarps * 32 / LW;  // elements in flight per block
   static constexpr int R = (N + LW - 1) / LW;
   // resident blocks per SM the register budget is sized for (shared memory
-  // allows about 4 blocks of 8 warps at degree <= 6 and 3 at degree 7)
-  static constexpr int MINB = R == 1 ? 4 : 2;
+  // allows about 4 blocks of 8 warps at degree <= 6 and 3 at degree 7; the
+  // one-kernel linear variant keeps 2 at degree 7, where 3 would spill)
+  static constexpr int MINB = R == 1 ? 4 : 3;
+  static constexpr int MINB_LIN = R == 1 ? 4 : 2;
   // operator image in shared memory (floats)
   static constexpr int PPT = 0;               // [n*Q + q]  = Pp(q, n)
   static constexpr int PW = PPT + N * Q;      // [q*N + i]  = Pp(q, i) wi(q)
