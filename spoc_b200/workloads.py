@@ -547,6 +547,37 @@ def regrid_step(p: Problem, s: api.Solver, fac1: float, fac2: float, fac3: float
     return p1, s1, info
 
 
+def ensemble_adaptive_run(problems: list, solvers: list, nsteps: int, every: int, thresholds,
+                          graph: bool = True, layout=(4, 2), precision: str = "mixed"):
+    """An ensemble of adaptive runs: the members are stepped together (one
+    cooperative launch per RK4 stage for all of them, api.Ensemble) and every
+    `every` steps each member goes through the adaptive pass (regrid_step:
+    cal_conv's indicator on the device, coarsening and refinement through its
+    refinement history, interpol and verif_rot on the device); a member whose
+    mesh changed continues on a new handle with the new mesh's time step and
+    the ensemble is set up again for the new meshes.  `thresholds(i, p, s)`
+    gives member i's (fac1, fac2, fac3).  Returns (problems, solvers, log)."""
+    problems, solvers = list(problems), list(solvers)
+    log = []
+    done = 0
+    while done < nsteps:
+        k = min(every, nsteps - done)
+        ens = api.Ensemble(solvers)
+        ens.configure(*layout)
+        ens.steps([p.dt for p in problems], k, graph)
+        ens.close()
+        done += k
+        if done >= nsteps:
+            break
+        for i, (p, s) in enumerate(zip(problems, solvers)):
+            p1, s1, info = regrid_step(p, s, *thresholds(i, p, s), precision=precision)
+            if s1 is not s:
+                problems[i], solvers[i] = p1, s1
+                log.append({"step": done, "member": i, "ne_old": info["ne_old"], "ne_new": info["ne_new"],
+                            "refined": info["refined"], "coarsened": info["coarsened"]})
+    return problems, solvers, log
+
+
 # ---------------------------------------------------------------------------
 # compare.f: error of a state against the analytic standing wave
 # ---------------------------------------------------------------------------

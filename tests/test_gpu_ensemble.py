@@ -120,3 +120,37 @@ def test_ensemble_rejects_fp64_members():
     with pytest.raises(api.SpocError) as ei:
         api.Ensemble([solver(p, "fp64")])
     assert ei.value.code == 7
+
+
+@pytest.mark.gpu
+def test_adaptive_ensemble_matches_members_run_alone():
+    """Members regridded inside a batched run (refined where cal_conv flags
+    jumps) end where the same adaptive runs end one member at a time."""
+    ps = small_members()[1:]
+
+    def thresholds(i, p, s):
+        amax = np.maximum.reduce(s.checkconv())
+        return float(np.quantile(amax, 0.9)), 0.0, 1e300
+
+    runs = []
+    for mode in ("ensemble", "alone"):
+        mem = [solver(p) for p in ps]
+        if mode == "ensemble":
+            p2, s2, log = W.ensemble_adaptive_run(ps, mem, 6, 3, thresholds)
+        else:
+            p2, s2, log = list(ps), mem, []
+            for i in range(len(ps)):
+                s2[i].rk4_steps(p2[i].dt, 3)
+                q, t, info = W.regrid_step(p2[i], s2[i], *thresholds(i, p2[i], s2[i]), precision="mixed")
+                if t is not s2[i]:
+                    log.append({"member": i, "ne_new": info["ne_new"]})
+                p2[i], s2[i] = q, t
+                s2[i].rk4_steps(p2[i].dt, 3)
+        runs.append((p2, states(s2), log))
+    (pe, se, loge), (pa, sa, loga) = runs
+    assert len(loge) == len(ps) and [l["ne_new"] for l in loge] == [l["ne_new"] for l in loga]
+    for p in pe:
+        assert p.adapt is not None
+    for got, ref in zip(se, sa):
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)
