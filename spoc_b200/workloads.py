@@ -12,7 +12,9 @@ configuration is generated here from seeded inputs:
 """
 from __future__ import annotations
 
+import copy
 from dataclasses import dataclass, field
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -476,7 +478,6 @@ def adapt_tree(p: Problem, fconv: np.ndarray, fderaff: np.ndarray | None = None,
     the other elements.  Depth on the new mesh: calh2 of `bathymetry(x, y)`,
     or the constant depth of p (newinter, src/adapt.f:238-265); no wind.
     Returns (Problem without state, tinter, (pt_elem, pt_x, pt_y), info)."""
-    import copy
     cfg, T = p.cfg, p.T
     ld = p.hb.shape[1]
     tree0, used0, leaf0, half0 = p.adapt if p.adapt is not None else _base_adapt(p)
@@ -503,7 +504,6 @@ def adapt_tree(p: Problem, fconv: np.ndarray, fderaff: np.ndarray | None = None,
     remap = np.full(max(int(used0.max()), int(used.max())) + 1, -1, dtype=np.int64)
     remap[used] = np.arange(used.size)
     old_in_new = (remap[old_tree] + 1).astype(np.int32)
-    from types import SimpleNamespace
     tinter = api.inter_only_new(SimpleNamespace(ne=p.mesh.ne, inn=old_in_new), inn)
     loc = api.locate_points(p.mesh, mesh, tinter, T)
     if bathymetry is None:
