@@ -217,7 +217,25 @@ __device__ __forceinline__ Sides sides_of(const DevMesh &m, int e) {
   return s;
 }
 
-// Stage NF fields of the three neighbours: nb[(k*NF + f)*N + i].
+// Neighbour buffers hold side k's NF fields at nb + k * nb_stride: NF*N
+// doubles and the least padding (an even number of doubles, keeping 16-byte
+// pairs aligned) that puts the three sides' entries a face loop reads at once
+// in different shared-memory bank groups (unpadded, NF*N = 168 doubles is a
+// multiple of 128 bytes: a 3-way conflict on every neighbour load).
+__host__ __device__ constexpr bool nb_banks_apart(int s) {
+  // 16-byte groups (8 per 128 bytes) of offsets 0, s, 2s doubles
+  return (s % 2) ? (s % 16 != 0 && (2 * s) % 16 != 0)
+                 : ((s / 2) % 8 != 0 && s % 8 != 0 && (s / 2) % 8 != s % 8);
+}
+template <class Dm, int NF>
+__host__ __device__ constexpr int nb_stride() {
+  const int base = NF * Dm::N;
+  for (int pad = 0; pad < 16; pad += 2)
+    if (nb_banks_apart(base + pad)) return base + pad;
+  return base;
+}
+
+// Stage NF fields of the three neighbours: nb[k*nb_stride + f*N + i].
 template <class Dm, int NF, class Fetch>
 __device__ __forceinline__ void stage_neighbours(const Sides &sd, double *nb, Fetch fetch) {
   const int l = lane_id();
@@ -230,7 +248,7 @@ __device__ __forceinline__ void stage_neighbours(const Sides &sd, double *nb, Fe
 #pragma unroll
       for (int r = 0; r < Dm::R; ++r) {
         const int i = l + 32 * r;
-        if (i < Dm::N) nb[(k * NF + f) * Dm::N + i] = fetch(f, t, i);
+        if (i < Dm::N) nb[k * nb_stride<Dm, NF>() + f * Dm::N + i] = fetch(f, t, i);
       }
   }
 }
@@ -245,7 +263,7 @@ __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Start the copies of NF fields of element e and of its three neighbours into
-// own[f*N + i] and nb[(k*NF + f)*N + i] (the layouts of load_vec and
+// own[f*N + i] and nb[k*nb_stride + f*N + i] (the layouts of load_vec and
 // stage_neighbours); field f is read from fields[f].  The buffers must not be
 // read until cp_async_wait_all() and a __syncwarp().
 template <class Dm, int NF>
@@ -268,7 +286,8 @@ __device__ __forceinline__ void prefetch_element(const double *const (&fields)[N
 #pragma unroll
       for (int r = 0; r < Dm::R; ++r) {
         const int i = l + 32 * r;
-        if (i < Dm::N) cp_async8(nb + (k * NF + f) * Dm::N + i, fields[f] + (size_t)t * Dm::N + i);
+        if (i < Dm::N)
+          cp_async8(nb + k * nb_stride<Dm, NF>() + f * Dm::N + i, fields[f] + (size_t)t * Dm::N + i);
       }
   }
 }
@@ -295,7 +314,7 @@ __device__ __forceinline__ void face_values(const double *pf, const DevMesh &m, 
         for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], own[q * N + n], pv);
       }
     } else {
-      const double *nbk = nb + k * NF * N;
+      const double *nbk = nb + k * nb_stride<Dm, NF>();
       const double *a1 = sd.first[k] ? own : nbk;
       const double *a2 = sd.first[k] ? nbk : own;
       const int s1 = __ldg(m.ssit + 2 * f), s2 = __ldg(m.ssit + 2 * f + 1);
@@ -628,7 +647,7 @@ __device__ __forceinline__ void stage_update(const StageArgs &sa, int fld, int e
 template <class Dm>
 struct __align__(16) QWarp {
   double own[2 * Dm::N];
-  double nb[3 * 2 * Dm::N];
+  double nb[3 * nb_stride<Dm, 2>()];
   double fr[2 * 32];
   double fb[4 * 32];
   double sm[64];
@@ -892,7 +911,7 @@ __global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) 
 template <class Dm>
 struct __align__(16) TWarp {
   double own[6 * Dm::N];       // fxx, fxy, fyx, fyy, uh, vh
-  double nb[3 * 6 * Dm::N];
+  double nb[3 * nb_stride<Dm, 6>()];
   double fb[6 * 32];           // face values, then fbdxx, fbdxy, fbdyx, fbdyy, fbdx, fbdy
   double sm[64];
 };
@@ -1015,7 +1034,7 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
 template <class Dm>
 struct __align__(16) LWarp {
   double own[3 * Dm::N];  // fxx = -g0 h, u, v
-  double nb[3 * 3 * Dm::N];
+  double nb[3 * nb_stride<Dm, 3>()];
   double xs[2 * Dm::N];   // u*hh0, v*hh0
   double fr[3 * 32];
   double fb[4 * 32];      // fbdxx, fbdyy, fbdx, fbdy
