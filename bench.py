@@ -253,7 +253,7 @@ def model_counts(cfg, ne, nf):
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel on
 # the workload: profiles/kf_kernels_c2_fs_p6.md, profiles/kx_kernels_c3_inv_p7.md
 NCU_TRAFFIC = {
-    "c2_fs_p6:kf_qphase": 19170816, "c2_fs_p6:kf_nlvol": 104526080, "c2_fs_p6:kf_tend": 105928960,
+    "c2_fs_p6:kf_qphase": 19072768, "c2_fs_p6:kf_nlvol": 103480320, "c2_fs_p6:kf_tend": 105977088,
     "c3_inv_p7:kx_vol": 246406656, "c3_inv_p7:kx_tend": 468452864,
     "c3_inv_p7:kt_vol": 250172160,
 }
