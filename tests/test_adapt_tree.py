@@ -201,3 +201,44 @@ def test_refining_next_to_a_coarser_leaf_refines_it_first():
     tree.mesh()                                   # raises if a rule were broken
     levels = [tree.level[t] for t in tree.leaves()]
     assert max(levels) == 2
+
+
+def test_refinement_at_the_walls_and_back():
+    """Refinement that reaches the walls and a corner (wall edges split, the
+    corner fix rotating wall elements), then coarsening back: conforming
+    meshes, valid mesh pointers, polynomials re-projected exactly, and the
+    base mesh again at the end."""
+    p, OT = _problem()
+    L = p.cfg.length
+
+    def wall_flags(mesh, d):
+        cy = mesh.ygr[mesh.inn - 1].mean(axis=1)
+        cx = mesh.xgr[mesh.inn - 1].mean(axis=1)
+        return (cy < -0.5 * L + d * L) | ((cx > 0.5 * L - d * L) & (cy > 0.5 * L - d * L))
+
+    def f(x, y):
+        s, t = x / L, y / L
+        return 0.3 + s - 2 * t + s * t + s ** p.cfg.nc - 0.5 * t ** p.cfg.nc
+
+    q, passes = p, []
+    for d in (0.15, 0.08):
+        q1, t1, _, i1 = W.adapt_tree(q, wall_flags(q.mesh, d))
+        assert i1["refined"] > 0
+        ok, _ = _conforming(q1.mesh)
+        M0, M1 = _omesh(p, q.mesh), _omesh(p, q1.mesh)
+        assert ok and M1.check == 0 and M1.its_rc == 0
+        a0, _, _ = O.calh(OT, M0, f)
+        a1, _, _ = O.calh(OT, M1, f)
+        got, *_ = O.interpol(OT, M0, M1, t1, a0)
+        assert O.mass_norm(OT, M1, got - a1) < 1e-11 * O.mass_norm(OT, M1, a1)
+        q = q1
+    assert _conforming(q.mesh)[1] > _conforming(p.mesh)[1]   # wall edges were split
+    for _ in range(4):
+        z = np.zeros(q.mesh.ne, bool)
+        q1, t1, _, i1 = W.adapt_tree(q, z, ~z)
+        if i1["coarsened"] == 0:
+            break
+        M1 = _omesh(p, q1.mesh)
+        assert _conforming(q1.mesh)[0] and M1.check == 0 and M1.its_rc == 0
+        q = q1
+    assert _tri_set(q.mesh) == _tri_set(p.mesh)
