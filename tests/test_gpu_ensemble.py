@@ -125,32 +125,41 @@ def test_ensemble_rejects_fp64_members():
 @pytest.mark.gpu
 def test_adaptive_ensemble_matches_members_run_alone():
     """Members regridded inside a batched run (refined where cal_conv flags
-    jumps) end where the same adaptive runs end one member at a time."""
+    jumps, then coarsened back once every element is flagged calm) end where
+    the same adaptive runs end one member at a time."""
     ps = small_members()[1:]
 
     def thresholds(i, p, s):
-        amax = np.maximum.reduce(s.checkconv())
-        return float(np.quantile(amax, 0.9)), 0.0, 1e300
+        if p.adapt is None:  # first pass: refine the jumpiest 10 %
+            amax = np.maximum.reduce(s.checkconv())
+            return float(np.quantile(amax, 0.9)), 0.0, 1e300
+        return 1e300, 1e300, 1e301  # second pass: everything calm
 
     runs = []
     for mode in ("ensemble", "alone"):
         mem = [solver(p) for p in ps]
         if mode == "ensemble":
-            p2, s2, log = W.ensemble_adaptive_run(ps, mem, 6, 3, thresholds)
+            p2, s2, log = W.ensemble_adaptive_run(ps, mem, 9, 3, thresholds)
         else:
             p2, s2, log = list(ps), mem, []
             for i in range(len(ps)):
-                s2[i].rk4_steps(p2[i].dt, 3)
-                q, t, info = W.regrid_step(p2[i], s2[i], *thresholds(i, p2[i], s2[i]), precision="mixed")
-                if t is not s2[i]:
-                    log.append({"member": i, "ne_new": info["ne_new"]})
-                p2[i], s2[i] = q, t
+                for _ in range(2):
+                    s2[i].rk4_steps(p2[i].dt, 3)
+                    q, t, info = W.regrid_step(p2[i], s2[i], *thresholds(i, p2[i], s2[i]),
+                                               precision="mixed")
+                    if t is not s2[i]:
+                        log.append({"member": i, "ne_new": info["ne_new"],
+                                    "coarsened": info["coarsened"]})
+                    p2[i], s2[i] = q, t
                 s2[i].rk4_steps(p2[i].dt, 3)
         runs.append((p2, states(s2), log))
     (pe, se, loge), (pa, sa, loga) = runs
-    assert len(loge) == len(ps) and [l["ne_new"] for l in loge] == [l["ne_new"] for l in loga]
-    for p in pe:
-        assert p.adapt is not None
+    assert len(loge) == 2 * len(ps)
+    key = lambda l: (l["member"], l["ne_new"], l["coarsened"])
+    assert sorted(map(key, loge)) == sorted(map(key, loga))
+    assert all(l["coarsened"] > 0 for l in loge if l["step"] == 6)
+    for p, p0 in zip(pe, ps):  # back to the base meshes
+        assert p.adapt is not None and p.mesh.ne == p0.mesh.ne
     for got, ref in zip(se, sa):
         for a, b in zip(got, ref):
             assert np.array_equal(a, b)
