@@ -17,6 +17,8 @@
 // or face points.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "spoc_device.cuh"
 #include "spoc_kernels.h"
 
@@ -48,6 +50,9 @@ struct Dims {
   static constexpr int G = G_;
   static constexpr int R = (N + 31) / 32;    // modal rows per lane
   static constexpr int RQ = (Q + 31) / 32;   // quadrature rows per lane
+  // threads per block of the tendency kernel: its per-warp scratch leaves
+  // room for 6 warps at two rows per lane (two blocks per SM)
+  static constexpr int TEND_THREADS = R == 1 ? 256 : 192;
   static constexpr int TRI = N * (N + 1) / 2;
   static constexpr int TRIR = NMR * (NMR + 1) / 2;
   static_assert(3 * G <= 32, "face points must fit one warp");
@@ -654,7 +659,7 @@ struct __align__(16) QWarp {
 };
 
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const double *__restrict__ su,
+__device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *__restrict__ su,
                                                  const double *__restrict__ sv, double *q) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
@@ -752,7 +757,7 @@ struct __align__(16) BWarp {
 };
 
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) {
+__device__ __forceinline__ void nlvol_body(DevOps op, DevMesh m, NlArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOpsQ<Dm> &S = *reinterpret_cast<SOpsQ<Dm> *>(smem);
   BWarp<Dm> &W = reinterpret_cast<BWarp<Dm> *>(smem + sizeof(SOpsQ<Dm>))[warp_in_block()];
@@ -917,7 +922,7 @@ struct __align__(16) TWarp {
 };
 
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
+__device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
   TWarp<Dm> &W = reinterpret_cast<TWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
@@ -1026,6 +1031,51 @@ __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a,
     stage_update<Dm>(sa, 2, e, hb);
     __syncwarp();
   }
+}
+
+// The nonlinear kernels.  At one row per lane the registers are left to the
+// compiler (about 120); at two rows per lane (degree 7) they are held to two
+// resident blocks per SM (kf_tend: 6 warps per block, which its per-warp
+// scratch allows), trading a few spilled words for twice the resident warps.
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const double *__restrict__ su,
+                                                 const double *__restrict__ sv, double *q) {
+  qphase_body<Dm, VAR>(op, m, su, sv, q);
+}
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256, 2) kf_qphase_r2(DevOps op, DevMesh m,
+                                                       const double *__restrict__ su,
+                                                       const double *__restrict__ sv, double *q) {
+  qphase_body<Dm, VAR>(op, m, su, sv, q);
+}
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) {
+  nlvol_body<Dm, VAR>(op, m, a);
+}
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256, 2) kf_nlvol_r2(DevOps op, DevMesh m, NlArgs a) {
+  nlvol_body<Dm, VAR>(op, m, a);
+}
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
+  tend_body<Dm, VAR>(op, m, a, sa);
+}
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(Dm::TEND_THREADS, 2) kf_tend_r2(DevOps op, DevMesh m, TendArgs a,
+                                                                  StageArgs sa) {
+  tend_body<Dm, VAR>(op, m, a, sa);
+}
+template <class Dm, int VAR>
+constexpr auto qphase_kernel() {
+  if constexpr (Dm::R == 1) return kf_qphase<Dm, VAR>; else return kf_qphase_r2<Dm, VAR>;
+}
+template <class Dm, int VAR>
+constexpr auto nlvol_kernel() {
+  if constexpr (Dm::R == 1) return kf_nlvol<Dm, VAR>; else return kf_nlvol_r2<Dm, VAR>;
+}
+template <class Dm, int VAR>
+constexpr auto tend_kernel() {
+  if constexpr (Dm::R == 1) return kf_tend<Dm, VAR>; else return kf_tend_r2<Dm, VAR>;
 }
 
 // ---------------------------------------------------------------------------
@@ -1180,26 +1230,29 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   if (ne_cached != m.ne) {
     wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
     wb = pick_warps(sizeof(SOpsQ<Dm>), sizeof(BWarp<Dm>));
-    wt = pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>));
+    wt = std::min(pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>)), Dm::TEND_THREADS / 32);
     sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
     sb = sizeof(SOpsQ<Dm>) + wb * sizeof(BWarp<Dm>);
     stt = sizeof(SOps<Dm>) + wt * sizeof(TWarp<Dm>);
-    cudaError_t e = prepare(kf_qphase<Dm, VAR>, sq);
-    if (e == cudaSuccess) e = prepare(kf_nlvol<Dm, VAR>, sb);
-    if (e == cudaSuccess) e = prepare(kf_tend<Dm, VAR>, stt);
+    cudaError_t e = prepare(qphase_kernel<Dm, VAR>(), sq);
+    if (e == cudaSuccess) e = prepare(nlvol_kernel<Dm, VAR>(), sb);
+    if (e == cudaSuccess) e = prepare(tend_kernel<Dm, VAR>(), stt);
     if (e != cudaSuccess) return e;
-    gq = resident_grid(kf_qphase<Dm, VAR>, 32 * wq, sq, sms, m.ne, wq);
-    gb = resident_grid(kf_nlvol<Dm, VAR>, 32 * wb, sb, sms, m.ne, wb);
-    gt = resident_grid(kf_tend<Dm, VAR>, 32 * wt, stt, sms, m.ne, wt);
+    gq = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq);
+    gb = resident_grid(nlvol_kernel<Dm, VAR>(), 32 * wb, sb, sms, m.ne, wb);
+    gt = resident_grid(tend_kernel<Dm, VAR>(), 32 * wt, stt, sms, m.ne, wt);
     ne_cached = m.ne;
   }
   mark(0);
-  kf_qphase<Dm, VAR><<<gq, 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
+  const auto kq = qphase_kernel<Dm, VAR>();
+  const auto kb = nlvol_kernel<Dm, VAR>();
+  const auto kt = tend_kernel<Dm, VAR>();
+  kq<<<gq, 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
   if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
   mark(1);
-  kf_nlvol<Dm, VAR><<<gb, 32 * wb, sb, st>>>(op, m, na);
+  kb<<<gb, 32 * wb, sb, st>>>(op, m, na);
   mark(2);
-  kf_tend<Dm, VAR><<<gt, 32 * wt, stt, st>>>(op, m, ta, sa);
+  kt<<<gt, 32 * wt, stt, st>>>(op, m, ta, sa);
   mark(3);
   return cudaGetLastError();
 }
@@ -1214,12 +1267,13 @@ cudaError_t run_q(const DevOps &op, const DevMesh &m, const double *su, const do
   if (ne_cached != m.ne) {
     wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
     sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
-    cudaError_t e = prepare(kf_qphase<Dm, VAR>, sq);
+    cudaError_t e = prepare(qphase_kernel<Dm, VAR>(), sq);
     if (e != cudaSuccess) return e;
-    gq = resident_grid(kf_qphase<Dm, VAR>, 32 * wq, sq, sms, m.ne, wq);
+    gq = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq);
     ne_cached = m.ne;
   }
-  kf_qphase<Dm, VAR><<<gq, 32 * wq, sq, st>>>(op, m, su, sv, q);
+  const auto kq = qphase_kernel<Dm, VAR>();
+  kq<<<gq, 32 * wq, sq, st>>>(op, m, su, sv, q);
   return cudaGetLastError();
 }
 
