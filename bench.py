@@ -24,11 +24,13 @@ OpenMP over all host cores) on the same workload: rank 0 only.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -45,6 +47,25 @@ def workload_desc(cfg, ne, nm):
     return (f"{cfg.name}: cal_var {cfg.variant} degree {cfg.nc} (nm={nm}), tri2_{cfg.ng}/legen{cfg.ngf}, "
             f"2x{cfg.n}x{cfg.n}={ne} triangles (jitter {cfg.jitter}), {cfg.length / 1e3:.0f} km basin, "
             f"f0={cfg.f0}, beta={cfg.beta}, mu0={cfg.mu0}, mb0={cfg.mb0}, H={cfg.depth}, ic={cfg.ic}")
+
+
+PRECISION_DESC = {
+    "fp64": "fp64, reference operation order (GPU bit-exact to the CPU oracle)",
+    "fp64_fma": "fp64 with fused multiply-adds (not bit-exact)",
+    "mixed": "FP32 contractions in the orthonormal basis, FP64 RK4 state",
+}
+
+
+def workload_config(cfg, ne, nm, dt, precision, n_gpus):
+    """The `config` object of both arms (identical on both for the same
+    workload, precision and GPU count)."""
+    return {"workload": workload_desc(cfg, ne, nm), "ne": ne, "nm": nm, "dt": dt,
+            "precision": PRECISION_DESC[precision],
+            "l2": "GPU arm: L2 flushed (256 MiB write) before every timed step; "
+                  "CPU arm: no flush (the state, 22 MB per field at C2, streams from DRAM)",
+            "parallelism": (f"replicas x{n_gpus} (GPU arm); CPU arm on rank 0's host cores"
+                            if n_gpus > 1 else
+                            "single device (GPU arm: one GPU; CPU arm: OpenMP over the host cores)")}
 
 
 def model_counts_mixed(cfg, ne):
@@ -146,7 +167,8 @@ def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, ts
         "kernel_ms_per_launch": per_launch,
         "roofline": {"kernel": dom, "bound": "fp32", "achieved": fl / dur / 1e12, "peak": fp32,
                      "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp32,
-                     "hbm_gbs": by / dur / 1e9, "traffic": NCU_TRAFFIC.get(f"{name}:{dom}"),
+                     "hbm_gbs": by / dur / 1e9, "traffic": ncu_traffic(name, dom)[0],
+                     "traffic_note": ncu_traffic(name, dom)[1],
                      "peak_source": "measured live: spoc_fp64_peak mode 2 (FP32 FMA chains)"},
         "tensor_core_path": {
             "volume_kernel": "kt_vol: tcgen05 TF32 MMAs (3-term split), accumulators in TMEM",
@@ -155,8 +177,22 @@ def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, ts
             "rel_l2_error_vs_fp64": errs("mixed_tensor"),
             "energy_drift": drift["mixed_tensor"],
             "kernel_ms_per_launch": per_launch_tc,
-            "traffic_kt_vol": NCU_TRAFFIC.get(f"{name}:kt_vol")},
+            "traffic_kt_vol": ncu_traffic(name, "kt_vol")[0]},
     }
+
+
+MIXED_RUNS = {"c1_lin_p3": 1000, "c2_fs_p6": 2000, "c4_ns_p4": 200}
+
+
+def mixed_errors_all(W):
+    """Mixed-precision form against FP64 on C1, C2 and C4 at their full sizes
+    and run lengths (C3 in mixed_measure, C5 in ensemble_measure): relative L2
+    errors of u, v, eta and both runs' energy drift."""
+    out = {}
+    for name, steps in MIXED_RUNS.items():
+        p = W.build_problem(W.CONFIGS[name])
+        out[name] = W.precision_errors(p, steps)
+    return out
 
 
 def ensemble_measure(torch, stream, W, api, replicas, rank=0, world=1, count=64, steps=500):
@@ -193,23 +229,27 @@ def ensemble_measure(torch, stream, W, api, replicas, rank=0, world=1, count=64,
     dof = sum(3.0 * p.T.nm * p.mesh.ne for p in ps)
     # members split across GPUs (replicas): all ranks' work over the slowest time
     ms_all, units = replicas.reduce_throughput(ms, dof * steps, world, "cuda")
-    errs = []
+    errs, uv_errs, drifts = [], [], []
     for p, s in zip(ps, mem):
-        f = W.make_solver(p, "fp64")
-        f.set_state(p.u, p.v, p.h)
-        f.rk4_steps(p.dt, steps)
+        ref = W.run_steps(p, "fp64", steps)
         mn = mnorm_factory(p)
-        x, y = s.get_state()[2], f.get_state()[2]
-        errs.append(mn(x - y) / mn(y))
-        f.close()
+        got = s.get_state()
+        e = [mn(got[i] - ref[0][i]) / mn(ref[0][i]) for i in range(3)]
+        errs.append(e[2])
+        uv_errs.append(max(e[0], e[1]))
+        e_end = s.energy()
+        drifts.append((W.energy_drift(ref[1], ref[2]), W.energy_drift(ref[1], e_end)))
     ens.close()
     for s in mem:
         s.close()
     if world > 1:
         import torch.distributed as dist
         gathered = [None] * world
-        dist.all_gather_object(gathered, errs)
-        errs = [e for g in gathered for e in g]
+        dist.all_gather_object(gathered, (errs, uv_errs, drifts))
+        errs = [e for g in gathered for e in g[0]]
+        uv_errs = [e for g in gathered for e in g[1]]
+        drifts = [e for g in gathered for e in g[2]]
+    ddiff = [abs(m - f) for f, m in drifts]
     ne = np.array([p.mesh.ne for p in ps])
     mb = np.array(info["member_blocks"])
     return {
@@ -227,8 +267,148 @@ def ensemble_measure(torch, stream, W, api, replicas, rank=0, world=1, count=64,
                       "elements_per_warp": {"degree 3-4": 2, "degree 5-6": 1}},
         "eta_rel_l2_error_vs_fp64": {"max": float(max(errs)), "median": float(np.median(errs)),
                                      "members": [float(e) for e in errs]},
+        "uv_rel_l2_error_vs_fp64": {"max": float(max(uv_errs)),
+                                    "median": float(np.median(uv_errs))},
+        "energy_drift": {"fp64_median": float(np.median([f for f, _ in drifts])),
+                         "mixed_median": float(np.median([m for _, m in drifts])),
+                         "max_abs_difference": float(max(ddiff))},
         "host_setup_s": build_s,
     }
+
+
+def host_rk4_step(rhs, u0, v0, h0, dt, w):
+    """One RK4 step driven the way the reference's loop drives cal_var
+    (src/shwwnl.f:233-284): four right-hand sides on host arrays, the stage
+    states and the final combination computed on the host in the same
+    operation order (numpy, in place; w holds the work arrays)."""
+    x0 = (u0, v0, h0)
+    d = w["d"]
+    y = w["y"]
+    t = w["t"]
+    for k in range(4):
+        rhs(*(x0 if k == 0 else y), *d[k])
+        if k < 3:
+            for f in range(3):
+                np.multiply(d[k][f], dt, out=t)
+                if k < 2:
+                    np.multiply(t, 0.5, out=t)
+                np.add(x0[f], t, out=y[f])
+    dt6 = dt / 6.0
+    for f in range(3):
+        np.multiply(d[1][f], 2.0, out=t)
+        np.add(d[0][f], t, out=t)
+        np.multiply(d[2][f], 2.0, out=y[f])
+        np.add(t, y[f], out=t)
+        np.add(t, d[3][f], out=t)
+        np.multiply(t, dt6, out=t)
+        np.add(x0[f], t, out=x0[f])
+
+
+def drop_in_measure(torch, W, api, p, steps=5):
+    """The literal drop-in, driven as the Fortran driver drives it: every RK4
+    step makes four cal_var calls on host arrays and does the stage AXPYs on
+    the host.  Two entries: cal_var_ (the reference's 31 by-reference
+    arguments, arrays with the reference's leading dimension nnmod = 45,
+    pageable memory) and the handle entry spoc_cal_var (packed ld = nm arrays
+    in pinned memory).  Host wall clock, synchronous calls; the final state
+    is checked bit for bit against the device-resident run."""
+    import ctypes as C
+    cfg, m = p.cfg, p.mesh
+    ne, nm, ld = m.ne, p.T.nm, 45
+    dof = 3.0 * nm * ne
+
+    def pad(a):
+        out = np.zeros((ne, ld))
+        out[:, :nm] = a[:, :nm]
+        return out
+
+    # reference: the device-resident path from the same state
+    s = W.make_solver(p)
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, steps + 1)
+    ref = s.get_state()
+    s.close()
+    res = {}
+    # ---- cal_var_ (31 by-reference arguments), ld = 45, pageable ----
+    lib = api.load_library()
+    T45 = p.T
+    ts = T45.struct()
+    assert lib.spoc_register_commons(C.byref(ts), api.VARIANTS[cfg.variant], api.FP64) == 0
+    keep = []
+
+    def ints(x):
+        keep.append(C.c_int(x))
+        return C.c_void_p(C.addressof(keep[-1]))
+
+    def dbl(x):
+        keep.append(C.c_double(x))
+        return C.c_void_p(C.addressof(keep[-1]))
+
+    ptr = lambda a: C.c_void_p(a.ctypes.data)
+    fc, w0, z0, hb = (pad(a) for a in (p.fc, p.w0, p.z0, p.hb))
+    pbdl = np.zeros(ne, np.int32)
+    pint = np.zeros(ne, np.int32)
+    fixed = dict(tseg=ptr(m.tseg), pseg=ptr(m.pseg), ssit=ptr(m.ssit), itm=ptr(m.itm),
+                 its=ptr(m.its), norm=ptr(m.norm), bdl=ptr(m.bdl), cip=ptr(T45.cip),
+                 vect=ptr(m.vect), normt=ptr(m.normt))
+
+    def cal_var_(u0, v0, h0, u1, v1, h1):
+        lib.cal_var_(ints(m.nf), ints(ne), ptr(u0), ptr(v0), ptr(h0), ptr(u1), ptr(v1), ptr(h1),
+                     fixed["tseg"], fixed["pseg"], fixed["ssit"], fixed["itm"], fixed["its"],
+                     fixed["norm"], ints(0), ptr(pbdl), ints(0), ptr(pint), fixed["bdl"],
+                     fixed["cip"], fixed["vect"], fixed["normt"], dbl(cfg.mu0), dbl(cfg.mb0),
+                     ptr(fc), dbl(cfg.beta), ptr(w0), ptr(z0), dbl(cfg.g0), ptr(hb), dbl(0.0))
+        del keep[:]
+        if lib.spoc_cal_var_status()[0] != 0:
+            raise RuntimeError("cal_var_ failed: " + str(lib.spoc_last_error()))
+
+    def run(rhs, alloc):
+        x = [alloc(a) for a in (p.u, p.v, p.h)]
+        w = {"d": [[alloc(None) for _ in range(3)] for _ in range(4)],
+             "y": [alloc(None) for _ in range(3)], "t": alloc(None)}
+        host_rk4_step(rhs, *x, p.dt, w)  # warm-up (upload of the mesh on the first call)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            host_rk4_step(rhs, *x, p.dt, w)
+        sec = time.perf_counter() - t0
+        same = all(np.array_equal(x[i][:, :nm], ref[i][:, :nm]) for i in range(3))
+        return sec, same
+
+    sec, same = run(cal_var_, lambda a: pad(a) if a is not None else np.zeros((ne, ld)))
+    lib.spoc_release_commons()
+    res["cal_var_"] = {
+        "value": dof * steps / sec, "unit": UNIT, "ms_per_step": 1e3 * sec / steps,
+        "h2d_bytes_per_step": 4 * 3 * ne * nm * 8, "d2h_bytes_per_step": 4 * 3 * ne * nm * 8,
+        "arrays": "pageable numpy, leading dimension 45 (nnmod)",
+        "bitwise_equal_to_device_resident_run": same}
+    # ---- spoc_cal_var (handle), ld = nm, pinned ----
+    s = W.make_solver(p)
+
+    def pinned(a):
+        t = torch.zeros((ne, nm), dtype=torch.float64).pin_memory()
+        if a is not None:
+            t.numpy()[...] = a[:, :nm]
+        keep_pin.append(t)
+        return t.numpy()
+
+    keep_pin = []
+
+    def handle_rhs(u0, v0, h0, u1, v1, h1):
+        api._check(api.load_library().spoc_cal_var(s._h, nm, api._d(u0), api._d(v0), api._d(h0),
+                                                   api._d(u1), api._d(v1), api._d(h1)),
+                   "cal_var")
+
+    sec, same = run(handle_rhs, pinned)
+    s.close()
+    res["spoc_cal_var"] = {
+        "value": dof * steps / sec, "unit": UNIT, "ms_per_step": 1e3 * sec / steps,
+        "h2d_bytes_per_step": 4 * 3 * ne * nm * 8, "d2h_bytes_per_step": 4 * 3 * ne * nm * 8,
+        "arrays": "pinned, packed (ld = nm)",
+        "bitwise_equal_to_device_resident_run": same}
+    res["note"] = ("4 cal_var calls per RK4 step on host arrays, stage AXPYs on the host "
+                   f"(numpy); host wall clock over {steps} steps after one warm-up step")
+    return res
 
 
 def model_counts(cfg, ne, nf):
@@ -250,13 +430,38 @@ def model_counts(cfg, ne, nf):
     }
 
 
-# DRAM bytes (read + write) per launch from one ncu capture of the kernel on
-# the workload: profiles/kf_kernels_c2_fs_p6.md, profiles/kx_kernels_c3_inv_p7.md
+# DRAM bytes (read + write) per launch of a kernel on a workload, each from one
+# ncu capture of that kernel, with the SHA-256 prefix of the kernel's source
+# file at the capture: a figure is reported only while the source is unchanged
+# (otherwise `traffic` is null, since it would describe another version).
+KERNEL_SOURCE = {"kf_": "spoc_fast.cu", "kx_": "spoc_mixed.cu", "kt_": "spoc_mixed_tc.cu"}
 NCU_TRAFFIC = {
-    "c2_fs_p6:kf_qphase": 19072768, "c2_fs_p6:kf_nlvol": 103480320, "c2_fs_p6:kf_tend": 105977088,
-    "c3_inv_p7:kx_vol": 246406656, "c3_inv_p7:kx_tend": 468452864,
-    "c3_inv_p7:kt_vol": 250172160,
+    "c2_fs_p6:kf_qphase": (19072768, None), "c2_fs_p6:kf_nlvol": (103480320, None),
+    "c2_fs_p6:kf_tend": (105977088, None),
+    "c3_inv_p7:kx_vol": (246406656, None), "c3_inv_p7:kx_tend": (468452864, None),
+    "c3_inv_p7:kt_vol": (250172160, None),
 }
+
+
+def source_digest(kernel: str):
+    for prefix, fname in KERNEL_SOURCE.items():
+        if kernel.startswith(prefix):
+            data = (ROOT / "spoc_b200" / "csrc" / fname).read_bytes()
+            return hashlib.sha256(data).hexdigest()[:16]
+    return None
+
+
+def ncu_traffic(config: str, kernel: str):
+    """(bytes per launch, note): the ncu figure if it was captured on this
+    version of the kernel's source, else (None, why)."""
+    ent = NCU_TRAFFIC.get(f"{config}:{kernel}")
+    if ent is None:
+        return None, "no ncu capture of this kernel on this workload"
+    nbytes, digest = ent
+    now = source_digest(kernel)
+    if digest is None or digest != now:
+        return None, f"ncu capture predates the current kernel source ({now})"
+    return nbytes, f"ncu dram__bytes_read.sum + dram__bytes_write.sum, kernel source {now}"
 
 
 def sample_clocks_start(out: Path):
@@ -301,22 +506,20 @@ def sample_clocks_stop(proc, fh, out: Path, gpu_index: int):
 
 
 def run_reference(args, cfg, rank):
-    """CPU restatement of the reference (oracle/), all host threads, rank 0 only."""
+    """CPU restatement of the reference (oracle/), all host threads, rank 0
+    only.  The workload is set up by the oracle itself (oracle.problems): the
+    CUDA library is not loaded by this arm."""
     if rank != 0:
         return
     from oracle import oracle as O
-    from spoc_b200 import workloads as W
+    from oracle.problems import oracle_problem
 
-    p = W.build_problem(cfg)
-    T = p.T
-    OT = O.Tables(cfg.nc, cfg.ng, cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
-    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, cfg.nc, cfg.f0, cfg.beta)
+    P = oracle_problem(cfg)
     threads = O.default_threads()
-    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    u, v, h = P.u.copy(), P.v.copy(), P.h.copy()
 
     def step():
-        O.rk4(cfg.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, cfg.mu0, cfg.mb0, cfg.g0,
-              p.dt, 1, threads)
+        P.rk4(u, v, h, 1, threads)
 
     nwarm = max(1, args.warmup)
     t0 = time.perf_counter()
@@ -329,13 +532,14 @@ def run_reference(args, cfg, rank):
     for _ in range(k):
         step()
     sec = time.perf_counter() - t0
-    dof = 3.0 * T.nm * p.mesh.ne
+    ne, nm = P.M.ne, P.T.nm
+    dof = 3.0 * nm * ne
     val = dof * k / sec
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": k, "warmup": nwarm, "ms_per_step": 1e3 * sec / k, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_desc(cfg, p.mesh.ne, T.nm), "ne": p.mesh.ne, "nm": T.nm},
+        "config": workload_config(cfg, ne, nm, P.dt, "fp64", args.gpus),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{k} full RK4 steps of the workload ({args.steps} requested, "
                                    f"capped at {budget:.0f} s)"},
@@ -344,35 +548,34 @@ def run_reference(args, cfg, rank):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(cfg, p):
-    """Oracle on the host cores, bounded to ~10-30 s (rank 0, N=1)."""
+def cpu_baseline(cfg):
+    """Oracle on the host cores, bounded to ~10-30 s (rank 0, N=1), on the
+    oracle's own set-up of the workload."""
     from oracle import oracle as O
-    T = p.T
-    OT = O.Tables(cfg.nc, cfg.ng, cfg.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
-    OM = O.Mesh(p.mesh.inn, p.mesh.xgr, p.mesh.ygr, cfg.nc, cfg.f0, cfg.beta)
+    from oracle.problems import oracle_problem
+    P = oracle_problem(cfg)
     threads = O.default_threads()
-    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    dof = 3.0 * P.T.nm * P.M.ne
+    u, v, h = P.u.copy(), P.v.copy(), P.h.copy()
     k, t0 = 0, time.perf_counter()
     while True:
-        O.rk4(cfg.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, cfg.mu0, cfg.mb0, cfg.g0,
-              p.dt, 1, threads)
+        P.rk4(u, v, h, 1, threads)
         k += 1
         sec = time.perf_counter() - t0
         if sec > 10.0 or k >= 50:
             break
     # the serial reference: one core, at least one step, about 6 s
-    u, v, h = p.u.copy(), p.v.copy(), p.h.copy()
+    u, v, h = P.u.copy(), P.v.copy(), P.h.copy()
     k1, t0 = 0, time.perf_counter()
     while True:
-        O.rk4(cfg.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, cfg.mu0, cfg.mb0, cfg.g0,
-              p.dt, 1, 1)
+        P.rk4(u, v, h, 1, 1)
         k1 += 1
         sec1 = time.perf_counter() - t0
         if sec1 > 6.0 or k1 >= 20:
             break
-    return {"value": 3.0 * T.nm * p.mesh.ne * k / sec, "unit": UNIT, "cores": threads,
+    return {"value": dof * k / sec, "unit": UNIT, "cores": threads,
             "kind": "port", "sample": f"{k} full RK4 steps of the workload, OpenMP over elements",
-            "serial": {"value": 3.0 * T.nm * p.mesh.ne * k1 / sec1, "unit": UNIT, "cores": 1,
+            "serial": {"value": dof * k1 / sec1, "unit": UNIT, "cores": 1,
                        "sample": f"{k1} full RK4 steps of the workload on one core"}}
 
 
@@ -385,17 +588,7 @@ def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
     p = W.build_problem(cfg)
     s = W.make_solver(p)
     s.set_stream(stream.cuda_stream)
-    elem, basis, _, _ = W.random_observations(p, nobs, seed=cfg.seed)
-    steps = np.array([50, 100, 150, 200], dtype=np.int32)
-    rng = np.random.Generator(np.random.PCG64(7))
-    truth = (p.u, p.v, p.h + 0.05 * rng.normal(size=p.h.shape) * (np.arange(p.h.shape[1]) < 1))
-    s.set_state(*truth)
-    vals, t_prev = [], 0
-    for st in steps:
-        s.rk4_steps(p.dt, int(st - t_prev))
-        t_prev = st
-        vals.append(np.sum(s.get_state()[2][elem - 1] * basis, axis=1))
-    s.set_observations(elem, basis, steps, np.array(vals))
+    W.assimilation_window(p, s, nobs, steps=(50, 100, 150, 200))
     x0 = (p.u, p.v, p.h)
     s.fwd_window(x0, p.dt, nsteps)  # warm-up
 
@@ -531,6 +724,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-regrid", action="store_true")
+    ap.add_argument("--no-drop-in", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma", "mixed"],
                     help="fp64: bit-exact reference order (headline); fp64_fma: fused "
                          "multiply-adds; mixed: FP32 contractions, FP64 state")
@@ -568,8 +762,8 @@ def main():
     s.rk4_steps(p.dt, args.warmup)
 
     # ---- timed region: device-resident state ----
-    clk_file = ROOT / "gpurun_out" / f"clocks_rank{rank}.csv"
-    clk_file.parent.mkdir(exist_ok=True)
+    clk_dir = tempfile.TemporaryDirectory(prefix="spoc_bench_clocks_")
+    clk_file = Path(clk_dir.name) / f"clocks_rank{rank}.csv"
     proc, fh = sample_clocks_start(clk_file) if rank == 0 else (None, None)
     if world > 1:
         dist.barrier()
@@ -617,6 +811,11 @@ def main():
     e2e = {"value": e_units / (e_ms * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": 3 * ne * nm * 8, "d2h_bytes_per_step": 3 * ne * nm * 8}
 
+    # ---- e2e through the literal drop-in: 4 cal_var calls per step ----
+    drop_in = None
+    if world == 1 and not args.no_drop_in and args.precision == "fp64":
+        drop_in = drop_in_measure(torch, W, api, p)
+
     # ---- per-kernel timing and roofline of the dominant kernel ----
     s.set_state(p.u, p.v, p.h)
     prof_steps = 2
@@ -629,28 +828,37 @@ def main():
     dur = per_launch_ms[dom] * 1e-3
     fp64_fma = api.fp64_peak(0)
     fp64_mul_add = api.fp64_peak(1)
-    hbm_peak = None
     try:
         hbm_peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
-        hbm_src = "measured"
+        hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
     except Exception:
-        hbm_peak, hbm_src = 6650.0, "fallback"
-    traffic = NCU_TRAFFIC.get(f"{cfg.name}:{dom}")
-    roof = {"kernel": dom, "bound": "hbm", "achieved": by / dur / 1e9, "peak": hbm_peak,
-            "unit": "GB/s", "frac": by / dur / 1e9 / hbm_peak, "traffic": traffic,
-            "peak_source": hbm_src, "algorithmic_bytes_per_launch": by}
+        hbm_peak, hbm_src = 6650.0, "fallback (6.65 TB/s, earlier measurement on this GPU type)"
+    traffic, traffic_note = ncu_traffic(cfg.name, dom)
+    hbm = {"achieved": by / dur / 1e9, "peak": hbm_peak, "unit": "GB/s",
+           "frac": by / dur / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": by,
+           "peak_source": hbm_src}
+    # the binding resource: the FP64 (or, mixed, FP32) pipe of the dominant
+    # kernel, against the measured peak of the arithmetic the kernel must use
     if args.precision == "mixed":
         fp32 = api.fp64_peak(2)
-        roof_fp64 = {"kernel": dom, "bound": "fp32", "achieved": fl / dur / 1e12, "peak": fp32,
-                     "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp32,
-                     "algorithmic_flops_per_launch": fl,
-                     "peak_source": "measured live: spoc_fp64_peak mode 2 (FP32 FMA chains)"}
+        roof = {"kernel": dom, "bound": "fp32", "achieved": fl / dur / 1e12, "peak": fp32,
+                "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp32, "traffic": traffic,
+                "traffic_note": traffic_note, "algorithmic_flops_per_launch": fl,
+                "launch_ms": per_launch_ms[dom],
+                "peak_source": "measured live: spoc_fp64_peak mode 2 (FP32 FMA chains)",
+                "hbm": hbm}
     else:
-        roof_fp64 = {"kernel": dom, "bound": "fp64", "achieved": fl / dur / 1e12,
-                     "peak": fp64_fma, "unit": "TFLOP/s", "frac": fl / dur / 1e12 / fp64_fma,
-                     "peak_mul_add": fp64_mul_add, "frac_of_mul_add": fl / dur / 1e12 / fp64_mul_add,
-                     "algorithmic_flops_per_launch": fl,
-                     "peak_source": "measured live: spoc_fp64_peak (DFMA chains, 148 SMs)"}
+        pk = fp64_mul_add if args.precision == "fp64" else fp64_fma
+        roof = {"kernel": dom, "bound": "fp64", "achieved": fl / dur / 1e12, "peak": pk,
+                "unit": "TFLOP/s", "frac": fl / dur / 1e12 / pk, "traffic": traffic,
+                "traffic_note": traffic_note, "algorithmic_flops_per_launch": fl,
+                "launch_ms": per_launch_ms[dom],
+                "peak_source": ("measured live: spoc_fp64_peak mode 1, separately rounded DMUL + "
+                                "DADD (the arithmetic the bit-exact path must use), 2 flops per pair"
+                                if args.precision == "fp64" else
+                                "measured live: spoc_fp64_peak mode 0, DFMA chains"),
+                "frac_of_dfma_peak": fl / dur / 1e12 / fp64_fma, "dfma_peak": fp64_fma,
+                "hbm": hbm}
 
     # the other precision modes on the same workload, and their distance from
     # the headline run after 100 steps
@@ -674,9 +882,10 @@ def main():
                            f: mnorm(st2[i] - ref_state[i]) / mnorm(ref_state[i])
                            for i, f in enumerate(("u", "v", "eta"))}})
 
-    mixed = None
+    mixed = mixed_all = None
     if world == 1 and not args.no_mixed:
         mixed = mixed_measure(torch, stream, flush, W, api)
+        mixed_all = mixed_errors_all(W)
     ensemble = None
     if not args.no_ensemble:
         ensemble = ensemble_measure(torch, stream, W, api, replicas, rank, world)
@@ -696,26 +905,22 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision != "mixed" else "f32 contractions / f64 state",
             "data": "synthetic",
-            "config": {"workload": workload_desc(cfg, ne, nm), "ne": ne, "nm": nm, "dt": p.dt,
-                       "precision": {"fp64": "fp64, reference operation order (bit-exact to the CPU oracle)",
-                                     "fp64_fma": "fp64 with fused multiply-adds (not bit-exact)",
-                                     "mixed": "FP32 contractions in the orthonormal basis, FP64 RK4 state"}[args.precision],
-                       "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": workload_config(cfg, ne, nm, p.dt, args.precision, world),
             "e2e": e2e,
+            "e2e_drop_in": drop_in,
             "gpu_launches": int(launches),
             "kernel_ms_per_launch": per_launch_ms,
             "roofline": roof,
-            ("roofline_fp32" if args.precision == "mixed" else "roofline_fp64"): roof_fp64,
             "other_precisions": others,
             "mixed_c3": mixed,
+            "mixed_errors": mixed_all,
             "ensemble_c5": ensemble,
             "adjoint": adjoint,
             "regrid": regrid,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(cfg, p)
+            line["cpu_baseline"] = cpu_baseline(cfg)
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:

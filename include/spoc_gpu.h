@@ -227,19 +227,22 @@ int spoc_tc_selftest(int K, int kpad, int n, int split, const float *A, const fl
  * mode 0: FP64 fused multiply-add, mode 1: FP64 separately rounded multiply
  * and add, mode 2: FP32 fused multiply-add. */
 int spoc_fp64_peak(int mode, double *tflops);
-/* Energy diagnostic that allocates nothing.  No counterpart in the reference
- * (it computes what src/energy.f:3-96 computes, like spoc_energy).  For
- * callers that cannot call cudaMalloc: it synchronises the device and is not
- * allowed during stream capture, or the host program owns all device memory.
+/* Energy diagnostic that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: cudaMalloc and cudaFree are
+ * prohibited while a stream is captured into a CUDA graph (default capture
+ * mode) and cudaFree synchronises the device, or the host program owns all
+ * device memory itself.  The result is the one spoc_energy gives.
  * Every argument is a DEVICE pointer owned by the caller: u, v, h, hb are
  * (ld, ne) fields, vect is (5, ne), pi2 is (ng, nm), wi is [ng], ammo1 is
  * column 1 of the mass matrix ammo [nm]; out receives (ke, pe, mass).  Work
  * is queued on `stream` (0 = legacy default stream) and nothing is allocated:
  * the per-element scratch is a static device array holding at most
  * SPOC_NOALLOC_MAX_NE elements (3 MiB on every GPU that loads the library);
- * larger ne returns SPOC_E_UNSUPPORTED.  The first call on a device looks up
- * that array's address and should come before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race on it. */
+ * larger ne returns SPOC_E_UNSUPPORTED.  The first call on a device (and
+ * the first after cudaDeviceReset) looks up that array's device address and
+ * should come before any stream capture.  All calls on a device share the
+ * array and it keeps the last call's contents (each call overwrites what it
+ * reads): calls that overlap on the GPU race on it. */
 #define SPOC_NOALLOC_MAX_NE 131072
 int spoc_energy_noalloc(int nc, int ng, int ne, int ld, double g0, const double *u,
                         const double *v, const double *h, const double *hb, const double *vect,
@@ -290,7 +293,9 @@ int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long long *adj_s
  * Register the COMMON contents once (after dpotrf), then link this library
  * instead of calvar*.o: cal_var_ has the reference argument list
  * (src/calvarnl_fs.f:9-12) with gfortran's by-reference, trailing-underscore
- * ABI.  A handle is created on the first call for (nf, ne) and reused.
+ * ABI.  A handle is created on the first call and reused while nf, ne and a
+ * content key of the mesh arrays and of fc, w0, z0, hb are unchanged (the
+ * adaptive driver rewrites them in place at a regrid).
  * Errors set *spoc_cal_var_status() (the reference `stop`s instead). */
 int spoc_register_commons(const spoc_tables *tables, int variant, int precision);
 void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, double *u1, double *v1,

@@ -31,7 +31,8 @@ SOURCES = ["spoc_kernels.cu", "spoc_fast.cu", "spoc_api.cu", "spoc_noalloc.cu", 
 # spoc_fast.cu is compiled a second time with fused multiply-adds
 VARIANT_SOURCES = [("spoc_fast.cu", "spoc_fast_fma", ["-DSPOC_FMA=1"])]
 HOST_SOURCES = ["spoc_host.cpp"]
-HEADERS = ["spoc_device.cuh", "spoc_kernels.h", "spoc_mixed.h", "spoc_tc.cuh", "spoc_mixed_dev.cuh"]
+HEADERS = ["spoc_device.cuh", "spoc_kernels.h", "spoc_launch.h", "spoc_bulk.cuh", "spoc_mixed.h", "spoc_tc.cuh",
+           "spoc_mixed_dev.cuh"]
 
 
 def _nvcc() -> str:

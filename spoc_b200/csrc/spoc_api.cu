@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -70,6 +71,11 @@ struct spoc_handle {
   int *flag = nullptr;
   unsigned long long *cflbits = nullptr;
   MixedCtx *mx = nullptr;  // SPOC_MIXED: the resident state lives here (psi basis)
+  // FP64: one RK4 step captured as a CUDA graph (replayed by spoc_rk4_steps),
+  // valid for the scalars baked into its kernel arguments
+  cudaGraphExec_t step_graph = nullptr;
+  double graph_key[6] = {};
+  long long graph_launches = 0;
 
   template <class T>
   cudaError_t alloc(T **p, size_t n) {
@@ -86,6 +92,7 @@ struct spoc_handle {
     return e;
   }
   ~spoc_handle() {
+    if (step_graph) cudaGraphExecDestroy(step_graph);
     if (mx) mixed_destroy(mx);
     for (void *p : allocs) cudaFree(p);
     if (side_ev) cudaEventDestroy(side_ev);
@@ -305,7 +312,7 @@ int check_flag(spoc_handle *h) {
   CK(cudaStreamSynchronize(h->st), "synchronize");
   if (flag) {
     CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->st), "clear flag");
-    if (flag & 2) return fail(SPOC_E_CUDA, "tensor-core wait limit reached");
+    if (flag & 2) return fail(SPOC_E_CUDA, "wait limit reached in a kernel (tensor-core or bulk-copy barrier)");
     if (flag & 4) return fail(SPOC_E_ARG, "interpol: element id out of range");
     return fail(SPOC_E_NONFINITE, "non-finite tendency detected");
   }
@@ -402,6 +409,18 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
     if (ce == cudaSuccess) ce = h->alloc(&h->escal, 4);
     if (ce == cudaSuccess) ce = h->alloc(&h->flag, 1);
     if (ce == cudaSuccess) ce = h->alloc(&h->cflbits, 1);
+    h->op.flag = h->flag;
+    if (ce == cudaSuccess && fast_available(nc, h->ng, h->ngf)) {
+      // operator images of the compile-time-sized kernels (bulk-copied into
+      // shared memory by every block)
+      void *img = nullptr, *imgq = nullptr;
+      ce = h->alloc(reinterpret_cast<char **>(&img), fast_image_bytes(nc, h->ng, h->ngf, 0));
+      if (ce == cudaSuccess)
+        ce = h->alloc(reinterpret_cast<char **>(&imgq), fast_image_bytes(nc, h->ng, h->ngf, 1));
+      if (ce == cudaSuccess) ce = fast_build_images(h->op, img, imgq, h->st);
+      h->op.img_ops = img;
+      h->op.img_q = imgq;
+    }
     for (int c = 0; c < 3 && ce == cudaSuccess; ++c)
       ce = cudaMemsetAsync(h->U0[c], 0, sizeof(double) * n, h->st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->hb, 0, sizeof(double) * n, h->st);
@@ -596,12 +615,62 @@ int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *bas
   return SPOC_OK;
 }
 
+// FP64 RK4 steps with the state resident: the launches of one step (3 or 1
+// kernels per stage, the same arguments every step) are captured once as a
+// CUDA graph and replayed, which removes the per-launch host and gap cost
+// that dominates small meshes.  The first step after any change of the
+// scalars in the kernel arguments (dt, mu0, mb0, g0, hb(1,1), kernel path)
+// runs directly, which also settles the launch configuration outside any
+// capture; the graph is captured from the next one.
+int graph_steps_fp64(spoc_handle *h, double dt, int nsteps) {
+  if (nsteps <= 0) return SPOC_OK;
+  // a caller capturing the handle's stream itself gets plain launches
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(h->st, &cap), "capture status");
+  if (cap != cudaStreamCaptureStatusNone) return enqueue_steps_fp64(h, dt, nsteps);
+  const double key[6] = {dt, h->mu0, h->mb0, h->g0, h->hh0, (double)h->path};
+  bool same = h->step_graph != nullptr;
+  for (int i = 0; i < 6 && same; ++i) same = key[i] == h->graph_key[i];
+  if (!same) {
+    if (h->step_graph) {
+      cudaGraphExecDestroy(h->step_graph);
+      h->step_graph = nullptr;
+    }
+    int rc = enqueue_steps_fp64(h, dt, 1);
+    if (rc || --nsteps == 0) return rc;
+    const long long l0 = h->launches;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    rc = enqueue_steps_fp64(h, dt, 1);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(h->st, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess) return fail(SPOC_E_CUDA, "end capture", ce);
+    const cudaError_t ie = cudaGraphInstantiate(&h->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      h->step_graph = nullptr;
+      return fail(SPOC_E_CUDA, "graph instantiate", ie);
+    }
+    h->graph_launches = h->launches - l0;
+    h->launches = l0;
+    for (int i = 0; i < 6; ++i) h->graph_key[i] = key[i];
+  }
+  for (int it = 0; it < nsteps; ++it) {
+    CK(cudaGraphLaunch(h->step_graph, h->st), "graph launch");
+    h->launches += h->graph_launches;
+  }
+  return SPOC_OK;
+}
+
 int enqueue_steps(spoc_handle *h, double dt, int nsteps) {
   if (h->mx) {
     CK(mixed_steps(h->mx, h->mesh, dt, nsteps, h->flag, h->st, &h->launches), "mixed RK4 steps");
     return SPOC_OK;
   }
-  return enqueue_steps_fp64(h, dt, nsteps);
+  return graph_steps_fp64(h, dt, nsteps);
 }
 }  // namespace
 
@@ -817,11 +886,55 @@ struct Commons {
   int ld_pi2 = 0, ld_p1 = 0, ld_p2 = 0;
   spoc_handle *h = nullptr;
   int h_ne = 0, h_nf = 0;
-  const void *h_keys[8] = {};
+  uint64_t h_key = 0;  // content key of the mesh and fields the handle holds
   int status = 0;
 };
 Commons g_commons;
 std::mutex g_commons_mu;
+
+// Content key of the arrays cal_var_ uploads.  The adaptive driver keeps its
+// mesh and field arrays at fixed addresses and rewrites them in place at
+// every regrid (src/shwwnl_adap.f:20, :397-433), possibly with the same
+// element and face counts, so a cached device copy is reused only while the
+// contents are unchanged.  Four independent multiply-xorshift lanes over
+// 64-bit words (the array lengths are mixed in too); only the nm used rows
+// of each (ld, ne) field are read.
+struct ContentKey {
+  uint64_t lane[4] = {0x243f6a8885a308d3ull, 0x13198a2e03707344ull, 0xa4093822299f31d0ull,
+                      0x082efa98ec4e6c89ull};
+  static uint64_t mix(uint64_t h, uint64_t w) {
+    h ^= w;
+    h *= 0x9e3779b97f4a7c15ull;
+    return h ^ (h >> 31);
+  }
+  void bytes(const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    size_t i = 0;
+    for (; i + 32 <= n; i += 32) {
+      uint64_t w[4];
+      std::memcpy(w, b + i, 32);
+      for (int k = 0; k < 4; ++k) lane[k] = mix(lane[k], w[k]);
+    }
+    for (; i < n; i += 8) {
+      uint64_t w = 0;
+      std::memcpy(&w, b + i, std::min<size_t>(8, n - i));
+      lane[0] = mix(lane[0], w);
+    }
+    lane[1] = mix(lane[1], (uint64_t)n);
+  }
+  void field(const double *a, int ld, int nm, int ne) {
+    if (!a) {
+      lane[2] = mix(lane[2], 0x6a09e667f3bcc908ull);
+      return;
+    }
+    for (int e = 0; e < ne; ++e) bytes(a + (size_t)e * ld, (size_t)nm * sizeof(double));
+  }
+  uint64_t digest() const {
+    uint64_t h = 0;
+    for (int k = 0; k < 4; ++k) h = mix(h, lane[k]);
+    return h;
+  }
+};
 }  // namespace
 
 extern "C" int *spoc_cal_var_status(void) { return &g_commons.status; }
@@ -884,9 +997,27 @@ extern "C" void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, d
     c.status = fail(SPOC_E_ARG, "spoc_register_commons not called");
     return;
   }
-  const void *keys[8] = {tseg, itm, its, norm, vect, fc, w0, hb};
-  bool same = c.h && c.h_ne == *ne && c.h_nf == *nf;
-  for (int i = 0; i < 8 && same; ++i) same = keys[i] == c.h_keys[i];
+  const int ne_ = *ne, nf_ = *nf;
+  if (ne_ <= 0 || nf_ <= 0 || !tseg || !itm || !its || !ssit || !norm || !vect || !normt || !bdl ||
+      !hb) {
+    c.status = fail(SPOC_E_ARG, "cal_var_: empty mesh or missing array");
+    return;
+  }
+  ContentKey ck;
+  ck.bytes(tseg, sizeof(int) * 2 * (size_t)nf_);
+  ck.bytes(ssit, sizeof(int) * 2 * (size_t)nf_);
+  ck.bytes(itm, sizeof(int) * 3 * (size_t)ne_);
+  ck.bytes(its, sizeof(int) * 3 * (size_t)ne_);
+  ck.bytes(bdl, sizeof(int) * (size_t)ne_);
+  ck.bytes(norm, sizeof(double) * 2 * (size_t)nf_);
+  ck.bytes(vect, sizeof(double) * 5 * (size_t)ne_);
+  ck.bytes(normt, sizeof(double) * 2 * (size_t)ne_);
+  ck.field(fc, c.ld, c.nm, ne_);
+  ck.field(w0, c.ld, c.nm, ne_);
+  ck.field(z0, c.ld, c.nm, ne_);
+  ck.field(hb, c.ld, c.nm, ne_);
+  const uint64_t key = ck.digest();
+  const bool same = c.h && c.h_ne == ne_ && c.h_nf == nf_ && c.h_key == key;
   if (!same) {
     if (c.h) {
       spoc_destroy(c.h);
@@ -914,9 +1045,9 @@ extern "C" void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, d
       c.status = rc;
       return;
     }
-    c.h_ne = *ne;
-    c.h_nf = *nf;
-    for (int i = 0; i < 8; ++i) c.h_keys[i] = keys[i];
+    c.h_ne = ne_;
+    c.h_nf = nf_;
+    c.h_key = key;
   } else {
     c.h->mu0 = *mu0;
     c.h->mb0 = *mb0;

@@ -45,6 +45,12 @@ struct DevOps {
   const int *inv_cnt;   // kind 1: chain length
   const double *ammo1;  // ammo(j,1), for the mass diagnostic
   const double *ammoT;  // [j*nm + i] = ammo(j,i)   (cal_b with ammo, verif_rot)
+  // images of the operators in the shared-memory layouts of the
+  // compile-time-sized kernels (copied into shared memory whole by the bulk
+  // copy engine); null where the degree has no such kernels
+  const void *img_ops;  // q-phase, tendency and linear kernels
+  const void *img_q;    // quadrature-point kernel
+  int *flag;            // the handle's error flags (bit 2: a wait limit ran out)
 };
 
 // Mesh pointers with 0-based ids; -1 marks a wall in tseg.

@@ -19,8 +19,10 @@
 
 #include <algorithm>
 
+#include "spoc_bulk.cuh"
 #include "spoc_device.cuh"
 #include "spoc_kernels.h"
+#include "spoc_launch.h"
 
 // SPOC_FMA selects the arithmetic of the multiply-add chains: 0 (default)
 // rounds every product separately, as the reference; 1 fuses each
@@ -676,8 +678,12 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
     sd_next = sides_of(m, warp_global());
     prefetch_element<Dm, 2>(fields, warp_global(), sd_next, W.own, W.nb);
   }
-  stage_ops(S, op);
-  __syncthreads();
+  // the operator image arrives whole through one bulk copy (TMA engine)
+  __shared__ __align__(8) uint64_t ops_bar;
+  if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) {
+    cp_async_wait_all();
+    return;
+  }
   const size_t fs = (size_t)m.ne * N;
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
     const Sides sd = PF ? sd_next : sides_of(m, e);
@@ -762,8 +768,8 @@ __device__ __forceinline__ void nlvol_body(DevOps op, DevMesh m, NlArgs a) {
   SOpsQ<Dm> &S = *reinterpret_cast<SOpsQ<Dm> *>(smem);
   BWarp<Dm> &W = reinterpret_cast<BWarp<Dm> *>(smem + sizeof(SOpsQ<Dm>))[warp_in_block()];
   constexpr int N = Dm::N, Q = Dm::Q, R = Dm::R, RQ = Dm::RQ;
-  stage_ops_q(S, op);
-  __syncthreads();
+  __shared__ __align__(8) uint64_t ops_bar;
+  if (!bulk::stage_block(&S, op.img_q, sizeof(SOpsQ<Dm>), &ops_bar, op.flag)) return;
   const int l = lane_id();
   const size_t fs = (size_t)m.ne * N;
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
@@ -939,8 +945,11 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
     sd_next = sides_of(m, warp_global());
     prefetch_element<Dm, 6>(src, warp_global(), sd_next, W.own, W.nb);
   }
-  stage_ops(S, op);
-  __syncthreads();
+  __shared__ __align__(8) uint64_t ops_bar;
+  if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) {
+    cp_async_wait_all();
+    return;
+  }
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
     const Sides sd = PF ? sd_next : sides_of(m, e);
     const int en = e + warp_count();
@@ -1049,7 +1058,7 @@ __global__ void __launch_bounds__(256, 2) kf_qphase_r2(DevOps op, DevMesh m,
   qphase_body<Dm, VAR>(op, m, su, sv, q);
 }
 template <class Dm, int VAR>
-__global__ void __launch_bounds__(256) kf_nlvol(DevOps op, DevMesh m, NlArgs a) {
+__global__ void __launch_bounds__(256, 2) kf_nlvol(DevOps op, DevMesh m, NlArgs a) {
   nlvol_body<Dm, VAR>(op, m, a);
 }
 template <class Dm, int VAR>
@@ -1097,8 +1106,8 @@ __global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, S
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
   LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
   constexpr int N = Dm::N, R = Dm::R;
-  stage_ops(S, op);
-  __syncthreads();
+  __shared__ __align__(8) uint64_t ops_bar;
+  if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) return;
   const int l = lane_id();
   const double mg0 = -a.g0, hh0 = a.hh0;
   for (int e = warp_global(); e < m.ne; e += warp_count()) {
@@ -1187,33 +1196,26 @@ __global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, S
 }
 
 // ---------------------------------------------------------------------------
-// launch plumbing
+// operator images: the shared-memory layouts of SOps / SOpsQ, written once per
+// handle into global memory so that each block stages them with bulk copies
 // ---------------------------------------------------------------------------
-template <class K>
-cudaError_t prepare(K kernel, size_t smem) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <class Dm>
+__global__ void __launch_bounds__(256) k_fast_images(DevOps op, SOps<Dm> *img, SOpsQ<Dm> *imgq) {
+  stage_ops(*img, op);
+  stage_ops_q(*imgq, op);
 }
 
+// ---------------------------------------------------------------------------
+// launch plumbing
+// ---------------------------------------------------------------------------
 // warps per block so that the per-block shared memory stays under ~113 KB
 // (two blocks per SM) when possible, else one block up to 8 warps.
-inline int pick_warps(size_t ops, size_t per_warp) {
+constexpr int pick_warps(size_t ops, size_t per_warp) {
   for (int w = 8; w >= 2; --w)
     if (ops + w * per_warp <= 113 * 1024) return w;
   for (int w = 8; w >= 1; --w)
     if (ops + w * per_warp <= 220 * 1024) return w;
   return 1;
-}
-
-// Persistent grid: exactly the number of blocks that can be resident.
-template <class K>
-int resident_grid(K kernel, int threads, size_t smem, int sms, int ne, int warps) {
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  const int need = (ne + warps - 1) / warps;
-  const int cap = sms * per_sm;
-  return need < cap ? need : cap;
 }
 
 template <class Dm, int VAR>
@@ -1225,24 +1227,17 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   NlArgs na{b.su, b.sv, b.sh, b.hb, b.w0, b.z0, b.fc, b.q, b.gx0, b.gy0, b.uh, b.vh, b.f,
             b.mu0, b.mb0, b.g0};
   TendArgs ta{b.gx0, b.gy0, b.uh, b.vh, b.f};
-  static int wq = 0, wb = 0, wt = 0, gq = 0, gb = 0, gt = 0, ne_cached = -1;
-  static size_t sq = 0, sb = 0, stt = 0;
-  if (ne_cached != m.ne) {
-    wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
-    wb = pick_warps(sizeof(SOpsQ<Dm>), sizeof(BWarp<Dm>));
-    wt = std::min(pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>)), Dm::TEND_THREADS / 32);
-    sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
-    sb = sizeof(SOpsQ<Dm>) + wb * sizeof(BWarp<Dm>);
-    stt = sizeof(SOps<Dm>) + wt * sizeof(TWarp<Dm>);
-    cudaError_t e = prepare(qphase_kernel<Dm, VAR>(), sq);
-    if (e == cudaSuccess) e = prepare(nlvol_kernel<Dm, VAR>(), sb);
-    if (e == cudaSuccess) e = prepare(tend_kernel<Dm, VAR>(), stt);
-    if (e != cudaSuccess) return e;
-    gq = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq);
-    gb = resident_grid(nlvol_kernel<Dm, VAR>(), 32 * wb, sb, sms, m.ne, wb);
-    gt = resident_grid(tend_kernel<Dm, VAR>(), 32 * wt, stt, sms, m.ne, wt);
-    ne_cached = m.ne;
-  }
+  constexpr int wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
+  constexpr int wb = pick_warps(sizeof(SOpsQ<Dm>), sizeof(BWarp<Dm>));
+  constexpr int wt = std::min(pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>)), Dm::TEND_THREADS / 32);
+  constexpr size_t sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
+  constexpr size_t sb = sizeof(SOpsQ<Dm>) + wb * sizeof(BWarp<Dm>);
+  constexpr size_t stt = sizeof(SOps<Dm>) + wt * sizeof(TWarp<Dm>);
+  int gq = 0, gb = 0, gt = 0;
+  cudaError_t e = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq, &gq);
+  if (e == cudaSuccess) e = resident_grid(nlvol_kernel<Dm, VAR>(), 32 * wb, sb, sms, m.ne, wb, &gb);
+  if (e == cudaSuccess) e = resident_grid(tend_kernel<Dm, VAR>(), 32 * wt, stt, sms, m.ne, wt, &gt);
+  if (e != cudaSuccess) return e;
   mark(0);
   const auto kq = qphase_kernel<Dm, VAR>();
   const auto kb = nlvol_kernel<Dm, VAR>();
@@ -1262,16 +1257,11 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
 template <class Dm, int VAR>
 cudaError_t run_q(const DevOps &op, const DevMesh &m, const double *su, const double *sv, double *q,
                   cudaStream_t st, int sms) {
-  static int wq = 0, gq = 0, ne_cached = -1;
-  static size_t sq = 0;
-  if (ne_cached != m.ne) {
-    wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
-    sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
-    cudaError_t e = prepare(qphase_kernel<Dm, VAR>(), sq);
-    if (e != cudaSuccess) return e;
-    gq = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq);
-    ne_cached = m.ne;
-  }
+  constexpr int wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
+  constexpr size_t sq = sizeof(SOps<Dm>) + wq * sizeof(QWarp<Dm>);
+  int gq = 0;
+  const cudaError_t e = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq, &gq);
+  if (e != cudaSuccess) return e;
   const auto kq = qphase_kernel<Dm, VAR>();
   kq<<<gq, 32 * wq, sq, st>>>(op, m, su, sv, q);
   return cudaGetLastError();
@@ -1280,16 +1270,11 @@ cudaError_t run_q(const DevOps &op, const DevMesh &m, const double *su, const do
 template <class Dm>
 cudaError_t run_lin(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
                     cudaStream_t st, int sms, cudaEvent_t *ev) {
-  static int w = 0, grid = 0, ne_cached = -1;
-  static size_t sm = 0;
-  if (ne_cached != m.ne) {
-    w = pick_warps(sizeof(SOps<Dm>), sizeof(LWarp<Dm>));
-    sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
-    cudaError_t e = prepare(kf_lin<Dm>, sm);
-    if (e != cudaSuccess) return e;
-    grid = resident_grid(kf_lin<Dm>, 32 * w, sm, sms, m.ne, w);
-    ne_cached = m.ne;
-  }
+  constexpr int w = pick_warps(sizeof(SOps<Dm>), sizeof(LWarp<Dm>));
+  constexpr size_t sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
+  int grid = 0;
+  const cudaError_t e = resident_grid(kf_lin<Dm>, 32 * w, sm, sms, m.ne, w, &grid);
+  if (e != cudaSuccess) return e;
   LinArgs la{b.su, b.sv, b.sh, b.g0, b.hh0};
   if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
   if (ev) cudaEventRecord(ev[0], st);
@@ -1326,6 +1311,39 @@ bool FAST_AVAILABLE(int nc, int ng, int ngf) {
 }
 
 #if !SPOC_FMA
+template <class F>
+bool with_fast_dims(int nc, int ng, int ngf, F &&f) {
+  if (nc == 3 && ng == 12 && ngf == 4) return f(Dims<3, 12, 4>{}), true;
+  if (nc == 4 && ng == 25 && ngf == 5) return f(Dims<4, 25, 5>{}), true;
+  if (nc == 5 && ng == 27 && ngf == 6) return f(Dims<5, 27, 6>{}), true;
+  if (nc == 6 && ng == 33 && ngf == 7) return f(Dims<6, 33, 7>{}), true;
+  if (nc == 7 && ng == 42 && ngf == 9) return f(Dims<7, 42, 9>{}), true;
+  return false;
+}
+
+size_t fast_image_bytes(int nc, int ng, int ngf, int which) {
+  size_t n = 0;
+  with_fast_dims(nc, ng, ngf, [&](auto d) {
+    using Dm = decltype(d);
+    n = which == 0 ? sizeof(SOps<Dm>) : sizeof(SOpsQ<Dm>);
+  });
+  return n;
+}
+
+cudaError_t fast_build_images(const DevOps &op, void *img, void *imgq, cudaStream_t st) {
+  cudaError_t e = cudaErrorNotSupported;
+  with_fast_dims(op.nc, op.ng, op.ngf, [&](auto d) {
+    using Dm = decltype(d);
+    e = cudaMemsetAsync(img, 0, sizeof(SOps<Dm>), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(imgq, 0, sizeof(SOpsQ<Dm>), st);
+    if (e != cudaSuccess) return;
+    k_fast_images<Dm><<<1, 256, 0, st>>>(op, static_cast<SOps<Dm> *>(img),
+                                          static_cast<SOpsQ<Dm> *>(imgq));
+    e = cudaGetLastError();
+  });
+  return e;
+}
+
 cudaError_t launch_qphase_fast(int variant, const DevOps &op, const DevMesh &m, const double *su,
                                const double *sv, double *q, cudaStream_t st, int sms) {
   const int nc = op.nc, ng = op.ng, ngf = op.ngf;

@@ -173,6 +173,11 @@ cudaError_t launch_obs_adj(int nel, int nm, const int *el_list, const int *el_st
 // Compile-time-sized kernels (spoc_fast.cu) for the tabulated degree /
 // quadrature combinations; identical results to launch_rhs.
 bool fast_available(int nc, int ng, int ngf);
+// Bytes of the operator images of the compile-time-sized kernels (which 0:
+// q-phase / tendency / linear kernels, 1: quadrature-point kernel; 0 when the
+// degree is not tabulated), and the kernel that writes them from op's tables.
+size_t fast_image_bytes(int nc, int ng, int ngf, int which);
+cudaError_t fast_build_images(const DevOps &op, void *img, void *imgq, cudaStream_t st);
 cudaError_t launch_rhs_fast(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
                             const StageArgs &sa, cudaStream_t st, int sms, long long *launches,
                             cudaEvent_t *ev = nullptr);

@@ -41,6 +41,7 @@
 #include <cstring>
 #include <vector>
 
+#include "spoc_launch.h"
 #include "spoc_mixed.h"
 #include "spoc_mixed_dev.cuh"
 
@@ -948,29 +949,11 @@ std::vector<float> ops_image(const PsiOps &p, const spoc_tables *t) {
   return o;
 }
 
-// Persistent grid: as many blocks as stay resident (occupancy x SMs), or
-// fewer when the elements run out.  Cached per kernel.
+// Persistent grid: as many blocks as stay resident (occupancy x SMs on the
+// current device), or fewer when the elements run out.
 using MxKernel = void (*)(MxArgs);
-int grid_for(MxKernel kernel, size_t smem, int sms, int ne, int slots) {
-  struct Entry {
-    MxKernel k;
-    int per_sm;
-  };
-  static std::vector<Entry> cache;
-  int per_sm = 0;
-  for (const Entry &x : cache)
-    if (x.k == kernel) per_sm = x.per_sm;
-  if (!per_sm) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * kMxWarps, smem) !=
-            cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
-    cache.push_back({kernel, per_sm});
-  }
-  const int need = (ne + slots - 1) / slots;
-  const int cap = sms * per_sm;
-  return need < cap ? need : cap;
+cudaError_t grid_for(MxKernel kernel, size_t smem, int sms, int ne, int slots, int *grid) {
+  return resident_grid(kernel, 32 * kMxWarps, smem, sms, ne, slots, grid);
 }
 
 template <class Dm>
@@ -987,7 +970,9 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
     if (ev) cudaEventRecord(ev[i], st);
   };
   if (c->variant == SPOC_LIN) {
-    const int g = grid_for(kx_lin<Dm>, smem, c->sms, c->ne, Dm::SLOTS);
+    int g = 0;
+    const cudaError_t ge = grid_for(kx_lin<Dm>, smem, c->sms, c->ne, Dm::SLOTS, &g);
+    if (ge != cudaSuccess) return ge;
     mark(0);
     kx_lin<Dm><<<g, 32 * kMxWarps, smem, st>>>(a);
     mark(1);
@@ -996,8 +981,10 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
   }
   cudaError_t tce = cudaSuccess;
   auto go = [&](MxKernel kv, MxKernel kt) {
-    const int gv = grid_for(kv, smem, c->sms, c->ne, Dm::SLOTS);
-    const int gt = grid_for(kt, smem, c->sms, c->ne, Dm::SLOTS);
+    int gv = 0, gt = 0;
+    tce = grid_for(kv, smem, c->sms, c->ne, Dm::SLOTS, &gv);
+    if (tce == cudaSuccess) tce = grid_for(kt, smem, c->sms, c->ne, Dm::SLOTS, &gt);
+    if (tce != cudaSuccess) return;
     mark(0);
     if (c->tc) {
       tce = mixed_tc_vol(c->variant, c->nc, c->Q, c->G, a, c->tcimg, c->sms, st);
@@ -1020,7 +1007,9 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
 template <class Dm>
 cudaError_t run_prep(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *launches) {
   constexpr size_t smem = mx_smem<Dm>();
-  const int g = grid_for(kx_prep<Dm>, smem, c->sms, c->ne, Dm::SLOTS);
+  int g = 0;
+  const cudaError_t ge = grid_for(kx_prep<Dm>, smem, c->sms, c->ne, Dm::SLOTS, &g);
+  if (ge != cudaSuccess) return ge;
   kx_prep<Dm><<<g, 32 * kMxWarps, smem, st>>>(a);
   if (launches) *launches += 1;
   return cudaGetLastError();

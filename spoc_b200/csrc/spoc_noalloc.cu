@@ -1,24 +1,32 @@
 // Energy diagnostic that allocates nothing: spoc_energy_noalloc.
 //
-// Why it exists: cudaMalloc and cudaFree synchronise the whole device and are
-// not allowed while a stream is being captured into a CUDA graph, and some
-// host programs own all device memory themselves (a Fortran driver with
-// OpenACC or CUDA Fortran device arrays, a framework with its own pool).
-// Such callers cannot use spoc_create, which allocates.  This entry point
-// takes every input and the output as device pointers the caller already
-// owns, and keeps its only scratch -- the per-element (ke, pe, mass) terms
-// summed afterwards -- in a file-scope static device array of fixed size.
+// Why it exists: some callers cannot call cudaMalloc.  cudaMalloc and
+// cudaFree are prohibited while a stream is captured into a CUDA graph in the
+// default capture mode and cudaFree synchronises the device, so a caller in
+// the middle of a capture, or one that must not stall other streams, cannot
+// use them; and some host programs own all device memory themselves (a
+// Fortran driver with OpenACC or CUDA Fortran device arrays, a framework
+// with its own pool).  Such callers cannot use spoc_create, which allocates.
+// This entry point takes every input and the output as device pointers the
+// caller already owns, and keeps its only scratch -- the per-element
+// (ke, pe, mass) terms summed afterwards -- in a file-scope static device
+// array of fixed size.
 //
 // Limits and sharing: at most SPOC_NOALLOC_MAX_NE elements (the array holds
 // 3 doubles per element, 3 MiB, resident on every GPU that loads the library
-// until the process exits); larger meshes get SPOC_E_UNSUPPORTED.  The first
-// call on a device looks up the array's device address (cudaGetSymbolAddress,
-// with that device current) and caches it; make that first call before any
-// stream capture.  All calls on a device share the array and it keeps the
-// previous call's contents; every call overwrites the ne*3 terms it reads, so
-// nothing needs clearing, but two calls that overlap on the GPU (different
-// streams, no ordering between them) race on it.
+// until the process exits); larger meshes get SPOC_E_UNSUPPORTED.  In host
+// code the array's name is not a device address: the first call on a device
+// looks up the address (cudaGetSymbolAddress, with that device current) and
+// caches it for that device's context; the lookup is made again after the
+// context is re-created (cudaDeviceReset), so the first call on a device, and
+// the first after a reset, should come before any stream capture.  All calls
+// on a device share the array and it keeps the previous call's contents;
+// every call overwrites the ne*3 terms it reads, so nothing needs clearing,
+// but two calls that overlap on the GPU (different streams, no ordering
+// between them) race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <mutex>
 
@@ -32,7 +40,11 @@ using namespace spoc;
 static __device__ __align__(256) double g_energy_scratch[3 * SPOC_NOALLOC_MAX_NE];
 
 constexpr int kMaxDevices = 64;
-double *g_scratch_ptr[kMaxDevices] = {};
+struct ScratchAddr {
+  double *ptr = nullptr;
+  unsigned long long ctx_id = 0;  // context the address belongs to
+};
+ScratchAddr g_scratch[kMaxDevices];
 std::mutex g_scratch_mu;
 
 // Per-element terms of src/energy.f:307-370, as k_energy_terms computes them,
@@ -104,21 +116,56 @@ __global__ void __launch_bounds__(1024) k_energy_sum_to(const double *terms, int
     for (int c = 0; c < 3; ++c) out[c] = part[c][0];
 }
 
-// Device address of the static scratch on the current device (looked up once
-// per device, with that device current).
+// Unique id of the current context (cuCtxGetId through the runtime's driver
+// entry points, so the library needs no link against the driver library);
+// it changes when cudaDeviceReset re-creates the device's context.  With no
+// context current on this thread, cudaSetDevice makes the device's primary
+// context current (it allocates nothing).
+cudaError_t current_context_id(int dev, unsigned long long *id) {
+  static PFN_cuCtxGetCurrent get_current = nullptr;
+  static PFN_cuCtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<PFN_cuCtxGetCurrent>(f);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PFN_cuCtxGetId>(f);
+  });
+  if (!get_current || !get_id) return cudaErrorNotSupported;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+  if (!ctx) {
+    const cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return e;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return cudaErrorDeviceUninitialized;
+  }
+  return get_id(ctx, id) == CUDA_SUCCESS ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
+
+// Device address of the static scratch on the current device: looked up with
+// that device current, once per device context.
 cudaError_t scratch_for_current_device(double **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  unsigned long long id = 0;
+  e = current_context_id(dev, &id);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+  ScratchAddr &a = g_scratch[dev];
+  if (!a.ptr || a.ctx_id != id) {
     double *p = nullptr;
     e = cudaGetSymbolAddress((void **)&p, g_energy_scratch);
     if (e != cudaSuccess) return e;
-    g_scratch_ptr[dev] = p;
+    a.ptr = p;
+    a.ctx_id = id;
   }
-  *out = g_scratch_ptr[dev];
+  *out = a.ptr;
   return cudaSuccess;
 }
 
@@ -142,8 +189,18 @@ extern "C" int spoc_energy_noalloc(int nc, int ng, int ne, int ld, double g0, co
     return SPOC_E_CUDA;
   int grid = (ne + 7) / 8;
   if (grid > sms * 8) grid = sms * 8;
-  k_energy_terms_ld<<<grid, 256, 0, st>>>(nm, ng, ne, ld, u, v, h, hb, vect, pi2, wi, ammo1, g0,
-                                          scratch);
-  k_energy_sum_to<<<1, 1024, 0, st>>>(scratch, ne, out);
-  return cudaGetLastError() == cudaSuccess ? SPOC_OK : SPOC_E_CUDA;
+  // cudaLaunchKernel returns the status of this launch itself, not an error
+  // left over from earlier work of the caller
+  void *ta[] = {(void *)&nm, (void *)&ng, (void *)&ne, (void *)&ld, (void *)&u, (void *)&v,
+                (void *)&h, (void *)&hb, (void *)&vect, (void *)&pi2, (void *)&wi,
+                (void *)&ammo1, (void *)&g0, (void *)&scratch};
+  if (cudaLaunchKernel((const void *)k_energy_terms_ld, dim3(grid), dim3(256), ta, 0, st) !=
+      cudaSuccess)
+    return SPOC_E_CUDA;
+  const double *terms = scratch;
+  void *sa[] = {(void *)&terms, (void *)&ne, (void *)&out};
+  if (cudaLaunchKernel((const void *)k_energy_sum_to, dim3(1), dim3(1024), sa, 0, st) !=
+      cudaSuccess)
+    return SPOC_E_CUDA;
+  return SPOC_OK;
 }

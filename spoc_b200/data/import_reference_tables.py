@@ -8,17 +8,22 @@ points, so they are imported verbatim: every entry keeps the decimal text of
 the .dat file, and is parsed at load time with a correctly rounded conversion,
 as Fortran list-directed input does.
 
-Usage: python spoc_b200/data/import_reference_tables.py [REFERENCE_INCLUDE_DIR]
+Usage: python spoc_b200/data/import_reference_tables.py REFERENCE_INCLUDE_DIR
+(the reference checkout's include/ directory, which holds the .dat files)
 """
 import json
 import sys
 from pathlib import Path
 
-SRC = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/include")
 OUT = Path(__file__).resolve().parent / "quadrature_tables.json"
 
 
 def main() -> None:
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    SRC = Path(sys.argv[1])
+    if not any(SRC.glob("tri2_*.dat")):
+        sys.exit(f"no tri2_*.dat in {SRC}")
     tables = {"triangle": {}, "edge": {}}
     for f in sorted(SRC.glob("tri2_*.dat")):
         ng = int(f.stem.split("_")[1])

@@ -87,8 +87,10 @@ def small(cfg: Config, n: int, **kw) -> Config:
     return Config(**d)
 
 
-def square_mesh(n: int, length: float = 1.0e6, jitter: float = 0.0, seed: int = 0):
-    """(nn, inn (ne,3) 1-based, xgr, ygr) of the rmal split, jittered, corner-fixed."""
+def square_mesh(n: int, length: float = 1.0e6, jitter: float = 0.0, seed: int = 0, fix=None):
+    """(nn, inn (ne,3) 1-based, xgr, ygr) of the rmal split, jittered, corner-fixed.
+
+    fix(inn, nn) applies the corner fix (default: the library's spoc_fix_mesh)."""
     nx = n + 1
     h = length / n
     xs = -0.5 * length + h * np.arange(nx)
@@ -110,7 +112,7 @@ def square_mesh(n: int, length: float = 1.0e6, jitter: float = 0.0, seed: int = 
     inn[0::2] = t1
     inn[1::2] = t2
     nn = nx * nx
-    inn = api.fix_mesh(inn, nn)
+    inn = (fix or api.fix_mesh)(inn, nn)
     return nn, inn, x, y
 
 
@@ -241,6 +243,45 @@ def make_solver(p: Problem, precision: str = "fp64") -> api.Solver:
     return s
 
 
+def mass_norm(p: Problem, a: np.ndarray) -> float:
+    """Physical L2 norm sqrt(sum_e det_e a_e^T ammo a_e) of a modal field."""
+    x = a[:, :p.T.nm]
+    return float(np.sqrt(np.sum(p.mesh.det * np.einsum("ei,ij,ej->e", x, p.T.ammo.T, x))))
+
+
+def run_steps(p: Problem, precision: str, steps: int, path: str = "auto"):
+    """(state, energy at the start, energy at the end) of `steps` RK4 steps
+    from the problem's state in the given precision form."""
+    s = make_solver(p, precision)
+    s.set_kernel_path(path)
+    s.set_state(p.u, p.v, p.h)
+    e0 = s.energy()
+    s.rk4_steps(p.dt, steps)
+    e1 = s.energy()
+    st = s.get_state()
+    s.close()
+    return st, e0, e1
+
+
+def energy_drift(e0, e1) -> float:
+    """Relative change of the total energy KE + PE (src/energy.f:3-96)."""
+    return ((e1[0] + e1[1]) - (e0[0] + e0[1])) / (e0[0] + e0[1])
+
+
+def precision_errors(p: Problem, steps: int, precision: str = "mixed", path: str = "auto",
+                     ref=None) -> dict:
+    """Relative L2 (mass-norm) errors of u, v, eta of a precision form against
+    the FP64 form (bit-identical to the CPU oracle) after `steps` steps, and
+    both runs' energy drift.  ref: an FP64 run_steps result to reuse."""
+    ref = ref or run_steps(p, "fp64", steps)
+    got = run_steps(p, precision, steps, path)
+    err = {f: mass_norm(p, got[0][i] - ref[0][i]) / max(mass_norm(p, ref[0][i]), 1e-300)
+           for i, f in enumerate(("u", "v", "eta"))}
+    return {"steps": steps, "rel_l2_error_vs_fp64": err,
+            "energy_drift": {"fp64": energy_drift(ref[1], ref[2]),
+                             precision: energy_drift(got[1], got[2])}}
+
+
 def locate(mesh: api.Mesh, px: np.ndarray, py: np.ndarray):
     """Element (1-based) and reference coordinates (xi, eta) of each point.
 
@@ -288,6 +329,29 @@ def random_observations(p: Problem, nobs: int, seed: int):
     py = rng.uniform(-0.5 * L, 0.5 * L, nobs)
     elem, xi, eta = locate(p.mesh, px, py)
     return elem, basis_at(p.cfg.nc, xi, eta), px, py
+
+
+def assimilation_window(p: Problem, s: api.Solver, nobs: int = 500,
+                        steps=(50, 100, 150, 200), seed: int | None = None):
+    """The C4 assimilation set-up: nobs seeded points uniform in the basin,
+    eta observed at the given steps of a truth run that starts from the
+    problem's state with seeded noise on the element means of eta; the
+    observations are registered on solver s.  Returns (elem, basis, steps,
+    values)."""
+    seed = p.cfg.seed if seed is None else seed
+    elem, basis, _, _ = random_observations(p, nobs, seed=seed)
+    steps = np.asarray(steps, dtype=np.int32)
+    rng = np.random.Generator(np.random.PCG64(7))
+    truth = (p.u, p.v, p.h + 0.05 * rng.normal(size=p.h.shape) * (np.arange(p.h.shape[1]) < 1))
+    s.set_state(*truth)
+    vals, t_prev = [], 0
+    for st in steps:
+        s.rk4_steps(p.dt, int(st - t_prev))
+        t_prev = st
+        vals.append(np.sum(s.get_state()[2][elem - 1] * basis, axis=1))
+    vals = np.array(vals)
+    s.set_observations(elem, basis, steps, vals)
+    return elem, basis, steps, vals
 
 
 # ---------------------------------------------------------------------------

@@ -34,3 +34,20 @@ def test_reference_arm_line():
 
 def test_reference_arm_other_ranks_print_nothing():
     assert run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
+
+
+def test_reference_arm_does_not_load_the_cuda_library():
+    """The reference arm sets the workload up with the oracle alone: the
+    product library is never mapped into its process."""
+    code = (
+        "import sys, types\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1']\n"
+        "import bench\n"
+        "bench.main()\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('LOADED' if 'libspoc_gpu.so' in maps else 'NOT_LOADED')\n"
+    )
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "NOT_LOADED"

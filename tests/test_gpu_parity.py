@@ -217,6 +217,62 @@ def test_fortran_drop_in_cal_var_(gpu_lib):
 
 
 @pytest.mark.gpu
+def test_fortran_drop_in_mesh_rewritten_in_place(gpu_lib):
+    """The adaptive driver rewrites its mesh, geometry and depth arrays in place
+    at a regrid (src/shwwnl_adap.f:397-433), possibly with the same ne and nf:
+    the second cal_var_ call, on a different mesh at the same addresses, must
+    use the new mesh."""
+    cfg = W.small(W.CONFIGS["c2_fs_p6"], 6)
+    p = W.build_problem(cfg)
+    q = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 6, seed=9))  # other jitter
+    assert (q.mesh.ne, q.mesh.nf) == (p.mesh.ne, p.mesh.nf)
+    assert not np.array_equal(q.mesh.vect, p.mesh.vect)
+    q.hb[:, 0] = 3500.0
+    lib = api.load_library()
+    ts = p.T.struct()
+    assert lib.spoc_register_commons(C.byref(ts), api.FS, api.FP64) == 0
+    m, c = p.mesh, p.cfg
+    # the driver's arrays, at fixed addresses for both calls
+    arr = {k: getattr(m, k).copy() for k in ("tseg", "pseg", "ssit", "itm", "its", "norm", "bdl",
+                                                 "vect", "normt")}
+    fc, w0, z0, hb = p.fc.copy(), p.w0.copy(), p.z0.copy(), p.hb.copy()
+    outs = [np.zeros_like(p.u) for _ in range(3)]
+    keep = []
+
+    def ints(x):
+        keep.append(C.c_int(x))
+        return C.c_void_p(C.addressof(keep[-1]))
+
+    def dbl(x):
+        keep.append(C.c_double(x))
+        return C.c_void_p(C.addressof(keep[-1]))
+
+    ptr = lambda a: C.c_void_p(a.ctypes.data)
+    pbdl = np.zeros(m.ne, np.int32)
+    pint = np.zeros(m.ne, np.int32)
+    args = [ints(m.nf), ints(m.ne), ptr(p.u), ptr(p.v), ptr(p.h), *map(ptr, outs),
+            ptr(arr["tseg"]), ptr(arr["pseg"]), ptr(arr["ssit"]), ptr(arr["itm"]),
+            ptr(arr["its"]), ptr(arr["norm"]), ints(0), ptr(pbdl), ints(0), ptr(pint),
+            ptr(arr["bdl"]), ptr(p.T.cip), ptr(arr["vect"]), ptr(arr["normt"]), dbl(c.mu0),
+            dbl(c.mb0), ptr(fc), dbl(c.beta), ptr(w0), ptr(z0), dbl(c.g0), ptr(hb), dbl(0.0)]
+    lib.cal_var_(*args)
+    assert lib.spoc_cal_var_status()[0] == 0
+    OT, OM = oracle_for(p)
+    assert_bitwise(outs, oracle_rhs(p, OT, OM, p.u, p.v, p.h), p.T.nm)
+    # regrid in place: same ne, nf and addresses, new contents
+    for k in arr:
+        arr[k][...] = getattr(q.mesh, k)
+    fc[...], hb[...] = q.fc, q.hb
+    lib.cal_var_(*args)
+    assert lib.spoc_cal_var_status()[0] == 0
+    OTq, OMq = oracle_for(q)
+    ref = O.cal_var(c.variant, OTq, OMq, p.u, p.v, p.h, OMq.fc, q.w0, q.z0, q.hb, c.mu0, c.mb0,
+                    c.g0)
+    assert_bitwise(outs, ref, p.T.nm)
+    lib.spoc_release_commons()
+
+
+@pytest.mark.gpu
 def test_nonfinite_state_is_reported(gpu_lib):
     p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 4))
     s = W.make_solver(p)

@@ -1,11 +1,12 @@
 """spoc_energy_noalloc: the energy diagnostic for callers that cannot allocate.
 
-Callers that may not call cudaMalloc (it synchronises the device and is not
-allowed during stream capture, or their host program owns all device memory)
-pass device arrays they already own; the entry point keeps its per-element
-scratch in a static device array.  Its result must equal the handle entry
-point spoc_energy (same kernels, same summation order; the energy tolerance
-of the other tests, 1e-13 relative, is the bound), on two calls in a row so a
+Some callers may not call cudaMalloc: it and cudaFree are prohibited while a
+stream is captured into a CUDA graph and cudaFree synchronises the device, or
+their host program owns all device memory.  They pass device arrays they
+already own; the entry point keeps its per-element scratch in a static device
+array.  Its result must equal the handle entry point spoc_energy (same
+kernels, same summation order) and the CPU oracle's energy (1e-13 relative,
+the energy tolerance of the other tests), on two calls in a row so that a
 stale scratch would show.  This file is collected last on purpose.
 """
 import ctypes as C
@@ -13,6 +14,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from spoc_b200 import api
 from spoc_b200 import workloads as W
 
@@ -40,9 +42,13 @@ def test_energy_noalloc_matches_handle_entry_point():
     ammo1 = _dev(torch, T.ammo[0, :])  # ammo(j, 1)
     hb = _dev(torch, p.hb)
     out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    OT = O.Tables(T.nc, T.ng, T.ngf, T.wi, T.xi, T.yi, T.wif, T.tif)
+    OM = O.Mesh(m.inn, m.xgr, m.ygr, T.nc, p.cfg.f0, p.cfg.beta, ld=45)
     for u, v, h in states:  # two calls in a row through the shared scratch
         s.set_state(u, v, h)
         ref = s.energy()
+        ora = O.energy(OT, OM, np.ascontiguousarray(u), np.ascontiguousarray(v),
+                       np.ascontiguousarray(h), p.hb, p.cfg.g0)
         du, dv, dh = (_dev(torch, a) for a in (u, v, h))
         torch.cuda.synchronize()
         rc = lib.spoc_energy_noalloc(T.nc, T.ng, m.ne, 45, p.cfg.g0, du.data_ptr(), dv.data_ptr(),
@@ -52,8 +58,9 @@ def test_energy_noalloc_matches_handle_entry_point():
         assert rc == 0
         torch.cuda.synchronize()
         got = out.cpu().numpy()
-        for g, r in zip(got, ref):
+        for g, r, o in zip(got, ref, ora):
             assert g == pytest.approx(r, rel=1e-13, abs=1e-300)
+            assert g == pytest.approx(o, rel=1e-13, abs=1e-300)
 
 
 @pytest.mark.gpu
