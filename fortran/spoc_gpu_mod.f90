@@ -51,6 +51,9 @@ module spoc_gpu_mod
       type(c_ptr) :: spoc_cal_var_status
     end function
 
+    subroutine spoc_cal_var_refresh() bind(c, name='spoc_cal_var_refresh')
+    end subroutine
+
     subroutine spoc_release_commons() bind(c, name='spoc_release_commons')
     end subroutine
 

@@ -293,9 +293,11 @@ int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long long *adj_s
  * Register the COMMON contents once (after dpotrf), then link this library
  * instead of calvar*.o: cal_var_ has the reference argument list
  * (src/calvarnl_fs.f:9-12) with gfortran's by-reference, trailing-underscore
- * ABI.  A handle is created on the first call and reused while nf, ne and a
- * content key of the mesh arrays and of fc, w0, z0, hb are unchanged (the
- * adaptive driver rewrites them in place at a regrid).
+ * ABI.  A handle is created on the first call and reused while nf, ne, a
+ * content key of the mesh arrays (tseg, ssit, itm, its, bdl, norm, vect,
+ * normt: the adaptive driver rewrites them in place at a regrid) and the
+ * addresses of fc, w0, z0, hb are unchanged; spoc_cal_var_refresh() makes the
+ * next call upload everything (fields rewritten in place on the same mesh).
  * Errors set *spoc_cal_var_status() (the reference `stop`s instead). */
 int spoc_register_commons(const spoc_tables *tables, int variant, int precision);
 void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, double *u1, double *v1,
@@ -304,6 +306,7 @@ void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, double *u1, 
               double *normt, double *mu0, double *mb0, double *fc, double *beta, double *w0,
               double *z0, double *g0, double *hb, double *time);
 int *spoc_cal_var_status(void);
+void spoc_cal_var_refresh(void);
 void spoc_release_commons(void);
 
 /* ---- host set-up helpers (no CUDA) ----

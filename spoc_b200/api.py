@@ -137,6 +137,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "spoc_register_commons": (C.c_int, [C.POINTER(_Tables), C.c_int, C.c_int]),
         "spoc_cal_var_status": (_IP, []),
         "spoc_release_commons": (None, []),
+        "spoc_cal_var_refresh": (None, []),
         "spoc_build_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP,
                                         _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _IP]),
         "spoc_build_mesh": (C.c_int, [C.c_int, C.c_int, _IP, _DP, _DP, C.c_int, C.c_double,

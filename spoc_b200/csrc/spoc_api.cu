@@ -886,19 +886,25 @@ struct Commons {
   int ld_pi2 = 0, ld_p1 = 0, ld_p2 = 0;
   spoc_handle *h = nullptr;
   int h_ne = 0, h_nf = 0;
-  uint64_t h_key = 0;  // content key of the mesh and fields the handle holds
+  uint64_t h_key = 0;    // content key of the mesh the handle holds
+  bool refresh = false;  // spoc_cal_var_refresh: upload everything on the next call
   int status = 0;
 };
 Commons g_commons;
 std::mutex g_commons_mu;
 
-// Content key of the arrays cal_var_ uploads.  The adaptive driver keeps its
-// mesh and field arrays at fixed addresses and rewrites them in place at
-// every regrid (src/shwwnl_adap.f:20, :397-433), possibly with the same
-// element and face counts, so a cached device copy is reused only while the
-// contents are unchanged.  Four independent multiply-xorshift lanes over
-// 64-bit words (the array lengths are mixed in too); only the nm used rows
-// of each (ld, ne) field are read.
+// Content key of the mesh cal_var_ uploads.  The adaptive driver keeps its
+// mesh arrays at fixed addresses and rewrites them in place at every regrid
+// (src/shwwnl_adap.f:20, :397-433), possibly with the same element and face
+// counts, so the device copy is reused only while the connectivity and
+// geometry (tseg, ssit, itm, its, bdl, norm, vect, normt: ~4 MB at 32768
+// elements) hash to the same key.  The per-element fields fc, w0, z0, hb
+// change with the mesh (the driver re-projects them at a regrid,
+// src/adapt.f:303-373); their addresses enter the key, and a caller that
+// rewrites them in place on an unchanged mesh calls spoc_cal_var_refresh().
+// Hashing them too would read ~30 MB per call (about 4 ms at one host core's
+// bandwidth, more than the right-hand side itself).  Four CRC-32C streams
+// where the host has SSE4.2 (memory-bound), else four multiply-xorshift lanes.
 struct ContentKey {
   uint64_t lane[4] = {0x243f6a8885a308d3ull, 0x13198a2e03707344ull, 0xa4093822299f31d0ull,
                       0x082efa98ec4e6c89ull};
@@ -907,28 +913,56 @@ struct ContentKey {
     h *= 0x9e3779b97f4a7c15ull;
     return h ^ (h >> 31);
   }
+#if defined(__x86_64__)
+  __attribute__((target("sse4.2"))) void crc_words(const unsigned char *b, size_t nw) {
+    uint64_t c[4] = {lane[0], lane[1], lane[2], lane[3]};
+    size_t i = 0;
+    for (; i + 4 <= nw; i += 4) {
+      uint64_t w[4];
+      std::memcpy(w, b + 8 * i, 32);
+      for (int k = 0; k < 4; ++k) c[k] = __builtin_ia32_crc32di(c[k], w[k]);
+    }
+    for (; i < nw; ++i) {
+      uint64_t w;
+      std::memcpy(&w, b + 8 * i, 8);
+      c[0] = __builtin_ia32_crc32di(c[0], w);
+    }
+    for (int k = 0; k < 4; ++k) lane[k] = c[k];
+  }
+  static bool have_crc() {
+    static const bool ok = __builtin_cpu_supports("sse4.2");
+    return ok;
+  }
+#endif
   void bytes(const void *p, size_t n) {
     const unsigned char *b = static_cast<const unsigned char *>(p);
-    size_t i = 0;
-    for (; i + 32 <= n; i += 32) {
-      uint64_t w[4];
-      std::memcpy(w, b + i, 32);
-      for (int k = 0; k < 4; ++k) lane[k] = mix(lane[k], w[k]);
+    const size_t nw = n / 8;
+#if defined(__x86_64__)
+    if (have_crc()) {
+      crc_words(b, nw);
+    } else
+#endif
+    {
+      size_t i = 0;
+      for (; i + 4 <= nw; i += 4) {
+        uint64_t w[4];
+        std::memcpy(w, b + 8 * i, 32);
+        for (int k = 0; k < 4; ++k) lane[k] = mix(lane[k], w[k]);
+      }
+      for (; i < nw; ++i) {
+        uint64_t w;
+        std::memcpy(&w, b + 8 * i, 8);
+        lane[0] = mix(lane[0], w);
+      }
     }
-    for (; i < n; i += 8) {
+    if (n % 8) {
       uint64_t w = 0;
-      std::memcpy(&w, b + i, std::min<size_t>(8, n - i));
+      std::memcpy(&w, b + 8 * nw, n % 8);
       lane[0] = mix(lane[0], w);
     }
     lane[1] = mix(lane[1], (uint64_t)n);
   }
-  void field(const double *a, int ld, int nm, int ne) {
-    if (!a) {
-      lane[2] = mix(lane[2], 0x6a09e667f3bcc908ull);
-      return;
-    }
-    for (int e = 0; e < ne; ++e) bytes(a + (size_t)e * ld, (size_t)nm * sizeof(double));
-  }
+  void word(uint64_t w) { lane[2] = mix(lane[2], w); }
   uint64_t digest() const {
     uint64_t h = 0;
     for (int k = 0; k < 4; ++k) h = mix(h, lane[k]);
@@ -978,6 +1012,11 @@ extern "C" int spoc_register_commons(const spoc_tables *t, int variant, int prec
   return SPOC_OK;
 }
 
+extern "C" void spoc_cal_var_refresh(void) {
+  std::lock_guard<std::mutex> lk(g_commons_mu);
+  g_commons.refresh = true;
+}
+
 extern "C" void spoc_release_commons(void) {
   std::lock_guard<std::mutex> lk(g_commons_mu);
   if (g_commons.h) spoc_destroy(g_commons.h);
@@ -1012,12 +1051,9 @@ extern "C" void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, d
   ck.bytes(norm, sizeof(double) * 2 * (size_t)nf_);
   ck.bytes(vect, sizeof(double) * 5 * (size_t)ne_);
   ck.bytes(normt, sizeof(double) * 2 * (size_t)ne_);
-  ck.field(fc, c.ld, c.nm, ne_);
-  ck.field(w0, c.ld, c.nm, ne_);
-  ck.field(z0, c.ld, c.nm, ne_);
-  ck.field(hb, c.ld, c.nm, ne_);
+  for (const double *a : {fc, w0, z0, hb}) ck.word((uint64_t)(uintptr_t)a);
   const uint64_t key = ck.digest();
-  const bool same = c.h && c.h_ne == ne_ && c.h_nf == nf_ && c.h_key == key;
+  const bool same = c.h && !c.refresh && c.h_ne == ne_ && c.h_nf == nf_ && c.h_key == key;
   if (!same) {
     if (c.h) {
       spoc_destroy(c.h);
@@ -1048,6 +1084,7 @@ extern "C" void cal_var_(int *nf, int *ne, double *u0, double *v0, double *h0, d
     c.h_ne = ne_;
     c.h_nf = nf_;
     c.h_key = key;
+    c.refresh = false;
   } else {
     c.h->mu0 = *mu0;
     c.h->mb0 = *mb0;

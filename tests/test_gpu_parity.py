@@ -269,6 +269,13 @@ def test_fortran_drop_in_mesh_rewritten_in_place(gpu_lib):
     ref = O.cal_var(c.variant, OTq, OMq, p.u, p.v, p.h, OMq.fc, q.w0, q.z0, q.hb, c.mu0, c.mb0,
                     c.g0)
     assert_bitwise(outs, ref, p.T.nm)
+    # depth rewritten in place on the same mesh: announced with spoc_cal_var_refresh
+    hb[:, 0] = 3000.0
+    lib.spoc_cal_var_refresh()
+    lib.cal_var_(*args)
+    assert lib.spoc_cal_var_status()[0] == 0
+    ref = O.cal_var(c.variant, OTq, OMq, p.u, p.v, p.h, OMq.fc, q.w0, q.z0, hb, c.mu0, c.mb0, c.g0)
+    assert_bitwise(outs, ref, p.T.nm)
     lib.spoc_release_commons()
 
 
