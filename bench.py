@@ -181,6 +181,25 @@ def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, ts
     }
 
 
+def fp64_configs_measure(torch, stream, flush, W, names=("c1_lin_p3", "c4_ns_p4"), steps=20):
+    """Plain FP64 step of the other single-GPU configurations (C3 in
+    mixed_measure): ms per RK4 step, L2 flushed before each, and DOF-updates/s."""
+    out = {}
+    for name in names:
+        p = W.build_problem(W.CONFIGS[name])
+        s = W.make_solver(p)
+        s.set_stream(stream.cuda_stream)
+        s.set_state(p.u, p.v, p.h)
+        s.rk4_steps(p.dt, 3)
+        l0 = s.launches
+        ms = timed_steps(torch, stream, flush, s, p.dt, steps)
+        out[name] = {"ne": p.mesh.ne, "nm": p.T.nm, "ms_per_step": ms,
+                     "value": 3.0 * p.T.nm * p.mesh.ne / (ms * 1e-3), "unit": UNIT,
+                     "launches_per_step": (s.launches - l0) / steps}
+        s.close()
+    return out
+
+
 MIXED_RUNS = {"c1_lin_p3": 1000, "c2_fs_p6": 2000, "c4_ns_p4": 200}
 
 
@@ -332,7 +351,17 @@ def drop_in_measure(torch, W, api, p, steps=5):
     # ---- cal_var_ (31 by-reference arguments), ld = 45, pageable ----
     lib = api.load_library()
     T45 = p.T
-    ts = T45.struct()
+    # the COMMON matrices with the reference's leading dimension nnmod = 45,
+    # which is also the leading dimension cal_var_ takes for the state arrays
+    mats = {}
+    for name in ("amm", "amml", "agx", "agy", "ammo"):
+        a = np.zeros((nm, ld))
+        a[:, :nm] = getattr(T45, name)
+        mats[name] = a
+    ts = api._Tables(T45.nc, nm, T45.ng, T45.ngf, api._d(T45.wi), api._d(T45.xi), api._d(T45.yi),
+                     api._d(T45.wif), api._d(T45.tif), api._d(T45.pi2), T45.ng, api._d(T45.pico),
+                     T45.ngf, nm, api._d(mats["amm"]), api._d(mats["amml"]), api._d(mats["agx"]),
+                     api._d(mats["agy"]), api._d(mats["ammo"]), ld, api._i(T45.cip))
     assert lib.spoc_register_commons(C.byref(ts), api.VARIANTS[cfg.variant], api.FP64) == 0
     keep = []
 
@@ -362,15 +391,24 @@ def drop_in_measure(torch, W, api, p, steps=5):
         if lib.spoc_cal_var_status()[0] != 0:
             raise RuntimeError("cal_var_ failed: " + str(lib.spoc_last_error()))
 
+    in_calls = [0.0]
+
     def run(rhs, alloc):
         x = [alloc(a) for a in (p.u, p.v, p.h)]
         w = {"d": [[alloc(None) for _ in range(3)] for _ in range(4)],
              "y": [alloc(None) for _ in range(3)], "t": alloc(None)}
+
+        def timed_rhs(*args):
+            t = time.perf_counter()
+            rhs(*args)
+            in_calls[0] += time.perf_counter() - t
+
         host_rk4_step(rhs, *x, p.dt, w)  # warm-up (upload of the mesh on the first call)
         torch.cuda.synchronize()
+        in_calls[0] = 0.0
         t0 = time.perf_counter()
         for _ in range(steps):
-            host_rk4_step(rhs, *x, p.dt, w)
+            host_rk4_step(timed_rhs, *x, p.dt, w)
         sec = time.perf_counter() - t0
         same = all(np.array_equal(x[i][:, :nm], ref[i][:, :nm]) for i in range(3))
         return sec, same
@@ -379,6 +417,8 @@ def drop_in_measure(torch, W, api, p, steps=5):
     lib.spoc_release_commons()
     res["cal_var_"] = {
         "value": dof * steps / sec, "unit": UNIT, "ms_per_step": 1e3 * sec / steps,
+        "ms_per_call": 1e3 * in_calls[0] / (4 * steps),
+        "host_axpy_ms_per_step": 1e3 * (sec - in_calls[0]) / steps,
         "h2d_bytes_per_step": 4 * 3 * ne * nm * 8, "d2h_bytes_per_step": 4 * 3 * ne * nm * 8,
         "arrays": "pageable numpy, leading dimension 45 (nnmod)",
         "bitwise_equal_to_device_resident_run": same}
@@ -403,6 +443,8 @@ def drop_in_measure(torch, W, api, p, steps=5):
     s.close()
     res["spoc_cal_var"] = {
         "value": dof * steps / sec, "unit": UNIT, "ms_per_step": 1e3 * sec / steps,
+        "ms_per_call": 1e3 * in_calls[0] / (4 * steps),
+        "host_axpy_ms_per_step": 1e3 * (sec - in_calls[0]) / steps,
         "h2d_bytes_per_step": 4 * 3 * ne * nm * 8, "d2h_bytes_per_step": 4 * 3 * ne * nm * 8,
         "arrays": "pinned, packed (ld = nm)",
         "bitwise_equal_to_device_resident_run": same}
@@ -882,6 +924,9 @@ def main():
                            f: mnorm(st2[i] - ref_state[i]) / mnorm(ref_state[i])
                            for i, f in enumerate(("u", "v", "eta"))}})
 
+    fp64_configs = None
+    if world == 1 and args.precision == "fp64":
+        fp64_configs = fp64_configs_measure(torch, stream, flush, W)
     mixed = mixed_all = None
     if world == 1 and not args.no_mixed:
         mixed = mixed_measure(torch, stream, flush, W, api)
@@ -912,6 +957,7 @@ def main():
             "kernel_ms_per_launch": per_launch_ms,
             "roofline": roof,
             "other_precisions": others,
+            "fp64_other_configs": fp64_configs,
             "mixed_c3": mixed,
             "mixed_errors": mixed_all,
             "ensemble_c5": ensemble,

@@ -74,6 +74,11 @@ struct spoc_handle {
   // FP64: one RK4 step captured as a CUDA graph (replayed by spoc_rk4_steps),
   // valid for the scalars baked into its kernel arguments
   cudaGraphExec_t step_graph = nullptr;
+  // spoc_cal_var with strided (ld > nm) host arrays: a device copy of one
+  // whole caller array, and pinned bounce buffers of the packed outputs
+  double *ld_stage = nullptr;
+  size_t ld_stage_n = 0;
+  double *bounce[3] = {};
   double graph_key[6] = {};
   long long graph_launches = 0;
 
@@ -93,6 +98,8 @@ struct spoc_handle {
   }
   ~spoc_handle() {
     if (step_graph) cudaGraphExecDestroy(step_graph);
+    for (double *b : bounce)
+      if (b) cudaFreeHost(b);
     if (mx) mixed_destroy(mx);
     for (void *p : allocs) cudaFree(p);
     if (side_ev) cudaEventDestroy(side_ev);
@@ -517,15 +524,48 @@ extern "C" int spoc_cal_var(spoc_handle *h, int ld, const double *u0, const doub
   if (!h || !u0 || !v0 || !h0 || !u1 || !v1 || !h1) return fail(SPOC_E_ARG, "null argument");
   if (ld < h->nm) return fail(SPOC_E_ARG, "ld < nm");
   if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
-  CK(copy_in(h, h->SIN[0], u0, ld, cudaMemcpyHostToDevice), "upload u0");
-  CK(copy_in(h, h->SIN[1], v0, ld, cudaMemcpyHostToDevice), "upload v0");
-  CK(copy_in(h, h->SIN[2], h0, ld, cudaMemcpyHostToDevice), "upload h0");
+  if (ld == h->nm) {
+    CK(copy_in(h, h->SIN[0], u0, ld, cudaMemcpyHostToDevice), "upload u0");
+    CK(copy_in(h, h->SIN[1], v0, ld, cudaMemcpyHostToDevice), "upload v0");
+    CK(copy_in(h, h->SIN[2], h0, ld, cudaMemcpyHostToDevice), "upload h0");
+    int rc = run_rhs_tend(h, h->SIN);
+    if (rc) return rc;
+    CK(copy_out(h, u1, h->TEND[0], ld, cudaMemcpyDeviceToHost), "download u1");
+    CK(copy_out(h, v1, h->TEND[1], ld, cudaMemcpyDeviceToHost), "download v1");
+    CK(copy_out(h, h1, h->TEND[2], ld, cudaMemcpyDeviceToHost), "download h1");
+    return check_flag(h);
+  }
+  // Strided caller arrays (the reference's (nnmod, ne) layout): each input
+  // moves as one contiguous copy of the whole array and is packed on the
+  // device; each output comes back packed into pinned memory and is spread
+  // into the caller's rows on the host, which leaves rows nm+1..ld of the
+  // caller's arrays untouched, as the reference does (a copy of ne rows of nm
+  // doubles runs far below the link bandwidth from pageable memory).
+  const size_t nld = (size_t)ld * h->ne, npk = fsize(h);
+  if (h->ld_stage_n < nld) {
+    h->ld_stage = nullptr;
+    CK(h->alloc(&h->ld_stage, nld), "staging allocation");
+    h->ld_stage_n = nld;
+  }
+  for (int c = 0; c < 3; ++c)
+    if (!h->bounce[c]) CK(cudaHostAlloc((void **)&h->bounce[c], sizeof(double) * npk, 0), "pinned allocation");
+  const double *in[3] = {u0, v0, h0};
+  for (int c = 0; c < 3; ++c) {
+    CK(cudaMemcpyAsync(h->ld_stage, in[c], sizeof(double) * nld, cudaMemcpyHostToDevice, h->st),
+       "upload state");
+    CK(launch_pack_rows(h->ne, h->nm, ld, h->ld_stage, h->SIN[c], h->st, h->sms), "pack state");
+  }
   int rc = run_rhs_tend(h, h->SIN);
   if (rc) return rc;
-  CK(copy_out(h, u1, h->TEND[0], ld, cudaMemcpyDeviceToHost), "download u1");
-  CK(copy_out(h, v1, h->TEND[1], ld, cudaMemcpyDeviceToHost), "download v1");
-  CK(copy_out(h, h1, h->TEND[2], ld, cudaMemcpyDeviceToHost), "download h1");
-  return check_flag(h);
+  for (int c = 0; c < 3; ++c)
+    CK(cudaMemcpyAsync(h->bounce[c], h->TEND[c], sizeof(double) * npk, cudaMemcpyDeviceToHost, h->st),
+       "download tendency");
+  rc = check_flag(h);  // synchronises the stream
+  double *out[3] = {u1, v1, h1};
+  for (int c = 0; c < 3; ++c)
+    for (int e = 0; e < h->ne; ++e)
+      std::memcpy(out[c] + (size_t)e * ld, h->bounce[c] + (size_t)e * h->nm, sizeof(double) * h->nm);
+  return rc;
 }
 
 extern "C" int spoc_cal_var_dev(spoc_handle *h, int ld, const double *u0, const double *v0,

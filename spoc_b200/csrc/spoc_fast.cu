@@ -660,6 +660,63 @@ struct __align__(16) QWarp {
   double sm[64];
 };
 
+// One element of the q-phase from the face-value chains on: own / nb hold the
+// element's and its neighbours' u, v; prefetch() is called once they are free
+// (after the mat-vecs); gq receives gxx, gxy, gyx, gyy.
+template <class Dm, int VAR, class Prefetch>
+__device__ __forceinline__ void qphase_elem(const SOps<Dm> &S, const DevMesh &m, int e,
+                                            const Sides &sd, const double *own, const double *nb,
+                                            double *fr, double *fb, double *sm, Prefetch prefetch,
+                                            double (&gq)[4][Dm::R]) {
+  constexpr int N = Dm::N, R = Dm::R;
+  const Geo g = geo(m, e);
+  int isg[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
+  face_values<Dm, 2>(S.pf, m, sd, own, nb, fr);
+  __syncwarp();
+  scale_face<Dm>(m, sd, fr, fb + 0, 0);
+  scale_face<Dm>(m, sd, fr, fb + 32, 1);
+  scale_face<Dm>(m, sd, fr + 32, fb + 64, 0);
+  scale_face<Dm>(m, sd, fr + 32, fb + 96, 1);
+  double ax[2][R], bx[2][R];
+  matvec2<Dm, 2>(S.agx, S.agy, own, N, ax, bx);
+  __syncwarp();  // own / nb are free from here on
+  prefetch();
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const double gx1 = add(0.0, mul(ax[c][r], -1.0)), gy1 = add(0.0, mul(bx[c][r], -1.0));
+      gq[2 * c][r] = mul(sub(mul(g.by, gx1), mul(g.ay, gy1)), g.detai);
+      gq[2 * c + 1][r] = mul(add(-mul(g.bx, gx1), mul(g.ax, gy1)), g.detai);
+    }
+  double t[4][3][R];
+  lift_sums<Dm, 4>(S, isg, fb, t);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) apply_lift<R>(gq[c], t[c], isg, g.detai);
+  if (VAR == kFS && __ldg(m.bdl + e)) {
+    // calvarnl_fs.f:171-204
+    const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+    double gnx[R], gtx[R], gny[R], gty[R], gtn[R], bu[1][R];
+    double fs3[3][R];  // gnn, gnt, gtt
+    rot<R>(gnx, gtx, gq[0], gq[2], dnx, dny);
+    rot<R>(gny, gty, gq[1], gq[3], dnx, dny);
+    rot<R>(fs3[0], fs3[1], gnx, gny, dnx, dny);
+    rot<R>(gtn, fs3[2], gtx, gty, dnx, dny);
+    reduc<Dm>(S, gtn, bu[0], sm);
+    solve_full_b<Dm, SOps<Dm>, 3>(S, fs3);
+    solve_red_b<Dm, SOps<Dm>, 1>(S, bu);
+    reduc_inv<Dm>(S, bu[0], gtn, sm);
+    rot<R>(gnx, gny, fs3[0], fs3[1], dnx, dny);
+    rot<R>(gtx, gty, gtn, fs3[2], dnx, dny);
+    rot<R>(gq[0], gq[2], gnx, gtx, dnx, dny);
+    rot<R>(gq[1], gq[3], gny, gty, dnx, dny);
+  } else {
+    solve_full_b<Dm, SOps<Dm>, 4>(S, gq);
+  }
+}
+
 template <class Dm, int VAR>
 __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *__restrict__ su,
                                                  const double *__restrict__ sv, double *q) {
@@ -689,10 +746,6 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
     const Sides sd = PF ? sd_next : sides_of(m, e);
     const int en = e + warp_count();
     if (PF && en < m.ne) sd_next = sides_of(m, en);
-    const Geo g = geo(m, e);
-    int isg[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
     if constexpr (PF) {
       cp_async_wait_all();
     } else {
@@ -701,49 +754,10 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
       stage_neighbours<Dm, 2>(sd, W.nb, [&](int f, int t, int i) { return fields[f][(size_t)t * N + i]; });
     }
     __syncwarp();
-    face_values<Dm, 2>(S.pf, m, sd, W.own, W.nb, W.fr);
-    __syncwarp();
-    scale_face<Dm>(m, sd, W.fr, W.fb + 0, 0);
-    scale_face<Dm>(m, sd, W.fr, W.fb + 32, 1);
-    scale_face<Dm>(m, sd, W.fr + 32, W.fb + 64, 0);
-    scale_face<Dm>(m, sd, W.fr + 32, W.fb + 96, 1);
-    double ax[2][R], bx[2][R];
-    matvec2<Dm, 2>(S.agx, S.agy, W.own, N, ax, bx);
-    __syncwarp();  // W.own / W.nb are free from here on
-    if (PF && en < m.ne) prefetch_element<Dm, 2>(fields, en, sd_next, W.own, W.nb);
     double gq[4][R];  // gxx, gxy, gyx, gyy
-#pragma unroll
-    for (int c = 0; c < 2; ++c)
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const double gx1 = add(0.0, mul(ax[c][r], -1.0)), gy1 = add(0.0, mul(bx[c][r], -1.0));
-        gq[2 * c][r] = mul(sub(mul(g.by, gx1), mul(g.ay, gy1)), g.detai);
-        gq[2 * c + 1][r] = mul(add(-mul(g.bx, gx1), mul(g.ax, gy1)), g.detai);
-      }
-    double t[4][3][R];
-    lift_sums<Dm, 4>(S, isg, W.fb, t);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) apply_lift<R>(gq[c], t[c], isg, g.detai);
-    if (VAR == kFS && __ldg(m.bdl + e)) {
-      // calvarnl_fs.f:171-204
-      const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
-      double gnx[R], gtx[R], gny[R], gty[R], gtn[R], bu[1][R];
-      double fs3[3][R];  // gnn, gnt, gtt
-      rot<R>(gnx, gtx, gq[0], gq[2], dnx, dny);
-      rot<R>(gny, gty, gq[1], gq[3], dnx, dny);
-      rot<R>(fs3[0], fs3[1], gnx, gny, dnx, dny);
-      rot<R>(gtn, fs3[2], gtx, gty, dnx, dny);
-      reduc<Dm>(S, gtn, bu[0], W.sm);
-      solve_full_b<Dm, SOps<Dm>, 3>(S, fs3);
-      solve_red_b<Dm, SOps<Dm>, 1>(S, bu);
-      reduc_inv<Dm>(S, bu[0], gtn, W.sm);
-      rot<R>(gnx, gny, fs3[0], fs3[1], dnx, dny);
-      rot<R>(gtx, gty, gtn, fs3[2], dnx, dny);
-      rot<R>(gq[0], gq[2], gnx, gtx, dnx, dny);
-      rot<R>(gq[1], gq[3], gny, gty, dnx, dny);
-    } else {
-      solve_full_b<Dm, SOps<Dm>, 4>(S, gq);
-    }
+    qphase_elem<Dm, VAR>(S, m, e, sd, W.own, W.nb, W.fr, W.fb, W.sm, [&] {
+      if (PF && en < m.ne) prefetch_element<Dm, 2>(fields, en, sd_next, W.own, W.nb);
+    }, gq);
 #pragma unroll
     for (int c = 0; c < 4; ++c) store_reg<Dm>(q + c * fs, gq[c], e);
     __syncwarp();
@@ -760,20 +774,53 @@ struct __align__(16) BWarp {
   double wp[8 * Dm::Q];
   double tail[9 * T];  // values of the nine fields at those points
   double sm[64];
+  // one row per lane: the element's su, sv, sh, hb, w0, z0, fc and q (4
+  // fields), copied ahead while the previous element is computed
+  double rows[Dm::R == 1 ? 11 * Dm::N : 2];
 };
 
-template <class Dm, int VAR>
-__device__ __forceinline__ void nlvol_body(DevOps op, DevMesh m, NlArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  SOpsQ<Dm> &S = *reinterpret_cast<SOpsQ<Dm> *>(smem);
-  BWarp<Dm> &W = reinterpret_cast<BWarp<Dm> *>(smem + sizeof(SOpsQ<Dm>))[warp_in_block()];
+// cp.async copies of element e's eleven input rows of the quadrature-point
+// phase into rows[f*N + lane]
+template <class Dm>
+__device__ __forceinline__ void prefetch_nl_rows(const NlArgs &a, int e, size_t fs, double *rows) {
+  const int l = lane_id();
+  if (l >= Dm::N) return;
+  const size_t o = (size_t)e * Dm::N + l;
+  const double *const src[11] = {a.su, a.sv, a.sh, a.hb, a.w0, a.z0, a.fc,
+                                 a.q, a.q + fs, a.q + 2 * fs, a.q + 3 * fs};
+#pragma unroll
+  for (int f = 0; f < 11; ++f) cp_async8(rows + f * Dm::N + l, src[f] + o);
+}
+
+// One element of the quadrature-point phase, given its q (qq): spectoxy of
+// the nine fields, the products, xytospec, the uh / vh solves (wall
+// projections included) and the stores of gx0, gy0, uh, vh, F.  so holds the
+// solve operators and index maps (SOps or SOpsQ), p2 / p2t / wi the
+// quadrature tables; vin, wp, tail, sm are the warp's scratch.
+// rows: the element's input rows already in shared memory (one row per
+// lane), or null to load them from global memory; after_load() runs once
+// they are in registers.
+template <class Dm, int VAR, class Ops, class AfterLoad>
+__device__ __forceinline__ void nlvol_elem(const Ops &S, const double *p2, const double *p2t,
+                                           const double *wi, double *vin, double *wp, double *tail,
+                                           double *sm, const DevMesh &m, const NlArgs &a, int e,
+                                           const double (&qq)[4][Dm::R], const double *rows,
+                                           AfterLoad after_load) {
   constexpr int N = Dm::N, Q = Dm::Q, R = Dm::R, RQ = Dm::RQ;
-  __shared__ __align__(8) uint64_t ops_bar;
-  if (!bulk::stage_block(&S, op.img_q, sizeof(SOpsQ<Dm>), &ops_bar, op.flag)) return;
+  constexpr int T = Dm::Q > 32 ? Dm::Q - 32 : 1;  // quadrature points past lane 31
   const int l = lane_id();
   const size_t fs = (size_t)m.ne * N;
-  for (int e = warp_global(); e < m.ne; e += warp_count()) {
-    double uk[R], vk[R], hh[R], qq[4][R], fc[R], hb[R], w0[R], z0[R];
+  double uk[R], vk[R], hh[R], fc[R], hb[R], w0[R], z0[R];
+  if (rows) {
+    const bool in = l < N;
+    uk[0] = in ? rows[0 * N + l] : 0.0;
+    vk[0] = in ? rows[1 * N + l] : 0.0;
+    hh[0] = in ? rows[2 * N + l] : 0.0;
+    hb[0] = in ? rows[3 * N + l] : 0.0;
+    w0[0] = in ? rows[4 * N + l] : 0.0;
+    z0[0] = in ? rows[5 * N + l] : 0.0;
+    fc[0] = in ? rows[6 * N + l] : 0.0;
+  } else {
     load_reg<Dm>(uk, a.su, e);
     load_reg<Dm>(vk, a.sv, e);
     load_reg<Dm>(hh, a.sh, e);
@@ -781,137 +828,170 @@ __device__ __forceinline__ void nlvol_body(DevOps op, DevMesh m, NlArgs a) {
     load_reg<Dm>(w0, a.w0, e);
     load_reg<Dm>(z0, a.z0, e);
     load_reg<Dm>(fc, a.fc, e);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) load_reg<Dm>(qq[c], a.q + c * fs, e);
-    // uk,vk,hk=h+hb,wk=w-mb0 u,zk=z-mb0 v,gxx=qxx,gxy=qxy-fc,gyx=qyx+fc,gyy=qyy (:245-255)
-    {
-      double v9[9][R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        v9[0][r] = uk[r];
-        v9[1][r] = vk[r];
-        v9[2][r] = qq[0][r];
-        v9[3][r] = sub(qq[1][r], fc[r]);
-        v9[4][r] = add(qq[2][r], fc[r]);
-        v9[5][r] = qq[3][r];
-        v9[6][r] = add(hh[r], hb[r]);
-        v9[7][r] = sub(w0[r], mul(a.mb0, uk[r]));
-        v9[8][r] = sub(z0[r], mul(a.mb0, vk[r]));
-      }
-#pragma unroll
-      for (int f = 0; f < 9; ++f) reg_to_sm<Dm>(W.vin + f * N, v9[f]);
-    }
-    __syncwarp();
-    // spectoxy (src/nonlin.f:62-86) for the nine fields; lanes over points.
-    // Points past lane 31 (degree 6: one, degree 7: ten) would cost a second
-    // pass of nine full chains on a few lanes: their (field, point) chains are
-    // spread over the lanes instead, each still summed over n in order.
-    auto products = [&](int qp, const double (&mv)[9]) {
-      const double w = S.wi[qp];
-      W.wp[0 * Q + qp] = mul(w, mul(mv[0], mv[2]));
-      W.wp[1 * Q + qp] = mul(w, mul(mv[1], mv[3]));
-      W.wp[2 * Q + qp] = mul(w, mul(mv[0], mv[4]));
-      W.wp[3 * Q + qp] = mul(w, mul(mv[1], mv[5]));
-      W.wp[4 * Q + qp] = mul(w, mul(mv[0], mv[6]));
-      W.wp[5 * Q + qp] = mul(w, mul(mv[1], mv[6]));
-      W.wp[6 * Q + qp] = mul(w, __ddiv_rn(mv[7], mv[6]));
-      W.wp[7 * Q + qp] = mul(w, __ddiv_rn(mv[8], mv[6]));
-    };
-    if (l < Q) {
-      double mv[9];
-#pragma unroll
-      for (int f = 0; f < 9; ++f) mv[f] = 0.0;
-#pragma unroll 4
-      for (int n = 0; n < N; ++n) {
-        const double p = S.p2[n * Q + l];
-#pragma unroll
-        for (int f = 0; f < 9; ++f) mv[f] = macc(mv[f], W.vin[f * N + n], p);
-      }
-      products(l, mv);
-    }
-    if (RQ > 1) {
-      constexpr int T = BWarp<Dm>::T;
-#pragma unroll
-      for (int c0 = 0; c0 < 9 * T; c0 += 32) {
-        const int c = c0 + l;
-        if (c < 9 * T) {
-          const int f = c / T, t = c - f * T;
-          double v = 0.0;
-#pragma unroll 4
-          for (int n = 0; n < N; ++n) v = macc(v, W.vin[f * N + n], S.p2[n * Q + 32 + t]);
-          W.tail[c] = v;
-        }
-      }
-      __syncwarp();
-      if (l < T) {
-        double mv[9];
-#pragma unroll
-        for (int f = 0; f < 9; ++f) mv[f] = W.tail[f * T + l];
-        products(32 + l, mv);
-      }
-    }
-    __syncwarp();
-    // xytospec (src/nonlin.f:35-57, :91-107); lanes over modes
-    double X[8][R];
-#pragma unroll
-    for (int f = 0; f < 8; ++f)
-#pragma unroll
-      for (int r = 0; r < R; ++r) X[f][r] = 0.0;
-#pragma unroll 4
-    for (int qp = 0; qp < Q; ++qp) {
-      double p[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int n = l + 32 * r;
-        p[r] = n < N ? S.p2t[qp * N + n] : 0.0;
-      }
-#pragma unroll
-      for (int f = 0; f < 8; ++f) {
-        const double wv = W.wp[f * Q + qp];
-#pragma unroll
-        for (int r = 0; r < R; ++r) X[f][r] = macc(X[f][r], wv, p[r]);
-      }
-    }
-    double uv[2][R];
-    copy<R>(uv[0], X[4]);
-    copy<R>(uv[1], X[5]);
-    if (__ldg(m.bdl + e)) {
-      if (VAR == kNS) {
-        double bu[2][R];  // calvarnl_ns.f:249-265
-        reduc<Dm>(S, uv[0], bu[0], W.sm);
-        reduc<Dm>(S, uv[1], bu[1], W.sm);
-        solve_red_b<Dm, SOpsQ<Dm>, 2>(S, bu);
-        reduc_inv<Dm>(S, bu[0], uv[0], W.sm);
-        reduc_inv<Dm>(S, bu[1], uv[1], W.sm);
-      } else {
-        const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
-        double gn[R], gt[1][R], bu[1][R];
-        rot<R>(gn, gt[0], uv[0], uv[1], dnx, dny);
-        reduc<Dm>(S, gn, bu[0], W.sm);
-        solve_red_b<Dm, SOpsQ<Dm>, 1>(S, bu);
-        solve_full_b<Dm, SOpsQ<Dm>, 1>(S, gt);
-        reduc_inv<Dm>(S, bu[0], gn, W.sm);
-        rot<R>(uv[0], uv[1], gn, gt[0], dnx, dny);
-      }
-    } else {
-      solve_full_b<Dm, SOpsQ<Dm>, 2>(S, uv);
-    }
-    double gx0[R], gy0[R], f4[4][R];
+  }
+  after_load();
+  // uk,vk,hk=h+hb,wk=w-mb0 u,zk=z-mb0 v,gxx=qxx,gxy=qxy-fc,gyx=qyx+fc,gyy=qyy (:245-255)
+  {
+    double v9[9][R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      gx0[r] = add(-add(X[0][r], X[1][r]), X[6][r]);
-      gy0[r] = add(-add(X[2][r], X[3][r]), X[7][r]);
-      f4[0][r] = sub(mul(a.mu0, qq[0][r]), mul(a.g0, hh[r]));
-      f4[1][r] = mul(a.mu0, qq[1][r]);
-      f4[2][r] = mul(a.mu0, qq[2][r]);
-      f4[3][r] = sub(mul(a.mu0, qq[3][r]), mul(a.g0, hh[r]));
+      v9[0][r] = uk[r];
+      v9[1][r] = vk[r];
+      v9[2][r] = qq[0][r];
+      v9[3][r] = sub(qq[1][r], fc[r]);
+      v9[4][r] = add(qq[2][r], fc[r]);
+      v9[5][r] = qq[3][r];
+      v9[6][r] = add(hh[r], hb[r]);
+      v9[7][r] = sub(w0[r], mul(a.mb0, uk[r]));
+      v9[8][r] = sub(z0[r], mul(a.mb0, vk[r]));
     }
-    store_reg<Dm>(a.gx0, gx0, e);
-    store_reg<Dm>(a.gy0, gy0, e);
-    store_reg<Dm>(a.uh, uv[0], e);
-    store_reg<Dm>(a.vh, uv[1], e);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) store_reg<Dm>(a.f + c * fs, f4[c], e);
+    for (int f = 0; f < 9; ++f) reg_to_sm<Dm>(vin + f * N, v9[f]);
+  }
+  __syncwarp();
+  // spectoxy (src/nonlin.f:62-86) for the nine fields; lanes over points.
+  // Points past lane 31 (degree 6: one, degree 7: ten) would cost a second
+  // pass of nine full chains on a few lanes: their (field, point) chains are
+  // spread over the lanes instead, each still summed over n in order.
+  auto products = [&](int qp, const double (&mv)[9]) {
+    const double w = wi[qp];
+    wp[0 * Q + qp] = mul(w, mul(mv[0], mv[2]));
+    wp[1 * Q + qp] = mul(w, mul(mv[1], mv[3]));
+    wp[2 * Q + qp] = mul(w, mul(mv[0], mv[4]));
+    wp[3 * Q + qp] = mul(w, mul(mv[1], mv[5]));
+    wp[4 * Q + qp] = mul(w, mul(mv[0], mv[6]));
+    wp[5 * Q + qp] = mul(w, mul(mv[1], mv[6]));
+    wp[6 * Q + qp] = mul(w, __ddiv_rn(mv[7], mv[6]));
+    wp[7 * Q + qp] = mul(w, __ddiv_rn(mv[8], mv[6]));
+  };
+  if (l < Q) {
+    double mv[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) mv[f] = 0.0;
+#pragma unroll 4
+    for (int n = 0; n < N; ++n) {
+      const double p = p2[n * Q + l];
+#pragma unroll
+      for (int f = 0; f < 9; ++f) mv[f] = macc(mv[f], vin[f * N + n], p);
+    }
+    products(l, mv);
+  }
+  if (RQ > 1) {
+#pragma unroll
+    for (int c0 = 0; c0 < 9 * T; c0 += 32) {
+      const int c = c0 + l;
+      if (c < 9 * T) {
+        const int f = c / T, t = c - f * T;
+        double v = 0.0;
+#pragma unroll 4
+        for (int n = 0; n < N; ++n) v = macc(v, vin[f * N + n], p2[n * Q + 32 + t]);
+        tail[c] = v;
+      }
+    }
+    __syncwarp();
+    if (l < T) {
+      double mv[9];
+#pragma unroll
+      for (int f = 0; f < 9; ++f) mv[f] = tail[f * T + l];
+      products(32 + l, mv);
+    }
+  }
+  __syncwarp();
+  // xytospec (src/nonlin.f:35-57, :91-107); lanes over modes
+  double X[8][R];
+#pragma unroll
+  for (int f = 0; f < 8; ++f)
+#pragma unroll
+    for (int r = 0; r < R; ++r) X[f][r] = 0.0;
+#pragma unroll 4
+  for (int qp = 0; qp < Q; ++qp) {
+    double p[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int n = l + 32 * r;
+      p[r] = n < N ? p2t[qp * N + n] : 0.0;
+    }
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      const double wv = wp[f * Q + qp];
+#pragma unroll
+      for (int r = 0; r < R; ++r) X[f][r] = macc(X[f][r], wv, p[r]);
+    }
+  }
+  double uv[2][R];
+  copy<R>(uv[0], X[4]);
+  copy<R>(uv[1], X[5]);
+  if (__ldg(m.bdl + e)) {
+    if (VAR == kNS) {
+      double bu[2][R];  // calvarnl_ns.f:249-265
+      reduc<Dm>(S, uv[0], bu[0], sm);
+      reduc<Dm>(S, uv[1], bu[1], sm);
+      solve_red_b<Dm, Ops, 2>(S, bu);
+      reduc_inv<Dm>(S, bu[0], uv[0], sm);
+      reduc_inv<Dm>(S, bu[1], uv[1], sm);
+    } else {
+      const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
+      double gn[R], gt[1][R], bu[1][R];
+      rot<R>(gn, gt[0], uv[0], uv[1], dnx, dny);
+      reduc<Dm>(S, gn, bu[0], sm);
+      solve_red_b<Dm, Ops, 1>(S, bu);
+      solve_full_b<Dm, Ops, 1>(S, gt);
+      reduc_inv<Dm>(S, bu[0], gn, sm);
+      rot<R>(uv[0], uv[1], gn, gt[0], dnx, dny);
+    }
+  } else {
+    solve_full_b<Dm, Ops, 2>(S, uv);
+  }
+  double gx0[R], gy0[R], f4[4][R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    gx0[r] = add(-add(X[0][r], X[1][r]), X[6][r]);
+    gy0[r] = add(-add(X[2][r], X[3][r]), X[7][r]);
+    f4[0][r] = sub(mul(a.mu0, qq[0][r]), mul(a.g0, hh[r]));
+    f4[1][r] = mul(a.mu0, qq[1][r]);
+    f4[2][r] = mul(a.mu0, qq[2][r]);
+    f4[3][r] = sub(mul(a.mu0, qq[3][r]), mul(a.g0, hh[r]));
+  }
+  store_reg<Dm>(a.gx0, gx0, e);
+  store_reg<Dm>(a.gy0, gy0, e);
+  store_reg<Dm>(a.uh, uv[0], e);
+  store_reg<Dm>(a.vh, uv[1], e);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) store_reg<Dm>(a.f + c * fs, f4[c], e);
+}
+
+template <class Dm, int VAR>
+__device__ __forceinline__ void nlvol_body(DevOps op, DevMesh m, NlArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SOpsQ<Dm> &S = *reinterpret_cast<SOpsQ<Dm> *>(smem);
+  BWarp<Dm> &W = reinterpret_cast<BWarp<Dm> *>(smem + sizeof(SOpsQ<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, R = Dm::R;
+  __shared__ __align__(8) uint64_t ops_bar;
+  if (!bulk::stage_block(&S, op.img_q, sizeof(SOpsQ<Dm>), &ops_bar, op.flag)) return;
+  const size_t fs = (size_t)m.ne * N;
+  // one row per lane: the next element's input rows are copied into W.rows
+  // while the current one is computed
+  constexpr bool PF = Dm::R == 1;
+  if (PF && warp_global() < m.ne) prefetch_nl_rows<Dm>(a, warp_global(), fs, W.rows);
+  for (int e = warp_global(); e < m.ne; e += warp_count()) {
+    const int en = e + warp_count();
+    double qq[4][R];
+    if constexpr (PF) {
+      cp_async_wait_all();
+      __syncwarp();
+      const int l = lane_id();
+#pragma unroll
+      for (int c = 0; c < 4; ++c) qq[c][0] = l < N ? W.rows[(7 + c) * N + l] : 0.0;
+      nlvol_elem<Dm, VAR>(S, S.p2, S.p2t, S.wi, W.vin, W.wp, W.tail, W.sm, m, a, e, qq, W.rows, [&] {
+        __syncwarp();  // every lane has its rows in registers
+        if (en < m.ne) prefetch_nl_rows<Dm>(a, en, fs, W.rows);
+      });
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) load_reg<Dm>(qq[c], a.q + c * fs, e);
+      nlvol_elem<Dm, VAR>(S, S.p2, S.p2t, S.wi, W.vin, W.wp, W.tail, W.sm, m, a, e, qq,
+                          static_cast<const double *>(nullptr), [] {});
+    }
     __syncwarp();
   }
 }
@@ -925,7 +1005,62 @@ struct __align__(16) TWarp {
   double nb[3 * nb_stride<Dm, 6>()];
   double fb[6 * 32];           // face values, then fbdxx, fbdxy, fbdyx, fbdyy, fbdx, fbdy
   double sm[64];
+  // one row per lane: the element's gx0, gy0 and the RK4 base and
+  // accumulator rows of u, v, h, copied ahead like the coefficients
+  double aux[Dm::R == 1 ? 8 * Dm::N : 2];
 };
+
+// cp.async copies of element e's gx0, gy0 rows into aux[0..2N)
+template <class Dm>
+__device__ __forceinline__ void prefetch_gxy(const TendArgs &a, int e, double *aux) {
+  const int l = lane_id();
+  if (l < Dm::N) {
+    cp_async8(aux + l, a.gx0 + (size_t)e * Dm::N + l);
+    cp_async8(aux + Dm::N + l, a.gy0 + (size_t)e * Dm::N + l);
+  }
+}
+// cp.async copies of element e's RK4 base rows (aux[2N..5N)) and, from the
+// second stage on, accumulator rows (aux[5N..8N))
+template <class Dm>
+__device__ __forceinline__ void prefetch_stage(const StageArgs &sa, int e, double *aux) {
+  const int l = lane_id();
+  if (sa.stage < 0 || l >= Dm::N) return;
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    cp_async8(aux + (2 + f) * Dm::N + l, sa.base[f] + (size_t)e * Dm::N + l);
+    if (sa.stage > 0) cp_async8(aux + (5 + f) * Dm::N + l, sa.acc[f] + (size_t)e * Dm::N + l);
+  }
+}
+
+// stage_update with the element's base and accumulator rows already in
+// shared memory (one row per lane); same operations
+template <class Dm>
+__device__ __forceinline__ void stage_update_sm(const StageArgs &sa, int fld, int e, double d,
+                                                const double *aux) {
+  const int n = lane_id();
+  if (n >= Dm::N) return;
+  const size_t i = (size_t)e * Dm::N + n;
+  if (!isfinite(d)) atomicOr(sa.flag, 1);
+  if (sa.stage < 0) {
+    sa.tend[fld][i] = d;
+    return;
+  }
+  const double u0 = aux[(2 + fld) * Dm::N + n];
+  if (sa.stage == 0) {
+    sa.acc[fld][i] = d;
+    sa.out[fld][i] = add(u0, mul(mul(sa.dt, d), 0.5));
+  } else if (sa.stage == 1) {
+    sa.acc[fld][i] = add(aux[(5 + fld) * Dm::N + n], mul(2.0, d));
+    sa.out[fld][i] = add(u0, mul(mul(sa.dt, d), 0.5));
+  } else if (sa.stage == 2) {
+    sa.acc[fld][i] = add(aux[(5 + fld) * Dm::N + n], mul(2.0, d));
+    sa.out[fld][i] = add(u0, mul(sa.dt, d));
+  } else {
+    const double nv = add(u0, mul(sa.dt6, add(aux[(5 + fld) * Dm::N + n], d)));
+    sa.base[fld][i] = nv;
+    if (sa.host[fld]) sa.host[fld][(size_t)e * sa.host_ld + n] = nv;
+  }
+}
 
 template <class Dm, int VAR>
 __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
@@ -944,6 +1079,8 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
   if (PF && warp_global() < m.ne) {
     sd_next = sides_of(m, warp_global());
     prefetch_element<Dm, 6>(src, warp_global(), sd_next, W.own, W.nb);
+    prefetch_gxy<Dm>(a, warp_global(), W.aux);
+    prefetch_stage<Dm>(sa, warp_global(), W.aux);
   }
   __shared__ __align__(8) uint64_t ops_bar;
   if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) {
@@ -974,8 +1111,13 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
     double ax[6][R], bx[6][R];
     matvec2<Dm, 6>(S.agx, S.agy, W.own, N, ax, bx);
     double gx[R], gy[R], hb[R];
-    load_reg<Dm>(gx, a.gx0, e);
-    load_reg<Dm>(gy, a.gy0, e);
+    if constexpr (PF) {
+      gx[0] = lane_id() < N ? W.aux[lane_id()] : 0.0;
+      gy[0] = lane_id() < N ? W.aux[N + lane_id()] : 0.0;
+    } else {
+      load_reg<Dm>(gx, a.gx0, e);
+      load_reg<Dm>(gy, a.gy0, e);
+    }
     const double cby = mul(g.by, g.detai), cay = mul(g.ay, g.detai);
     const double cbx = mul(g.bx, g.detai), cax = mul(g.ax, g.detai);
     axpy<R>(gx, ax[0], -cby);
@@ -992,8 +1134,11 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
     axpy<R>(hb, bx[4], -cay);
     axpy<R>(hb, ax[5], -cbx);
     axpy<R>(hb, bx[5], cax);
-    __syncwarp();  // W.own / W.nb are free from here on
-    if (PF && en < m.ne) prefetch_element<Dm, 6>(src, en, sd_next, W.own, W.nb);
+    __syncwarp();  // W.own / W.nb and the gx0, gy0 rows are free from here on
+    if (PF && en < m.ne) {
+      prefetch_element<Dm, 6>(src, en, sd_next, W.own, W.nb);
+      prefetch_gxy<Dm>(a, en, W.aux);
+    }
     double t[6][3][R];
     lift_sums<Dm, 6>(S, isg, W.fb, t);
     apply_lift<R>(gx, t[0], isg, g.detai);
@@ -1035,9 +1180,17 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
       copy<R>(gy, s3[1]);
       copy<R>(hb, s3[2]);
     }
-    stage_update<Dm>(sa, 0, e, gx);
-    stage_update<Dm>(sa, 1, e, gy);
-    stage_update<Dm>(sa, 2, e, hb);
+    if constexpr (PF) {
+      stage_update_sm<Dm>(sa, 0, e, gx[0], W.aux);
+      stage_update_sm<Dm>(sa, 1, e, gy[0], W.aux);
+      stage_update_sm<Dm>(sa, 2, e, hb[0], W.aux);
+      __syncwarp();  // the base and accumulator rows are free
+      if (en < m.ne) prefetch_stage<Dm>(sa, en, W.aux);
+    } else {
+      stage_update<Dm>(sa, 0, e, gx);
+      stage_update<Dm>(sa, 1, e, gy);
+      stage_update<Dm>(sa, 2, e, hb);
+    }
     __syncwarp();
   }
 }
@@ -1220,7 +1373,7 @@ constexpr int pick_warps(size_t ops, size_t per_warp) {
 
 template <class Dm, int VAR>
 cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
-                   cudaStream_t st, int sms, cudaEvent_t *ev) {
+                   cudaStream_t st, int sms, cudaEvent_t *ev, long long *launches) {
   auto mark = [&](int i) {
     if (ev) cudaEventRecord(ev[i], st);
   };
@@ -1234,9 +1387,10 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   constexpr size_t sb = sizeof(SOpsQ<Dm>) + wb * sizeof(BWarp<Dm>);
   constexpr size_t stt = sizeof(SOps<Dm>) + wt * sizeof(TWarp<Dm>);
   int gq = 0, gb = 0, gt = 0;
-  cudaError_t e = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq, &gq);
+  cudaError_t e = resident_grid(tend_kernel<Dm, VAR>(), 32 * wt, stt, sms, m.ne, wt, &gt);
+  if (e != cudaSuccess) return e;
+  e = resident_grid(qphase_kernel<Dm, VAR>(), 32 * wq, sq, sms, m.ne, wq, &gq);
   if (e == cudaSuccess) e = resident_grid(nlvol_kernel<Dm, VAR>(), 32 * wb, sb, sms, m.ne, wb, &gb);
-  if (e == cudaSuccess) e = resident_grid(tend_kernel<Dm, VAR>(), 32 * wt, stt, sms, m.ne, wt, &gt);
   if (e != cudaSuccess) return e;
   mark(0);
   const auto kq = qphase_kernel<Dm, VAR>();
@@ -1249,7 +1403,9 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   mark(2);
   kt<<<gt, 32 * wt, stt, st>>>(op, m, ta, sa);
   mark(3);
-  return cudaGetLastError();
+  e = cudaGetLastError();
+  if (e == cudaSuccess) *launches += 3;
+  return e;
 }
 
 // The q-phase alone (the base state's q of the tangent-linear and adjoint
@@ -1285,12 +1441,13 @@ cudaError_t run_lin(const DevOps &op, const DevMesh &m, const RhsBuffers &b, con
 
 template <class Dm>
 cudaError_t run_any(int variant, const DevOps &op, const DevMesh &m, const RhsBuffers &b,
-                    const StageArgs &sa, cudaStream_t st, int sms, cudaEvent_t *ev) {
+                    const StageArgs &sa, cudaStream_t st, int sms, cudaEvent_t *ev,
+                    long long *launches) {
   switch (variant) {
     case kLIN: return run_lin<Dm>(op, m, b, sa, st, sms, ev);
-    case kFS: return run_nl<Dm, kFS>(op, m, b, sa, st, sms, ev);
-    case kNS: return run_nl<Dm, kNS>(op, m, b, sa, st, sms, ev);
-    default: return run_nl<Dm, kINV>(op, m, b, sa, st, sms, ev);
+    case kFS: return run_nl<Dm, kFS>(op, m, b, sa, st, sms, ev, launches);
+    case kNS: return run_nl<Dm, kNS>(op, m, b, sa, st, sms, ev, launches);
+    default: return run_nl<Dm, kINV>(op, m, b, sa, st, sms, ev, launches);
   }
 }
 
@@ -1370,12 +1527,12 @@ cudaError_t LAUNCH_FAST(int variant, const DevOps &op, const DevMesh &m, const R
                         cudaEvent_t *ev) {
   cudaError_t e = cudaErrorNotSupported;
   const int nc = op.nc, ng = op.ng, ngf = op.ngf;
-  if (nc == 3 && ng == 12 && ngf == 4) e = run_any<Dims<3, 12, 4>>(variant, op, m, b, sa, st, sms, ev);
-  else if (nc == 4 && ng == 25 && ngf == 5) e = run_any<Dims<4, 25, 5>>(variant, op, m, b, sa, st, sms, ev);
-  else if (nc == 5 && ng == 27 && ngf == 6) e = run_any<Dims<5, 27, 6>>(variant, op, m, b, sa, st, sms, ev);
-  else if (nc == 6 && ng == 33 && ngf == 7) e = run_any<Dims<6, 33, 7>>(variant, op, m, b, sa, st, sms, ev);
-  else if (nc == 7 && ng == 42 && ngf == 9) e = run_any<Dims<7, 42, 9>>(variant, op, m, b, sa, st, sms, ev);
-  if (e == cudaSuccess) *launches += variant == kLIN ? 1 : 3;
+  if (nc == 3 && ng == 12 && ngf == 4) e = run_any<Dims<3, 12, 4>>(variant, op, m, b, sa, st, sms, ev, launches);
+  else if (nc == 4 && ng == 25 && ngf == 5) e = run_any<Dims<4, 25, 5>>(variant, op, m, b, sa, st, sms, ev, launches);
+  else if (nc == 5 && ng == 27 && ngf == 6) e = run_any<Dims<5, 27, 6>>(variant, op, m, b, sa, st, sms, ev, launches);
+  else if (nc == 6 && ng == 33 && ngf == 7) e = run_any<Dims<6, 33, 7>>(variant, op, m, b, sa, st, sms, ev, launches);
+  else if (nc == 7 && ng == 42 && ngf == 9) e = run_any<Dims<7, 42, 9>>(variant, op, m, b, sa, st, sms, ev, launches);
+  if (e == cudaSuccess && variant == kLIN) *launches += 1;
   return e;
 }
 

@@ -8,14 +8,16 @@ lengths, through the C ABI.
   have the oracle's state bit for bit (SHA-256 of the u, v, h bytes) and the
   oracle's energy diagnostic (src/energy.f:3-96, the values src/shwwnl.f:
   291-298 writes) to the fixed-order-sum tolerance: 1e-13 relative for the
-  positive KE and PE sums, 1e-12 for the signed mass sum.  C2 runs its 2000
-  steps with the energy every 100 steps.
+  positive KE and PE sums, 1e-13 of the summed term magnitudes for the signed
+  mass sum (near zero for C3's zero-mean field).  C2 runs its 2000 steps with
+  the energy every 100 steps.
 * The C4 assimilation window at full size (32768 triangles, degree 4, 200
   steps, 500 observation points at steps 50/100/150/200, 20 binomial
   snapshots): the dot-product test of the 200-step tangent-linear and adjoint
   models, and the gradient against central differences (eps 1e-6) in 20
   seeded random directions.
 """
+import functools
 import hashlib
 import json
 from pathlib import Path
@@ -29,6 +31,19 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 FIXTURES = sorted(GOLDEN.glob("*_trajectory.json"))
 
 
+@functools.lru_cache(maxsize=None)
+def problem(name):
+    """Full-size configurations, set up once per test session (C3's initial
+    state alone takes about a minute of host time)."""
+    return W.build_problem(W.CONFIGS[name])
+
+
+def mass_scale(p, h):
+    """sum_e |det_e| sum_j |ammo(j,1) h_j|: the size of the terms the signed
+    mass sum adds (src/energy.f:327-329), the scale of its rounding."""
+    return float(np.sum(np.abs(p.mesh.det)[:, None] * np.abs(p.T.ammo[0, :][None, :] * h[:, :p.T.nm])))
+
+
 def digest(u, v, h, nm):
     m = hashlib.sha256()
     for a in (u, v, h):
@@ -40,8 +55,7 @@ def digest(u, v, h, nm):
 @pytest.mark.parametrize("path", FIXTURES, ids=[f.name.split("_trajectory")[0] for f in FIXTURES])
 def test_trajectory_matches_oracle_fixture(gpu_lib, path):
     rec = json.loads(path.read_text())
-    cfg = W.CONFIGS[rec["config"]]
-    p = W.build_problem(cfg)
+    p = problem(rec["config"])
     nm = p.T.nm
     assert (p.mesh.ne, nm, p.dt) == (rec["ne"], rec["nm"], rec["dt"])
     assert digest(p.u, p.v, p.h, nm) == rec["initial_sha256"], "set-up differs from the oracle's"
@@ -57,7 +71,7 @@ def test_trajectory_matches_oracle_fixture(gpu_lib, path):
         ke, pe, mass = s.energy()
         assert ke == pytest.approx(r["ke"], rel=1e-13), f"ke at step {prev}"
         assert pe == pytest.approx(r["pe"], rel=1e-13), f"pe at step {prev}"
-        assert mass == pytest.approx(r["mass"], rel=1e-12), f"mass at step {prev}"
+        assert abs(mass - r["mass"]) <= 1e-13 * mass_scale(p, h), f"mass at step {prev}"
     assert prev == rec["steps"]
 
 
@@ -67,8 +81,7 @@ def dot(a, b):
 
 @pytest.fixture(scope="module")
 def c4_window(gpu_lib):
-    cfg = W.CONFIGS["c4_ns_p4"]
-    p = W.build_problem(cfg)
+    p = problem("c4_ns_p4")
     s = W.make_solver(p)
     W.assimilation_window(p, s, 500, steps=(50, 100, 150, 200))
     yield p, s
@@ -127,7 +140,7 @@ MIXED_BOUNDS = {  # name: (steps, eta bound, u/v bound)
 @pytest.mark.parametrize("name", sorted(MIXED_BOUNDS))
 def test_mixed_errors_full_size(gpu_lib, name):
     steps, eta_tol, uv_tol = MIXED_BOUNDS[name]
-    p = W.build_problem(W.CONFIGS[name])
+    p = problem(name)
     r = W.precision_errors(p, steps)
     err = r["rel_l2_error_vs_fp64"]
     print(name, r)
