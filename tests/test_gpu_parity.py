@@ -381,3 +381,45 @@ def test_fma_mode_c1_1000_steps_within_1e10(gpu_lib):
     c = p.cfg
     O.rk4(c.variant, OT, OM, u, v, h, OM.fc, p.w0, p.z0, p.hb, c.mu0, c.mb0, c.g0, p.dt, 1000)
     assert rel_mass_diff(OT, OM, s.get_state(), (u, v, h)) < 1e-10
+
+
+# every tabulated degree with every nonlinear variant through the
+# compile-time-sized kernels (one and two rows per lane, wall branches)
+DEGREES = [(3, 12, 4), (4, 25, 5), (5, 27, 6), (6, 33, 7), (7, 42, 9)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["fs", "ns", "inv"])
+@pytest.mark.parametrize("deg", DEGREES, ids=[f"p{d[0]}" for d in DEGREES])
+def test_every_degree_and_variant_bitwise(gpu_lib, deg, variant):
+    import dataclasses
+    nc, ng, ngf = deg
+    base = W.small(W.CONFIGS["c2_fs_p6"], 5)
+    cfg = dataclasses.replace(base, nc=nc, ng=ng, ngf=ngf, variant=variant)
+    p = W.build_problem(cfg)
+    OT, OM = oracle_for(p)
+    s = W.make_solver(p)
+    s.set_kernel_path("templated")
+    rng = np.random.default_rng(nc)
+    u, v = p.u + 0.1 * rng.normal(size=p.u.shape), p.v + 0.1 * rng.normal(size=p.v.shape)
+    assert_bitwise(s.cal_var(u, v, p.h), oracle_rhs(p, OT, OM, u, v, p.h), p.T.nm)
+    s.set_state(p.u, p.v, p.h)
+    s.rk4_steps(p.dt, 3)
+    x = [p.u.copy(), p.v.copy(), p.h.copy()]
+    O.rk4(variant, OT, OM, *x, OM.fc, p.w0, p.z0, p.hb, cfg.mu0, cfg.mb0, cfg.g0, p.dt, 3)
+    assert_bitwise(s.get_state(), x, p.T.nm)
+
+
+@pytest.mark.gpu
+def test_strided_cal_var_leaves_padding_rows(gpu_lib):
+    """spoc_cal_var with ld = 45 arrays writes rows 1..nm of the outputs only,
+    as the reference's loops do (the rows past nm keep the caller's values)."""
+    p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 6), ld=45)
+    s = W.make_solver(p)
+    lib = api.load_library()
+    outs = [np.full_like(p.u, 7.0) for _ in range(3)]
+    rc = lib.spoc_cal_var(s._h, 45, api._d(p.u), api._d(p.v), api._d(p.h), *map(api._d, outs))
+    assert rc == 0
+    OT, OM = oracle_for(p)
+    assert_bitwise(outs, oracle_rhs(p, OT, OM, p.u, p.v, p.h), p.T.nm)
+    assert all((o[:, p.T.nm:] == 7.0).all() for o in outs)
