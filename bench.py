@@ -478,10 +478,11 @@ def model_counts(cfg, ne, nf):
 # (otherwise `traffic` is null, since it would describe another version).
 KERNEL_SOURCE = {"kf_": "spoc_fast.cu", "kx_": "spoc_mixed.cu", "kt_": "spoc_mixed_tc.cu"}
 NCU_TRAFFIC = {
-    "c2_fs_p6:kf_qphase": (19072768, None), "c2_fs_p6:kf_nlvol": (103480320, None),
-    "c2_fs_p6:kf_tend": (105977088, None),
-    "c3_inv_p7:kx_vol": (246406656, None), "c3_inv_p7:kx_tend": (468452864, None),
-    "c3_inv_p7:kt_vol": (250172160, None),
+    "c2_fs_p6:kf_qphase": (19388416, "96d09c3350079ef8"),
+    "c2_fs_p6:kf_nlvol": (97662720, "96d09c3350079ef8"),
+    "c2_fs_p6:kf_tend": (105278720, "96d09c3350079ef8"),
+    "c3_inv_p7:kx_vol": (247323136, "61a8985a532a517c"),
+    "c3_inv_p7:kx_tend": (464581888, "61a8985a532a517c"),
 }
 
 

@@ -299,6 +299,71 @@ __device__ __forceinline__ void prefetch_element(const double *const (&fields)[N
   }
 }
 
+// The copies of prefetch_element, made by the bulk-copy (TMA) engine where
+// a coefficient row is a whole number of 16-byte units (even N): lane r
+// issues row r (the element's NF rows, then NF rows per existing neighbour),
+// all completing on the warp's mbarrier; at odd N the per-value cp.async
+// copies of prefetch_element.  Rows land in the same layout either way.
+template <class Dm, int NF>
+struct RowCopy {
+  static constexpr bool kBulk = Dm::N % 2 == 0;
+  uint64_t *bar;
+  uint32_t phase;
+  __device__ __forceinline__ void init(uint64_t *b) {
+    bar = b;
+    phase = 0;
+    if (kBulk && lane_id() == 0) {
+      tc::mbar_init(bar, 1);
+      tc::fence_mbar_init();
+    }
+    __syncwarp();
+  }
+  __device__ __forceinline__ void issue(const double *const (&fields)[NF], int e, const Sides &sd,
+                                        double *own, double *nb) {
+    if constexpr (kBulk) {
+      constexpr uint32_t RB = Dm::N * sizeof(double);
+      const int have[3] = {sd.nb[0] >= 0, sd.nb[1] >= 0, sd.nb[2] >= 0};
+      const int rows = NF * (1 + have[0] + have[1] + have[2]);
+      const int l = lane_id();
+      if (l == 0) bulk::arrive_expect_tx(bar, (uint32_t)rows * RB);
+      __syncwarp();
+      if (l < rows) {
+        const int slot = l / NF;  // 0: the element, then the existing neighbours in side order
+        const int f = l - slot * NF;
+        const double *src = fields[f] + (size_t)e * Dm::N;
+        double *dst = own + f * Dm::N;
+        if (slot > 0) {
+          // side of the slot-th existing neighbour
+          const int k = (slot == 1) ? (have[0] ? 0 : have[1] ? 1 : 2)
+                      : (slot == 2) ? ((have[0] && have[1]) ? 1 : 2)
+                                    : 2;
+          src = fields[f] + (size_t)sd.nb[k] * Dm::N;
+          dst = nb + k * nb_stride<Dm, NF>() + f * Dm::N;
+        }
+        bulk::copy_g2s(dst, src, RB, bar);
+      }
+    } else {
+      prefetch_element<Dm, NF>(fields, e, sd, own, nb);
+    }
+  }
+  // Waits for the rows of the last issue(); false when the wait limit ran
+  // out (bit 2 of *flag set, after one more bounded wait for the copies).
+  __device__ __forceinline__ bool wait(int *flag) {
+    if constexpr (kBulk) {
+      const bool ok = tc::mbar_wait(bar, phase, bulk::kWaitLimit);
+      if (!ok) {
+        if (lane_id() == 0 && flag) atomicOr(flag, 2);
+        tc::mbar_wait(bar, phase, bulk::kWaitLimit);
+      }
+      phase ^= 1;
+      return __all_sync(0xffffffffu, ok);
+    } else {
+      cp_async_wait_all();
+      return true;
+    }
+  }
+};
+
 // Face values of NF fields by the cal_flu chain (src/calflu.f:31-62): lane
 // k*G + j computes point j of the face of side k; fb[f*32 + k*G + j].
 template <class Dm, int NF>
@@ -658,6 +723,7 @@ struct __align__(16) QWarp {
   double fr[2 * 32];
   double fb[4 * 32];
   double sm[64];
+  uint64_t bar;  // completion of the bulk row copies
 };
 
 // One element of the q-phase from the face-value chains on: own / nb hold the
@@ -731,14 +797,16 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
   // (one row per lane only: at two rows the registers are not there)
   constexpr bool PF = Dm::R == 1;
   Sides sd_next{};
+  RowCopy<Dm, 2> rows;
+  if (PF) rows.init(&W.bar);
   if (PF && warp_global() < m.ne) {
     sd_next = sides_of(m, warp_global());
-    prefetch_element<Dm, 2>(fields, warp_global(), sd_next, W.own, W.nb);
+    rows.issue(fields, warp_global(), sd_next, W.own, W.nb);
   }
   // the operator image arrives whole through one bulk copy (TMA engine)
   __shared__ __align__(8) uint64_t ops_bar;
   if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) {
-    cp_async_wait_all();
+    if (PF && warp_global() < m.ne) rows.wait(op.flag);
     return;
   }
   const size_t fs = (size_t)m.ne * N;
@@ -747,7 +815,7 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
     const int en = e + warp_count();
     if (PF && en < m.ne) sd_next = sides_of(m, en);
     if constexpr (PF) {
-      cp_async_wait_all();
+      if (!rows.wait(op.flag)) return;
     } else {
       load_vec<Dm>(W.own, su, e);
       load_vec<Dm>(W.own + N, sv, e);
@@ -756,7 +824,7 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
     __syncwarp();
     double gq[4][R];  // gxx, gxy, gyx, gyy
     qphase_elem<Dm, VAR>(S, m, e, sd, W.own, W.nb, W.fr, W.fb, W.sm, [&] {
-      if (PF && en < m.ne) prefetch_element<Dm, 2>(fields, en, sd_next, W.own, W.nb);
+      if (PF && en < m.ne) rows.issue(fields, en, sd_next, W.own, W.nb);
     }, gq);
 #pragma unroll
     for (int c = 0; c < 4; ++c) store_reg<Dm>(q + c * fs, gq[c], e);
@@ -1008,6 +1076,7 @@ struct __align__(16) TWarp {
   // one row per lane: the element's gx0, gy0 and the RK4 base and
   // accumulator rows of u, v, h, copied ahead like the coefficients
   double aux[Dm::R == 1 ? 8 * Dm::N : 2];
+  uint64_t bar;  // completion of the bulk row copies
 };
 
 // cp.async copies of element e's gx0, gy0 rows into aux[0..2N)
@@ -1076,14 +1145,17 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
   // (one row per lane only: at two rows the registers are not there)
   constexpr bool PF = Dm::R == 1;
   Sides sd_next{};
+  RowCopy<Dm, 6> rows;
+  if (PF) rows.init(&W.bar);
   if (PF && warp_global() < m.ne) {
     sd_next = sides_of(m, warp_global());
-    prefetch_element<Dm, 6>(src, warp_global(), sd_next, W.own, W.nb);
+    rows.issue(src, warp_global(), sd_next, W.own, W.nb);
     prefetch_gxy<Dm>(a, warp_global(), W.aux);
     prefetch_stage<Dm>(sa, warp_global(), W.aux);
   }
   __shared__ __align__(8) uint64_t ops_bar;
   if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) {
+    if (PF && warp_global() < m.ne) rows.wait(op.flag);
     cp_async_wait_all();
     return;
   }
@@ -1096,7 +1168,9 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
 #pragma unroll
     for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
     if constexpr (PF) {
+      const bool ok = rows.wait(op.flag);
       cp_async_wait_all();
+      if (!ok) return;
     } else {
 #pragma unroll
       for (int f = 0; f < 6; ++f) load_vec<Dm>(W.own + f * N, src[f], e);
@@ -1136,7 +1210,7 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
     axpy<R>(hb, bx[5], cax);
     __syncwarp();  // W.own / W.nb and the gx0, gy0 rows are free from here on
     if (PF && en < m.ne) {
-      prefetch_element<Dm, 6>(src, en, sd_next, W.own, W.nb);
+      rows.issue(src, en, sd_next, W.own, W.nb);
       prefetch_gxy<Dm>(a, en, W.aux);
     }
     double t[6][3][R];
