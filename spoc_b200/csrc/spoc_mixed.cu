@@ -187,23 +187,6 @@ __device__ void wall_vec(const float *o, float *tmp, float (&gx)[Dm::R], float (
   }
 }
 
-// RK4 bookkeeping of src/shwwnl.f:242-284 on one psi coefficient, FP64;
-// returns the next stage input.
-__device__ __forceinline__ double rk4_update(const MxArgs &a, size_t i, double d) {
-  double *c = a.c64 + i, *acc = a.acc + i;
-  const double u0 = *c;
-  switch (a.stage) {
-    case 0: *acc = d; return u0 + a.dt * d * 0.5;
-    case 1: *acc = *acc + 2.0 * d; return u0 + a.dt * d * 0.5;
-    case 2: *acc = *acc + 2.0 * d; return u0 + a.dt * d;
-    default: {
-      const double u1 = u0 + a.dt6 * (*acc + d);
-      *c = u1;
-      return u1;
-    }
-  }
-}
-
 // Finishes an element: non-finite check, RK4 update (or tendency output),
 // next stage input and its traces.  t[3][R] holds the psi tendencies.
 template <class Dm>
@@ -993,7 +976,12 @@ cudaError_t run_stage(MixedCtx *c, const MxArgs &a, cudaStream_t st, long long *
       kv<<<gv, 32 * kMxWarps, smem, st>>>(a);
     }
     mark(1);
-    kt<<<gt, 32 * kMxWarps, smem, st>>>(a);
+    if (c->tc) {
+      tce = mixed_tc_tend(c->variant, c->nc, c->Q, c->G, a, c->tcimg, c->sms, st);
+      if (tce != cudaSuccess) return;
+    } else {
+      kt<<<gt, 32 * kMxWarps, smem, st>>>(a);
+    }
     mark(2);
     if (launches) *launches += 2;
   };

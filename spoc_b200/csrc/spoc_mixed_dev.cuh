@@ -126,6 +126,23 @@ __device__ __forceinline__ float face_value(const float *tr, const FaceRef &r, i
   return 0.5f * (own + nb[r.s2 * G + (G - 1 - j)] + (nb[TG] - tr[(size_t)e * TS + TG]));
 }
 
+// RK4 bookkeeping of src/shwwnl.f:242-284 on one psi coefficient, FP64;
+// returns the next stage input.
+__device__ __forceinline__ double rk4_update(const MxArgs &a, size_t i, double d) {
+  double *c = a.c64 + i, *acc = a.acc + i;
+  const double u0 = *c;
+  switch (a.stage) {
+    case 0: *acc = d; return u0 + a.dt * d * 0.5;
+    case 1: *acc = *acc + 2.0 * d; return u0 + a.dt * d * 0.5;
+    case 2: *acc = *acc + 2.0 * d; return u0 + a.dt * d;
+    default: {
+      const double u1 = u0 + a.dt6 * (*acc + d);
+      *c = u1;
+      return u1;
+    }
+  }
+}
+
 }  // namespace mx
 
 // psi-basis operators built on the host in FP64 (spoc_mixed.cu).
@@ -138,6 +155,9 @@ struct PsiOps {
 bool mixed_tc_available(int nc, int ng, int ngf);
 std::vector<float> mixed_tc_image(int nc, int ng, int ngf, const PsiOps &p, const double *wi);
 cudaError_t mixed_tc_vol(int variant, int nc, int ng, int ngf, const mx::MxArgs &a, const float *img,
+                         int sms, cudaStream_t st);
+// The tendency kernel on the tensor cores (face lifts, wall projection, traces).
+cudaError_t mixed_tc_tend(int variant, int nc, int ng, int ngf, const mx::MxArgs &a, const float *img,
                          int sms, cudaStream_t st);
 
 }  // namespace spoc

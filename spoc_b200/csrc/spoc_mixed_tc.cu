@@ -672,6 +672,326 @@ __global__ void __launch_bounds__(kTcThreads, 1) kt_vol(const MxArgs a, const fl
   if (warp == 0) tc::tmem_dealloc(tm, T::TCOLS);
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core tendency kernel (kt_tend): the face lifts of phases C, D, the
+// wall projections and the traces of the next stage input as tcgen05 MMA
+// groups, the RK4 update in FP64 between them; the same mathematics as
+// kx_tend (spoc_mixed.cu).  Per 128-element tile:
+//   1. face fluxes of the three tendencies at the 3 ngf face points (from the
+//      trace records of q, uh, vh and of the stage input's h) -> three A
+//      tiles; D_f (128 x W) = A_f TR  (the lift TR_s^T, all modes);
+//   2. t_f = D_f + the partial load vectors of the volume kernel; wall
+//      elements: projection onto the wall subspace by an MMA with Pwall;
+//   3. RK4 update (FP64 psi state and accumulator) -> next stage input y;
+//   4. D_f (128 x WT) = y_f TRm^T -> mean-free trace records, then the mean.
+// Shared memory: the TRm, Pwall and lift blocks of the tensor-core image
+// (head and TF32 tail of each) and three A tiles (head and tail).
+template <class Dm>
+struct TcTend {
+  using T = TcDims<Dm>;
+  static constexpr int W = T::W, WT = T::WT, KN = T::KN, KT = T::KT;
+  static constexpr int KA = KN > KT ? KN : KT;
+  static constexpr int O_TR = 0, L_TR = WT * KN;        // trace rows (K = KN)
+  static constexpr int O_PW = O_TR + 2 * L_TR, L_PW = W * KN;
+  static constexpr int O_L = O_PW + 2 * L_PW, L_L = W * KT;
+  static constexpr int IMG = O_L + 2 * L_L;
+  static constexpr int O_A = IMG, ABUF = 2 * 128 * KA;  // one A tile: head, tail
+  static constexpr size_t SMEM = sizeof(float) * (IMG + 3 * ABUF) + 64;
+  // TMEM: the three lifted tendencies, then two projection outputs; the
+  // trace outputs reuse columns 0 .. 3 WT once the lifts are read
+  static constexpr int C_S = 3 * W, C_END = 5 * W;
+  static constexpr int TCOLS = pow2_cols(C_END);
+  static_assert(C_END <= 512 && 3 * WT <= 3 * W, "tensor memory plan");
+  static_assert(SMEM <= 227 * 1024, "shared memory plan exceeds 227 KB");
+  static_assert(IMG % 4 == 0 && ABUF % 4 == 0 && T::R_TR % 8 == 0 && T::R_PW % 8 == 0,
+                "16-byte staging of whole row groups");
+};
+
+// MMA group on explicit operand addresses (thread 0): D[dcol .. dcol+n) (+)=
+// A B^T, A and B K-major with kpad columns, heads at ah / bh, tails at al / bl.
+__device__ __forceinline__ void issue_ab(uint32_t tm, uint32_t ah, uint32_t al, uint32_t bh,
+                                         uint32_t bl, int kpad, int n, int dcol, bool acc0) {
+  if (threadIdx.x != 0) return;
+  const uint32_t id = tc::idesc_tf32(128, n);
+  for (int s = 0; s < kpad / 8; ++s) {
+    const uint32_t o = (uint32_t)s * 256u;
+    tc::mma_tf32(tm + dcol, tc::sdesc(ah + o, kpad), tc::sdesc(bh + o, kpad), id,
+                 (s > 0 || acc0) ? 1u : 0u);
+    tc::mma_tf32(tm + dcol, tc::sdesc(al + o, kpad), tc::sdesc(bh + o, kpad), id, 1u);
+    tc::mma_tf32(tm + dcol, tc::sdesc(ah + o, kpad), tc::sdesc(bl + o, kpad), id, 1u);
+  }
+}
+
+// Three A tiles, one mbarrier each (the two-buffer Pipe of kt_vol, widened).
+struct Pipe3 {
+  uint64_t *mbar;
+  uint32_t issued[3], waited[3];
+  int *flag;
+  __device__ __forceinline__ void wait(int b) {
+    if (issued[b] > waited[b]) {
+      if (!tc::mbar_wait(&mbar[b], (issued[b] - 1) & 1u, kWaitLimit) && threadIdx.x == 0)
+        atomicOr(flag, 2);
+      waited[b] = issued[b];
+      tc::fence_after();
+    }
+  }
+  __device__ __forceinline__ void wait_all() {
+    wait(0);
+    wait(1);
+    wait(2);
+  }
+  __device__ __forceinline__ void commit(int b) {
+    if (threadIdx.x == 0) tc::commit(&mbar[b]);
+    ++issued[b];
+  }
+};
+
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(kTcThreads, 1) kt_tend(const MxArgs a, const float *__restrict__ img) {
+  using T = TcDims<Dm>;
+  using U = TcTend<Dm>;
+  constexpr int N = Dm::N, G = Dm::G, TG = Dm::TG, TS = Dm::TS;
+  constexpr int W = U::W, WT = U::WT, KN = U::KN, KT = U::KT, KA = U::KA;
+  extern __shared__ __align__(1024) float sm[];
+  const int t = threadIdx.x, warp = t >> 5, row = t & 127, half = t >> 7;
+  auto own = [&](int c) { return ((c >> 3) & 1) == half; };
+  // the TRm and Pwall row groups of the operator block and the lift block
+  {
+    const float4 *g = reinterpret_cast<const float4 *>(img);
+    float4 *d = reinterpret_cast<float4 *>(sm);
+    auto copy = [&](int dst, int src, int n) {
+      for (int i = t; i < n / 4; i += kTcThreads) d[dst / 4 + i] = g[src / 4 + i];
+    };
+    const int tr = T::O_BK + (T::R_TR / 8) * (KN * 8), pw = T::O_BK + (T::R_PW / 8) * (KN * 8);
+    const int tail = T::RB * KN;
+    copy(U::O_TR, tr, U::L_TR);
+    copy(U::O_TR + U::L_TR, tr + tail, U::L_TR);
+    copy(U::O_PW, pw, U::L_PW);
+    copy(U::O_PW + U::L_PW, pw + tail, U::L_PW);
+    copy(U::O_L, T::O_BL, U::L_L);
+    copy(U::O_L + U::L_L, T::O_BL + T::L_BL, U::L_L);
+  }
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + U::O_A + 3 * U::ABUF);
+  uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 3);
+  if (warp == 0) tc::tmem_alloc(slot, U::TCOLS);
+  if (t == 0) {
+    for (int b = 0; b < 3; ++b) tc::mbar_init(&mbar[b], 1);
+    tc::fence_mbar_init();
+  }
+  sync_for_mma();
+  const uint32_t tm = *slot;
+  const uint32_t lrow = (uint32_t)((warp & 3) * 32) << 16;
+  Pipe3 p{mbar, {0u, 0u, 0u}, {0u, 0u, 0u}, a.flag};
+  const size_t fn = (size_t)a.ne * N, tn = (size_t)a.ne * TS;
+  auto ld = [&](int col, float (&v)[8]) { tc::tmem_ld8(tm + lrow + (uint32_t)col, v); };
+  auto ldw = [&]() { tc::tmem_wait_ld(); };
+  auto abuf = [&](int b) { return sm + U::O_A + b * U::ABUF; };
+  // this thread's row of A tile b (kpad columns): eight values at column k
+  auto put8a = [&](int b, int kpad, int k, const float (&x)[8]) {
+    float *hi = abuf(b);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      float4 h, l;
+      tc::split_tf32(x[4 * q + 0], h.x, l.x);
+      tc::split_tf32(x[4 * q + 1], h.y, l.y);
+      tc::split_tf32(x[4 * q + 2], h.z, l.z);
+      tc::split_tf32(x[4 * q + 3], h.w, l.w);
+      const uint32_t o = tc::kmaj_off(row, k + 4 * q, kpad) / 4;
+      *reinterpret_cast<float4 *>(hi + o) = h;
+      *reinterpret_cast<float4 *>(hi + 128 * KA + o) = l;
+    }
+  };
+  auto group = [&](int b, int kpad, int bo, int lb, int n, int dcol) {
+    const uint32_t ah = tc::smem_u32(abuf(b)), al = ah + 128u * KA * 4u;
+    issue_ab(tm, ah, al, tc::smem_u32(sm + bo), tc::smem_u32(sm + bo + lb), kpad, n, dcol, false);
+  };
+
+  for (int tile = blockIdx.x; tile * 128 < a.ne; tile += gridDim.x) {
+    const int e = tile * 128 + row;
+    const bool valid = e < a.ne;
+    float di = 0.f, wnx = 0.f, wny = 0.f;
+    bool wall = false;
+    FaceRef fr[3];
+    if (valid) {
+      di = (float)a.m.vect[5 * (size_t)e + 4];
+      wall = a.m.bdl[e] != 0;
+      wnx = (float)a.m.normt[2 * (size_t)e];
+      wny = (float)a.m.normt[2 * (size_t)e + 1];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) fr[k] = face_ref(a.m, e, k);
+    }
+
+    // ---- 1. face fluxes of the three tendencies, lifted by the MMA
+    p.wait_all();
+#pragma unroll
+    for (int c = 0; c < KT; c += 8)
+      if (own(c)) {
+        float x[3][8];
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int l = c + jj;
+          x[0][jj] = x[1][jj] = x[2][jj] = 0.f;
+          if (valid && l < TG) {
+            const int side = l / G, j = l - side * G;
+            const FaceRef &r = fr[side];
+            const float fqxx = face_value<G>(a.trq, r, e, l, j);
+            const float fqxy = face_value<G>(a.trq + tn, r, e, l, j);
+            const float fqyx = face_value<G>(a.trq + 2 * tn, r, e, l, j);
+            const float fqyy = face_value<G>(a.trq + 3 * tn, r, e, l, j);
+            const float fuh = face_value<G>(a.trq + 4 * tn, r, e, l, j);
+            const float fvh = face_value<G>(a.trq + 5 * tn, r, e, l, j);
+            const float fh = face_value<G>(a.tr_in + 2 * tn, r, e, l, j);
+            const float Fxx = a.mu0 * fqxx - a.g0 * fh, Fxy = a.mu0 * fqxy;
+            const float Fyx = a.mu0 * fqyx, Fyy = a.mu0 * fqyy - a.g0 * fh;
+            const float s = r.sig * di * a.wif[r.sig > 0.f ? j : G - 1 - j];
+            x[0][jj] = s * (r.nx * Fxx + r.ny * Fxy);
+            x[1][jj] = s * (r.nx * Fyx + r.ny * Fyy);
+            x[2][jj] = -s * (r.nx * fuh + r.ny * fvh);
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) put8a(f, KT, c, x[f]);
+      }
+    sync_for_mma();
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      group(f, KT, U::O_L, U::L_L, W, f * W);
+      p.commit(f);
+    }
+    p.wait_all();
+
+    // ---- 2. tendencies: lifts + partial load vectors; wall projection
+    const bool any_wall = __syncthreads_or(wall);
+    if (any_wall) {
+      // FS / INV: the normal component gn = n.(gx, gy) is projected; NS:
+      // both components
+      for (int c = 0; c < KN; c += 8)
+        if (own(c)) {
+          float dx[8], dy[8], g0v[8], g1v[8];
+          ld(0 * W + c, dx);
+          ld(1 * W + c, dy);
+          ldw();
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int i = c + jj;
+            const bool in = valid && i < N;
+            const float tx = in ? dx[jj] + a.part[(size_t)e * N + i] : 0.f;
+            const float ty = in ? dy[jj] + a.part[fn + (size_t)e * N + i] : 0.f;
+            if (VAR == SPOC_NS) {
+              g0v[jj] = wall ? tx : 0.f;
+              g1v[jj] = wall ? ty : 0.f;
+            } else {
+              g0v[jj] = wall ? wnx * tx + wny * ty : 0.f;
+              g1v[jj] = 0.f;
+            }
+          }
+          put8a(0, KN, c, g0v);
+          if (VAR == SPOC_NS) put8a(1, KN, c, g1v);
+        }
+      sync_for_mma();
+      group(0, KN, U::O_PW, U::L_PW, W, U::C_S);
+      p.commit(0);
+      if (VAR == SPOC_NS) {
+        group(1, KN, U::O_PW, U::L_PW, W, U::C_S + W);
+        p.commit(1);
+      }
+      p.wait_all();
+    }
+
+    // ---- 3. RK4 update (FP64 psi state); the next stage input as A tiles
+    bool bad = false;
+    for (int c = 0; c < KN; c += 8)
+      if (own(c)) {
+        float d[3][8], pg0[8], pg1[8];
+        ld(0 * W + c, d[0]);
+        ld(1 * W + c, d[1]);
+        ld(2 * W + c, d[2]);
+        if (any_wall) {
+          ld(U::C_S + c, pg0);
+          if (VAR == SPOC_NS) ld(U::C_S + W + c, pg1);
+        }
+        ldw();
+        float y[3][8];
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int i = c + jj;
+          const bool in = valid && i < N;
+          float tf[3];
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            tf[f] = in ? d[f][jj] + a.part[f * fn + (size_t)e * N + i] : 0.f;
+          if (in && wall) {
+            if (VAR == SPOC_NS) {
+              tf[0] = pg0[jj];
+              tf[1] = pg1[jj];
+            } else {
+              const float gn = wnx * tf[0] + wny * tf[1];
+              const float dd = pg0[jj] - gn;
+              tf[0] += wnx * dd;
+              tf[1] += wny * dd;
+            }
+          }
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            y[f][jj] = 0.f;
+            if (!in) continue;
+            bad |= !isfinite(tf[f]);
+            const size_t gi = f * fn + (size_t)e * N + i;
+            if (a.stage < 0) {
+              a.k64[gi] = (double)tf[f];
+            } else {
+              const float y32 = (float)rk4_update(a, gi, (double)tf[f]);
+              a.y[gi] = y32;
+              y[f][jj] = y32;
+            }
+          }
+        }
+        if (a.stage >= 0) {
+#pragma unroll
+          for (int f = 0; f < 3; ++f) put8a(f, KN, c, y[f]);
+        }
+        if (a.stage >= 0 && c == 0 && valid) {
+          // the mean of each field: the constant mode's coefficient
+#pragma unroll
+          for (int f = 0; f < 3; ++f) a.tr_out[f * tn + (size_t)e * TS + TG] = a.psi0 * y[f][0];
+        }
+      }
+    if (bad) atomicOr(a.flag, 1);
+    if (a.stage < 0) continue;
+
+    // ---- 4. mean-free traces of the next stage input
+    tc::tmem_wait_ld();  // the lifted columns are read: the traces reuse them
+    sync_for_mma();
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      group(f, KN, U::O_TR, U::L_TR, WT, f * WT);
+      p.commit(f);
+    }
+    p.wait_all();
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      float *rec = a.tr_out + f * tn + (size_t)(valid ? e : 0) * TS;
+      for (int c = 0; c < WT; c += 8)
+        if (own(c)) {
+          float v[8];
+          ld(f * WT + c, v);
+          ldw();
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj)
+            if (valid && c + jj < TG) rec[c + jj] = v[jj];
+        }
+    }
+    // the trace columns are read before the next tile's lifts overwrite them
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+  }
+  p.wait_all();
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tm, U::TCOLS);
+}
+
 // tf32 head of x: round to nearest on the 13 dropped mantissa bits, ties away
 float tf32_head(float x) {
   uint32_t u;
@@ -753,6 +1073,27 @@ cudaError_t mixed_tc_vol(int variant, int nc, int ng, int ngf, const MxArgs &a, 
     if (variant == SPOC_FS) go(kt_vol<Dm, SPOC_FS>);
     else if (variant == SPOC_NS) go(kt_vol<Dm, SPOC_NS>);
     else go(kt_vol<Dm, SPOC_INV>);
+  });
+  return ce;
+}
+
+cudaError_t mixed_tc_tend(int variant, int nc, int ng, int ngf, const MxArgs &a, const float *img,
+                          int sms, cudaStream_t st) {
+  cudaError_t ce = cudaErrorInvalidValue;
+  tc_dims(nc, ng, ngf, [&](auto d) {
+    using Dm = decltype(d);
+    using U = TcTend<Dm>;
+    auto go = [&](auto kern) {
+      ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)U::SMEM);
+      if (ce != cudaSuccess) return;
+      const int tiles = (a.ne + 127) / 128;
+      const int grid = tiles < sms ? tiles : sms;
+      kern<<<grid, kTcThreads, U::SMEM, st>>>(a, img);
+      ce = cudaGetLastError();
+    };
+    if (variant == SPOC_FS) go(kt_tend<Dm, SPOC_FS>);
+    else if (variant == SPOC_NS) go(kt_tend<Dm, SPOC_NS>);
+    else go(kt_tend<Dm, SPOC_INV>);
   });
   return ce;
 }
