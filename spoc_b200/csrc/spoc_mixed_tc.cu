@@ -1005,10 +1005,12 @@ float tf32_head(float x) {
 // operator block (rows x kpad, K-major core-matrix layout): head at o, tail
 // at o + rows * kpad
 void put_block(std::vector<float> &img, int o, int rows, int kpad, int r, int k, double v) {
-  const float x = (float)v, h = tf32_head(x);
+  // head and tail both rounded to TF32 (the tensor core truncates the bits
+  // below), the tail taken from the FP64 value
+  const float h = tf32_head((float)v), l = tf32_head((float)(v - (double)h));
   const uint32_t off = tc::kmaj_off(r, k, kpad) / 4;
   img[o + off] = h;
-  img[o + rows * kpad + off] = x - h;
+  img[o + rows * kpad + off] = l;
 }
 
 template <class Dm>

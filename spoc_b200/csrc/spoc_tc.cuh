@@ -135,13 +135,17 @@ __device__ __forceinline__ void tmem_wait_st() {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
-// x = hi + lo with hi rounded to TF32 (10 explicit mantissa bits, round to
-// nearest, ties away) and lo = x - hi exact in FP32.
+// x ~ hi + lo with hi rounded to TF32 (10 explicit mantissa bits, round to
+// nearest, ties away) and lo = x - hi (exact in FP32) rounded to TF32 as well:
+// the tensor core reads only the top 19 bits of a 32-bit operand, so an
+// unrounded tail would be truncated (a biased error that accumulates over
+// the steps of a run); rounded, the tail's error is unbiased.
 __device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
-  uint32_t h;
+  uint32_t h, l;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
   hi = __uint_as_float(h);
-  lo = x - hi;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - hi));
+  lo = __uint_as_float(l);
 }
 
 }  // namespace tc
