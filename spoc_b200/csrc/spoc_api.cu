@@ -67,6 +67,7 @@ struct spoc_handle {
   double *U0[3]{}, *SA[3]{}, *SB[3]{}, *ACC[3]{}, *TEND[3]{}, *SIN[3]{};
   double *hb = nullptr, *w0 = nullptr, *z0 = nullptr, *fc = nullptr;
   double *q = nullptr, *f = nullptr, *gx0 = nullptr, *gy0 = nullptr, *uh = nullptr, *vh = nullptr;
+  double *fv = nullptr;  // [nf][6][ngf] face values of the tendency kernel
   double *eterms = nullptr, *escal = nullptr;
   int *flag = nullptr;
   unsigned long long *cflbits = nullptr;
@@ -290,6 +291,7 @@ RhsBuffers rhs_buffers(spoc_handle *h, double *const s[3]) {
   b.gy0 = h->gy0;
   b.uh = h->uh;
   b.vh = h->vh;
+  b.fv = h->fv;
   b.mu0 = h->mu0;
   b.mb0 = h->mb0;
   b.g0 = h->g0;
@@ -411,6 +413,7 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
       if (ce == cudaSuccess) ce = h->alloc(&h->gy0, n);
       if (ce == cudaSuccess) ce = h->alloc(&h->uh, n);
       if (ce == cudaSuccess) ce = h->alloc(&h->vh, n);
+      if (ce == cudaSuccess) ce = h->alloc(&h->fv, 6 * (size_t)h->ngf * h->nf);
     }
     if (ce == cudaSuccess) ce = h->alloc(&h->eterms, 3 * (size_t)h->ne);
     if (ce == cudaSuccess) ce = h->alloc(&h->escal, 4);

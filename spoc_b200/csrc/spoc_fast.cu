@@ -346,6 +346,25 @@ struct RowCopy {
       prefetch_element<Dm, NF>(fields, e, sd, own, nb);
     }
   }
+  // The element's NF rows (lanes 0..NF-1) and the records of its three
+  // faces (lanes NF..NF+2: rec floats each, from frec + face * rec into
+  // fdst + k * rec), bulk copies only (even N; rec * 8 a multiple of 16).
+  __device__ __forceinline__ void issue_own_faces(const double *const (&fields)[NF], int e,
+                                                  const Sides &sd, double *own,
+                                                  const double *frec, double *fdst, int rec) {
+    static_assert(kBulk, "bulk copies need 16-byte rows");
+    constexpr uint32_t RB = Dm::N * sizeof(double);
+    const int l = lane_id();
+    if (l == 0) bulk::arrive_expect_tx(bar, NF * RB + 3u * (uint32_t)rec * sizeof(double));
+    __syncwarp();
+    if (l < NF) {
+      bulk::copy_g2s(own + l * Dm::N, fields[l] + (size_t)e * Dm::N, RB, bar);
+    } else if (l < NF + 3) {
+      const int k = l - NF;
+      bulk::copy_g2s(fdst + k * rec, frec + (size_t)sd.face[k] * rec, (uint32_t)rec * sizeof(double),
+                     bar);
+    }
+  }
   // Waits for the rows of the last issue(); false when the wait limit ran
   // out (bit 2 of *flag set, after one more bounded wait for the copies).
   __device__ __forceinline__ bool wait(int *flag) {
@@ -1065,12 +1084,74 @@ __device__ __forceinline__ void nlvol_body(DevOps op, DevMesh m, NlArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// face values once per face (src/calflu.f:22-66): the cal_flu chain of NF
+// fields at every point of every face, in the order of the first element of
+// the face (the values face_values computes on either side, bit for bit)
+// ---------------------------------------------------------------------------
+struct FaceArgs {
+  const double *f[6];  // the fields, [ne][N] each
+  double *out;         // [nf][NF][G]
+};
+
+template <class Dm, int NF>
+__global__ void __launch_bounds__(256) kf_faces(DevOps op, DevMesh m, FaceArgs fa) {
+  constexpr int N = Dm::N, G = Dm::G;
+  __shared__ double spf[3 * N * G];  // [(s*N + n)*G + j] = pico(j,n,s)
+  for (int i = threadIdx.x; i < 3 * N * G; i += blockDim.x) spf[i] = op.picoF[i];
+  __syncthreads();
+  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= m.nf * G) return;
+  const int f = item / G, j = item - f * G;
+  const int t1 = __ldg(m.tseg + 2 * f), t2 = __ldg(m.tseg + 2 * f + 1);
+  double acc[NF];
+#pragma unroll
+  for (int q = 0; q < NF; ++q) acc[q] = 0.0;
+  // the chain over one element's modes (16-byte pairs at even N: the same
+  // operations in the same order)
+  auto chain = [&](int t, const double *p) {
+    if constexpr (N % 2 == 0) {
+#pragma unroll 2
+      for (int n = 0; n < N; n += 2) {
+        const double pv0 = p[n * G], pv1 = p[(n + 1) * G];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) {
+          const double2 c = __ldg(reinterpret_cast<const double2 *>(fa.f[q] + (size_t)t * N + n));
+          acc[q] = macc(acc[q], c.x, pv0);
+          acc[q] = macc(acc[q], c.y, pv1);
+        }
+      }
+    } else {
+#pragma unroll 2
+      for (int n = 0; n < N; ++n) {
+        const double pv = p[n * G];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) acc[q] = macc(acc[q], __ldg(fa.f[q] + (size_t)t * N + n), pv);
+      }
+    }
+  };
+  if (t2 < 0) {
+    chain(t1, spf + j);  // wall faces are traced on side 1 of their element
+  } else {
+    const int s1 = __ldg(m.ssit + 2 * f), s2 = __ldg(m.ssit + 2 * f + 1);
+    chain(t1, spf + s1 * N * G + j);
+    chain(t2, spf + s2 * N * G + (G - 1 - j));
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = mul(0.5, acc[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < NF; ++q) fa.out[((size_t)f * NF + q) * G + j] = acc[q];
+}
+
+// ---------------------------------------------------------------------------
 // tendencies and the RK4 stage update (calvarnl_fs.f:350-544)
 // ---------------------------------------------------------------------------
-template <class Dm>
+// FACES: the face values come from kf_faces (the records of the element's
+// three faces are copied instead of its neighbours' coefficients).
+template <class Dm, bool FACES = false>
 struct __align__(16) TWarp {
   double own[6 * Dm::N];       // fxx, fxy, fyx, fyy, uh, vh
-  double nb[3 * nb_stride<Dm, 6>()];
+  double nb[FACES ? 2 : 3 * nb_stride<Dm, 6>()];
+  double fvs[FACES ? 3 * 6 * Dm::G : 2];  // side k: [k][field][point]
   double fb[6 * 32];           // face values, then fbdxx, fbdxy, fbdyx, fbdyy, fbdx, fbdy
   double sm[64];
   // one row per lane: the element's gx0, gy0 and the RK4 base and
@@ -1131,12 +1212,22 @@ __device__ __forceinline__ void stage_update_sm(const StageArgs &sa, int fld, in
   }
 }
 
-template <class Dm, int VAR>
+template <class Dm, int VAR, bool FACES = false>
 __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
-  TWarp<Dm> &W = reinterpret_cast<TWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
-  constexpr int N = Dm::N, R = Dm::R;
+  TWarp<Dm, FACES> &W =
+      reinterpret_cast<TWarp<Dm, FACES> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, R = Dm::R, G = Dm::G;
+  static_assert(!FACES || (Dm::R == 1 && Dm::N % 2 == 0), "face records need bulk row copies");
+  // issue the copies of element e: its rows and its neighbours' rows, or its
+  // rows and its three face records
+  auto issue = [&](RowCopy<Dm, 6> &rc, const double *const (&fields)[6], int e, const Sides &sd) {
+    if constexpr (FACES)
+      rc.issue_own_faces(fields, e, sd, W.own, a.fv, W.fvs, 6 * G);
+    else
+      rc.issue(fields, e, sd, W.own, W.nb);
+  };
   const size_t fs = (size_t)m.ne * N;
   const double *const src[6] = {a.f, a.f + fs, a.f + 2 * fs, a.f + 3 * fs, a.uh, a.vh};
   // the coefficients of the warp's next element are copied into W.own / W.nb
@@ -1149,7 +1240,7 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
   if (PF) rows.init(&W.bar);
   if (PF && warp_global() < m.ne) {
     sd_next = sides_of(m, warp_global());
-    rows.issue(src, warp_global(), sd_next, W.own, W.nb);
+    issue(rows, src, warp_global(), sd_next);
     prefetch_gxy<Dm>(a, warp_global(), W.aux);
     prefetch_stage<Dm>(sa, warp_global(), W.aux);
   }
@@ -1177,7 +1268,16 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
       stage_neighbours<Dm, 6>(sd, W.nb, [&](int f, int t, int i) { return src[f][(size_t)t * N + i]; });
     }
     __syncwarp();
-    face_values<Dm, 6>(S.pf, m, sd, W.own, W.nb, W.fb);
+    if constexpr (FACES) {
+      const int l = lane_id();
+      if (l < 3 * G) {
+        const int k = l / G, j = l - k * G;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) W.fb[f * 32 + l] = W.fvs[(k * 6 + f) * G + j];
+      }
+    } else {
+      face_values<Dm, 6>(S.pf, m, sd, W.own, W.nb, W.fb);
+    }
     __syncwarp();
     // each lane scales the values it computed (fbd * norm(1|2, face))
 #pragma unroll
@@ -1210,7 +1310,7 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
     axpy<R>(hb, bx[5], cax);
     __syncwarp();  // W.own / W.nb and the gx0, gy0 rows are free from here on
     if (PF && en < m.ne) {
-      rows.issue(src, en, sd_next, W.own, W.nb);
+      issue(rows, src, en, sd_next);
       prefetch_gxy<Dm>(a, en, W.aux);
     }
     double t[6][3][R];
@@ -1295,6 +1395,11 @@ __global__ void __launch_bounds__(256, 2) kf_nlvol_r2(DevOps op, DevMesh m, NlAr
 template <class Dm, int VAR>
 __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
   tend_body<Dm, VAR>(op, m, a, sa);
+}
+// the tendency kernel on the face values of kf_faces (one row per lane, even N)
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_tendf(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
+  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) tend_body<Dm, VAR, true>(op, m, a, sa);
 }
 template <class Dm, int VAR>
 __global__ void __launch_bounds__(Dm::TEND_THREADS, 2) kf_tend_r2(DevOps op, DevMesh m, TendArgs a,
@@ -1453,7 +1558,7 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   };
   NlArgs na{b.su, b.sv, b.sh, b.hb, b.w0, b.z0, b.fc, b.q, b.gx0, b.gy0, b.uh, b.vh, b.f,
             b.mu0, b.mb0, b.g0};
-  TendArgs ta{b.gx0, b.gy0, b.uh, b.vh, b.f};
+  TendArgs ta{b.gx0, b.gy0, b.uh, b.vh, b.f, b.fv};
   constexpr int wq = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm>));
   constexpr int wb = pick_warps(sizeof(SOpsQ<Dm>), sizeof(BWarp<Dm>));
   constexpr int wt = std::min(pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm>)), Dm::TEND_THREADS / 32);
@@ -1475,6 +1580,27 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   mark(1);
   kb<<<gb, 32 * wb, sb, st>>>(op, m, na);
   mark(2);
+  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) {
+    if (b.fv) {
+      // face values once per face, then the tendency kernel on them (the
+      // face kernel's time is counted with the tendency kernel's)
+      constexpr int wf = std::min(pick_warps(sizeof(SOps<Dm>), sizeof(TWarp<Dm, true>)),
+                                  Dm::TEND_THREADS / 32);
+      constexpr size_t sf = sizeof(SOps<Dm>) + wf * sizeof(TWarp<Dm, true>);
+      int gf = 0;
+      e = resident_grid(kf_tendf<Dm, VAR>, 32 * wf, sf, sms, m.ne, wf, &gf);
+      if (e != cudaSuccess) return e;
+      const size_t fs = (size_t)m.ne * Dm::N;
+      FaceArgs fa{{b.f, b.f + fs, b.f + 2 * fs, b.f + 3 * fs, b.uh, b.vh}, b.fv};
+      const int items = m.nf * Dm::G;
+      kf_faces<Dm, 6><<<(items + 255) / 256, 256, 0, st>>>(op, m, fa);
+      kf_tendf<Dm, VAR><<<gf, 32 * wf, sf, st>>>(op, m, ta, sa);
+      mark(3);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) *launches += 4;
+      return e;
+    }
+  }
   kt<<<gt, 32 * wt, stt, st>>>(op, m, ta, sa);
   mark(3);
   e = cudaGetLastError();

@@ -32,6 +32,7 @@ struct NlArgs {
 
 struct TendArgs {
   const double *gx0, *gy0, *uh, *vh, *f;
+  const double *fv = nullptr;  // [nf][6][ngf] face values of f, uh, vh, or null
 };
 
 struct LinArgs {
@@ -86,6 +87,9 @@ struct RhsBuffers {
   const double *su, *sv, *sh;          // stage input
   const double *hb, *w0, *z0, *fc;     // time-constant fields
   double *q, *f, *gx0, *gy0, *uh, *vh; // nonlinear intermediates
+  // optional: [nf][6][ngf] face values of the tendency kernel's six fields
+  // (computed once per face instead of once per side)
+  double *fv = nullptr;
   double mu0, mb0, g0, hh0;
   // optional: recorded when sh is in place (the kernels that read sh wait
   // for it; the q-phase, which reads only su and sv, does not)
