@@ -70,6 +70,7 @@ struct spoc_handle {
   double *fv = nullptr;  // [nf][6][ngf] face values of the tendency kernel
   double *eterms = nullptr, *escal = nullptr;
   int *flag = nullptr;
+  unsigned *gbar = nullptr;  // grid-barrier word of the multi-step linear kernel
   unsigned long long *cflbits = nullptr;
   MixedCtx *mx = nullptr;  // SPOC_MIXED: the resident state lives here (psi basis)
   // FP64: one RK4 step captured as a CUDA graph (replayed by spoc_rk4_steps),
@@ -418,6 +419,7 @@ extern "C" int spoc_create(const spoc_tables *t, const spoc_mesh *m, int variant
     if (ce == cudaSuccess) ce = h->alloc(&h->eterms, 3 * (size_t)h->ne);
     if (ce == cudaSuccess) ce = h->alloc(&h->escal, 4);
     if (ce == cudaSuccess) ce = h->alloc(&h->flag, 1);
+    if (ce == cudaSuccess) ce = h->alloc(&h->gbar, 1);
     if (ce == cudaSuccess) ce = h->alloc(&h->cflbits, 1);
     h->op.flag = h->flag;
     if (ce == cudaSuccess && fast_available(nc, h->ng, h->ngf)) {
@@ -628,6 +630,40 @@ bool mapped_host(const double *p, double **dev) {
 // arrays; the last stage of the last step stores the new state there too.
 // sh_ready (optional): the first right-hand side's kernels that read h wait
 // for it.
+// The linear variant on the compile-time-sized path runs all the steps in one
+// cooperative launch when the mesh fits one pass of the resident warps
+// (cudaErrorNotSupported: it does not, nothing was launched; nsteps 0 only
+// asks whether it applies).
+cudaError_t lin_steps(spoc_handle *h, const StageArgs &sa, int nsteps, double *const *host,
+                      cudaEvent_t sh_ready) {
+  if (h->variant != SPOC_LIN || h->path == SPOC_PATH_GENERIC ||
+      !fast_available(h->nc, h->ng, h->ngf))
+    return cudaErrorNotSupported;
+  // a cooperative launch is not captured into a caller's graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(h->st, &cap);
+  if (e != cudaSuccess) return e;
+  if (cap != cudaStreamCaptureStatusNone) return cudaErrorNotSupported;
+  LinSteps ls{};
+  ls.sa = sa;
+  for (int c = 0; c < 3; ++c) {
+    ls.bufa[c] = h->SA[c];
+    ls.bufb[c] = h->SB[c];
+    ls.host[c] = host ? host[c] : nullptr;
+  }
+  ls.g0 = h->g0;
+  ls.hh0 = h->hh0;
+  ls.nsteps = nsteps;
+  ls.count = h->gbar;
+  if (sh_ready) {
+    e = cudaStreamWaitEvent(h->st, sh_ready, 0);
+    if (e != cudaSuccess) return e;
+  }
+  return h->precision == SPOC_FP64_FMA
+             ? lin_steps_fast_fma(h->op, h->mesh, ls, h->st, h->sms, &h->launches)
+             : lin_steps_fast(h->op, h->mesh, ls, h->st, h->sms, &h->launches);
+}
+
 int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *base = nullptr,
                        double *const *host = nullptr, int host_ld = 0,
                        cudaEvent_t sh_ready = nullptr) {
@@ -639,6 +675,12 @@ int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *bas
   for (int c = 0; c < 3; ++c) {
     sa.base[c] = base[c];
     sa.acc[c] = h->ACC[c];
+  }
+  sa.host_ld = host_ld;
+  if (nsteps > 0) {
+    const cudaError_t le = lin_steps(h, sa, nsteps, host, sh_ready);
+    if (le == cudaSuccess) return SPOC_OK;
+    if (le != cudaErrorNotSupported) return fail(SPOC_E_CUDA, "multi-step linear launch", le);
   }
   for (int it = 0; it < nsteps; ++it) {
     for (int s = 0; s < 4; ++s) {
@@ -667,6 +709,12 @@ int enqueue_steps_fp64(spoc_handle *h, double dt, int nsteps, double *const *bas
 // capture; the graph is captured from the next one.
 int graph_steps_fp64(spoc_handle *h, double dt, int nsteps) {
   if (nsteps <= 0) return SPOC_OK;
+  if (h->variant == SPOC_LIN) {
+    // the multi-step linear kernel needs no graph (nsteps 0: does it apply?)
+    const StageArgs probe{};
+    if (lin_steps(h, probe, 0, nullptr, nullptr) == cudaSuccess)
+      return enqueue_steps_fp64(h, dt, nsteps);
+  }
   // a caller capturing the handle's stream itself gets plain launches
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(h->st, &cap), "capture status");

@@ -735,10 +735,11 @@ __device__ __forceinline__ void stage_update(const StageArgs &sa, int fld, int e
 // ---------------------------------------------------------------------------
 // q-phase (calvarnl_fs.f:88-226)
 // ---------------------------------------------------------------------------
-template <class Dm>
+template <class Dm, bool FACES = false>
 struct __align__(16) QWarp {
   double own[2 * Dm::N];
-  double nb[3 * nb_stride<Dm, 2>()];
+  double nb[FACES ? 2 : 3 * nb_stride<Dm, 2>()];
+  double fvs[FACES ? 3 * 2 * Dm::G : 2];  // face records of u, v (FACES)
   double fr[2 * 32];
   double fb[4 * 32];
   double sm[64];
@@ -746,19 +747,29 @@ struct __align__(16) QWarp {
 };
 
 // One element of the q-phase from the face-value chains on: own / nb hold the
-// element's and its neighbours' u, v; prefetch() is called once they are free
+// element's and its neighbours' u, v (FACES: nb holds the face records of
+// kf_faces, [side][field][point]); prefetch() is called once they are free
 // (after the mat-vecs); gq receives gxx, gxy, gyx, gyy.
-template <class Dm, int VAR, class Prefetch>
+template <class Dm, int VAR, bool FACES = false, class Prefetch>
 __device__ __forceinline__ void qphase_elem(const SOps<Dm> &S, const DevMesh &m, int e,
                                             const Sides &sd, const double *own, const double *nb,
                                             double *fr, double *fb, double *sm, Prefetch prefetch,
                                             double (&gq)[4][Dm::R]) {
-  constexpr int N = Dm::N, R = Dm::R;
+  constexpr int N = Dm::N, R = Dm::R, G = Dm::G;
   const Geo g = geo(m, e);
   int isg[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
-  face_values<Dm, 2>(S.pf, m, sd, own, nb, fr);
+  if constexpr (FACES) {
+    const int l = lane_id();
+    if (l < 3 * G) {
+      const int k = l / G, j = l - k * G;
+      fr[l] = nb[(k * 2) * G + j];
+      fr[32 + l] = nb[(k * 2 + 1) * G + j];
+    }
+  } else {
+    face_values<Dm, 2>(S.pf, m, sd, own, nb, fr);
+  }
   __syncwarp();
   scale_face<Dm>(m, sd, fr, fb + 0, 0);
   scale_face<Dm>(m, sd, fr, fb + 32, 1);
@@ -802,14 +813,26 @@ __device__ __forceinline__ void qphase_elem(const SOps<Dm> &S, const DevMesh &m,
   }
 }
 
-template <class Dm, int VAR>
+template <class Dm, int VAR, bool FACES = false>
 __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *__restrict__ su,
-                                                 const double *__restrict__ sv, double *q) {
+                                            const double *__restrict__ sv, double *q,
+                                            const double *fv = nullptr) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
-  QWarp<Dm> &W = reinterpret_cast<QWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
-  constexpr int N = Dm::N, R = Dm::R;
+  QWarp<Dm, FACES> &W =
+      reinterpret_cast<QWarp<Dm, FACES> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, R = Dm::R, G = Dm::G;
+  static_assert(!FACES || (Dm::R == 1 && Dm::N % 2 == 0), "face records need bulk row copies");
   const double *const fields[2] = {su, sv};
+  // the copies of element e: its rows and its neighbours' rows, or its rows
+  // and its three face records (FACES: W.fvs stands in for W.nb)
+  double *const nbs = FACES ? W.fvs : W.nb;
+  auto issue = [&](RowCopy<Dm, 2> &rc, int e, const Sides &sd) {
+    if constexpr (FACES)
+      rc.issue_own_faces(fields, e, sd, W.own, fv, W.fvs, 2 * G);
+    else
+      rc.issue(fields, e, sd, W.own, W.nb);
+  };
   // the coefficients of the warp's next element are copied into W.own / W.nb
   // while it works on the current one (the first copy overlaps the staging
   // of the operators)
@@ -820,7 +843,7 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
   if (PF) rows.init(&W.bar);
   if (PF && warp_global() < m.ne) {
     sd_next = sides_of(m, warp_global());
-    rows.issue(fields, warp_global(), sd_next, W.own, W.nb);
+    issue(rows, warp_global(), sd_next);
   }
   // the operator image arrives whole through one bulk copy (TMA engine)
   __shared__ __align__(8) uint64_t ops_bar;
@@ -842,8 +865,8 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
     }
     __syncwarp();
     double gq[4][R];  // gxx, gxy, gyx, gyy
-    qphase_elem<Dm, VAR>(S, m, e, sd, W.own, W.nb, W.fr, W.fb, W.sm, [&] {
-      if (PF && en < m.ne) rows.issue(fields, en, sd_next, W.own, W.nb);
+    qphase_elem<Dm, VAR, FACES>(S, m, e, sd, W.own, nbs, W.fr, W.fb, W.sm, [&] {
+      if (PF && en < m.ne) issue(rows, en, sd_next);
     }, gq);
 #pragma unroll
     for (int c = 0; c < 4; ++c) store_reg<Dm>(q + c * fs, gq[c], e);
@@ -1378,6 +1401,14 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
                                                  const double *__restrict__ sv, double *q) {
   qphase_body<Dm, VAR>(op, m, su, sv, q);
 }
+// the q-phase on the face values of kf_faces (one row per lane, even N)
+template <class Dm, int VAR>
+__global__ void __launch_bounds__(256) kf_qphasef(DevOps op, DevMesh m,
+                                                  const double *__restrict__ su,
+                                                  const double *__restrict__ sv, double *q,
+                                                  const double *__restrict__ fv) {
+  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) qphase_body<Dm, VAR, true>(op, m, su, sv, q, fv);
+}
 template <class Dm, int VAR>
 __global__ void __launch_bounds__(256, 2) kf_qphase_r2(DevOps op, DevMesh m,
                                                        const double *__restrict__ su,
@@ -1432,26 +1463,36 @@ struct __align__(16) LWarp {
   double sm[64];
 };
 
-template <class Dm>
-__global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, StageArgs sa) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
-  LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+// A load of the stage state: plain, or through L2 only (ld.global.cg) in the
+// multi-step kernel, whose blocks read rows that other blocks wrote earlier
+// in the same launch (behind a grid barrier).
+template <bool CG>
+__device__ __forceinline__ double ld_state(const double *p) {
+  if constexpr (CG) return __ldcg(p); else return *p;
+}
+
+// One element of the linear right-hand side and its RK4 stage update.
+template <class Dm, bool CG>
+__device__ __forceinline__ void lin_elem(const SOps<Dm> &S, LWarp<Dm> &W, const DevMesh &m,
+                                         const LinArgs &a, const StageArgs &sa, int e) {
   constexpr int N = Dm::N, R = Dm::R;
-  __shared__ __align__(8) uint64_t ops_bar;
-  if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) return;
   const int l = lane_id();
   const double mg0 = -a.g0, hh0 = a.hh0;
-  for (int e = warp_global(); e < m.ne; e += warp_count()) {
+  {
     const Sides sd = sides_of(m, e);
     const Geo g = geo(m, e);
     int isg[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
     double uk[R], vk[R], hk[R];
-    load_reg<Dm>(uk, a.su, e);
-    load_reg<Dm>(vk, a.sv, e);
-    load_reg<Dm>(hk, a.sh, e);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = l + 32 * r;
+      const size_t o = (size_t)e * N + i;
+      uk[r] = i < N ? ld_state<CG>(a.su + o) : 0.0;
+      vk[r] = i < N ? ld_state<CG>(a.sv + o) : 0.0;
+      hk[r] = i < N ? ld_state<CG>(a.sh + o) : 0.0;
+    }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int i = l + 32 * r;
@@ -1465,7 +1506,8 @@ __global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, S
     }
     stage_neighbours<Dm, 3>(sd, W.nb, [&](int f, int t, int i) {
       const size_t o = (size_t)t * N + i;
-      return f == 0 ? mul(mg0, a.sh[o]) : (f == 1 ? a.su[o] : a.sv[o]);
+      return f == 0 ? mul(mg0, ld_state<CG>(a.sh + o))
+                    : (f == 1 ? ld_state<CG>(a.su + o) : ld_state<CG>(a.sv + o));
     });
     __syncwarp();
     face_values<Dm, 3>(S.pf, m, sd, W.own, W.nb, W.fr);
@@ -1527,6 +1569,80 @@ __global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, S
   }
 }
 
+template <class Dm>
+__global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, StageArgs sa) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
+  LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  __shared__ __align__(8) uint64_t ops_bar;
+  if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) return;
+  for (int e = warp_global(); e < m.ne; e += warp_count()) lin_elem<Dm, false>(S, W, m, a, sa, e);
+}
+
+// Grid-wide barrier of a cooperative launch: every block adds one to *count
+// and waits until it reaches `target` (a multiple of the grid size).  The
+// wait is bounded: past kGridWaitLimit polls bit 2 of *flag is set and false
+// returned (the caller leaves the kernel).
+constexpr long long kGridWaitLimit = 1ll << 24;
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, int *flag) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+    bool done = false;
+    for (long long it = 0; it < kGridWaitLimit; ++it) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+      if (v >= target) {
+        done = true;
+        break;
+      }
+      __nanosleep(32);
+    }
+    if (!done) atomicOr(flag, 2);
+    __threadfence();
+    ok = done;
+  }
+  __syncthreads();
+  return ok;
+}
+
+// Several RK4 steps of the linear variant in one cooperative launch: the
+// operator image is staged once, the stages are separated by grid barriers
+// instead of kernel boundaries.  The stage buffers rotate as in one launch
+// per stage (input u0, A, B, A; output A, B, A, u0 in place), so the
+// arithmetic and its order are those of kf_lin.
+template <class Dm>
+__global__ void __launch_bounds__(256) kf_lin_steps(DevOps op, DevMesh m, LinSteps ls) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
+  LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  __shared__ __align__(8) uint64_t ops_bar;
+  const bool staged = bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag);
+  StageArgs sa = ls.sa;
+  unsigned target = 0;
+  for (int it = 0; it < ls.nsteps; ++it) {
+    for (int st = 0; st < 4; ++st) {
+      const bool last = it == ls.nsteps - 1 && st == 3;
+      sa.stage = st;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sa.out[c] = st == 1 ? ls.bufb[c] : ls.bufa[c];
+        sa.host[c] = last ? ls.host[c] : nullptr;
+      }
+      const LinArgs a{st == 0 ? ls.sa.base[0] : (st == 2 ? ls.bufb[0] : ls.bufa[0]),
+                      st == 0 ? ls.sa.base[1] : (st == 2 ? ls.bufb[1] : ls.bufa[1]),
+                      st == 0 ? ls.sa.base[2] : (st == 2 ? ls.bufb[2] : ls.bufa[2]), ls.g0, ls.hh0};
+      if (staged)
+        for (int e = warp_global(); e < m.ne; e += warp_count()) lin_elem<Dm, true>(S, W, m, a, sa, e);
+      if (last) return;
+      target += gridDim.x;
+      if (!grid_barrier(ls.count, target, op.flag)) return;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // operator images: the shared-memory layouts of SOps / SOpsQ, written once per
 // handle into global memory so that each block stages them with bulk copies
@@ -1575,7 +1691,24 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   const auto kq = qphase_kernel<Dm, VAR>();
   const auto kb = nlvol_kernel<Dm, VAR>();
   const auto kt = tend_kernel<Dm, VAR>();
-  kq<<<gq, 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
+  // face values of u, v once per face (counted with the q-phase)
+  bool qfaces = false;
+  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) {
+    if (b.fv) {
+      constexpr int wf = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm, true>));
+      constexpr size_t sf = sizeof(SOps<Dm>) + wf * sizeof(QWarp<Dm, true>);
+      int gf = 0;
+      e = resident_grid(kf_qphasef<Dm, VAR>, 32 * wf, sf, sms, m.ne, wf, &gf);
+      if (e != cudaSuccess) return e;
+      FaceArgs fa{{b.su, b.sv}, b.fv};
+      const int items = m.nf * Dm::G;
+      kf_faces<Dm, 2><<<(items + 255) / 256, 256, 0, st>>>(op, m, fa);
+      kf_qphasef<Dm, VAR><<<gf, 32 * wf, sf, st>>>(op, m, b.su, b.sv, b.q, b.fv);
+      *launches += 1;
+      qfaces = true;
+    }
+  }
+  if (!qfaces) kq<<<gq, 32 * wq, sq, st>>>(op, m, b.su, b.sv, b.q);
   if (b.sh_ready) cudaStreamWaitEvent(st, b.sh_ready, 0);
   mark(1);
   kb<<<gb, 32 * wb, sb, st>>>(op, m, na);
@@ -1623,6 +1756,34 @@ cudaError_t run_q(const DevOps &op, const DevMesh &m, const double *su, const do
   return cudaGetLastError();
 }
 
+// The multi-step linear kernel when one pass of the resident warps covers the
+// mesh (small meshes, where the per-stage launches dominate); else
+// cudaErrorNotSupported.
+template <class Dm>
+cudaError_t run_lin_steps(const DevOps &op, const DevMesh &m, const LinSteps &ls, cudaStream_t st,
+                          int sms, long long *launches) {
+  constexpr int w = pick_warps(sizeof(SOps<Dm>), sizeof(LWarp<Dm>));
+  constexpr size_t sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
+  int per_sm = 0;
+  cudaError_t e = device_blocks_per_sm(kf_lin_steps<Dm>, 32 * w, sm, &per_sm);
+  if (e != cudaSuccess) return e;
+  if ((long long)sms * per_sm * w < m.ne) return cudaErrorNotSupported;
+  int grid = 0;
+  e = resident_grid(kf_lin_steps<Dm>, 32 * w, sm, sms, m.ne, w, &grid);
+  if (e != cudaSuccess) return e;
+  if (ls.nsteps <= 0) return cudaSuccess;
+  e = cudaMemsetAsync(ls.count, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  DevOps o = op;
+  DevMesh mm = m;
+  LinSteps l = ls;
+  void *args[] = {&o, &mm, &l};
+  e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kf_lin_steps<Dm>), dim3(grid),
+                                  dim3(32 * w), args, sm, st);
+  if (e == cudaSuccess) *launches += 1;
+  return e;
+}
+
 template <class Dm>
 cudaError_t run_lin(const DevOps &op, const DevMesh &m, const RhsBuffers &b, const StageArgs &sa,
                     cudaStream_t st, int sms, cudaEvent_t *ev) {
@@ -1656,9 +1817,11 @@ cudaError_t run_any(int variant, const DevOps &op, const DevMesh &m, const RhsBu
 #if SPOC_FMA
 #define FAST_AVAILABLE fast_available_fma
 #define LAUNCH_FAST launch_rhs_fast_fma
+#define LIN_STEPS_FAST lin_steps_fast_fma
 #else
 #define FAST_AVAILABLE fast_available
 #define LAUNCH_FAST launch_rhs_fast
+#define LIN_STEPS_FAST lin_steps_fast
 #endif
 
 bool FAST_AVAILABLE(int nc, int ng, int ngf) {
@@ -1734,6 +1897,17 @@ cudaError_t LAUNCH_FAST(int variant, const DevOps &op, const DevMesh &m, const R
   else if (nc == 7 && ng == 42 && ngf == 9) e = run_any<Dims<7, 42, 9>>(variant, op, m, b, sa, st, sms, ev, launches);
   if (e == cudaSuccess && variant == kLIN) *launches += 1;
   return e;
+}
+
+cudaError_t LIN_STEPS_FAST(const DevOps &op, const DevMesh &m, const LinSteps &ls, cudaStream_t st,
+                           int sms, long long *launches) {
+  const int nc = op.nc, ng = op.ng, ngf = op.ngf;
+  if (nc == 3 && ng == 12 && ngf == 4) return run_lin_steps<Dims<3, 12, 4>>(op, m, ls, st, sms, launches);
+  if (nc == 4 && ng == 25 && ngf == 5) return run_lin_steps<Dims<4, 25, 5>>(op, m, ls, st, sms, launches);
+  if (nc == 5 && ng == 27 && ngf == 6) return run_lin_steps<Dims<5, 27, 6>>(op, m, ls, st, sms, launches);
+  if (nc == 6 && ng == 33 && ngf == 7) return run_lin_steps<Dims<6, 33, 7>>(op, m, ls, st, sms, launches);
+  if (nc == 7 && ng == 42 && ngf == 9) return run_lin_steps<Dims<7, 42, 9>>(op, m, ls, st, sms, launches);
+  return cudaErrorNotSupported;
 }
 
 }  // namespace spoc

@@ -40,6 +40,20 @@ struct LinArgs {
   double g0, hh0;
 };
 
+// Several RK4 steps of the linear variant in one launch: sa carries dt, dt6,
+// base (u0, updated in place), acc, flag and host_ld; bufa / bufb are the
+// two stage buffers; host (optional) receives the final state; count is a
+// device word for the grid barrier (zeroed by the launcher).
+struct LinSteps {
+  StageArgs sa;
+  double *bufa[3];
+  double *bufb[3];
+  double *host[3];
+  double g0, hh0;
+  int nsteps;
+  unsigned *count;
+};
+
 // Tangent-linear quadrature-point stage: base state (su.., q) and perturbation
 // (du, dv, dh, dq) in; perturbations of gx0, gy0, uh, vh, F out.
 struct TlmArgs {
@@ -195,11 +209,20 @@ cudaError_t launch_rhs_fast(int variant, const DevOps &op, const DevMesh &m, con
 cudaError_t launch_qphase_fast(int variant, const DevOps &op, const DevMesh &m, const double *su,
                                const double *sv, double *q, cudaStream_t st, int sms);
 
+// Several RK4 steps of the linear variant in one cooperative launch of the
+// compile-time-sized kernel, bit-identical to one launch per stage; returns
+// cudaErrorNotSupported (nothing launched) when the degree is not tabulated
+// or the mesh needs more than one pass of the resident warps.
+cudaError_t lin_steps_fast(const DevOps &op, const DevMesh &m, const LinSteps &ls, cudaStream_t st,
+                           int sms, long long *launches);
+
 // The same kernels with fused multiply-adds (spoc_fast.cu built with SPOC_FMA=1).
 bool fast_available_fma(int nc, int ng, int ngf);
 cudaError_t launch_rhs_fast_fma(int variant, const DevOps &op, const DevMesh &m,
                                 const RhsBuffers &b, const StageArgs &sa, cudaStream_t st, int sms,
                                 long long *launches, cudaEvent_t *ev = nullptr);
+cudaError_t lin_steps_fast_fma(const DevOps &op, const DevMesh &m, const LinSteps &ls,
+                               cudaStream_t st, int sms, long long *launches);
 
 // 8 independent chains of `iters` multiply-adds per thread, sms*8 blocks of 256;
 // mode 0 FP64 fused, 1 FP64 separately rounded, 2 FP32 fused

@@ -101,14 +101,15 @@ def test_rk4_host_entry_matches_resident(gpu_lib):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c2_fs_p6", "c1_lin_p3"])
 @pytest.mark.parametrize("ld", [28, 45])
 @pytest.mark.parametrize("path", ["templated", "generic"])
-def test_rk4_host_entry_pinned_buffers(gpu_lib, ld, path):
+def test_rk4_host_entry_pinned_buffers(gpu_lib, ld, path, name):
     """Mapped pinned caller arrays take the direct path (the last stage stores
     the new state into them); the result is the resident run's, bit for bit,
     and the rows past nm of an ld-strided array are left alone."""
     import torch
-    p = W.build_problem(W.small(W.CONFIGS["c2_fs_p6"], 8), ld=ld)
+    p = W.build_problem(W.small(W.CONFIGS[name], 8), ld=ld)
     s = W.make_solver(p)
     s.set_kernel_path(path)
     pin = [torch.from_numpy(a.copy()).pin_memory() for a in (p.u, p.v, p.h)]
@@ -128,6 +129,28 @@ def test_rk4_host_entry_pinned_buffers(gpu_lib, ld, path):
     before = [a.copy() for a in host]
     s.rk4_steps_host(*host, p.dt, 0)
     assert all(np.array_equal(a, b) for a, b in zip(host, before))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("steps", [1, 7])
+def test_lin_steps_in_one_launch(gpu_lib, steps):
+    """The linear variant's RK4 steps run as one cooperative launch on a mesh
+    that one pass of the resident warps covers (grid barriers between the
+    stages), bit-identical to one launch per stage (generic kernels)."""
+    p = W.build_problem(W.CONFIGS["c1_lin_p3"])
+    s = W.make_solver(p)
+    s.set_kernel_path("templated")
+    s.set_state(p.u, p.v, p.h)
+    l0 = s.launches
+    s.rk4_steps(p.dt, steps)
+    assert s.launches - l0 == 1
+    g = W.make_solver(p)
+    g.set_kernel_path("generic")
+    g.set_state(p.u, p.v, p.h)
+    l0 = g.launches
+    g.rk4_steps(p.dt, steps)
+    assert g.launches - l0 == 4 * steps
+    assert_bitwise(s.get_state(), g.get_state(), p.T.nm)
 
 
 @pytest.mark.gpu
@@ -389,7 +412,7 @@ DEGREES = [(3, 12, 4), (4, 25, 5), (5, 27, 6), (6, 33, 7), (7, 42, 9)]
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", ["fs", "ns", "inv"])
+@pytest.mark.parametrize("variant", ["lin", "fs", "ns", "inv"])
 @pytest.mark.parametrize("deg", DEGREES, ids=[f"p{d[0]}" for d in DEGREES])
 def test_every_degree_and_variant_bitwise(gpu_lib, deg, variant):
     import dataclasses
