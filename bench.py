@@ -115,6 +115,23 @@ def timed_steps(torch, stream, flush, s, dt, nsteps):
     return sum(out) / nsteps
 
 
+def timed_call(torch, stream, flush, s, dt, nsteps, repeats=3):
+    """ms per RK4 step of one rk4_steps(dt, nsteps) call (L2 flushed before
+    the call), the median of `repeats` calls."""
+    out = []
+    for _ in range(repeats):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            a.record(stream)
+        s.rk4_steps(dt, nsteps)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        b.synchronize()
+        out.append(a.elapsed_time(b) / nsteps)
+    return sorted(out)[len(out) // 2]
+
+
 def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, tsteps=10):
     """Mixed-precision form against plain FP64 on one configuration, with the
     volume work on the FP32 pipes (the default) and on the tensor cores: ms
@@ -181,9 +198,14 @@ def mixed_measure(torch, stream, flush, W, api, name="c3_inv_p7", steps=1000, ts
     }
 
 
-def fp64_configs_measure(torch, stream, flush, W, names=("c1_lin_p3", "c4_ns_p4"), steps=20):
+def fp64_configs_measure(torch, stream, flush, W, names=("c1_lin_p3", "c4_ns_p4"), steps=20,
+                         call_steps=100):
     """Plain FP64 step of the other single-GPU configurations (C3 in
-    mixed_measure): ms per RK4 step, L2 flushed before each, and DOF-updates/s."""
+    mixed_measure), DOF-updates/s from ms per RK4 step of one
+    rk4_steps(dt, call_steps) call (L2 flushed before the call: how a run of
+    many steps is made); beside it the ms per step of single-step calls (L2
+    flushed before each; host launch cost and the per-call flag read
+    included)."""
     out = {}
     for name in names:
         p = W.build_problem(W.CONFIGS[name])
@@ -192,10 +214,16 @@ def fp64_configs_measure(torch, stream, flush, W, names=("c1_lin_p3", "c4_ns_p4"
         s.set_state(p.u, p.v, p.h)
         s.rk4_steps(p.dt, 3)
         l0 = s.launches
-        ms = timed_steps(torch, stream, flush, s, p.dt, steps)
+        ms1 = timed_steps(torch, stream, flush, s, p.dt, steps)
+        per1 = (s.launches - l0) / steps
+        l0 = s.launches
+        ms = timed_call(torch, stream, flush, s, p.dt, call_steps)
         out[name] = {"ne": p.mesh.ne, "nm": p.T.nm, "ms_per_step": ms,
                      "value": 3.0 * p.T.nm * p.mesh.ne / (ms * 1e-3), "unit": UNIT,
-                     "launches_per_step": (s.launches - l0) / steps}
+                     "steps_per_call": call_steps,
+                     "launches_per_call": (s.launches - l0) / 3,
+                     "ms_per_step_single_step_calls": ms1,
+                     "launches_per_single_step_call": per1}
         s.close()
     return out
 

@@ -1471,102 +1471,125 @@ __device__ __forceinline__ double ld_state(const double *p) {
   if constexpr (CG) return __ldcg(p); else return *p;
 }
 
-// One element of the linear right-hand side and its RK4 stage update.
+// The mesh record of one element of the linear kernels (read once per
+// element; the multi-step kernel keeps it for the whole launch).
+struct LinElem {
+  Sides sd;
+  Geo g;
+  int isg[3];
+  bool wall;
+  double dnx, dny;
+};
+__device__ __forceinline__ LinElem lin_elem_mesh(const DevMesh &m, int e) {
+  LinElem r;
+  r.sd = sides_of(m, e);
+  r.g = geo(m, e);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) r.isg[k] = __ldg(m.its + 3 * e + k);
+  r.wall = __ldg(m.bdl + e) != 0;
+  r.dnx = r.wall ? __ldg(m.normt + 2 * e) : 0.0;
+  r.dny = r.wall ? __ldg(m.normt + 2 * e + 1) : 0.0;
+  return r;
+}
+
+// The linear right-hand side of one element (calvar_lin.f:7-287) from its
+// own u, v, h (registers) and its neighbours' rows of a.su, a.sv, a.sh:
+// gx, gy, hb receive the tendencies of u, v, h after the mass solves.
 template <class Dm, bool CG>
-__device__ __forceinline__ void lin_elem(const SOps<Dm> &S, LWarp<Dm> &W, const DevMesh &m,
-                                         const LinArgs &a, const StageArgs &sa, int e) {
+__device__ __forceinline__ void lin_rhs(const SOps<Dm> &S, LWarp<Dm> &W, const DevMesh &m,
+                                        const LinElem &lm, const LinArgs &a,
+                                        const double (&uk)[Dm::R], const double (&vk)[Dm::R],
+                                        const double (&hk)[Dm::R], double (&gx)[Dm::R],
+                                        double (&gy)[Dm::R], double (&hb)[Dm::R]) {
   constexpr int N = Dm::N, R = Dm::R;
   const int l = lane_id();
   const double mg0 = -a.g0, hh0 = a.hh0;
-  {
-    const Sides sd = sides_of(m, e);
-    const Geo g = geo(m, e);
-    int isg[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) isg[k] = __ldg(m.its + 3 * e + k);
-    double uk[R], vk[R], hk[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = l + 32 * r;
-      const size_t o = (size_t)e * N + i;
-      uk[r] = i < N ? ld_state<CG>(a.su + o) : 0.0;
-      vk[r] = i < N ? ld_state<CG>(a.sv + o) : 0.0;
-      hk[r] = i < N ? ld_state<CG>(a.sh + o) : 0.0;
+  for (int r = 0; r < R; ++r) {
+    const int i = l + 32 * r;
+    if (i < N) {
+      W.own[i] = mul(mg0, hk[r]);  // fxx = fyy = -g0 h (calvar_lin.f:76-79)
+      W.own[N + i] = uk[r];
+      W.own[2 * N + i] = vk[r];
+      W.xs[i] = mul(uk[r], hh0);
+      W.xs[N + i] = mul(vk[r], hh0);
     }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = l + 32 * r;
-      if (i < N) {
-        W.own[i] = mul(mg0, hk[r]);  // fxx = fyy = -g0 h (calvar_lin.f:76-79)
-        W.own[N + i] = uk[r];
-        W.own[2 * N + i] = vk[r];
-        W.xs[i] = mul(uk[r], hh0);
-        W.xs[N + i] = mul(vk[r], hh0);
-      }
-    }
-    stage_neighbours<Dm, 3>(sd, W.nb, [&](int f, int t, int i) {
-      const size_t o = (size_t)t * N + i;
-      return f == 0 ? mul(mg0, ld_state<CG>(a.sh + o))
-                    : (f == 1 ? ld_state<CG>(a.su + o) : ld_state<CG>(a.sv + o));
-    });
-    __syncwarp();
-    face_values<Dm, 3>(S.pf, m, sd, W.own, W.nb, W.fr);
-    __syncwarp();
-    scale_face<Dm>(m, sd, W.fr, W.fb, 0);        // fbdxx
-    scale_face<Dm>(m, sd, W.fr, W.fb + 32, 1);   // fbdyy
-    scale_face_h<Dm>(m, sd, W.fr + 32, W.fb + 64, 0, hh0);  // fbdx
-    scale_face_h<Dm>(m, sd, W.fr + 64, W.fb + 96, 1, hh0);  // fbdy
-    double af[1][R], bf[1][R], ah[2][R], bh[2][R];
-    matvec2<Dm, 1>(S.agx, S.agy, W.own, N, af, bf);
-    matvec2<Dm, 2>(S.agx, S.agy, W.xs, N, ah, bh);
-    __syncwarp();
-    const double cby = mul(g.by, g.detai), cay = mul(g.ay, g.detai);
-    const double cbx = mul(g.bx, g.detai), cax = mul(g.ax, g.detai);
-    double gx[R], gy[R], hb[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) gx[r] = gy[r] = hb[r] = 0.0;
-    // u, v (calvar_lin.f:143-166); the zero fields fxy, fyx contribute exact zeros
-    axpy<R>(gx, af[0], -cby);
-    axpy<R>(gx, bf[0], cay);
-    axpy<R>(gy, af[0], cbx);
-    axpy<R>(gy, bf[0], -cax);
-    // h (calvar_lin.f:256-270)
-    axpy<R>(hb, ah[0], cby);
-    axpy<R>(hb, bh[0], -cay);
-    axpy<R>(hb, ah[1], -cbx);
-    axpy<R>(hb, bh[1], cax);
-    double t[4][3][R];
-    lift_sums<Dm, 4>(S, isg, W.fb, t);
-    apply_lift<R>(gx, t[0], isg, g.detai);
-    apply_lift<R>(gy, t[1], isg, g.detai);
-    apply_lift<R>(hb, t[2], isg, -g.detai);
-    apply_lift<R>(hb, t[3], isg, -g.detai);
-    if (__ldg(m.bdl + e)) {
-      const double dnx = __ldg(m.normt + 2 * e), dny = __ldg(m.normt + 2 * e + 1);
-      double gn[R], full2[2][R], bu[1][R];
-      rot<R>(gn, full2[0], gx, gy, dnx, dny);
-      copy<R>(full2[1], hb);
-      reduc<Dm>(S, gn, bu[0], W.sm);
-      solve_red_b<Dm, SOps<Dm>, 1>(S, bu);
-      solve_full_b<Dm, SOps<Dm>, 2>(S, full2);
-      reduc_inv<Dm>(S, bu[0], gn, W.sm);
-      rot<R>(gx, gy, gn, full2[0], dnx, dny);
-      copy<R>(hb, full2[1]);
-    } else {
-      double s3[3][R];
-      copy<R>(s3[0], gx);
-      copy<R>(s3[1], gy);
-      copy<R>(s3[2], hb);
-      solve_full_b<Dm, SOps<Dm>, 3>(S, s3);
-      copy<R>(gx, s3[0]);
-      copy<R>(gy, s3[1]);
-      copy<R>(hb, s3[2]);
-    }
-    stage_update<Dm>(sa, 0, e, gx);
-    stage_update<Dm>(sa, 1, e, gy);
-    stage_update<Dm>(sa, 2, e, hb);
-    __syncwarp();
   }
+  stage_neighbours<Dm, 3>(lm.sd, W.nb, [&](int f, int t, int i) {
+    const size_t o = (size_t)t * N + i;
+    return f == 0 ? mul(mg0, ld_state<CG>(a.sh + o))
+                  : (f == 1 ? ld_state<CG>(a.su + o) : ld_state<CG>(a.sv + o));
+  });
+  __syncwarp();
+  face_values<Dm, 3>(S.pf, m, lm.sd, W.own, W.nb, W.fr);
+  __syncwarp();
+  scale_face<Dm>(m, lm.sd, W.fr, W.fb, 0);        // fbdxx
+  scale_face<Dm>(m, lm.sd, W.fr, W.fb + 32, 1);   // fbdyy
+  scale_face_h<Dm>(m, lm.sd, W.fr + 32, W.fb + 64, 0, hh0);  // fbdx
+  scale_face_h<Dm>(m, lm.sd, W.fr + 64, W.fb + 96, 1, hh0);  // fbdy
+  double af[1][R], bf[1][R], ah[2][R], bh[2][R];
+  matvec2<Dm, 1>(S.agx, S.agy, W.own, N, af, bf);
+  matvec2<Dm, 2>(S.agx, S.agy, W.xs, N, ah, bh);
+  __syncwarp();
+  const double cby = mul(lm.g.by, lm.g.detai), cay = mul(lm.g.ay, lm.g.detai);
+  const double cbx = mul(lm.g.bx, lm.g.detai), cax = mul(lm.g.ax, lm.g.detai);
+#pragma unroll
+  for (int r = 0; r < R; ++r) gx[r] = gy[r] = hb[r] = 0.0;
+  // u, v (calvar_lin.f:143-166); the zero fields fxy, fyx contribute exact zeros
+  axpy<R>(gx, af[0], -cby);
+  axpy<R>(gx, bf[0], cay);
+  axpy<R>(gy, af[0], cbx);
+  axpy<R>(gy, bf[0], -cax);
+  // h (calvar_lin.f:256-270)
+  axpy<R>(hb, ah[0], cby);
+  axpy<R>(hb, bh[0], -cay);
+  axpy<R>(hb, ah[1], -cbx);
+  axpy<R>(hb, bh[1], cax);
+  double t[4][3][R];
+  lift_sums<Dm, 4>(S, lm.isg, W.fb, t);
+  apply_lift<R>(gx, t[0], lm.isg, lm.g.detai);
+  apply_lift<R>(gy, t[1], lm.isg, lm.g.detai);
+  apply_lift<R>(hb, t[2], lm.isg, -lm.g.detai);
+  apply_lift<R>(hb, t[3], lm.isg, -lm.g.detai);
+  if (lm.wall) {
+    const double dnx = lm.dnx, dny = lm.dny;
+    double gn[R], full2[2][R], bu[1][R];
+    rot<R>(gn, full2[0], gx, gy, dnx, dny);
+    copy<R>(full2[1], hb);
+    reduc<Dm>(S, gn, bu[0], W.sm);
+    solve_red_b<Dm, SOps<Dm>, 1>(S, bu);
+    solve_full_b<Dm, SOps<Dm>, 2>(S, full2);
+    reduc_inv<Dm>(S, bu[0], gn, W.sm);
+    rot<R>(gx, gy, gn, full2[0], dnx, dny);
+    copy<R>(hb, full2[1]);
+  } else {
+    double s3[3][R];
+    copy<R>(s3[0], gx);
+    copy<R>(s3[1], gy);
+    copy<R>(s3[2], hb);
+    solve_full_b<Dm, SOps<Dm>, 3>(S, s3);
+    copy<R>(gx, s3[0]);
+    copy<R>(gy, s3[1]);
+    copy<R>(hb, s3[2]);
+  }
+}
+
+// One element of the linear right-hand side and its RK4 stage update.
+template <class Dm>
+__device__ __forceinline__ void lin_elem(const SOps<Dm> &S, LWarp<Dm> &W, const DevMesh &m,
+                                         const LinArgs &a, const StageArgs &sa, int e) {
+  constexpr int R = Dm::R;
+  const LinElem lm = lin_elem_mesh(m, e);
+  double uk[R], vk[R], hk[R];
+  load_reg<Dm>(uk, a.su, e);
+  load_reg<Dm>(vk, a.sv, e);
+  load_reg<Dm>(hk, a.sh, e);
+  double gx[R], gy[R], hb[R];
+  lin_rhs<Dm, false>(S, W, m, lm, a, uk, vk, hk, gx, gy, hb);
+  stage_update<Dm>(sa, 0, e, gx);
+  stage_update<Dm>(sa, 1, e, gy);
+  stage_update<Dm>(sa, 2, e, hb);
+  __syncwarp();
 }
 
 template <class Dm>
@@ -1576,7 +1599,7 @@ __global__ void __launch_bounds__(256) kf_lin(DevOps op, DevMesh m, LinArgs a, S
   LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
   __shared__ __align__(8) uint64_t ops_bar;
   if (!bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag)) return;
-  for (int e = warp_global(); e < m.ne; e += warp_count()) lin_elem<Dm, false>(S, W, m, a, sa, e);
+  for (int e = warp_global(); e < m.ne; e += warp_count()) lin_elem<Dm>(S, W, m, a, sa, e);
 }
 
 // Grid-wide barrier of a cooperative launch: every block adds one to *count
@@ -1608,34 +1631,88 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, i
   return ok;
 }
 
-// Several RK4 steps of the linear variant in one cooperative launch: the
-// operator image is staged once, the stages are separated by grid barriers
-// instead of kernel boundaries.  The stage buffers rotate as in one launch
-// per stage (input u0, A, B, A; output A, B, A, u0 in place), so the
-// arithmetic and its order are those of kf_lin.
+// Several RK4 steps of the linear variant in one cooperative launch, one
+// element per warp for the whole launch: the operator image is staged once,
+// the element's mesh record, its u0 and RK4 accumulator rows and its stage
+// values stay in registers, and only the neighbours' stage rows are read
+// (through L2 only: other blocks wrote them earlier in the launch, behind a
+// grid barrier).  The stage buffers rotate as in one launch per stage (input
+// u0, A, B, A; output A, B, A, u0 in place); the arithmetic and its order are
+// those of kf_lin and stage_update.
+constexpr int kLinStepsMaxWarps = 20;
 template <class Dm>
-__global__ void __launch_bounds__(256) kf_lin_steps(DevOps op, DevMesh m, LinSteps ls) {
+__global__ void __launch_bounds__(32 * kLinStepsMaxWarps) kf_lin_steps(DevOps op, DevMesh m,
+                                                                     LinSteps ls) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
   LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
+  constexpr int N = Dm::N, R = Dm::R;
   __shared__ __align__(8) uint64_t ops_bar;
   const bool staged = bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag);
-  StageArgs sa = ls.sa;
+  const int l = lane_id();
+  const int e = warp_global();
+  const bool active = staged && e < m.ne;
+  LinElem lm{};
+  double u0[3][R], acc[3][R], x[3][R];  // u0, du1 + 2 du2 + 2 du3, stage input
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < R; ++r) u0[c][r] = acc[c][r] = x[c][r] = 0.0;
+  if (active) {
+    lm = lin_elem_mesh(m, e);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = l + 32 * r;
+        u0[c][r] = x[c][r] = i < N ? __ldcg(ls.sa.base[c] + (size_t)e * N + i) : 0.0;
+      }
+  }
+  const double dt = ls.sa.dt, dt6 = ls.sa.dt6;
   unsigned target = 0;
   for (int it = 0; it < ls.nsteps; ++it) {
     for (int st = 0; st < 4; ++st) {
       const bool last = it == ls.nsteps - 1 && st == 3;
-      sa.stage = st;
+      if (active) {
+        const LinArgs a{st == 0 ? ls.sa.base[0] : (st == 2 ? ls.bufb[0] : ls.bufa[0]),
+                        st == 0 ? ls.sa.base[1] : (st == 2 ? ls.bufb[1] : ls.bufa[1]),
+                        st == 0 ? ls.sa.base[2] : (st == 2 ? ls.bufb[2] : ls.bufa[2]), ls.g0,
+                        ls.hh0};
+        double d[3][R];
+        lin_rhs<Dm, true>(S, W, m, lm, a, x[0], x[1], x[2], d[0], d[1], d[2]);
+        // stage_update with u0 and the accumulator in registers
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        sa.out[c] = st == 1 ? ls.bufb[c] : ls.bufa[c];
-        sa.host[c] = last ? ls.host[c] : nullptr;
+        for (int c = 0; c < 3; ++c) {
+          double *const out = st == 1 ? ls.bufb[c] : ls.bufa[c];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = l + 32 * r;
+            if (i >= N) continue;
+            const size_t o = (size_t)e * N + i;
+            const double dd = d[c][r];
+            if (!isfinite(dd)) atomicOr(ls.sa.flag, 1);
+            if (st == 0) {
+              acc[c][r] = dd;
+              x[c][r] = add(u0[c][r], mul(mul(dt, dd), 0.5));
+              out[o] = x[c][r];
+            } else if (st == 1) {
+              acc[c][r] = add(acc[c][r], mul(2.0, dd));
+              x[c][r] = add(u0[c][r], mul(mul(dt, dd), 0.5));
+              out[o] = x[c][r];
+            } else if (st == 2) {
+              acc[c][r] = add(acc[c][r], mul(2.0, dd));
+              x[c][r] = add(u0[c][r], mul(dt, dd));
+              out[o] = x[c][r];
+            } else {
+              const double nv = add(u0[c][r], mul(dt6, add(acc[c][r], dd)));
+              u0[c][r] = x[c][r] = nv;
+              ls.sa.base[c][o] = nv;
+              if (last && ls.host[c]) ls.host[c][(size_t)e * ls.sa.host_ld + i] = nv;
+            }
+          }
+        }
+        __syncwarp();
       }
-      const LinArgs a{st == 0 ? ls.sa.base[0] : (st == 2 ? ls.bufb[0] : ls.bufa[0]),
-                      st == 0 ? ls.sa.base[1] : (st == 2 ? ls.bufb[1] : ls.bufa[1]),
-                      st == 0 ? ls.sa.base[2] : (st == 2 ? ls.bufb[2] : ls.bufa[2]), ls.g0, ls.hh0};
-      if (staged)
-        for (int e = warp_global(); e < m.ne; e += warp_count()) lin_elem<Dm, true>(S, W, m, a, sa, e);
       if (last) return;
       target += gridDim.x;
       if (!grid_barrier(ls.count, target, op.flag)) return;
@@ -1756,21 +1833,23 @@ cudaError_t run_q(const DevOps &op, const DevMesh &m, const double *su, const do
   return cudaGetLastError();
 }
 
-// The multi-step linear kernel when one pass of the resident warps covers the
-// mesh (small meshes, where the per-stage launches dominate); else
-// cudaErrorNotSupported.
+// The multi-step linear kernel when the mesh fits one block per SM with one
+// element per warp (small meshes, where the per-stage launches and
+// the operator staging dominate): the elements are spread evenly, ceil(ne /
+// sms) warps per block, so no SM carries twice the work of another between
+// two barriers.  Else cudaErrorNotSupported.
 template <class Dm>
 cudaError_t run_lin_steps(const DevOps &op, const DevMesh &m, const LinSteps &ls, cudaStream_t st,
                           int sms, long long *launches) {
-  constexpr int w = pick_warps(sizeof(SOps<Dm>), sizeof(LWarp<Dm>));
-  constexpr size_t sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
+  if (m.ne < 1 || sms < 1) return cudaErrorNotSupported;
+  const int w = (m.ne + sms - 1) / sms;
+  if (w > kLinStepsMaxWarps) return cudaErrorNotSupported;
+  const size_t sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
   int per_sm = 0;
   cudaError_t e = device_blocks_per_sm(kf_lin_steps<Dm>, 32 * w, sm, &per_sm);
+  if (e == cudaErrorInvalidConfiguration) return cudaErrorNotSupported;  // no room on an SM
   if (e != cudaSuccess) return e;
-  if ((long long)sms * per_sm * w < m.ne) return cudaErrorNotSupported;
-  int grid = 0;
-  e = resident_grid(kf_lin_steps<Dm>, 32 * w, sm, sms, m.ne, w, &grid);
-  if (e != cudaSuccess) return e;
+  const int grid = (m.ne + w - 1) / w;  // <= sms blocks, one resident per SM at least
   if (ls.nsteps <= 0) return cudaSuccess;
   e = cudaMemsetAsync(ls.count, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;

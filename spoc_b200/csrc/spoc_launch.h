@@ -17,7 +17,8 @@ namespace spoc {
 
 // Resident blocks per SM of `kernel` at `threads` threads and `smem` bytes of
 // dynamic shared memory on the current device; raises the kernel's dynamic
-// shared-memory limit to `smem` there on first use.
+// shared-memory limit there on first use (cudaErrorInvalidConfiguration: the
+// block does not fit an SM).
 template <class K>
 cudaError_t device_blocks_per_sm(K kernel, int threads, size_t smem, int *per_sm) {
   static std::mutex mu;
@@ -32,7 +33,18 @@ cudaError_t device_blocks_per_sm(K kernel, int threads, size_t smem, int *per_sm
     *per_sm = it->second;
     return cudaSuccess;
   }
-  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the limit is raised to the most the device allows beside the kernel's
+  // static shared memory, not to `smem`: a kernel launched with several
+  // shared-memory sizes keeps them all valid
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes fa{};
+  e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  const int dyn_max = optin - (int)fa.sharedSizeBytes;
+  if (dyn_max < 0 || smem > (size_t)dyn_max) return cudaErrorInvalidConfiguration;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max);
   if (e != cudaSuccess) return e;
   int n = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem);
