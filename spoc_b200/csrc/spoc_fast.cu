@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "spoc_bulk.cuh"
 #include "spoc_device.cuh"
@@ -57,9 +58,23 @@ struct Dims {
   static constexpr int TEND_THREADS = R == 1 ? 256 : 192;
   static constexpr int TRI = N * (N + 1) / 2;
   static constexpr int TRIR = NMR * (NMR + 1) / 2;
+  static constexpr int LW = 32;              // lanes per element
   static_assert(3 * G <= 32, "face points must fit one warp");
   static_assert(N <= 64 && Q <= 64, "two rows per lane at most");
 };
+
+// The same sizes with two elements per warp, one per 16-lane half (degrees
+// whose modes and 3 * ngf face points fit 16 lanes).  The operator layouts
+// (SOps) are those of D.
+template <class D>
+struct Half : D {
+  static constexpr int LW = 16;
+  static_assert(D::N <= 16 && 3 * D::G <= 16 && D::R == 1, "one element per 16 lanes");
+};
+template <class D>
+constexpr bool fits_half() {
+  return D::N <= 16 && 3 * D::G <= 16;
+}
 
 // Packed upper-triangular factor U (row k of U is U(k, k..m-1); column k is
 // U(0..k, k)).  Row k starts at k*m - k*(k-1)/2; column k at k*(k+1)/2.
@@ -160,6 +175,18 @@ __device__ __forceinline__ int warp_in_block() { return threadIdx.x >> 5; }
 __device__ __forceinline__ int warp_global() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 __device__ __forceinline__ int warp_count() { return (gridDim.x * blockDim.x) >> 5; }
 
+// Lanes of one element: the whole warp (LW = 32), or a 16-lane half of it for
+// degrees whose modes and face points fit 16 lanes (two elements per warp).
+template <int LW>
+__device__ __forceinline__ int tile_lane() {
+  if constexpr (LW == 32) return lane_id(); else return lane_id() & (LW - 1);
+}
+template <int LW>
+__device__ __forceinline__ unsigned tile_mask() {
+  if constexpr (LW == 32) return 0xffffffffu;
+  else return ((1u << LW) - 1) << (lane_id() & ~(LW - 1));
+}
+
 // ---------------------------------------------------------------------------
 // warp building blocks (lanes over modes unless stated otherwise)
 // ---------------------------------------------------------------------------
@@ -167,40 +194,40 @@ __device__ __forceinline__ int warp_count() { return (gridDim.x * blockDim.x) >>
 // own field: lanes load v[e*N + i] into sm[i]
 template <class Dm>
 __device__ __forceinline__ void load_vec(double *sm, const double *__restrict__ g, int e) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int r = 0; r < Dm::R; ++r) {
-    const int i = l + 32 * r;
+    const int i = l + Dm::LW * r;
     if (i < Dm::N) sm[i] = g[(size_t)e * Dm::N + i];
   }
 }
 
 template <class Dm>
 __device__ __forceinline__ void load_reg(double (&x)[Dm::R], const double *__restrict__ g, int e) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int r = 0; r < Dm::R; ++r) {
-    const int i = l + 32 * r;
+    const int i = l + Dm::LW * r;
     x[r] = i < Dm::N ? g[(size_t)e * Dm::N + i] : 0.0;
   }
 }
 
 template <class Dm>
 __device__ __forceinline__ void store_reg(double *g, const double (&x)[Dm::R], int e) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int r = 0; r < Dm::R; ++r) {
-    const int i = l + 32 * r;
+    const int i = l + Dm::LW * r;
     if (i < Dm::N) g[(size_t)e * Dm::N + i] = x[r];
   }
 }
 
 template <class Dm>
 __device__ __forceinline__ void reg_to_sm(double *sm, const double (&x)[Dm::R]) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int r = 0; r < Dm::R; ++r) {
-    const int i = l + 32 * r;
+    const int i = l + Dm::LW * r;
     if (i < Dm::N) sm[i] = x[r];
   }
 }
@@ -245,7 +272,7 @@ __host__ __device__ constexpr int nb_stride() {
 // Stage NF fields of the three neighbours: nb[k*nb_stride + f*N + i].
 template <class Dm, int NF, class Fetch>
 __device__ __forceinline__ void stage_neighbours(const Sides &sd, double *nb, Fetch fetch) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int t = sd.nb[k];
@@ -254,7 +281,7 @@ __device__ __forceinline__ void stage_neighbours(const Sides &sd, double *nb, Fe
     for (int f = 0; f < NF; ++f)
 #pragma unroll
       for (int r = 0; r < Dm::R; ++r) {
-        const int i = l + 32 * r;
+        const int i = l + Dm::LW * r;
         if (i < Dm::N) nb[k * nb_stride<Dm, NF>() + f * Dm::N + i] = fetch(f, t, i);
       }
   }
@@ -389,7 +416,7 @@ template <class Dm, int NF>
 __device__ __forceinline__ void face_values(const double *pf, const DevMesh &m, const Sides &sd,
                                             const double *own, const double *nb, double *fb) {
   constexpr int N = Dm::N, G = Dm::G;
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
   if (l < 3 * G) {
     const int k = l / G, j = l - k * G;
     const int f = sd.face[k];
@@ -449,7 +476,7 @@ template <class Dm, int NF>
 __device__ __forceinline__ void matvec2(const double *A, const double *B, const double *X, int XS,
                                         double (&ax)[NF][Dm::R], double (&bx)[NF][Dm::R]) {
   constexpr int N = Dm::N, R = Dm::R;
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int f = 0; f < NF; ++f)
 #pragma unroll
@@ -458,7 +485,7 @@ __device__ __forceinline__ void matvec2(const double *A, const double *B, const 
     double a[R], b[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = l + 32 * r;
+      const int i = l + Dm::LW * r;
       a[r] = (i < N) ? A[j * N + i] : 0.0;
       b[r] = (i < N) ? B[j * N + i] : 0.0;
     }
@@ -509,7 +536,7 @@ template <class Dm, int NF>
 __device__ __forceinline__ void lift_sums(const SOps<Dm> &s, const int (&isg)[3], const double *fb,
                                           double (&t)[NF][3][Dm::R]) {
   constexpr int N = Dm::N, G = Dm::G, R = Dm::R;
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int isg2 = (G + 1) * (1 - isg[k]) / 2;
@@ -525,7 +552,7 @@ __device__ __forceinline__ void lift_sums(const SOps<Dm> &s, const int (&isg)[3]
       double p[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int i = l + 32 * r;
+        const int i = l + Dm::LW * r;
         p[r] = i < N ? pr[i] : 0.0;
       }
 #pragma unroll
@@ -552,24 +579,24 @@ __device__ __forceinline__ void apply_lift(double (&b)[R], const double (&t)[3][
 
 // S simultaneous DTRSM4 solves (src/dtrsm1.f:47-82) of size M with a packed
 // factor; rows i = lane + 32 r.
-template <int M, int R, int S>
+template <int M, int R, int S, int LW = 32>
 __device__ __forceinline__ void solve_batch(double (&t)[S][R], const double *row, const double *col,
                                             const double *dia) {
-  const int l = lane_id();
+  const int l = tile_lane<LW>();
 #pragma unroll
   for (int k = 0; k < M; ++k) {
-    const int kl = k & 31, kr = k >> 5;
+    const int kl = k % LW, kr = k / LW;
     const double d = dia[k];
     double xk[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       if (l == kl) t[s][kr] = mul(t[s][kr], d);
-      xk[s] = __shfl_sync(0xffffffffu, t[s][kr], kl);
+      xk[s] = __shfl_sync(tile_mask<LW>(), t[s][kr], kl, LW);
     }
     const double *u = row + row_off(k, M) - k;  // u[i] = U(k,i)
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = l + 32 * r;
+      const int i = l + LW * r;
       if (i > k && i < M) {
         const double uk = u[i];
 #pragma unroll
@@ -579,18 +606,18 @@ __device__ __forceinline__ void solve_batch(double (&t)[S][R], const double *row
   }
 #pragma unroll
   for (int k = M - 1; k >= 0; --k) {
-    const int kl = k & 31, kr = k >> 5;
+    const int kl = k % LW, kr = k / LW;
     const double d = dia[k];
     double bk[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       if (l == kl) t[s][kr] = mul(t[s][kr], d);
-      bk[s] = __shfl_sync(0xffffffffu, t[s][kr], kl);
+      bk[s] = __shfl_sync(tile_mask<LW>(), t[s][kr], kl, LW);
     }
     const double *u = col + col_off(k);  // u[i] = U(i,k)
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int i = l + 32 * r;
+      const int i = l + LW * r;
       if (i < k) {
         const double uk = u[i];
 #pragma unroll
@@ -602,23 +629,23 @@ __device__ __forceinline__ void solve_batch(double (&t)[S][R], const double *row
 
 template <class Dm, class Ops, int S>
 __device__ __forceinline__ void solve_full_b(const Ops &s, double (&t)[S][Dm::R]) {
-  solve_batch<Dm::N, Dm::R, S>(t, s.urow, s.ucol, s.dia1);
+  solve_batch<Dm::N, Dm::R, S, Dm::LW>(t, s.urow, s.ucol, s.dia1);
 }
 template <class Dm, class Ops, int S>
 __device__ __forceinline__ void solve_red_b(const Ops &s, double (&t)[S][Dm::R]) {
-  solve_batch<Dm::NMR, Dm::R, S>(t, s.lrow, s.lcol, s.dia2);
+  solve_batch<Dm::NMR, Dm::R, S, Dm::LW>(t, s.lrow, s.lcol, s.dia2);
 }
 
 // reduc_gn (src/mat1.f:418-439) through a warp scratch vector
 template <class Dm, class Ops>
 __device__ __forceinline__ void reduc(const Ops &s, const double (&gn)[Dm::R], double (&r)[Dm::R],
                                       double *sm) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
   reg_to_sm<Dm>(sm, gn);
-  __syncwarp();
+  __syncwarp(tile_mask<Dm::LW>());
 #pragma unroll
   for (int h = 0; h < Dm::R; ++h) {
-    const int rr = l + 32 * h;
+    const int rr = l + Dm::LW * h;
     double v = 0.0;
     if (rr < Dm::NMR) {
       const double a = sm[s.red_k[rr]], c = sm[s.red_i0[rr]];
@@ -626,23 +653,23 @@ __device__ __forceinline__ void reduc(const Ops &s, const double (&gn)[Dm::R], d
     }
     r[h] = v;
   }
-  __syncwarp();
+  __syncwarp(tile_mask<Dm::LW>());
 }
 
 // reduc_inv_gn (src/mat1.f:445-473)
 template <class Dm, class Ops>
 __device__ __forceinline__ void reduc_inv(const Ops &s, const double (&gr)[Dm::R],
                                           double (&gn)[Dm::R], double *sm) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
 #pragma unroll
   for (int h = 0; h < Dm::R; ++h) {
-    const int i = l + 32 * h;
+    const int i = l + Dm::LW * h;
     if (i < Dm::NMR) sm[i] = gr[h];
   }
-  __syncwarp();
+  __syncwarp(tile_mask<Dm::LW>());
 #pragma unroll
   for (int h = 0; h < Dm::R; ++h) {
-    const int n = l + 32 * h;
+    const int n = l + Dm::LW * h;
     double v = 0.0;
     if (n < Dm::N) {
       const int kind = s.inv_kind[n];
@@ -656,7 +683,7 @@ __device__ __forceinline__ void reduc_inv(const Ops &s, const double (&gr)[Dm::R
     }
     gn[h] = v;
   }
-  __syncwarp();
+  __syncwarp(tile_mask<Dm::LW>());
 }
 
 template <int R>
@@ -688,13 +715,13 @@ __device__ __forceinline__ Geo geo(const DevMesh &m, int e) {
 template <class Dm>
 __device__ __forceinline__ void scale_face(const DevMesh &m, const Sides &sd, const double *fb,
                                            double *out, int c) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
   if (l < 3 * Dm::G) out[l] = mul(fb[l], __ldg(m.norm + 2 * sd.face[l / Dm::G] + c));
 }
 template <class Dm>
 __device__ __forceinline__ void scale_face_h(const DevMesh &m, const Sides &sd, const double *fb,
                                              double *out, int c, double scale) {
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
   if (l < 3 * Dm::G) out[l] = mul(mul(fb[l], __ldg(m.norm + 2 * sd.face[l / Dm::G] + c)), scale);
 }
 
@@ -1502,11 +1529,11 @@ __device__ __forceinline__ void lin_rhs(const SOps<Dm> &S, LWarp<Dm> &W, const D
                                         const double (&hk)[Dm::R], double (&gx)[Dm::R],
                                         double (&gy)[Dm::R], double (&hb)[Dm::R]) {
   constexpr int N = Dm::N, R = Dm::R;
-  const int l = lane_id();
+  const int l = tile_lane<Dm::LW>();
   const double mg0 = -a.g0, hh0 = a.hh0;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const int i = l + 32 * r;
+    const int i = l + Dm::LW * r;
     if (i < N) {
       W.own[i] = mul(mg0, hk[r]);  // fxx = fyy = -g0 h (calvar_lin.f:76-79)
       W.own[N + i] = uk[r];
@@ -1520,9 +1547,9 @@ __device__ __forceinline__ void lin_rhs(const SOps<Dm> &S, LWarp<Dm> &W, const D
     return f == 0 ? mul(mg0, ld_state<CG>(a.sh + o))
                   : (f == 1 ? ld_state<CG>(a.su + o) : ld_state<CG>(a.sv + o));
   });
-  __syncwarp();
+  __syncwarp(tile_mask<Dm::LW>());
   face_values<Dm, 3>(S.pf, m, lm.sd, W.own, W.nb, W.fr);
-  __syncwarp();
+  __syncwarp(tile_mask<Dm::LW>());
   scale_face<Dm>(m, lm.sd, W.fr, W.fb, 0);        // fbdxx
   scale_face<Dm>(m, lm.sd, W.fr, W.fb + 32, 1);   // fbdyy
   scale_face_h<Dm>(m, lm.sd, W.fr + 32, W.fb + 64, 0, hh0);  // fbdx
@@ -1530,7 +1557,7 @@ __device__ __forceinline__ void lin_rhs(const SOps<Dm> &S, LWarp<Dm> &W, const D
   double af[1][R], bf[1][R], ah[2][R], bh[2][R];
   matvec2<Dm, 1>(S.agx, S.agy, W.own, N, af, bf);
   matvec2<Dm, 2>(S.agx, S.agy, W.xs, N, ah, bh);
-  __syncwarp();
+  __syncwarp(tile_mask<Dm::LW>());
   const double cby = mul(lm.g.by, lm.g.detai), cay = mul(lm.g.ay, lm.g.detai);
   const double cbx = mul(lm.g.bx, lm.g.detai), cax = mul(lm.g.ax, lm.g.detai);
 #pragma unroll
@@ -1631,26 +1658,29 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, i
   return ok;
 }
 
-// Several RK4 steps of the linear variant in one cooperative launch, one
-// element per warp for the whole launch: the operator image is staged once,
-// the element's mesh record, its u0 and RK4 accumulator rows and its stage
-// values stay in registers, and only the neighbours' stage rows are read
-// (through L2 only: other blocks wrote them earlier in the launch, behind a
-// grid barrier).  The stage buffers rotate as in one launch per stage (input
-// u0, A, B, A; output A, B, A, u0 in place); the arithmetic and its order are
-// those of kf_lin and stage_update.
+// Several RK4 steps of the linear variant in one cooperative launch (every
+// block resident), one element per warp or half-warp for the whole launch:
+// the operator image is staged once, the element's mesh record, its u0 and
+// RK4 accumulator rows and its stage values stay in registers, and only the
+// neighbours' stage rows are read (through L2 only: other blocks wrote them
+// earlier in the launch, behind a grid barrier).  The stage buffers rotate as
+// in one launch per stage (input u0, A, B, A; output A, B, A, u0 in place);
+// the arithmetic and its order are those of kf_lin and stage_update.  (Per-
+// element stage counters polled by the neighbours instead of the barrier
+// measured three times slower.)
 constexpr int kLinStepsMaxWarps = 20;
 template <class Dm>
 __global__ void __launch_bounds__(32 * kLinStepsMaxWarps) kf_lin_steps(DevOps op, DevMesh m,
                                                                      LinSteps ls) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
-  LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
-  constexpr int N = Dm::N, R = Dm::R;
+  constexpr int N = Dm::N, R = Dm::R, TPW = 32 / Dm::LW;  // elements per warp
+  LWarp<Dm> &W = reinterpret_cast<LWarp<Dm> *>(
+      smem + sizeof(SOps<Dm>))[warp_in_block() * TPW + lane_id() / Dm::LW];
   __shared__ __align__(8) uint64_t ops_bar;
   const bool staged = bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag);
-  const int l = lane_id();
-  const int e = warp_global();
+  const int l = tile_lane<Dm::LW>();
+  const int e = warp_global() * TPW + lane_id() / Dm::LW;
   const bool active = staged && e < m.ne;
   LinElem lm{};
   double u0[3][R], acc[3][R], x[3][R];  // u0, du1 + 2 du2 + 2 du3, stage input
@@ -1664,7 +1694,7 @@ __global__ void __launch_bounds__(32 * kLinStepsMaxWarps) kf_lin_steps(DevOps op
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int i = l + 32 * r;
+        const int i = l + Dm::LW * r;
         u0[c][r] = x[c][r] = i < N ? __ldcg(ls.sa.base[c] + (size_t)e * N + i) : 0.0;
       }
   }
@@ -1686,7 +1716,7 @@ __global__ void __launch_bounds__(32 * kLinStepsMaxWarps) kf_lin_steps(DevOps op
           double *const out = st == 1 ? ls.bufb[c] : ls.bufa[c];
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            const int i = l + 32 * r;
+            const int i = l + Dm::LW * r;
             if (i >= N) continue;
             const size_t o = (size_t)e * N + i;
             const double dd = d[c][r];
@@ -1711,7 +1741,7 @@ __global__ void __launch_bounds__(32 * kLinStepsMaxWarps) kf_lin_steps(DevOps op
             }
           }
         }
-        __syncwarp();
+        __syncwarp(tile_mask<Dm::LW>());
       }
       if (last) return;
       target += gridDim.x;
@@ -1838,18 +1868,22 @@ cudaError_t run_q(const DevOps &op, const DevMesh &m, const double *su, const do
 // the operator staging dominate): the elements are spread evenly, ceil(ne /
 // sms) warps per block, so no SM carries twice the work of another between
 // two barriers.  Else cudaErrorNotSupported.
-template <class Dm>
+template <class D>
 cudaError_t run_lin_steps(const DevOps &op, const DevMesh &m, const LinSteps &ls, cudaStream_t st,
                           int sms, long long *launches) {
+  // two elements per warp where an element fits 16 lanes
+  using Dm = std::conditional_t<fits_half<D>(), Half<D>, D>;
+  static_assert(sizeof(SOps<Dm>) == sizeof(SOps<D>), "one operator image for both layouts");
+  constexpr int TPW = 32 / Dm::LW;
   if (m.ne < 1 || sms < 1) return cudaErrorNotSupported;
-  const int w = (m.ne + sms - 1) / sms;
+  const int w = (m.ne + TPW * sms - 1) / (TPW * sms);
   if (w > kLinStepsMaxWarps) return cudaErrorNotSupported;
-  const size_t sm = sizeof(SOps<Dm>) + w * sizeof(LWarp<Dm>);
+  const size_t sm = sizeof(SOps<Dm>) + TPW * w * sizeof(LWarp<Dm>);
   int per_sm = 0;
   cudaError_t e = device_blocks_per_sm(kf_lin_steps<Dm>, 32 * w, sm, &per_sm);
   if (e == cudaErrorInvalidConfiguration) return cudaErrorNotSupported;  // no room on an SM
   if (e != cudaSuccess) return e;
-  const int grid = (m.ne + w - 1) / w;  // <= sms blocks, one resident per SM at least
+  const int grid = (m.ne + TPW * w - 1) / (TPW * w);  // <= sms blocks, one per SM
   if (ls.nsteps <= 0) return cudaSuccess;
   e = cudaMemsetAsync(ls.count, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
