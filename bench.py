@@ -218,13 +218,23 @@ def fp64_configs_measure(torch, stream, flush, W, names=("c1_lin_p3", "c4_ns_p4"
         per1 = (s.launches - l0) / steps
         l0 = s.launches
         ms = timed_call(torch, stream, flush, s, p.dt, call_steps)
+        dof = 3.0 * p.T.nm * p.mesh.ne
         out[name] = {"ne": p.mesh.ne, "nm": p.T.nm, "ms_per_step": ms,
-                     "value": 3.0 * p.T.nm * p.mesh.ne / (ms * 1e-3), "unit": UNIT,
+                     "value": dof / (ms * 1e-3), "unit": UNIT,
                      "steps_per_call": call_steps,
                      "launches_per_call": (s.launches - l0) / 3,
                      "ms_per_step_single_step_calls": ms1,
                      "launches_per_single_step_call": per1}
         s.close()
+        # the mixed-precision form on the same workload, timed the same way
+        m = W.make_solver(p, "mixed")
+        m.set_stream(stream.cuda_stream)
+        m.set_state(p.u, p.v, p.h)
+        m.rk4_steps(p.dt, 3)
+        mms = timed_call(torch, stream, flush, m, p.dt, call_steps)
+        out[name].update({"mixed_ms_per_step": mms, "mixed_value": dof / (mms * 1e-3),
+                          "mixed_speedup": ms / mms})
+        m.close()
     return out
 
 
@@ -505,13 +515,21 @@ def model_counts(cfg, ne, nf):
 # file at the capture: a figure is reported only while the source is unchanged
 # (otherwise `traffic` is null, since it would describe another version).
 KERNEL_SOURCE = {"kf_": "spoc_fast.cu", "kx_": "spoc_mixed.cu", "kt_": "spoc_mixed_tc.cu"}
+# At C2 the q-phase and tendency phases are two launches each (the face values
+# once per face, kf_faces, then kf_qphasef / kf_tendf): their figures are the
+# sums over the phase's two kernels.
 NCU_TRAFFIC = {
-    "c2_fs_p6:kf_qphase": (19388416, "96d09c3350079ef8"),
-    "c2_fs_p6:kf_nlvol": (97662720, "96d09c3350079ef8"),
-    "c2_fs_p6:kf_tend": (105278720, "96d09c3350079ef8"),
-    "c3_inv_p7:kx_vol": (247323136, "61a8985a532a517c"),
-    "c3_inv_p7:kx_tend": (464581888, "61a8985a532a517c"),
+    "c2_fs_p6:kf_qphase": (39760640, "f663cfa91067b3df"),
+    "c2_fs_p6:kf_nlvol": (97545216, "f663cfa91067b3df"),
+    "c2_fs_p6:kf_tend": (167038976, "f663cfa91067b3df"),
+    "c3_inv_p7:kx_vol": (248066048, "6bbf3e429a3ee218"),
+    "c3_inv_p7:kx_tend": (578007040, "6bbf3e429a3ee218"),
 }
+# The kernels behind each timed phase of the FP64 nonlinear RHS at the
+# degrees whose mode count is even and fits one row per lane (3 and 6).
+PHASE_KERNELS = {"kf_qphase": "kf_faces<NF=2> (face values of u, v) + kf_qphasef",
+                 "kf_nlvol": "kf_nlvol",
+                 "kf_tend": "kf_faces<NF=6> (face values of f, uh, vh) + kf_tendf"}
 
 
 def source_digest(kernel: str):
@@ -681,11 +699,27 @@ def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
     nf, na = s.adjoint_counters()
     nf, na = nf // 3, na // 3
     s.close()
+    # the mixed-precision forward over the same window (the RK4 steps alone,
+    # one call, median of three)
+    m = W.make_solver(p, "mixed")
+    m.set_stream(stream.cuda_stream)
+    m.set_state(*x0)
+    m.rk4_steps(p.dt, nsteps)
+    t_mix = []
+    for _ in range(3):
+        m.set_state(*x0)
+        t_mix.append(timed(lambda: m.rk4_steps(p.dt, nsteps))[1])
+    t_mix = float(np.median(t_mix))
+    m.close()
     return {"config": f"c4_ns_p4: {p.mesh.ne} triangles, nm={p.T.nm}, window {nsteps} steps, "
                       f"{snaps} binomial snapshots, {nobs} observation points at steps 50/100/150/200",
             "cost": J, "forward_window_ms": t_fwd, "gradient_ms": t_bwd,
             "timing": "median of three runs of each window",
             "gradient_over_forward": t_bwd / t_fwd,
+            "mixed_forward_window_ms": t_mix,
+            "gradient_over_mixed_forward": t_bwd / t_mix,
+            "gradient_precision": "fp64 (the gradient of the FP64 forward; no mixed-precision "
+                                  "tangent-linear or adjoint kernels)",
             "forward_steps_run_by_gradient": nf, "adjoint_steps": na,
             "checks": "dot-product, central differences (20 directions) and checkpointing invariance in tests/test_gpu_adjoint.py"}
 
@@ -984,6 +1018,8 @@ def main():
             "e2e_drop_in": drop_in,
             "gpu_launches": int(launches),
             "kernel_ms_per_launch": per_launch_ms,
+            "phase_kernels": (PHASE_KERNELS if args.precision == "fp64" and cfg.variant != "lin"
+                              and nm % 2 == 0 and nm <= 32 else None),
             "roofline": roof,
             "other_precisions": others,
             "fp64_other_configs": fp64_configs,
