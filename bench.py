@@ -698,6 +698,13 @@ def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
     (J2, g), t_bwd = bw[0][0], float(np.median([t for _, t in bw]))
     nf, na = s.adjoint_counters()
     nf, na = nf // 3, na // 3
+    # the forward sweeps in the mixed-precision form (adjoint kernels FP64)
+    s.set_adjoint_sweeps("mixed")
+    bm = [timed(lambda: s.bwd_window(x0, p.dt, nsteps, snaps)) for _ in range(3)]
+    (Jm, gm), t_bm = bm[0][0], float(np.median([t for _, t in bm]))
+    s.set_adjoint_sweeps("fp64")
+    g_rel = (sum(float(np.sum((a - b) ** 2)) for a, b in zip(gm, g)) /
+             sum(float(np.sum(b * b)) for b in g)) ** 0.5
     s.close()
     # the mixed-precision forward over the same window (the RK4 steps alone,
     # one call, median of three)
@@ -720,6 +727,14 @@ def adjoint_measure(torch, stream, nsteps=200, snaps=20, nobs=500):
             "gradient_over_mixed_forward": t_bwd / t_mix,
             "gradient_precision": "fp64 (the gradient of the FP64 forward; no mixed-precision "
                                   "tangent-linear or adjoint kernels)",
+            "mixed_sweeps": {
+                "what": "spoc_set_adjoint_sweeps(SPOC_MIXED): the cost sweep, the checkpoint "
+                        "sweeps and the re-advances in the mixed-precision form; tangent-linear "
+                        "and adjoint kernels FP64, linearised about that trajectory",
+                "gradient_ms": t_bm, "gradient_over_forward": t_bm / t_fwd,
+                "gradient_over_mixed_forward": t_bm / t_mix,
+                "gradient_rel_l2_difference_vs_fp64": g_rel,
+                "cost_rel_difference_vs_fp64": abs(Jm - J2) / abs(J2)},
             "forward_steps_run_by_gradient": nf, "adjoint_steps": na,
             "checks": "dot-product, central differences (20 directions) and checkpointing invariance in tests/test_gpu_adjoint.py"}
 

@@ -269,7 +269,14 @@ const char *spoc_last_error(void);
  *   with respect to the initial modal coefficients (gu,gv,gh), reversing the
  *   window with binomial checkpointing in `snaps` device snapshots.
  * spoc_adjoint_counters: forward and adjoint RK4 steps run since the last
- *   call (recomputation included). */
+ *   call (recomputation included).
+ * spoc_set_adjoint_sweeps (no reference counterpart): precision of the
+ *   forward steps that spoc_fwd_window, spoc_bwd_window, spoc_tlm_steps and
+ *   spoc_adj_steps run (the cost sweep, the checkpoint sweeps and the
+ *   re-advances of the reversal): SPOC_FP64 (default) or SPOC_MIXED (the
+ *   mixed-precision form, built from `tables`, which must be the handle's).
+ *   The tangent-linear and adjoint kernels stay FP64; with SPOC_MIXED they
+ *   are linearised about the mixed-precision trajectory. */
 int spoc_tlm_rhs(spoc_handle *h, int ld, const double *u, const double *v, const double *hh,
                  const double *du, const double *dv, const double *dh, double *ou, double *ov,
                  double *oh);
@@ -288,6 +295,7 @@ int spoc_bwd_window(spoc_handle *h, int ld, const double *u0, const double *v0, 
                     double dt, int nsteps, int snaps, double *cost, double *gu, double *gv,
                     double *gh);
 int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long long *adj_steps);
+int spoc_set_adjoint_sweeps(spoc_handle *h, const spoc_tables *tables, int precision);
 
 /* ---- Fortran drop-in ----
  * Register the COMMON contents once (after dpotrf), then link this library

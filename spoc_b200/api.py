@@ -133,6 +133,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "spoc_bwd_window": (C.c_int, [vp, C.c_int, _DP, _DP, _DP, C.c_double, C.c_int, C.c_int,
                                       _DP, _DP, _DP, _DP]),
         "spoc_adjoint_counters": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+        "spoc_set_adjoint_sweeps": (C.c_int, [vp, C.POINTER(_Tables), C.c_int]),
         "spoc_last_error": (C.c_char_p, []),
         "spoc_register_commons": (C.c_int, [C.POINTER(_Tables), C.c_int, C.c_int]),
         "spoc_cal_var_status": (_IP, []),
@@ -614,6 +615,15 @@ class Solver:
         _check(self.lib.spoc_bwd_window(self._h, x0[0].shape[1], *map(_d, x0), dt, nsteps, snaps,
                                         C.byref(J), *map(_d, g)), "bwd_window")
         return J.value, tuple(g)
+
+    def set_adjoint_sweeps(self, precision: int | str) -> None:
+        """Precision of the forward steps of the window and tangent-linear /
+        adjoint step functions: 'fp64' (default) or 'mixed'."""
+        if isinstance(precision, str):
+            precision = PRECISIONS[precision]
+        ts = self.T.struct()
+        _check(self.lib.spoc_set_adjoint_sweeps(self._h, C.byref(ts), precision),
+               "set_adjoint_sweeps")
 
     def adjoint_counters(self):
         f, a = C.c_longlong(), C.c_longlong()

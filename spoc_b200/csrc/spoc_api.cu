@@ -60,6 +60,7 @@ struct spoc_handle {
   long long launches = 0;
   double mu0 = 0, mb0 = 0, g0 = 9.81, hh0 = 0;
   bool have_params = false;
+  bool w0z0_zero = true;  // w0 and z0 identically zero (the mixed form skips their terms)
   std::vector<void *> allocs;
   DevOps op{};
   DevMesh mesh{};
@@ -509,12 +510,13 @@ extern "C" int spoc_set_params(spoc_handle *h, const spoc_params *p) {
   else CK(cudaMemsetAsync(h->z0, 0, sizeof(double) * n, h->st), "zero z0");
   if (p->fc) CK(copy_in(h, h->fc, p->fc, p->ld, cudaMemcpyHostToDevice), "upload fc");
   else CK(cudaMemsetAsync(h->fc, 0, sizeof(double) * n, h->st), "zero fc");
+  bool zero = true;
+  for (const double *w : {p->w0, p->z0})
+    if (w)
+      for (int e = 0; e < h->ne && zero; ++e)
+        for (int i = 0; i < h->nm && zero; ++i) zero = w[(size_t)e * p->ld + i] == 0.0;
+  h->w0z0_zero = zero;
   if (h->mx) {
-    bool zero = true;
-    for (const double *w : {p->w0, p->z0})
-      if (w)
-        for (int e = 0; e < h->ne && zero; ++e)
-          for (int i = 0; i < h->nm && zero; ++i) zero = w[(size_t)e * p->ld + i] == 0.0;
     CK(mixed_set_params(h->mx, h->op, h->hb, h->fc, h->w0, h->z0, zero, h->mu0, h->mb0, h->g0,
                         h->hh0, h->st),
        "mixed-precision parameters");
@@ -1211,6 +1213,12 @@ struct AdjCtx {
   // checkpoints
   std::vector<double *> snaps;
   long long fwd_steps = 0, adj_steps = 0;
+  // forward sweeps (advance) in the mixed-precision form: its context, owned
+  // here; null when the sweeps are FP64
+  MixedCtx *sweep_mx = nullptr;
+  ~AdjCtx() {
+    if (sweep_mx) mixed_destroy(sweep_mx);
+  }
 };
 
 std::mutex g_adj_mu;
@@ -1368,9 +1376,28 @@ int stages(spoc_handle *h, AdjCtx *c, double *const x[3], double dt) {
 // Advance a state by nsteps forward RK4 steps in place.
 int advance(spoc_handle *h, AdjCtx *c, double *const x[3], double dt, int nsteps) {
   if (nsteps <= 0) return SPOC_OK;
-  int rc = enqueue_steps_fp64(h, dt, nsteps, x);
-  if (rc) return rc;
+  if (c->sweep_mx) {
+    // mixed-precision steps: x (reference basis) -> psi state -> x
+    CK(mixed_set_state(c->sweep_mx, h->mesh, x, h->st, &h->launches), "sweep state in");
+    CK(mixed_steps(c->sweep_mx, h->mesh, dt, nsteps, h->flag, h->st, &h->launches),
+       "mixed-precision sweep");
+    CK(mixed_get_state(c->sweep_mx, x, h->st, &h->launches), "sweep state out");
+  } else {
+    const int rc = enqueue_steps_fp64(h, dt, nsteps, x);
+    if (rc) return rc;
+  }
   c->fwd_steps += nsteps;
+  return SPOC_OK;
+}
+
+// The mixed-precision sweep context takes the handle's current parameters
+// (they may have changed since the last window call).
+int sweep_params(spoc_handle *h, AdjCtx *c) {
+  if (!c->sweep_mx) return SPOC_OK;
+  if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
+  CK(mixed_set_params(c->sweep_mx, h->op, h->hb, h->fc, h->w0, h->z0, h->w0z0_zero, h->mu0,
+                      h->mb0, h->g0, h->hh0, h->st),
+     "sweep parameters");
   return SPOC_OK;
 }
 
@@ -1575,6 +1602,7 @@ extern "C" int spoc_tlm_steps(spoc_handle *h, int ld, const double *u0, const do
   if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
   AdjCtx *c = ctx_of(h);
   int rc = adj_init(h, c);
+  if (!rc) rc = sweep_params(h, c);
   double *const *x = c->V[3], *const *d = c->V[4];
   if (!rc) rc = host_to_dev3(h, x, ld, u0, v0, h0);
   if (!rc) rc = host_to_dev3(h, d, ld, du, dv, dh);
@@ -1594,6 +1622,7 @@ extern "C" int spoc_adj_steps(spoc_handle *h, int ld, const double *u0, const do
   if (!h->have_params) return fail(SPOC_E_ARG, "spoc_set_params not called");
   AdjCtx *c = ctx_of(h);
   int rc = adj_init(h, c);
+  if (!rc) rc = sweep_params(h, c);
   double *const *x = c->V[4], *const *lam = c->V[5];
   if (!rc) rc = host_to_dev3(h, x, ld, u0, v0, h0);
   if (!rc) rc = host_to_dev3(h, lam, ld, bu, bv, bh);
@@ -1661,6 +1690,7 @@ extern "C" int spoc_fwd_window(spoc_handle *h, int ld, const double *u0, const d
   AdjCtx *c = ctx_of(h);
   if (!c->nobs) return fail(SPOC_E_ARG, "spoc_set_observations not called");
   int rc = adj_init(h, c);
+  if (!rc) rc = sweep_params(h, c);
   double *const *x = c->V[4];
   if (!rc) rc = host_to_dev3(h, x, ld, u0, v0, h0);
   double J = 0.0;
@@ -1688,6 +1718,7 @@ extern "C" int spoc_bwd_window(spoc_handle *h, int ld, const double *u0, const d
   AdjCtx *c = ctx_of(h);
   if (!c->nobs) return fail(SPOC_E_ARG, "spoc_set_observations not called");
   int rc = adj_init(h, c);
+  if (!rc) rc = sweep_params(h, c);
   if (rc) return rc;
   // snapshot buffers
   while ((int)c->snaps.size() < snaps) {
@@ -1734,6 +1765,32 @@ extern "C" int spoc_bwd_window(spoc_handle *h, int ld, const double *u0, const d
   if (!rc) rc = reverse(h, c, 0, nsteps, x0, snaps, lam, dt, true);
   if (!rc) rc = dev_to_host3(h, gu, gv, gh, ld, lam);
   return rc ? rc : check_flag(h);
+}
+
+extern "C" int spoc_set_adjoint_sweeps(spoc_handle *h, const spoc_tables *t, int precision) {
+  if (!h) return fail(SPOC_E_ARG, "null handle");
+  if (precision != SPOC_FP64 && precision != SPOC_MIXED)
+    return fail(SPOC_E_ARG, "sweep precision must be SPOC_FP64 or SPOC_MIXED");
+  AdjCtx *c = ctx_of(h);
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  if (precision == SPOC_FP64) {
+    if (c->sweep_mx) mixed_destroy(c->sweep_mx);
+    c->sweep_mx = nullptr;
+    return SPOC_OK;
+  }
+  if (!t) return fail(SPOC_E_ARG, "tables needed for the mixed-precision sweeps");
+  if (t->nc != h->nc || t->ng != h->ng || t->ngf != h->ngf)
+    return fail(SPOC_E_ARG, "tables do not match the handle");
+  if (!mixed_available(h->nc, h->ng, h->ngf))
+    return fail(SPOC_E_ARG, "no mixed-precision form at this degree");
+  if (c->sweep_mx) return SPOC_OK;
+  std::string err;
+  const int rc = mixed_create(&c->sweep_mx, t, h->variant, h->ne, h->sms, &err);
+  if (rc) {
+    c->sweep_mx = nullptr;
+    return fail(rc, err.c_str());
+  }
+  return SPOC_OK;
 }
 
 extern "C" int spoc_adjoint_counters(spoc_handle *h, long long *fwd_steps, long long *adj_steps) {
