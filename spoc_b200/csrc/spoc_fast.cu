@@ -1638,8 +1638,10 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, i
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(count, 1u);
+    // release: the block's stores (ordered before this thread by the block
+    // barrier) are visible to whoever acquires the count after this add
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(count) : "memory");
     bool done = false;
     for (long long it = 0; it < kGridWaitLimit; ++it) {
       unsigned v;
@@ -1651,7 +1653,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, i
       __nanosleep(32);
     }
     if (!done) atomicOr(flag, 2);
-    __threadfence();
     ok = done;
   }
   __syncthreads();
@@ -1668,10 +1669,11 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, i
 // the arithmetic and its order are those of kf_lin and stage_update.  (Per-
 // element stage counters polled by the neighbours instead of the barrier
 // measured three times slower.)
+// MAXW: the most warps per block the instance is built for (8: the
+// registers are left to the compiler; 20: held to 96)
 constexpr int kLinStepsMaxWarps = 20;
-template <class Dm>
-__global__ void __launch_bounds__(32 * kLinStepsMaxWarps) kf_lin_steps(DevOps op, DevMesh m,
-                                                                     LinSteps ls) {
+template <class Dm, int MAXW>
+__global__ void __launch_bounds__(32 * MAXW) kf_lin_steps(DevOps op, DevMesh m, LinSteps ls) {
   extern __shared__ __align__(16) unsigned char smem[];
   SOps<Dm> &S = *reinterpret_cast<SOps<Dm> *>(smem);
   constexpr int N = Dm::N, R = Dm::R, TPW = 32 / Dm::LW;  // elements per warp
@@ -1879,8 +1881,9 @@ cudaError_t run_lin_steps(const DevOps &op, const DevMesh &m, const LinSteps &ls
   const int w = (m.ne + TPW * sms - 1) / (TPW * sms);
   if (w > kLinStepsMaxWarps) return cudaErrorNotSupported;
   const size_t sm = sizeof(SOps<Dm>) + TPW * w * sizeof(LWarp<Dm>);
+  const auto kern = w <= 8 ? kf_lin_steps<Dm, 8> : kf_lin_steps<Dm, kLinStepsMaxWarps>;
   int per_sm = 0;
-  cudaError_t e = device_blocks_per_sm(kf_lin_steps<Dm>, 32 * w, sm, &per_sm);
+  cudaError_t e = device_blocks_per_sm(kern, 32 * w, sm, &per_sm);
   if (e == cudaErrorInvalidConfiguration) return cudaErrorNotSupported;  // no room on an SM
   if (e != cudaSuccess) return e;
   const int grid = (m.ne + TPW * w - 1) / (TPW * w);  // <= sms blocks, one per SM
@@ -1891,7 +1894,7 @@ cudaError_t run_lin_steps(const DevOps &op, const DevMesh &m, const LinSteps &ls
   DevMesh mm = m;
   LinSteps l = ls;
   void *args[] = {&o, &mm, &l};
-  e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kf_lin_steps<Dm>), dim3(grid),
+  e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid),
                                   dim3(32 * w), args, sm, st);
   if (e == cudaSuccess) *launches += 1;
   return e;
