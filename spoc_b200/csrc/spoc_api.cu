@@ -72,6 +72,8 @@ struct spoc_handle {
   double *eterms = nullptr, *escal = nullptr;
   int *flag = nullptr;
   unsigned *gbar = nullptr;  // grid-barrier word of the multi-step linear kernel
+  int *lin_order = nullptr;  // element order of its 16-lane tiles (built on first use)
+  int lin_norder = 0;
   unsigned long long *cflbits = nullptr;
   MixedCtx *mx = nullptr;  // SPOC_MIXED: the resident state lives here (psi basis)
   // FP64: one RK4 step captured as a CUDA graph (replayed by spoc_rk4_steps),
@@ -632,6 +634,47 @@ bool mapped_host(const double *p, double **dev) {
 // arrays; the last stage of the last step stores the new state there too.
 // sh_ready (optional): the first right-hand side's kernels that read h wait
 // for it.
+// Element order of the multi-step linear kernel's 16-lane tiles: elements
+// paired by their wall flag (the two halves of a warp take the same branch
+// of the wall projection instead of running both one after the other), the
+// wall pairs spread evenly among the interior pairs (every block gets its
+// share).  A permutation of all elements (tiles with -1 are idle), so the
+// results do not depend on it.
+int build_lin_order(spoc_handle *h) {
+  const int ne = h->ne;
+  std::vector<int> bdl(ne);
+  CK(cudaMemcpyAsync(bdl.data(), h->mesh.bdl, sizeof(int) * ne, cudaMemcpyDeviceToHost, h->st),
+     "read bdl");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  std::vector<int> inner, wall;
+  for (int e = 0; e < ne; ++e) (bdl[e] ? wall : inner).push_back(e);
+  auto pairs = [](const std::vector<int> &v) {
+    std::vector<std::pair<int, int>> p;
+    for (size_t i = 0; i < v.size(); i += 2) p.push_back({v[i], i + 1 < v.size() ? v[i + 1] : -1});
+    return p;
+  };
+  const auto pi = pairs(inner), pw = pairs(wall);
+  const size_t np = pi.size() + pw.size();
+  std::vector<int> order;
+  order.reserve(2 * np);
+  size_t ii = 0, iw = 0;
+  for (size_t k = 0; k < np; ++k) {
+    // wall pair j sits at position floor((j + 0.5) np / |pw|)
+    const bool take_wall =
+        iw < pw.size() && (double)k >= std::floor((iw + 0.5) * (double)np / (double)pw.size());
+    const auto &q = (take_wall || ii >= pi.size()) ? pw[iw++] : pi[ii++];
+    order.push_back(q.first);
+    order.push_back(q.second);
+  }
+  if (h->lin_order == nullptr) CK(h->alloc(&h->lin_order, order.size()), "element order");
+  CK(cudaMemcpyAsync(h->lin_order, order.data(), sizeof(int) * order.size(),
+                     cudaMemcpyHostToDevice, h->st),
+     "upload element order");
+  CK(cudaStreamSynchronize(h->st), "synchronize");
+  h->lin_norder = (int)order.size();
+  return SPOC_OK;
+}
+
 // The linear variant on the compile-time-sized path runs all the steps in one
 // cooperative launch when the mesh fits one pass of the resident warps
 // (cudaErrorNotSupported: it does not, nothing was launched; nsteps 0 only
@@ -657,6 +700,9 @@ cudaError_t lin_steps(spoc_handle *h, const StageArgs &sa, int nsteps, double *c
   ls.hh0 = h->hh0;
   ls.nsteps = nsteps;
   ls.count = h->gbar;
+  if (!h->lin_order && build_lin_order(h)) return cudaErrorUnknown;
+  ls.order = h->lin_order;
+  ls.norder = h->lin_norder;
   if (sh_ready) {
     e = cudaStreamWaitEvent(h->st, sh_ready, 0);
     if (e != cudaSuccess) return e;

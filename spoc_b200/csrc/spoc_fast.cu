@@ -1682,8 +1682,9 @@ __global__ void __launch_bounds__(32 * MAXW) kf_lin_steps(DevOps op, DevMesh m, 
   __shared__ __align__(8) uint64_t ops_bar;
   const bool staged = bulk::stage_block(&S, op.img_ops, sizeof(SOps<Dm>), &ops_bar, op.flag);
   const int l = tile_lane<Dm::LW>();
-  const int e = warp_global() * TPW + lane_id() / Dm::LW;
-  const bool active = staged && e < m.ne;
+  const int tile = warp_global() * TPW + lane_id() / Dm::LW;
+  const int e = ls.order ? (tile < ls.norder ? __ldg(ls.order + tile) : -1) : tile;
+  const bool active = staged && e >= 0 && e < m.ne;
   LinElem lm{};
   double u0[3][R], acc[3][R], x[3][R];  // u0, du1 + 2 du2 + 2 du3, stage input
 #pragma unroll
@@ -1878,7 +1879,15 @@ cudaError_t run_lin_steps(const DevOps &op, const DevMesh &m, const LinSteps &ls
   static_assert(sizeof(SOps<Dm>) == sizeof(SOps<D>), "one operator image for both layouts");
   constexpr int TPW = 32 / Dm::LW;
   if (m.ne < 1 || sms < 1) return cudaErrorNotSupported;
-  const int w = (m.ne + TPW * sms - 1) / (TPW * sms);
+  // the element order pairs the halves of a warp; one element per warp has
+  // no halves to pair
+  LinSteps l = ls;
+  if (TPW == 1 || l.norder < m.ne) {
+    l.order = nullptr;
+    l.norder = 0;
+  }
+  const int tiles = l.order ? l.norder : m.ne;
+  const int w = (tiles + TPW * sms - 1) / (TPW * sms);
   if (w > kLinStepsMaxWarps) return cudaErrorNotSupported;
   const size_t sm = sizeof(SOps<Dm>) + TPW * w * sizeof(LWarp<Dm>);
   const auto kern = w <= 8 ? kf_lin_steps<Dm, 8> : kf_lin_steps<Dm, kLinStepsMaxWarps>;
@@ -1886,13 +1895,12 @@ cudaError_t run_lin_steps(const DevOps &op, const DevMesh &m, const LinSteps &ls
   cudaError_t e = device_blocks_per_sm(kern, 32 * w, sm, &per_sm);
   if (e == cudaErrorInvalidConfiguration) return cudaErrorNotSupported;  // no room on an SM
   if (e != cudaSuccess) return e;
-  const int grid = (m.ne + TPW * w - 1) / (TPW * w);  // <= sms blocks, one per SM
+  const int grid = (tiles + TPW * w - 1) / (TPW * w);  // <= sms blocks, one per SM
   if (ls.nsteps <= 0) return cudaSuccess;
   e = cudaMemsetAsync(ls.count, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
   DevOps o = op;
   DevMesh mm = m;
-  LinSteps l = ls;
   void *args[] = {&o, &mm, &l};
   e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid),
                                   dim3(32 * w), args, sm, st);

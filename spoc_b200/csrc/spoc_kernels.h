@@ -52,6 +52,11 @@ struct LinSteps {
   double g0, hh0;
   int nsteps;
   unsigned *count;
+  // optional element order of the 16-lane tiles (order[t] = element of tile t,
+  // -1 for none; norder entries): pairs the two elements of a warp by their
+  // wall flag, so that a warp's halves take the same wall or interior branch
+  const int *order = nullptr;
+  int norder = 0;
 };
 
 // Tangent-linear quadrature-point stage: base state (su.., q) and perturbation
