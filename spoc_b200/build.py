@@ -79,7 +79,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             raise RuntimeError(f"compile failed on {src} ({' '.join(cmd[-6:])}):\n{r.stderr}")
     objs = [j[1] for j in jobs]
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
+    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")

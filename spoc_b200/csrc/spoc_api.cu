@@ -10,6 +10,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/spoc_gpu.h"
@@ -79,10 +80,9 @@ struct spoc_handle {
   // FP64: one RK4 step captured as a CUDA graph (replayed by spoc_rk4_steps),
   // valid for the scalars baked into its kernel arguments
   cudaGraphExec_t step_graph = nullptr;
-  // spoc_cal_var with strided (ld > nm) host arrays: a device copy of one
-  // whole caller array, and pinned bounce buffers of the packed outputs
-  double *ld_stage = nullptr;
-  size_t ld_stage_n = 0;
+  // spoc_cal_var with strided (ld > nm) host arrays: pinned bounce buffers of
+  // the packed inputs and outputs
+  double *bounce_in[3] = {};
   double *bounce[3] = {};
   double graph_key[6] = {};
   long long graph_launches = 0;
@@ -104,6 +104,8 @@ struct spoc_handle {
   ~spoc_handle() {
     if (step_graph) cudaGraphExecDestroy(step_graph);
     for (double *b : bounce)
+      if (b) cudaFreeHost(b);
+    for (double *b : bounce_in)
       if (b) cudaFreeHost(b);
     if (mx) mixed_destroy(mx);
     for (void *p : allocs) cudaFree(p);
@@ -528,6 +530,38 @@ extern "C" int spoc_set_params(spoc_handle *h, const spoc_params *p) {
   return SPOC_OK;
 }
 
+namespace {
+// Rows 0..ne-1 (nm doubles each) of three fields from ld-strided `src` to
+// `dst` (stride dld), split over up to 8 host threads for large fields.
+void copy_rows(int ne, int nm, const double *const *src, int sld, double *const *dst, int dld) {
+  auto work = [&](int e0, int e1) {
+    for (int c = 0; c < 3; ++c)
+      for (int e = e0; e < e1; ++e)
+        std::memcpy(dst[c] + (size_t)e * dld, src[c] + (size_t)e * sld, sizeof(double) * nm);
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::min<unsigned>(hw ? hw : 1u, 8u);
+  if (nt <= 1 || ne < 4096) {
+    work(0, ne);
+    return;
+  }
+  const int chunk = (ne + nt - 1) / nt;
+  std::vector<std::thread> th;
+  int done_to = chunk;  // rows [0, chunk) stay with this thread
+  try {
+    for (int t = 1; t < nt && t * chunk < ne; ++t) {
+      th.emplace_back(work, t * chunk, std::min(ne, (t + 1) * chunk));
+      done_to = std::min(ne, (t + 1) * chunk);
+    }
+  } catch (...) {
+    // no more threads: the rows not handed out are copied here
+  }
+  work(0, std::min(ne, chunk));
+  if (done_to < ne) work(done_to, ne);
+  for (auto &x : th) x.join();
+}
+}  // namespace
+
 extern "C" int spoc_cal_var(spoc_handle *h, int ld, const double *u0, const double *v0,
                             const double *h0, double *u1, double *v1, double *h1) {
   if (!h || !u0 || !v0 || !h0 || !u1 || !v1 || !h1) return fail(SPOC_E_ARG, "null argument");
@@ -544,36 +578,33 @@ extern "C" int spoc_cal_var(spoc_handle *h, int ld, const double *u0, const doub
     CK(copy_out(h, h1, h->TEND[2], ld, cudaMemcpyDeviceToHost), "download h1");
     return check_flag(h);
   }
-  // Strided caller arrays (the reference's (nnmod, ne) layout): each input
-  // moves as one contiguous copy of the whole array and is packed on the
-  // device; each output comes back packed into pinned memory and is spread
-  // into the caller's rows on the host, which leaves rows nm+1..ld of the
-  // caller's arrays untouched, as the reference does (a copy of ne rows of nm
-  // doubles runs far below the link bandwidth from pageable memory).
-  const size_t nld = (size_t)ld * h->ne, npk = fsize(h);
-  if (h->ld_stage_n < nld) {
-    h->ld_stage = nullptr;
-    CK(h->alloc(&h->ld_stage, nld), "staging allocation");
-    h->ld_stage_n = nld;
-  }
-  for (int c = 0; c < 3; ++c)
-    if (!h->bounce[c]) CK(cudaHostAlloc((void **)&h->bounce[c], sizeof(double) * npk, 0), "pinned allocation");
-  const double *in[3] = {u0, v0, h0};
+  // Strided caller arrays (the reference's (nnmod, ne) layout): the inputs are
+  // packed on the host into pinned memory by several threads and move as one
+  // contiguous copy each; the outputs come back packed into pinned memory and
+  // are spread into rows 1..nm of the caller's arrays the same way, which
+  // leaves rows nm+1..ld untouched, as the reference does.  (Copies of ne
+  // rows of nm doubles run far below the link bandwidth, and one thread's
+  // host copy of a few MB takes milliseconds.)
+  const size_t npk = fsize(h);
   for (int c = 0; c < 3; ++c) {
-    CK(cudaMemcpyAsync(h->ld_stage, in[c], sizeof(double) * nld, cudaMemcpyHostToDevice, h->st),
-       "upload state");
-    CK(launch_pack_rows(h->ne, h->nm, ld, h->ld_stage, h->SIN[c], h->st, h->sms), "pack state");
+    if (!h->bounce[c]) CK(cudaHostAlloc((void **)&h->bounce[c], sizeof(double) * npk, 0), "pinned allocation");
+    if (!h->bounce_in[c])
+      CK(cudaHostAlloc((void **)&h->bounce_in[c], sizeof(double) * npk, 0), "pinned allocation");
   }
+  const double *const in[3] = {u0, v0, h0};
+  copy_rows(h->ne, h->nm, in, ld, h->bounce_in, h->nm);
+  for (int c = 0; c < 3; ++c)
+    CK(cudaMemcpyAsync(h->SIN[c], h->bounce_in[c], sizeof(double) * npk, cudaMemcpyHostToDevice,
+                       h->st),
+       "upload state");
   int rc = run_rhs_tend(h, h->SIN);
   if (rc) return rc;
   for (int c = 0; c < 3; ++c)
     CK(cudaMemcpyAsync(h->bounce[c], h->TEND[c], sizeof(double) * npk, cudaMemcpyDeviceToHost, h->st),
        "download tendency");
-  rc = check_flag(h);  // synchronises the stream
-  double *out[3] = {u1, v1, h1};
-  for (int c = 0; c < 3; ++c)
-    for (int e = 0; e < h->ne; ++e)
-      std::memcpy(out[c] + (size_t)e * ld, h->bounce[c] + (size_t)e * h->nm, sizeof(double) * h->nm);
+  rc = check_flag(h);  // synchronises the stream (the pinned inputs are free again)
+  double *const out[3] = {u1, v1, h1};
+  copy_rows(h->ne, h->nm, h->bounce, h->nm, out, ld);
   return rc;
 }
 

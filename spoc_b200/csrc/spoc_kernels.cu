@@ -730,27 +730,4 @@ cudaError_t launch_fp64_peak(int mode, int sms, int iters, double *out, cudaStre
     k_fp32_peak<<<grid, 256, 0, st>>>(out, iters, 0.999999f, 1e-9f);
   return cudaGetLastError();
 }
-// dst[e*nm + k] = src[e*ld + k], k < nm: the packed device layout of a
-// (ld, ne) caller array copied to the device whole (one contiguous transfer
-// instead of ne rows of nm doubles)
-__global__ void __launch_bounds__(256) k_pack_rows(int ne, int nm, int ld,
-                                                   const double *__restrict__ src,
-                                                   double *__restrict__ dst) {
-  const size_t n = (size_t)ne * nm;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const size_t e = i / nm, k = i - e * nm;
-    dst[i] = src[e * ld + k];
-  }
-}
-
-cudaError_t launch_pack_rows(int ne, int nm, int ld, const double *src, double *dst,
-                             cudaStream_t st, int sms) {
-  size_t blocks = ((size_t)ne * nm + 255) / 256;
-  if (blocks > (size_t)sms * 16) blocks = (size_t)sms * 16;
-  if (blocks < 1) blocks = 1;
-  k_pack_rows<<<(unsigned)blocks, 256, 0, st>>>(ne, nm, ld, src, dst);
-  return cudaGetLastError();
-}
-
 }  // namespace spoc

@@ -127,9 +127,6 @@ cudaError_t launch_tend(int variant, const DevOps &op, const DevMesh &m, const T
 cudaError_t launch_lin(const DevOps &op, const DevMesh &m, const LinArgs &la, const StageArgs &sa,
                        cudaStream_t st, int sms);
 
-// dst[e*nm + k] = src[e*ld + k] for k < nm (device to device)
-cudaError_t launch_pack_rows(int ne, int nm, int ld, const double *src, double *dst,
-                             cudaStream_t st, int sms);
 
 cudaError_t launch_energy(const DevOps &op, const DevMesh &m, const double *su, const double *sv,
                           const double *sh, const double *hb, double g0, double *terms,
