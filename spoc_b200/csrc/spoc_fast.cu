@@ -373,13 +373,29 @@ struct RowCopy {
       prefetch_element<Dm, NF>(fields, e, sd, own, nb);
     }
   }
-  // The element's NF rows (lanes 0..NF-1) and the records of its three
-  // faces (lanes NF..NF+2: rec floats each, from frec + face * rec into
-  // fdst + k * rec), bulk copies only (even N; rec * 8 a multiple of 16).
+  // The element's NF rows and the records of its three faces (rec doubles
+  // each, from frec + face * rec into fdst + k * rec): bulk copies at even N
+  // (lanes 0..NF-1 the rows, NF..NF+2 the records; rec * 8 a multiple of
+  // 16), else 8-byte cp.async copies spread over the lanes.
   __device__ __forceinline__ void issue_own_faces(const double *const (&fields)[NF], int e,
                                                   const Sides &sd, double *own,
                                                   const double *frec, double *fdst, int rec) {
-    static_assert(kBulk, "bulk copies need 16-byte rows");
+    if constexpr (!kBulk) {
+      const int l = lane_id();
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int r = 0; r < Dm::R; ++r) {
+          const int i = l + 32 * r;
+          if (i < Dm::N) cp_async8(own + f * Dm::N + i, fields[f] + (size_t)e * Dm::N + i);
+        }
+      for (int i = l; i < 3 * rec; i += 32) {
+        const int k = i / rec, j = i - k * rec;
+        const int face = k == 0 ? sd.face[0] : (k == 1 ? sd.face[1] : sd.face[2]);
+        cp_async8(fdst + i, frec + (size_t)face * rec + j);
+      }
+      return;
+    }
     constexpr uint32_t RB = Dm::N * sizeof(double);
     const int l = lane_id();
     if (l == 0) bulk::arrive_expect_tx(bar, NF * RB + 3u * (uint32_t)rec * sizeof(double));
@@ -849,7 +865,7 @@ __device__ __forceinline__ void qphase_body(DevOps op, DevMesh m, const double *
   QWarp<Dm, FACES> &W =
       reinterpret_cast<QWarp<Dm, FACES> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
   constexpr int N = Dm::N, R = Dm::R, G = Dm::G;
-  static_assert(!FACES || (Dm::R == 1 && Dm::N % 2 == 0), "face records need bulk row copies");
+  static_assert(!FACES || Dm::R == 1, "face records with one row per lane");
   const double *const fields[2] = {su, sv};
   // the copies of element e: its rows and its neighbours' rows, or its rows
   // and its three face records (FACES: W.fvs stands in for W.nb)
@@ -1269,7 +1285,7 @@ __device__ __forceinline__ void tend_body(DevOps op, DevMesh m, TendArgs a, Stag
   TWarp<Dm, FACES> &W =
       reinterpret_cast<TWarp<Dm, FACES> *>(smem + sizeof(SOps<Dm>))[warp_in_block()];
   constexpr int N = Dm::N, R = Dm::R, G = Dm::G;
-  static_assert(!FACES || (Dm::R == 1 && Dm::N % 2 == 0), "face records need bulk row copies");
+  static_assert(!FACES || Dm::R == 1, "face records with one row per lane");
   // issue the copies of element e: its rows and its neighbours' rows, or its
   // rows and its three face records
   auto issue = [&](RowCopy<Dm, 6> &rc, const double *const (&fields)[6], int e, const Sides &sd) {
@@ -1428,13 +1444,13 @@ __global__ void __launch_bounds__(256) kf_qphase(DevOps op, DevMesh m, const dou
                                                  const double *__restrict__ sv, double *q) {
   qphase_body<Dm, VAR>(op, m, su, sv, q);
 }
-// the q-phase on the face values of kf_faces (one row per lane, even N)
+// the q-phase on the face values of kf_faces (one row per lane)
 template <class Dm, int VAR>
 __global__ void __launch_bounds__(256) kf_qphasef(DevOps op, DevMesh m,
                                                   const double *__restrict__ su,
                                                   const double *__restrict__ sv, double *q,
                                                   const double *__restrict__ fv) {
-  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) qphase_body<Dm, VAR, true>(op, m, su, sv, q, fv);
+  if constexpr (Dm::R == 1) qphase_body<Dm, VAR, true>(op, m, su, sv, q, fv);
 }
 template <class Dm, int VAR>
 __global__ void __launch_bounds__(256, 2) kf_qphase_r2(DevOps op, DevMesh m,
@@ -1454,10 +1470,10 @@ template <class Dm, int VAR>
 __global__ void __launch_bounds__(256) kf_tend(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
   tend_body<Dm, VAR>(op, m, a, sa);
 }
-// the tendency kernel on the face values of kf_faces (one row per lane, even N)
+// the tendency kernel on the face values of kf_faces (one row per lane)
 template <class Dm, int VAR>
 __global__ void __launch_bounds__(256) kf_tendf(DevOps op, DevMesh m, TendArgs a, StageArgs sa) {
-  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) tend_body<Dm, VAR, true>(op, m, a, sa);
+  if constexpr (Dm::R == 1) tend_body<Dm, VAR, true>(op, m, a, sa);
 }
 template <class Dm, int VAR>
 __global__ void __launch_bounds__(Dm::TEND_THREADS, 2) kf_tend_r2(DevOps op, DevMesh m, TendArgs a,
@@ -1803,7 +1819,7 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   const auto kt = tend_kernel<Dm, VAR>();
   // face values of u, v once per face (counted with the q-phase)
   bool qfaces = false;
-  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) {
+  if constexpr (Dm::R == 1) {
     if (b.fv) {
       constexpr int wf = pick_warps(sizeof(SOps<Dm>), sizeof(QWarp<Dm, true>));
       constexpr size_t sf = sizeof(SOps<Dm>) + wf * sizeof(QWarp<Dm, true>);
@@ -1823,7 +1839,7 @@ cudaError_t run_nl(const DevOps &op, const DevMesh &m, const RhsBuffers &b, cons
   mark(1);
   kb<<<gb, 32 * wb, sb, st>>>(op, m, na);
   mark(2);
-  if constexpr (Dm::R == 1 && Dm::N % 2 == 0) {
+  if constexpr (Dm::R == 1) {
     if (b.fv) {
       // face values once per face, then the tendency kernel on them (the
       // face kernel's time is counted with the tendency kernel's)
