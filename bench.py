@@ -519,9 +519,9 @@ KERNEL_SOURCE = {"kf_": "spoc_fast.cu", "kx_": "spoc_mixed.cu", "kt_": "spoc_mix
 # once per face, kf_faces, then kf_qphasef / kf_tendf): their figures are the
 # sums over the phase's two kernels.
 NCU_TRAFFIC = {
-    "c2_fs_p6:kf_qphase": (39811328, "30527c38cd03f815"),
-    "c2_fs_p6:kf_nlvol": (97823232, "30527c38cd03f815"),
-    "c2_fs_p6:kf_tend": (167237120, "30527c38cd03f815"),
+    "c2_fs_p6:kf_qphase": (39800320, "3d82445bfb57b56a"),
+    "c2_fs_p6:kf_nlvol": (98205184, "3d82445bfb57b56a"),
+    "c2_fs_p6:kf_tend": (167291904, "3d82445bfb57b56a"),
     "c3_inv_p7:kx_vol": (248066048, "6bbf3e429a3ee218"),
     "c3_inv_p7:kx_tend": (578007040, "6bbf3e429a3ee218"),
 }
