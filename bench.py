@@ -526,7 +526,7 @@ NCU_TRAFFIC = {
     "c3_inv_p7:kx_tend": (578007040, "6bbf3e429a3ee218"),
 }
 # The kernels behind each timed phase of the FP64 nonlinear RHS at the
-# degrees whose mode count is even and fits one row per lane (3 and 6).
+# degrees whose modes fit one row per lane (3-6).
 PHASE_KERNELS = {"kf_qphase": "kf_faces<NF=2> (face values of u, v) + kf_qphasef",
                  "kf_nlvol": "kf_nlvol",
                  "kf_tend": "kf_faces<NF=6> (face values of f, uh, vh) + kf_tendf"}
@@ -1034,7 +1034,7 @@ def main():
             "gpu_launches": int(launches),
             "kernel_ms_per_launch": per_launch_ms,
             "phase_kernels": (PHASE_KERNELS if args.precision == "fp64" and cfg.variant != "lin"
-                              and nm % 2 == 0 and nm <= 32 else None),
+                              and nm <= 32 else None),
             "roofline": roof,
             "other_precisions": others,
             "fp64_other_configs": fp64_configs,
