@@ -185,6 +185,20 @@ def cal_var(variant, T: Tables, M: Mesh, u0, v0, h0, fc, w0, z0, hb, mu0, mb0, g
     return tuple(out)
 
 
+def cal_flu(T: Tables, M: Mesh, a0, nthreads=None):
+    """Face traces of one field (src/calflu.f:6-71): (nf, ngf), the central
+    average of both sides' traces at the ngf edge points (side 1's trace on
+    wall faces)."""
+    a0 = np.ascontiguousarray(a0, dtype=np.float64)
+    out = np.zeros((M.nf, T.ngf))
+    L = lib()
+    L.ora_cal_flu.argtypes = [C.POINTER(Common), C.c_int, _IP, _DP, C.c_int, _DP, C.c_int, _IP,
+                              C.c_int]
+    L.ora_cal_flu(C.byref(T.common), M.nf, i(M.tseg), d(out), T.ngf, d(a0), a0.shape[1],
+                  i(M.ssit), nthreads or default_threads())
+    return out
+
+
 def rk4(variant, T: Tables, M: Mesh, u, v, h, fc, w0, z0, hb, mu0, mb0, g0, dt, nsteps,
         nthreads=None):
     """nsteps RK4 steps in place on (u, v, h)."""

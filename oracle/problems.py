@@ -69,3 +69,23 @@ def oracle_problem(cfg: W.Config) -> OracleProblem:
     z0 = np.zeros_like(hb)
     dt = W.cfl_dt(cfg.nc, M, cfg.g0, cfg.depth) * cfg.dt_scale
     return OracleProblem(cfg, T, M, u, v, h, hb, w0, z0, dt)
+
+
+# Small known-answer cases (tests/golden/small_rhs.json): the C2 physics on a
+# 2 x 2 cell basin (8 triangles) at every tabulated degree and variant, with a
+# seeded perturbation of the initial state so the nonlinear terms are active.
+SMALL_DEGREES = [(3, 12, 4), (4, 25, 5), (5, 27, 6), (6, 33, 7), (7, 42, 9)]
+SMALL_VARIANTS = ["lin", "fs", "ns", "inv"]
+
+
+def small_case(nc: int, ng: int, ngf: int, variant: str) -> W.Config:
+    import dataclasses
+    return dataclasses.replace(W.small(W.CONFIGS["c2_fs_p6"], 2), nc=nc, ng=ng, ngf=ngf,
+                               variant=variant)
+
+
+def small_case_state(u, v, h, nc: int, variant: str):
+    """The perturbed state of a small case: u, v, h plus seeded noise."""
+    rng = np.random.default_rng(1000 * nc + SMALL_VARIANTS.index(variant))
+    return (u + 0.1 * rng.normal(size=u.shape), v + 0.1 * rng.normal(size=v.shape),
+            h + 0.05 * rng.normal(size=h.shape))

@@ -446,3 +446,36 @@ def test_strided_cal_var_leaves_padding_rows(gpu_lib):
     OT, OM = oracle_for(p)
     assert_bitwise(outs, oracle_rhs(p, OT, OM, p.u, p.v, p.h), p.T.nm)
     assert all((o[:, p.T.nm:] == 7.0).all() for o in outs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", PATHS)
+def test_small_golden_rhs(gpu_lib, path):
+    """The library's right-hand side on the committed 8-triangle known answers
+    (tests/golden/small_rhs.json, every tabulated degree and variant), set up
+    with the library's own code: input state and cal_var output bit for bit."""
+    import hashlib
+    import json
+    from pathlib import Path
+
+    from oracle.problems import SMALL_DEGREES, SMALL_VARIANTS, small_case, small_case_state
+
+    golden = json.loads((Path(__file__).parent / "golden" / "small_rhs.json").read_text())
+
+    def digest(*arrays):
+        m = hashlib.sha256()
+        for a in arrays:
+            m.update(np.ascontiguousarray(a[:, :nm], dtype="<f8").tobytes())
+        return m.hexdigest()
+
+    for nc, ng, ngf in SMALL_DEGREES:
+        for variant in SMALL_VARIANTS:
+            rec = golden[f"p{nc}_{variant}"]
+            p = W.build_problem(small_case(nc, ng, ngf, variant))
+            nm = p.T.nm
+            u, v, h = small_case_state(p.u, p.v, p.h, nc, variant)
+            assert digest(u, v, h) == rec["input_sha256"], (nc, variant)
+            s = W.make_solver(p)
+            s.set_kernel_path(path)
+            assert digest(*s.cal_var(u, v, h)) == rec["rhs_sha256"], (nc, variant, path)
+            s.close()
